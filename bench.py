@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the batched edge-step collision checker on one B200.
+
+Workload (the batched plain-GPU-checker configuration): 6-DOF arm whose
+links are hulls of 16 points on an ellipsoid (0.15/0.04/0.04 m), 64 hull
+obstacles of 12-32 points, 2^20 uniform samples in [-pi,pi]^6, the vertex
+check, then k=10 nearest free neighbours -> ~4M undirected edges of uneven
+length, discretised at dq = 0.01 rad; FP32 with the FP64 band recheck
+(|margin| < 1e-5 m).  All inputs are seeded synthetic data.
+
+One step = one pass of the edge checker over the whole edge batch.
+  value  nominal edge-step checks/s (sum of testnum / time) of the device
+         entry point on inputs resident in HBM (CUDA events on the launch
+         stream, max over ranks);
+  e2e    the same through the host-buffer C ABI (indicator2): host->device
+         copies of qs/qe and the device->host read of res inside the timed
+         region;
+  roofline  FP32 pipe: counted FP32 operations of the checked steps over
+         the FP32 check kernel's event-timed duration, against the measured
+         FP32 FMA peak of the device;
+  cpu_baseline  GPUPRM's own CPU checker (oracle/_ref, compiled from the
+         reference sources) on a bounded sample of the same edges, all host
+         cores, one checker instance per thread.
+
+--impl reference times only that CPU checker (same metric/config).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edge-step collision checks/s"
+UNIT = "edge-steps/s"
+WORKLOAD = dict(workload="hull6 batched edges: 6-DOF ellipsoid-hull arm, 64 hull obstacles, "
+                         "2^20 samples, kNN k=10, dq=0.01 rad, FP64 band 1e-5 m",
+                ndof=6, obstacles=64, samples=1 << 20, k=10, dq=0.01, band_m=1e-5)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--samples", type=int, default=1 << 20)
+    ap.add_argument("--k", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--policy", default="early", choices=["early", "all"])
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="gprm_clocks_", suffix=".csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU leg (GPUPRM's own CPU checker; the oracle restatement if it is absent)
+# --------------------------------------------------------------------------
+
+def cpu_reference_rate(scene, qs_np, qe_np, dq, seconds, seed=0):
+    """Times the reference CPU checker on a bounded sample of the edges with
+    all host cores.  Returns (dict for cpu_baseline, flops per step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(seed + 77)
+    order = rng.permutation(qs_np.shape[0])
+    orc = O.Oracle(scene)
+    # algorithmic FP32 work per step, counted by the instrumented restatement
+    cnt_idx = order[:256]
+    ops = orc.count_ops_edges(qs_np[cnt_idx], qe_np[cnt_idx], dq)
+    tn_cnt = orc.testnum(qs_np[cnt_idx], qe_np[cnt_idx], dq)
+    flops_per_step = (ops["add"] + ops["mul"] + ops["div"] + ops["sqrt"]) / max(1, int(tn_cnt.sum()))
+    if O.ref_available():
+        ref = O.RefChecker(scene, dq=dq, nbuf=4096)
+        kind = "reference"
+        run = lambda a, b: ref.check_edges_mt(a, b, cores, chunk=16)
+    else:
+        kind = "port"
+        cores = 1
+        run = lambda a, b: orc.check_edges(a, b, dq, O.FP32)[0]
+    # calibrate on a small slice, then size the sample to `seconds`
+    cal = order[256:256 + 64 * cores]
+    t0 = time.perf_counter()
+    run(qs_np[cal], qe_np[cal])
+    dt = max(1e-3, time.perf_counter() - t0)
+    n = int(len(cal) * seconds / dt)
+    n = max(64, min(n, qs_np.shape[0]))
+    idx = order[:n]
+    a, b = qs_np[idx], qe_np[idx]
+    steps = int(orc.testnum(a, b, dq).sum())
+    t0 = time.perf_counter()
+    run(a, b)
+    dt = time.perf_counter() - t0
+    return ({"value": steps / dt, "unit": UNIT, "cores": cores, "kind": kind,
+             "sample": f"{n} random edges of the workload ({steps} edge steps), indicator2 in chunks "
+                       f"of <=4096 edges per thread, {dt:.1f} s"}, flops_per_step)
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from gpuprm_b200 import workloads
+    from gpuprm_b200._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT, GPRM_MODE_FP64_BAND
+    from gpuprm_b200.configspace import measure_fp32_peak
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    ws = workloads.edge_workload("hull6", seed=args.seed + 7919 * rank, n_samples=args.samples, k=args.k,
+                                 dq=WORKLOAD["dq"], device=str(dev))
+    cs = ws["space"]
+    cs.set_mode(GPRM_MODE_FP64_BAND)
+    policy = GPRM_EDGES_EARLY_EXIT if args.policy == "early" else GPRM_EDGES_ALL_STEPS
+    cs.set_edge_policy(policy)
+    qs, qe = ws["qs"], ws["qe"]
+    E = qs.shape[1]
+    res = torch.empty(E, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        cs.check_edges_device(qs, qe, res)
+    torch.cuda.synchronize()
+    barrier()
+    s0 = cs.stats()
+    cs.profile_enable(True)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        cs.check_edges_device(qs, qe, res)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t = e0.elapsed_time(e1) / 1e3
+    clocks = clk.stop()
+    prof = cs.profile_read()
+    s1 = cs.stats()
+    cs.profile_enable(False)
+    nominal = (s1["edge_steps_nominal"] - s0["edge_steps_nominal"])
+    executed = (s1["edge_steps_executed"] - s0["edge_steps_executed"])
+    band = (s1["band_rechecks"] - s0["band_rechecks"])
+    launches = s1["launches"] - s0["launches"]
+    colliding = int((res != 0).sum().item())
+
+    # max over ranks of the device time; totals over ranks
+    t_max, nominal_all, executed_all = t, nominal, executed
+    if world > 1:
+        tt = torch.tensor([t], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_max = float(tt.item())
+        nn = torch.tensor([nominal, executed], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(nn)
+        nominal_all, executed_all = int(nn[0].item()), int(nn[1].item())
+
+    # e2e through the host-buffer C ABI (H2D + D2H inside the timed region)
+    qs_np = np.ascontiguousarray(qs.cpu().numpy())
+    qe_np = np.ascontiguousarray(qe.cpu().numpy())
+    res_np = np.zeros(E, np.int32)
+    cs.indicator2(qs_np, qe_np, res_np, E, E)   # warm-up (allocates pinned staging)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cs.indicator2(qs_np, qe_np, res_np, E, E)
+    t_e2e = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    assert np.array_equal(res_np, res.cpu().numpy()), "host and device entry points disagree"
+
+    if rank != 0:
+        return None
+    peak = measure_fp32_peak()
+    cpu = None
+    flops_per_step = None
+    if not args.no_cpu_baseline and world == 1:
+        qs_r = np.ascontiguousarray(qs_np.T)
+        qe_r = np.ascontiguousarray(qe_np.T)
+        cpu, flops_per_step = cpu_reference_rate(ws["scene"], qs_r, qe_r, WORKLOAD["dq"], args.cpu_seconds,
+                                                 args.seed)
+    k_ms = prof["fp32_ms"] / max(1, prof["fp32_launches"])
+    exec_per_launch = executed / max(1, args.steps)
+    roof = None
+    if flops_per_step is not None:
+        achieved = flops_per_step * exec_per_launch / (k_ms * 1e-3) / 1e12
+        roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured FP32 FMA probe on this device (2 flops/FMA); "
+                               "MEASURED_PEAKS.json has no FP32 entry",
+                "flops_per_step": flops_per_step, "kernel_ms": k_ms,
+                "fp64_recheck_ms_per_launch": prof["fp64_ms"] / max(1, prof["fp32_launches"])}
+    line = {
+        "metric": METRIC, "value": nominal_all / t_max, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (+f64 band)",
+        "data": "synthetic (seeded)",
+        "config": dict(WORKLOAD, edges_per_gpu=E, free_samples=ws["n_free"], policy=args.policy,
+                       l2="inputs (qs,qe: %.0f MB) larger than L2" % (2 * qs.numel() * 4 / 1e6)),
+        "executed_steps_per_s": executed_all / t_max,
+        "nominal_steps_per_step": nominal, "executed_steps_per_step_": executed / args.steps,
+        "colliding_edges": colliding, "band_rechecks_per_step": band / args.steps,
+        "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
+                "d2h_bytes_per_step": int(E * 4)},
+        "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+    }
+    return line
+
+
+# --------------------------------------------------------------------------
+# reference arm: GPUPRM's CPU checker on the same workload definition
+# --------------------------------------------------------------------------
+
+def run_reference(args):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from scipy.spatial import cKDTree
+    from gpuprm_b200 import scenes
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libgprm_ref.so was not built (reference tree absent at build time)"}
+    sc = scenes.make_scene("hull6", args.seed)
+    dq = WORKLOAD["dq"]
+    cores = os.cpu_count() or 1
+    ref = O.RefChecker(sc, dq=dq, nbuf=4096)
+    q = scenes.uniform_configs(sc, args.samples, args.seed + 1000)
+    codes = ref.check_configs_mt(q, cores, chunk=512)
+    free = q[codes == 0]
+    tree = cKDTree(free.astype(np.float64))
+    rng = np.random.default_rng(args.seed + 5)
+
+    def sample_edges(m):
+        src = rng.choice(free.shape[0], m, replace=False)
+        _, nb = tree.query(free[src].astype(np.float64), k=args.k + 1)
+        j = nb[np.arange(m), rng.integers(1, args.k + 1, m)]
+        return free[src], free[j]
+
+    # size one step to ~cpu_seconds of work
+    a, b = sample_edges(64 * cores)
+    t0 = time.perf_counter()
+    ref.check_edges_mt(a, b, cores, chunk=16)
+    per_edge = (time.perf_counter() - t0) / a.shape[0]
+    m = int(max(64, min(200000, args.cpu_seconds / max(per_edge, 1e-9))))
+    for _ in range(max(3, args.warmup)):
+        a, b = sample_edges(min(m, 256 * cores))
+        ref.check_edges_mt(a, b, cores, chunk=16)
+    steps = 0
+    t = 0.0
+    for _ in range(args.steps):
+        a, b = sample_edges(m)
+        steps += int(O.Oracle(sc).testnum(a, b, dq).sum())
+        t0 = time.perf_counter()
+        ref.check_edges_mt(a, b, cores, chunk=16)
+        t += time.perf_counter() - t0
+    v = steps / t
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": dict(WORKLOAD), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{m} kNN edges per step drawn from the workload's free samples"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,58 @@
+"""Builds libgprm_b200.so in-tree with nvcc for sm_100a (no JIT, no torch
+extension machinery: the library is a plain C-ABI shared object)."""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(PKG, "csrc")
+OUT = os.path.join(PKG, "libgprm_b200.so")
+SOURCES = ["gprm_api.cu", "gprm_kernels.cu"]
+HEADERS = ["gprm_device.cuh", "gprm_internal.h", "gprm_sincos64.h"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17",
+    # IEEE single precision everywhere, no FMA contraction: the FP32 kernels
+    # reproduce the reference's operation-by-operation rounding.
+    "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    "-Xcompiler", "-fPIC", "-shared", "-ccbin", "/usr/bin/g++",
+]
+
+
+def nvcc() -> str:
+    for c in ("/usr/local/cuda/bin/nvcc", "nvcc"):
+        if os.path.isabs(c) and os.path.exists(c):
+            return c
+    return "nvcc"
+
+
+def needs_build() -> bool:
+    if not os.path.exists(OUT):
+        return True
+    t = os.path.getmtime(OUT)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(PKG, "..", "include", "gprm_b200.h"))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
+    if not force and not needs_build():
+        return OUT
+    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + [
+        "-o", OUT] + [os.path.join(CSRC, f) for f in SOURCES]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building libgprm_b200.so")
+    if verbose or ptxas_info:
+        sys.stderr.write(r.stderr)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(verbose=True, force=True, ptxas_info="-v" in sys.argv)

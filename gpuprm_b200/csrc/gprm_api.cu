@@ -1,0 +1,804 @@
+/*
+ * gprm_api.cu - the C ABI of include/gprm_b200.h.
+ *
+ * Host side of RobotConfigspace<ndof> (prm/src/lib/robotspace/
+ * robotconfigspace.{h,cpp}) rebuilt for one B200:
+ *   - scene ingest and validation (load_config/construct,
+ *     robotconfigspace.cpp:20-208) into a device layout built for the
+ *     kernels (gprm_device.cuh), with every CRS index checked on the host
+ *     so that no kernel can read out of bounds;
+ *   - a request pool like the reference's buffer/stream pool
+ *     (robotconfigspace.cpp:627-650, 726-742): each in-flight request owns a
+ *     stream, pinned staging buffers and device buffers; wait() synchronises
+ *     the request's stream before copying results out (the reference relied
+ *     on pageable-memory copies being synchronous);
+ *   - every failure returns a status code and leaves a message instead of
+ *     asserting (util.hpp:44-46).
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <fstream>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/gprm_b200.h"
+#include "gprm_internal.h"
+
+using namespace gprm;
+
+namespace {
+
+thread_local std::string g_create_error = "no error";
+
+struct Request {
+    cudaStream_t st = nullptr;
+    Control* ctl = nullptr;       /* device */
+    Control* ctl_host = nullptr;  /* pinned copy read after the request */
+    float* d_a = nullptr;         /* q or qs (contiguous SoA, offset = n) */
+    float* d_b = nullptr;         /* qe */
+    int* d_res = nullptr;
+    unsigned* d_key = nullptr;
+    uint2* d_queue = nullptr;
+    float* h_a = nullptr;         /* pinned staging */
+    float* h_b = nullptr;
+    int* h_res = nullptr;
+    size_t cap_items = 0;         /* edges or configurations */
+    size_t cap_queue = 0;
+    bool busy = false;
+    /* the request in flight */
+    int kind = 0;                 /* 0 vertices, 1 edges */
+    int* user_res = nullptr;
+    int n = 0;
+    const float* user_a = nullptr;
+    const float* user_b = nullptr;
+    int user_offset = 0;
+};
+
+}  // namespace
+
+struct gprm_space {
+    int ndof = 0;
+    float dq = 0.01f;
+    int nbuf = 0;
+    float a[GPRM_MAX_DOF], alpha[GPRM_MAX_DOF], q0[GPRM_MAX_DOF], d0[GPRM_MAX_DOF];
+    float mins[GPRM_MAX_DOF], maxs[GPRM_MAX_DOF];
+    int types[GPRM_MAX_DOF];
+    int npoly = 0, npairs = 0, sumn = 0, summ = 0;
+    std::vector<float4> verts;
+    std::vector<uint8_t> dest;
+    std::vector<int4> pairs;
+
+    bool inited = false;
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    void* d_scene = nullptr;
+    DevScene dsc;
+    LaunchCfg cfg_v, cfg_e;
+
+    int mode = GPRM_MODE_FP64_BAND;
+    int policy = GPRM_EDGES_EARLY_EXIT;
+    float band = 1e-5f;
+
+    std::vector<Request> reqs;
+    std::map<int, int> live;       /* request id -> slot */
+    int next_id = 0;
+    Request dev;                   /* scratch of the device-pointer entry points */
+    Control* d_total = nullptr;    /* cumulative counters of all requests */
+    gprm_stats host_stats;         /* host-side counters */
+
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev32, ev64;   /* start/stop pairs */
+    size_t ev32_used = 0, ev64_used = 0;
+
+    std::string err = "no error";
+};
+
+namespace {
+
+int fail(gprm_space* h, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    else g_create_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                   \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((h), e_ == cudaErrorMemoryAllocation ? GPRM_ERR_NOMEM : GPRM_ERR_CUDA, \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+/* smallest float f with (double)f >= x */
+float float_ceil(double x)
+{
+    float f = (float)x;
+    if ((double)f < x) f = nextafterf(f, INFINITY);
+    while ((double)nextafterf(f, -INFINITY) >= x) f = nextafterf(f, -INFINITY);
+    return f;
+}
+
+int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
+{
+    if (!d || !out) return fail(nullptr, GPRM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->ndof < 1 || d->ndof > GPRM_MAX_DOF)
+        return fail(nullptr, GPRM_ERR_SCENE, "ndof %d outside 1..%d", d->ndof, GPRM_MAX_DOF);
+    if (d->num_polytopes < 1) return fail(nullptr, GPRM_ERR_SCENE, "N<=0");
+    if (d->num_pairs < 0) return fail(nullptr, GPRM_ERR_SCENE, "M<0");
+    if (!d->dh_a || !d->dh_alpha || !d->dh_q || !d->dh_d || !d->dh_types || !d->mins || !d->maxs ||
+        !d->poly_n || !d->poly_m || !d->vertices || !d->dsp || !d->cnt || !d->dest || !d->sys ||
+        (d->num_pairs > 0 && (!d->pair_from || !d->pair_to)))
+        return fail(nullptr, GPRM_ERR_ARG, "null array in scene description");
+    if (!(dq > 0.0f) || !isfinite(dq)) return fail(nullptr, GPRM_ERR_ARG, "dq must be positive");
+    if (nbuf < 0) return fail(nullptr, GPRM_ERR_ARG, "nbuf < 0");
+
+    gprm_space* h = new gprm_space();
+    h->ndof = d->ndof;
+    h->dq = dq;
+    h->nbuf = nbuf;
+    for (int i = 0; i < d->ndof; ++i) {
+        h->a[i] = d->dh_a[i]; h->alpha[i] = d->dh_alpha[i];
+        h->q0[i] = d->dh_q[i]; h->d0[i] = d->dh_d[i];
+        h->types[i] = d->dh_types[i];
+        h->mins[i] = d->mins[i]; h->maxs[i] = d->maxs[i];
+        if (h->types[i] != 0 && h->types[i] != 1) {
+            delete h;
+            return fail(nullptr, GPRM_ERR_SCENE, "joint %d: type %d is neither 0 nor 1", i, d->dh_types[i]);
+        }
+    }
+    h->npoly = d->num_polytopes;
+    std::vector<int> voff(h->npoly), moff(h->npoly);
+    long long sn = 0, sm = 0;
+    for (int k = 0; k < h->npoly; ++k) {
+        int n = d->poly_n[k], m = d->poly_m[k];
+        /* robotconfigspace.cpp:44-51 asserts cnt>0 and n<=100 */
+        if (n < 1 || n > GPRM_MAX_VERTICES || m < 0) {
+            delete h;
+            return fail(nullptr, GPRM_ERR_SCENE, "polytope %d: n=%d (1..%d) m=%d", k, n, GPRM_MAX_VERTICES, m);
+        }
+        if (d->sys[k] < 0 || d->sys[k] > d->ndof) {
+            delete h;
+            return fail(nullptr, GPRM_ERR_SCENE, "polytope %d: sys %d outside 0..%d", k, d->sys[k], d->ndof);
+        }
+        voff[k] = (int)sn; moff[k] = (int)sm;
+        sn += n; sm += m;
+    }
+    if (sm >= (1LL << 27) || sn >= (1LL << 30)) {
+        delete h;
+        return fail(nullptr, GPRM_ERR_SCENE, "scene too large (sum n=%lld, sum m=%lld)", sn, sm);
+    }
+    h->sumn = (int)sn;
+    h->summ = (int)sm;
+    h->verts.resize(h->sumn);
+    h->dest.assign(((size_t)h->summ + 15) & ~(size_t)15, 0);
+    for (int k = 0; k < h->npoly; ++k) {
+        int n = d->poly_n[k], m = d->poly_m[k];
+        for (int i = 0; i < n; ++i) {
+            int g = voff[k] + i;
+            int ds = d->dsp[g], c = d->cnt[g];
+            if (c < 1 || c > 255 || ds < 0 || ds + c > m || ds >= (1 << 23)) {
+                delete h;
+                return fail(nullptr, GPRM_ERR_SCENE,
+                            "polytope %d vertex %d: dsp=%d cnt=%d (need cnt in 1..255, dsp+cnt<=m=%d)", k, i, ds, c, m);
+            }
+            float x = d->vertices[3 * (size_t)g], y = d->vertices[3 * (size_t)g + 1], z = d->vertices[3 * (size_t)g + 2];
+            if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+                delete h;
+                return fail(nullptr, GPRM_ERR_SCENE, "polytope %d vertex %d is not finite", k, i);
+            }
+            int packed = (ds << 8) | c;
+            float w;
+            memcpy(&w, &packed, 4);
+            h->verts[g] = make_float4(x, y, z, w);
+        }
+        for (int j = 0; j < m; ++j) {
+            int v = d->dest[moff[k] + j];
+            if (v < 0 || v >= n) {
+                delete h;
+                return fail(nullptr, GPRM_ERR_SCENE, "polytope %d: dest[%d]=%d outside 0..%d", k, j, v, n - 1);
+            }
+            h->dest[moff[k] + j] = (uint8_t)v;
+        }
+    }
+    h->npairs = d->num_pairs;
+    h->pairs.resize(h->npairs);
+    for (int j = 0; j < h->npairs; ++j) {
+        int f = d->pair_from[j], t = d->pair_to[j];
+        if (f < 0 || f >= h->npoly || t < 0 || t >= h->npoly) {
+            delete h;
+            return fail(nullptr, GPRM_ERR_SCENE, "pair %d: (%d,%d) outside 0..%d", j, f, t, h->npoly - 1);
+        }
+        /* polytope4data::build orders pairs in CRS by `from` (polytope4data.h:268-288) */
+        if (j > 0 && f < d->pair_from[j - 1]) {
+            delete h;
+            return fail(nullptr, GPRM_ERR_SCENE, "pairs must be sorted by from (pair %d)", j);
+        }
+        h->pairs[j] = make_int4(voff[f], moff[f] | (d->sys[f] << 28), voff[t], moff[t] | (d->sys[t] << 28));
+    }
+    *out = h;
+    return GPRM_OK;
+}
+
+template <class T>
+bool read_bin(const std::string& path, T* dst, size_t n)
+{
+    std::ifstream f(path.c_str(), std::ios::in | std::ios::binary);
+    if (!f) return false;
+    f.read((char*)dst, (std::streamsize)(n * sizeof(T)));
+    return (size_t)f.gcount() == n * sizeof(T);
+}
+
+void release_request(Request& r)
+{
+    if (r.st) cudaStreamDestroy(r.st);
+    cudaFree(r.ctl);
+    cudaFree(r.d_a);
+    cudaFree(r.d_b);
+    cudaFree(r.d_res);
+    cudaFree(r.d_key);
+    cudaFree(r.d_queue);
+    cudaFreeHost(r.ctl_host);
+    cudaFreeHost(r.h_a);
+    cudaFreeHost(r.h_b);
+    cudaFreeHost(r.h_res);
+    r = Request();
+}
+
+/* Grows the buffers of `r` to hold `n` items of `kind`; the stream and
+ * the control block are created on first use.  with_host: pinned staging. */
+int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host, bool own_stream)
+{
+    if (own_stream && !r.st) CUDA_TRY(h, cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking));
+    if (!r.ctl) {
+        CUDA_TRY(h, cudaMalloc((void**)&r.ctl, sizeof(Control)));
+        CUDA_TRY(h, cudaHostAlloc((void**)&r.ctl_host, sizeof(Control), cudaHostAllocDefault));
+    }
+    size_t need_q = (kind == 0) ? n : 4 * n + 65536;
+    if (n > r.cap_items || need_q > r.cap_queue || (with_host && !r.h_res && n > 0)) {
+        size_t cap = n > r.cap_items ? n + n / 4 + 64 : r.cap_items;
+        size_t qcap = (need_q > r.cap_queue) ? need_q + need_q / 4 : r.cap_queue;
+        if (qcap < cap * 4 + 65536) qcap = cap * 4 + 65536;
+        cudaFree(r.d_a); cudaFree(r.d_b); cudaFree(r.d_res); cudaFree(r.d_key); cudaFree(r.d_queue);
+        r.d_a = r.d_b = nullptr; r.d_res = nullptr; r.d_key = nullptr; r.d_queue = nullptr;
+        size_t nd = (size_t)h->ndof;
+        CUDA_TRY(h, cudaMalloc((void**)&r.d_res, cap * sizeof(int)));
+        CUDA_TRY(h, cudaMalloc((void**)&r.d_key, cap * sizeof(unsigned)));
+        CUDA_TRY(h, cudaMalloc((void**)&r.d_queue, qcap * sizeof(uint2)));
+        if (with_host) {
+            CUDA_TRY(h, cudaMalloc((void**)&r.d_a, cap * nd * sizeof(float)));
+            CUDA_TRY(h, cudaMalloc((void**)&r.d_b, cap * nd * sizeof(float)));
+            cudaFreeHost(r.h_a); cudaFreeHost(r.h_b); cudaFreeHost(r.h_res);
+            r.h_a = r.h_b = nullptr; r.h_res = nullptr;
+            CUDA_TRY(h, cudaHostAlloc((void**)&r.h_a, cap * nd * sizeof(float), cudaHostAllocDefault));
+            CUDA_TRY(h, cudaHostAlloc((void**)&r.h_b, cap * nd * sizeof(float), cudaHostAllocDefault));
+            CUDA_TRY(h, cudaHostAlloc((void**)&r.h_res, cap * sizeof(int), cudaHostAllocDefault));
+        }
+        r.cap_items = cap;
+        r.cap_queue = qcap;
+    }
+    return GPRM_OK;
+}
+
+/* Returns a start/stop event pair from the handle's pool (grown on demand). */
+int event_pair(gprm_space* h, std::vector<cudaEvent_t>& pool, size_t& used, cudaEvent_t* a, cudaEvent_t* b)
+{
+    while (pool.size() < used + 2) {
+        cudaEvent_t e;
+        CUDA_TRY(h, cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    *a = pool[used];
+    *b = pool[used + 1];
+    used += 2;
+    return GPRM_OK;
+}
+
+__global__ void k_accumulate(const Control* c, Control* total)
+{
+    total->steps_nominal += c->steps_nominal;
+    total->steps_exec += c->steps_exec;
+    total->band_checks += c->band_checks;
+    total->band_flips += c->band_flips;
+    total->flags |= c->flags;
+    total->next += 1;  /* requests completed */
+}
+
+/* Enqueues one request on stream `st` with device inputs/outputs.
+ * kind 0: q -> res.  kind 1: (qs, qe) -> res. */
+int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
+            long long offset, cudaStream_t st)
+{
+    const int band_on = h->mode == GPRM_MODE_FP64_BAND;
+    CUDA_TRY(h, cudaMemsetAsync(r.ctl, 0, sizeof(Control), st));
+    int recheck_blocks = h->sms * 4;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+    if (h->profiling) {
+        int rc = event_pair(h, h->ev32, h->ev32_used, &e0, &e1);
+        if (rc) return rc;
+        if (band_on && (rc = event_pair(h, h->ev64, h->ev64_used, &e2, &e3))) return rc;
+    }
+    if (kind == 1)
+        CUDA_TRY(h, cudaMemsetAsync(r.d_key, h->policy == GPRM_EDGES_EARLY_EXIT ? 0xff : 0x00,
+                                    (size_t)n * sizeof(unsigned), st));
+    if (e0) CUDA_TRY(h, cudaEventRecord(e0, st));
+    if (kind == 0)
+        CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, a, n, offset, res, band_on, h->band, r.d_queue,
+                                         (unsigned)r.cap_queue, r.ctl, st));
+    else
+        CUDA_TRY(h, launch_check_edges(h->dsc, h->cfg_e, a, b, n, offset, h->dq, h->policy, r.d_key, band_on,
+                                       h->band, r.d_queue, (unsigned)r.cap_queue, r.ctl, st));
+    if (e1) CUDA_TRY(h, cudaEventRecord(e1, st));
+    if (band_on) {
+        if (e2) CUDA_TRY(h, cudaEventRecord(e2, st));
+        if (kind == 0)
+            CUDA_TRY(h, launch_recheck(h->dsc, recheck_blocks, 0, a, nullptr, nullptr, offset, h->dq, h->policy,
+                                       res, nullptr, r.d_queue, (unsigned)r.cap_queue, r.ctl, st));
+        else
+            CUDA_TRY(h, launch_recheck(h->dsc, recheck_blocks, 1, nullptr, a, b, offset, h->dq, h->policy,
+                                       nullptr, r.d_key, r.d_queue, (unsigned)r.cap_queue, r.ctl, st));
+        if (e3) CUDA_TRY(h, cudaEventRecord(e3, st));
+    }
+    if (kind == 1) CUDA_TRY(h, launch_finalize_edges(n, h->policy, r.d_key, res, st));
+    /* check + accumulate, plus recheck and finalize where they run */
+    h->host_stats.launches += 2 + (band_on ? 1 : 0) + (kind == 1 ? 1 : 0);
+    k_accumulate<<<1, 1, 0, st>>>(r.ctl, h->d_total);
+    CUDA_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+int check_ready(gprm_space* h)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (!h->inited) return fail(h, GPRM_ERR_STATE, "gprm_init has not been called");
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    return GPRM_OK;
+}
+
+/* Host-buffer request: gather into pinned staging, copy, enqueue. */
+int submit_host(gprm_space* h, int kind, const float* a, const float* b, int* res, int n, int offset, int* slot_out)
+{
+    int slot = -1;
+    for (size_t i = 0; i < h->reqs.size(); ++i)
+        if (!h->reqs[i].busy) { slot = (int)i; break; }
+    if (slot < 0) {
+        h->reqs.emplace_back();
+        slot = (int)h->reqs.size() - 1;
+    }
+    Request& r = h->reqs[slot];
+    int rc = ensure_request(h, r, kind, (size_t)(n > 0 ? n : 1), true, true);
+    if (rc) return rc;
+    const int nd = h->ndof;
+    for (int j = 0; j < nd; ++j) {
+        memcpy(r.h_a + (size_t)j * n, a + (size_t)offset * j, (size_t)n * sizeof(float));
+        if (kind == 1) memcpy(r.h_b + (size_t)j * n, b + (size_t)offset * j, (size_t)n * sizeof(float));
+    }
+    if (n > 0) {
+        CUDA_TRY(h, cudaMemcpyAsync(r.d_a, r.h_a, (size_t)n * nd * sizeof(float), cudaMemcpyHostToDevice, r.st));
+        if (kind == 1)
+            CUDA_TRY(h, cudaMemcpyAsync(r.d_b, r.h_b, (size_t)n * nd * sizeof(float), cudaMemcpyHostToDevice, r.st));
+        rc = enqueue(h, r, kind, r.d_a, kind == 1 ? r.d_b : nullptr, r.d_res, n, n, r.st);
+        if (rc) return rc;
+        CUDA_TRY(h, cudaMemcpyAsync(r.h_res, r.d_res, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, r.st));
+        CUDA_TRY(h, cudaMemcpyAsync(r.ctl_host, r.ctl, sizeof(Control), cudaMemcpyDeviceToHost, r.st));
+    }
+    r.busy = true;
+    r.kind = kind;
+    r.user_res = res;
+    r.n = n;
+    r.user_a = a;
+    r.user_b = b;
+    r.user_offset = offset;
+    *slot_out = slot;
+    return GPRM_OK;
+}
+
+int complete_host(gprm_space* h, int slot)
+{
+    Request& r = h->reqs[slot];
+    r.busy = false;
+    if (r.n == 0) return GPRM_OK;
+    CUDA_TRY(h, cudaStreamSynchronize(r.st));
+    Control c = *r.ctl_host;
+    if (c.flags & GPRM_DEVFLAG_BAD_EDGE)
+        return fail(h, GPRM_ERR_ARG, "an edge has a non-finite or oversized length (|qe-qs|/dq >= 1e8)");
+    if (c.flags & GPRM_DEVFLAG_QUEUE_FULL) {
+        /* rerun with a queue that holds every check of the request */
+        size_t need = (r.kind == 0) ? (size_t)r.n : (size_t)c.steps_nominal + 1;
+        cudaFree(r.d_queue);
+        r.d_queue = nullptr;
+        CUDA_TRY(h, cudaMalloc((void**)&r.d_queue, need * sizeof(uint2)));
+        r.cap_queue = need;
+        int rc = enqueue(h, r, r.kind, r.d_a, r.kind == 1 ? r.d_b : nullptr, r.d_res, r.n, r.n, r.st);
+        if (rc) return rc;
+        CUDA_TRY(h, cudaMemcpyAsync(r.h_res, r.d_res, (size_t)r.n * sizeof(int), cudaMemcpyDeviceToHost, r.st));
+        CUDA_TRY(h, cudaMemcpyAsync(r.ctl_host, r.ctl, sizeof(Control), cudaMemcpyDeviceToHost, r.st));
+        CUDA_TRY(h, cudaStreamSynchronize(r.st));
+        c = *r.ctl_host;
+        if (c.flags) return fail(h, GPRM_ERR_DEVICE, "device flags 0x%x after rerun", c.flags);
+    }
+    memcpy(r.user_res, r.h_res, (size_t)r.n * sizeof(int));
+    /* edge-step and band counters accumulate on the device (d_total) */
+    if (r.kind == 0) h->host_stats.vertex_checks += r.n;
+    return GPRM_OK;
+}
+
+}  // namespace
+
+/* ====================================================================== */
+
+extern "C" {
+
+int gprm_create(const gprm_scene_desc* desc, float dq, int nbuf, gprm_space** out)
+{
+    return build_space(desc, dq, nbuf, out);
+}
+
+int gprm_create_from_dir(const char* path, int ndof, float dq, int nbuf, gprm_space** out)
+{
+    if (!path || !out) return fail(nullptr, GPRM_ERR_ARG, "null argument");
+    std::string p(path);
+    int nd = 0;
+    if (!read_bin(p + "/ndof.bin", &nd, 1)) return fail(nullptr, GPRM_ERR_IO, "cannot read %s/ndof.bin", path);
+    if (nd != ndof) return fail(nullptr, GPRM_ERR_SCENE, "wrong ndof: file has %d, caller asked for %d", nd, ndof);
+    if (nd < 1 || nd > GPRM_MAX_DOF) return fail(nullptr, GPRM_ERR_SCENE, "ndof %d unsupported", nd);
+    std::vector<float> a(nd), alpha(nd), q(nd), d(nd), mins(nd), maxs(nd);
+    std::vector<int> types(nd);
+    bool ok = read_bin(p + "/dh/a.bin", a.data(), nd) && read_bin(p + "/dh/alpha.bin", alpha.data(), nd) &&
+              read_bin(p + "/dh/q.bin", q.data(), nd) && read_bin(p + "/dh/d.bin", d.data(), nd) &&
+              read_bin(p + "/dh/types.bin", types.data(), nd) && read_bin(p + "/mins.bin", mins.data(), nd) &&
+              read_bin(p + "/maxs.bin", maxs.data(), nd);
+    if (!ok) return fail(nullptr, GPRM_ERR_IO, "cannot read the DH or bound files under %s", path);
+    int N = 0, M = 0;
+    if (!read_bin(p + "/polys/N.bin", &N, 1) || N <= 0) return fail(nullptr, GPRM_ERR_IO, "bad polys/N.bin");
+    if (!read_bin(p + "/pairs/M.bin", &M, 1) || M < 0) return fail(nullptr, GPRM_ERR_IO, "bad pairs/M.bin");
+    std::vector<int> sys(N), from(M > 0 ? M : 1), to(M > 0 ? M : 1), pn(N), pm(N);
+    if (!read_bin(p + "/polys/sys.bin", sys.data(), N) ||
+        (M > 0 && (!read_bin(p + "/pairs/from.bin", from.data(), M) || !read_bin(p + "/pairs/to.bin", to.data(), M))))
+        return fail(nullptr, GPRM_ERR_IO, "cannot read sys/from/to");
+    std::vector<float> verts;
+    std::vector<int> dsp, cnt, dest;
+    for (int i = 0; i < N; ++i) {
+        std::string pp = p + "/polys/poly" + std::to_string(i);
+        int size[2];
+        if (!read_bin(pp + "/size.bin", size, 2)) return fail(nullptr, GPRM_ERR_IO, "cannot read %s/size.bin", pp.c_str());
+        int n = size[0], m = size[1];
+        if (n < 1 || n > GPRM_MAX_VERTICES || m < 0)
+            return fail(nullptr, GPRM_ERR_SCENE, "polytope %d: n=%d m=%d", i, n, m);
+        pn[i] = n; pm[i] = m;
+        size_t v0 = verts.size(), c0 = dsp.size(), e0 = dest.size();
+        verts.resize(v0 + 3 * (size_t)n);
+        dsp.resize(c0 + n); cnt.resize(c0 + n); dest.resize(e0 + m);
+        if (!read_bin(pp + "/vertices.bin", verts.data() + v0, 3 * (size_t)n) ||
+            !read_bin(pp + "/dsp.bin", dsp.data() + c0, n) || !read_bin(pp + "/cnt.bin", cnt.data() + c0, n) ||
+            (m > 0 && !read_bin(pp + "/dest.bin", dest.data() + e0, m)))
+            return fail(nullptr, GPRM_ERR_IO, "cannot read polytope files under %s", pp.c_str());
+    }
+    gprm_scene_desc desc;
+    desc.ndof = nd;
+    desc.dh_a = a.data(); desc.dh_alpha = alpha.data(); desc.dh_q = q.data(); desc.dh_d = d.data();
+    desc.dh_types = types.data(); desc.mins = mins.data(); desc.maxs = maxs.data();
+    desc.num_polytopes = N; desc.poly_n = pn.data(); desc.poly_m = pm.data();
+    desc.vertices = verts.data(); desc.dsp = dsp.data(); desc.cnt = cnt.data();
+    desc.dest = dest.empty() ? pn.data() : dest.data();
+    desc.sys = sys.data(); desc.num_pairs = M; desc.pair_from = from.data(); desc.pair_to = to.data();
+    return build_space(&desc, dq, nbuf, out);
+}
+
+int gprm_init(gprm_space* h, int rank, int size)
+{
+    if (!h) return fail(nullptr, GPRM_ERR_ARG, "null handle");
+    if (h->inited) return GPRM_OK;
+    if (size < 1 || rank < 0 || rank >= size) return fail(h, GPRM_ERR_ARG, "rank %d / size %d", rank, size);
+    int devcount = 0;
+    CUDA_TRY(h, cudaGetDeviceCount(&devcount));
+    if (devcount < 1) return fail(h, GPRM_ERR_CUDA, "no CUDA device");
+    /* device = rank*devcount/size (robotconfigspace.cpp:229) */
+    h->device = (int)(((long long)rank * devcount) / size);
+    CUDA_TRY(h, cudaSetDevice(h->device));
+    CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+
+    size_t vb = (size_t)h->sumn * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4), db = h->dest.size();
+    CUDA_TRY(h, cudaMalloc(&h->d_scene, vb + pb + db + 64));
+    char* base = (char*)h->d_scene;
+    CUDA_TRY(h, cudaMemcpy(base, h->verts.data(), vb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + vb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
+    if (db) CUDA_TRY(h, cudaMemcpy(base + vb + pb, h->dest.data(), db, cudaMemcpyHostToDevice));
+
+    DevScene& s = h->dsc;
+    memset(&s, 0, sizeof(s));
+    s.ndof = h->ndof; s.npoly = h->npoly; s.npairs = h->npairs; s.sumn = h->sumn; s.summ = h->summ;
+    for (int i = 0; i < h->ndof; ++i) {
+        s.a[i] = h->a[i]; s.q0[i] = h->q0[i]; s.d0[i] = h->d0[i]; s.types[i] = h->types[i];
+        s.mins[i] = h->mins[i]; s.maxs[i] = h->maxs[i];
+        /* cos_/sin_(alpha) as the reference CPU build evaluates them (sincosf) */
+        float sa, ca;
+        sincosf(h->alpha[i], &sa, &ca);
+        s.ca[i] = ca; s.sa[i] = sa;
+        gprm_sincos64((double)h->alpha[i], &s.sa64[i], &s.ca64[i]);
+    }
+    s.sep_thr = float_ceil(-0.000001);
+    s.tiny_thr = float_ceil(0.000001);
+    s.verts = (const float4*)base;
+    s.pairs = (const int4*)(base + vb);
+    s.dest = (const uint8_t*)(base + vb + pb);
+
+    CUDA_TRY(h, plan_launch(s, 1, 128, &h->cfg_v));
+    CUDA_TRY(h, plan_launch(s, 0, 128, &h->cfg_e));
+    CUDA_TRY(h, cudaMalloc((void**)&h->d_total, sizeof(Control)));
+    CUDA_TRY(h, cudaMemset(h->d_total, 0, sizeof(Control)));
+    memset(&h->host_stats, 0, sizeof(h->host_stats));
+    h->inited = true;
+    return GPRM_OK;
+}
+
+void gprm_destroy(gprm_space* h)
+{
+    if (!h) return;
+    if (h->inited) {
+        cudaSetDevice(h->device);
+        for (auto& r : h->reqs) {
+            if (r.st) cudaStreamSynchronize(r.st);
+            release_request(r);
+        }
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        release_request(h->dev);
+        cudaFree(h->d_total);
+        cudaFree(h->d_scene);
+        if (h->stream) cudaStreamDestroy(h->stream);
+    }
+    delete h;
+}
+
+const char* gprm_last_error(const gprm_space* h)
+{
+    return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int gprm_set_mode(gprm_space* h, int mode)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (mode != GPRM_MODE_FP32 && mode != GPRM_MODE_FP64_BAND) return fail(h, GPRM_ERR_ARG, "unknown mode %d", mode);
+    h->mode = mode;
+    return GPRM_OK;
+}
+
+int gprm_set_edge_policy(gprm_space* h, int policy)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (policy != GPRM_EDGES_EARLY_EXIT && policy != GPRM_EDGES_ALL_STEPS)
+        return fail(h, GPRM_ERR_ARG, "unknown edge policy %d", policy);
+    h->policy = policy;
+    return GPRM_OK;
+}
+
+int gprm_set_band(gprm_space* h, float band_m)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (!(band_m >= 0.0f) || !isfinite(band_m)) return fail(h, GPRM_ERR_ARG, "band must be finite and >= 0");
+    h->band = band_m;
+    return GPRM_OK;
+}
+
+int gprm_get_stats(const gprm_space* hc, gprm_stats* out)
+{
+    gprm_space* h = const_cast<gprm_space*>(hc);
+    if (!h || !out) return GPRM_ERR_ARG;
+    *out = h->host_stats;
+    if (!h->inited) return GPRM_OK;
+    int rc = check_ready(h);
+    if (rc) return rc;
+    /* the edge-step and band counters of every request accumulate on the device */
+    Control tot;
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    CUDA_TRY(h, cudaMemcpy(&tot, h->d_total, sizeof(Control), cudaMemcpyDeviceToHost));
+    out->edge_steps_nominal = (int64_t)tot.steps_nominal;
+    out->edge_steps_executed = (int64_t)tot.steps_exec;
+    out->band_rechecks = (int64_t)tot.band_checks;
+    out->band_flips = (int64_t)tot.band_flips;
+    if (tot.flags & GPRM_DEVFLAG_QUEUE_FULL)
+        return fail(h, GPRM_ERR_DEVICE, "a device-pointer request overflowed the FP64 queue; its band results are incomplete");
+    if (tot.flags & GPRM_DEVFLAG_BAD_EDGE)
+        return fail(h, GPRM_ERR_DEVICE, "a device-pointer request held a non-finite or oversized edge");
+    return GPRM_OK;
+}
+
+int gprm_indicator_batch(gprm_space* h, const float* q, int* res, int n, int offset)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!q || !res)) || offset < n) return fail(h, GPRM_ERR_ARG, "bad q/res/n/offset (offset must be >= n)");
+    int slot;
+    rc = submit_host(h, 0, q, nullptr, res, n, offset, &slot);
+    if (rc) return rc;
+    return complete_host(h, slot);
+}
+
+int gprm_indicator(gprm_space* h, const float* q, int* code)
+{
+    if (!q || !code) return fail(h, GPRM_ERR_ARG, "null argument");
+    return gprm_indicator_batch(h, q, code, 1, 1);
+}
+
+int gprm_indicator2_async(gprm_space* h, const float* qs, const float* qe, int* res, int n, int offset, int* request)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!request || n < 0 || (n > 0 && (!qs || !qe || !res)) || offset < n)
+        return fail(h, GPRM_ERR_ARG, "bad qs/qe/res/n/offset/request (offset must be >= n)");
+    /* N <= nbuf (robotconfigspace.cpp:618-619) */
+    if (h->nbuf > 0 && n > h->nbuf) return fail(h, GPRM_ERR_ARG, "N=%d exceeds nbuf=%d", n, h->nbuf);
+    int slot;
+    rc = submit_host(h, 1, qs, qe, res, n, offset, &slot);
+    if (rc) return rc;
+    int id = ++h->next_id;
+    h->live[id] = slot;
+    *request = id;
+    return GPRM_OK;
+}
+
+int gprm_indicator2_wait(gprm_space* h, int request)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    auto it = h->live.find(request);
+    if (it == h->live.end()) return fail(h, GPRM_ERR_REQUEST, "unknown request %d", request);
+    int slot = it->second;
+    h->live.erase(it);
+    return complete_host(h, slot);
+}
+
+int gprm_indicator2(gprm_space* h, const float* qs, const float* qe, int* res, int n, int offset)
+{
+    int req;
+    int rc = gprm_indicator2_async(h, qs, qe, res, n, offset, &req);
+    if (rc) return rc;
+    return gprm_indicator2_wait(h, req);
+}
+
+int gprm_check_boundaries(gprm_space* h, const float* q, int* res, int n, int offset)
+{
+    if (!h || (n > 0 && (!q || !res)) || n < 0 || offset < n) return fail(h, GPRM_ERR_ARG, "bad arguments");
+    for (int i = 0; i < n; ++i) {
+        int r = 0;
+        for (int j = 0; j < h->ndof; ++j) {
+            float qi = q[i + (size_t)offset * j];
+            if (qi < h->mins[j] || qi > h->maxs[j]) { r = 1; break; }
+        }
+        res[i] = r;
+    }
+    return GPRM_OK;
+}
+
+int gprm_check_boundaries1(gprm_space* h, const float* q, int* out)
+{
+    if (!h || !q || !out) return fail(h, GPRM_ERR_ARG, "null argument");
+    return gprm_check_boundaries(h, q, out, 1, 1);
+}
+
+float gprm_min(const gprm_space* h, int i) { return (h && i >= 0 && i < h->ndof) ? h->mins[i] : NAN; }
+float gprm_max(const gprm_space* h, int i) { return (h && i >= 0 && i < h->ndof) ? h->maxs[i] : NAN; }
+float gprm_deltaq(const gprm_space* h) { return h ? h->dq : NAN; }
+int gprm_dim(const gprm_space* h) { return h ? h->ndof : GPRM_ERR_ARG; }
+
+int gprm_indicator_batch_device(gprm_space* h, const float* q, int* res, int n, int offset, void* stream)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!q || !res)) || offset < n) return fail(h, GPRM_ERR_ARG, "bad q/res/n/offset");
+    if (n == 0) return GPRM_OK;
+    rc = ensure_request(h, h->dev, 0, (size_t)n, false, false);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    h->host_stats.vertex_checks += n;
+    return enqueue(h, h->dev, 0, q, nullptr, res, n, offset, st);
+}
+
+int gprm_indicator2_device(gprm_space* h, const float* qs, const float* qe, int* res, int n, int offset, void* stream)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!qs || !qe || !res)) || offset < n) return fail(h, GPRM_ERR_ARG, "bad qs/qe/res/n/offset");
+    if (n == 0) return GPRM_OK;
+    rc = ensure_request(h, h->dev, 1, (size_t)n, false, false);
+    if (rc) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    return enqueue(h, h->dev, 1, qs, qe, res, n, offset, st);
+}
+
+/* ---- diagnostics ------------------------------------------------------ */
+
+int gprm_debug_fk(gprm_space* h, const float* q, float* out)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!q || !out) return fail(h, GPRM_ERR_ARG, "null argument");
+    float* d = nullptr;
+    size_t nf = (size_t)(h->ndof + 1) * 12;
+    CUDA_TRY(h, cudaMalloc((void**)&d, (nf + 8) * sizeof(float)));
+    cudaMemcpy(d + nf, q, h->ndof * sizeof(float), cudaMemcpyHostToDevice);
+    cudaError_t e = launch_fk_probe(h->dsc, d + nf, d, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, nf * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(h, GPRM_ERR_CUDA, "fk probe: %s", cudaGetErrorString(e));
+    return GPRM_OK;
+}
+
+int gprm_device_sm_count(const gprm_space* h) { return h ? h->sms : 0; }
+
+int gprm_profile_enable(gprm_space* h, int on)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    h->profiling = on != 0;
+    h->ev32_used = h->ev64_used = 0;
+    return GPRM_OK;
+}
+
+int gprm_profile_read(gprm_space* h, double* fp32_ms, double* fp64_ms, int64_t* fp32_launches)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!fp32_ms || !fp64_ms || !fp32_launches) return fail(h, GPRM_ERR_ARG, "null argument");
+    CUDA_TRY(h, cudaDeviceSynchronize());
+    double t32 = 0, t64 = 0;
+    for (size_t i = 0; i + 1 < h->ev32_used; i += 2) {
+        float ms = 0;
+        CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev32[i], h->ev32[i + 1]));
+        t32 += ms;
+    }
+    for (size_t i = 0; i + 1 < h->ev64_used; i += 2) {
+        float ms = 0;
+        CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev64[i], h->ev64[i + 1]));
+        t64 += ms;
+    }
+    *fp32_ms = t32;
+    *fp64_ms = t64;
+    *fp32_launches = (int64_t)(h->ev32_used / 2);
+    return GPRM_OK;
+}
+
+int gprm_measure_fp32_peak(double* tflops)
+{
+    if (!tflops) return GPRM_ERR_ARG;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GPRM_ERR_CUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    float* out = nullptr;
+    if (cudaMalloc((void**)&out, sizeof(float) * 1024 * 1024) != cudaSuccess) return GPRM_ERR_NOMEM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    gprm::launch_fma_probe(blocks, threads, iters, out, 0);   /* warm-up */
+    cudaEventRecord(a, 0);
+    gprm::launch_fma_probe(blocks, threads, iters, out, 0);
+    cudaEventRecord(b, 0);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e != cudaSuccess || ms <= 0) return GPRM_ERR_CUDA;
+    double flops = 2.0 * (double)blocks * threads * iters * GPRM_FMA_PROBE_CHAINS;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return GPRM_OK;
+}
+
+}  /* extern "C" */

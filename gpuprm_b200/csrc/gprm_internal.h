@@ -1,0 +1,74 @@
+/*
+ * gprm_internal.h - interface between the C ABI (gprm_api.cu) and the
+ * kernels (gprm_kernels.cu).  Not installed; not part of the public ABI.
+ */
+#ifndef GPRM_INTERNAL_H
+#define GPRM_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "gprm_device.cuh"
+
+namespace gprm {
+
+/* Per-request control block in device memory, zeroed before each request. */
+struct Control {
+    unsigned long long next;          /* work counter (items handed out) */
+    unsigned int qcount;              /* FP64 queue entries appended (may exceed capacity) */
+    unsigned int flags;               /* GPRM_DEVFLAG_* */
+    unsigned long long steps_nominal; /* sum of testnum of the request's edges */
+    unsigned long long steps_exec;    /* steps evaluated in FP32 */
+    unsigned long long band_checks;   /* checks recomputed in FP64 */
+    unsigned long long band_flips;    /* FP64 verdict differs from FP32 verdict */
+};
+
+#define GPRM_DEVFLAG_BAD_EDGE    1u   /* non-finite or oversized edge length */
+#define GPRM_DEVFLAG_QUEUE_FULL  2u   /* FP64 queue overflowed; rerun needed */
+
+/* How a launch reads its scene. */
+struct LaunchCfg {
+    int blocks;          /* persistent grid size */
+    int threads;         /* threads per block (multiple of 32) */
+    size_t smem_bytes;   /* dynamic shared memory (scene copy), 0 = global */
+};
+
+enum EdgePolicy { EDGE_EARLY_EXIT = 0, EDGE_ALL_STEPS = 1 };
+
+/* Scene bytes when staged in shared memory. */
+size_t scene_smem_bytes(const DevScene& sc);
+
+/* Vertex checks: res[i] = code of configuration q[i + offset*j]. */
+cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q,
+                                 long long n, long long offset, int* res, int band_on, float band,
+                                 uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
+
+/* Edge checks, FP32 pass: key[e] is set per the edge policy (see kernels). */
+cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs,
+                               const float* qe, long long n, long long offset, float dq, int policy,
+                               unsigned* key, int band_on, float band, uint2* queue, unsigned qcap,
+                               Control* ctl, cudaStream_t st);
+
+/* FP64 recheck of queued vertex (kind 0) or edge-step (kind 1) items. */
+cudaError_t launch_recheck(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,
+                           const float* qe, long long offset, float dq, int policy, int* res,
+                           unsigned* key, const uint2* queue, unsigned qcap, Control* ctl,
+                           cudaStream_t st);
+
+/* res[e] = code decoded from key[e] */
+cudaError_t launch_finalize_edges(long long n, int policy, const unsigned* key, int* res,
+                                  cudaStream_t st);
+
+/* Occupancy-derived persistent grid for the FP32 kernels. */
+cudaError_t plan_launch(const DevScene& sc, int vertex_kernel, int threads, LaunchCfg* cfg);
+
+/* FMA throughput probe: every thread runs `iters` rounds of
+ * GPRM_FMA_PROBE_CHAINS independent FMAs. */
+#define GPRM_FMA_PROBE_CHAINS 16
+cudaError_t launch_fma_probe(int blocks, int threads, int iters, float* out, cudaStream_t st);
+
+/* The FP32 per-configuration FK used by tests: out[(ndof+1)*12]. */
+cudaError_t launch_fk_probe(const DevScene& sc, const float* q, float* out, cudaStream_t st);
+
+}  // namespace gprm
+
+#endif

@@ -1,0 +1,441 @@
+/*
+ * gprm_kernels.cu - sm_100a kernels of the collision checker.
+ *
+ * Replaces kernel_indicator2 / kernel_indicator2_1 and set_kernel
+ * (prm/src/lib/robotspace/robotconfigspace.cpp:362-595) and the host loop
+ * over indicator(q) (robotconfigspace.cpp:313-346, prmsolver.cpp:2611).
+ *
+ * Work mapping (persistent grid, warps take work from a device counter):
+ *   vertex checks  a warp takes 32 configurations, one per lane; every lane
+ *                  runs FK and then the reference's pair loop with its own
+ *                  early exit, lanes stepping through the pairs together.
+ *   edge checks    a warp takes one edge; its lanes hold 32 steps of that
+ *                  edge (coarse-to-fine: round r, lane i -> step i*R + r with
+ *                  R = ceil(testnum/32); or descending steps when every step's
+ *                  code is wanted) and step through the pairs together.  Nearby
+ *                  steps take nearly the same path through the algorithm, so
+ *                  the lanes stay converged, and one warp vote after each pair
+ *                  ends the edge at its first colliding step.
+ * The scene (vertices with packed adjacency, neighbour bytes, pair table)
+ * is copied into shared memory per block when it fits.
+ *
+ * FP64 band: a check whose FP32 result is decided within the band (or by
+ * the iteration cap) is appended to a queue; k_recheck recomputes it in
+ * FP64, thread per item, and its verdict replaces the FP32 one.
+ */
+#include "gprm_internal.h"
+
+namespace gprm {
+
+#define FULL_MASK 0xffffffffu
+
+size_t scene_smem_bytes(const DevScene& sc)
+{
+    size_t v = (size_t)sc.sumn * 16, p = (size_t)sc.npairs * 16;
+    size_t d = ((size_t)sc.summ + 15) & ~(size_t)15;
+    return v + p + d;
+}
+
+struct SceneView {
+    const float4* verts;
+    const uint8_t* dest;
+    const int4* pairs;
+};
+
+template <bool SMEM>
+__device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned char* smem)
+{
+    SceneView s;
+    if (!SMEM) {
+        s.verts = sc.verts;
+        s.dest = sc.dest;
+        s.pairs = sc.pairs;
+        return s;
+    }
+    float4* v = reinterpret_cast<float4*>(smem);
+    int4* p = reinterpret_cast<int4*>(smem + (size_t)sc.sumn * 16);
+    uint32_t* d = reinterpret_cast<uint32_t*>(smem + (size_t)sc.sumn * 16 + (size_t)sc.npairs * 16);
+    for (int i = threadIdx.x; i < sc.sumn; i += blockDim.x) v[i] = sc.verts[i];
+    for (int i = threadIdx.x; i < sc.npairs; i += blockDim.x) p[i] = sc.pairs[i];
+    const uint32_t* dsrc = reinterpret_cast<const uint32_t*>(sc.dest);
+    for (int i = threadIdx.x; i < (sc.summ + 3) / 4; i += blockDim.x) d[i] = dsrc[i];
+    __syncthreads();
+    s.verts = v;
+    s.dest = reinterpret_cast<const uint8_t*>(d);
+    s.pairs = p;
+    return s;
+}
+
+/* Appends the items of the lanes with `want` set, one atomic per warp. */
+__device__ __forceinline__ void warp_append(bool want, uint2 item, uint2* queue, unsigned qcap,
+                                            Control* ctl)
+{
+    unsigned m = __ballot_sync(FULL_MASK, want);
+    if (!m) return;
+    int lane = threadIdx.x & 31;
+    unsigned base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(&ctl->qcount, (unsigned)__popc(m));
+    base = __shfl_sync(FULL_MASK, base, __ffs(m) - 1);
+    if (want) {
+        unsigned slot = base + __popc(m & ((1u << lane) - 1));
+        if (slot < qcap) queue[slot] = item;
+        else atomicOr(&ctl->flags, GPRM_DEVFLAG_QUEUE_FULL);
+    }
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
+{
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
+    return x;
+}
+
+/* ------------------------------------------------------------------ */
+/* vertex checks                                                        */
+/* ------------------------------------------------------------------ */
+
+template <bool SMEM>
+__global__ void __launch_bounds__(128) k_check_configs(DevScene sc, const float* __restrict__ q,
+                                                       long long n, long long offset,
+                                                       int* __restrict__ res, int band_on, float band,
+                                                       uint2* __restrict__ queue, unsigned qcap,
+                                                       Control* ctl)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const SceneView S = stage_scene<SMEM>(sc, smem);
+    const int lane = threadIdx.x & 31;
+    unsigned long long exec = 0;
+    Frame<float> F[GPRM_MAX_FRAMES];
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&ctl->next, 32ull);
+        base = __shfl_sync(FULL_MASK, base, 0);
+        if (base >= (unsigned long long)n) break;
+        const long long i = (long long)base + lane;
+        const bool valid = i < n;
+        float qi[GPRM_MAX_FRAMES];
+        int code = 0;
+        bool active = valid;
+        if (valid) {
+            for (int j = 0; j < sc.ndof; ++j) qi[j] = q[i + offset * j];
+            /* check_boundaries(q) (robotconfigspace.cpp:795-802) */
+            for (int j = 0; j < sc.ndof; ++j)
+                if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
+        }
+        if (active) forward_kinematics<PF32>(sc, qi, F);
+        float mmin = PF32::inf(), mdec = 0.0f;
+#pragma unroll 1
+        for (int j = 0; j < sc.npairs; ++j) {
+            if (!__any_sync(FULL_MASK, active)) break;
+            if (active) {
+                float m;
+                int r = pair_test<PF32>(sc, S.verts, S.dest, S.pairs[j], F, &m);
+                if (r != 0) { code = r; mdec = m; active = false; }
+                else mmin = min_nan(mmin, m);
+            }
+        }
+        if (valid) {
+            exec += (code != 1);
+            res[i] = code;
+        }
+        bool want = valid && band_on && code != 1 && in_band(code, code == 0 ? mmin : mdec, band);
+        warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), queue, qcap, ctl);
+    }
+    exec = warp_sum(exec);
+    if (lane == 0 && exec) atomicAdd(&ctl->steps_exec, exec);
+}
+
+/* ------------------------------------------------------------------ */
+/* edge checks                                                          */
+/* ------------------------------------------------------------------ */
+
+/* Edge keys (one uint32 per edge, decoded by k_finalize_edges):
+ *   early exit  min over colliding steps of (order << 4 | (code+1)),
+ *               0xffffffff = free
+ *   all steps   max over colliding steps of ((t+1) << 4 | (code+1)),
+ *               0 = free                                                   */
+__device__ __forceinline__ unsigned early_key(unsigned order, int code) { return (order << 4) | (unsigned)(code + 1); }
+__device__ __forceinline__ unsigned all_key(int t, int code) { return ((unsigned)(t + 1) << 4) | (unsigned)(code + 1); }
+
+template <bool SMEM, int POLICY>
+__global__ void __launch_bounds__(128) k_check_edges(DevScene sc, const float* __restrict__ qs,
+                                                     const float* __restrict__ qe, long long n,
+                                                     long long offset, float dq, unsigned* __restrict__ key,
+                                                     int band_on, float band, uint2* __restrict__ queue,
+                                                     unsigned qcap, Control* ctl)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const SceneView S = stage_scene<SMEM>(sc, smem);
+    const int lane = threadIdx.x & 31;
+    unsigned long long exec = 0, nominal = 0;
+    Frame<float> F[GPRM_MAX_FRAMES];
+    for (;;) {
+        unsigned long long eu = 0;
+        if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
+        eu = __shfl_sync(FULL_MASK, eu, 0);
+        if (eu >= (unsigned long long)n) break;
+        const long long e = (long long)eu;
+        const int tn = edge_testnum(qs, qe, e, offset, sc.ndof, dq);
+        if (tn < 0) {
+            if (lane == 0) atomicOr(&ctl->flags, GPRM_DEVFLAG_BAD_EDGE);
+            continue;
+        }
+        if (lane == 0) nominal += tn;
+        const int R = (tn + 31) >> 5;
+        bool decided = false;
+#pragma unroll 1
+        for (int r = 0; r < R && !decided; ++r) {
+            int t;
+            unsigned order;
+            bool valid;
+            if (POLICY == EDGE_EARLY_EXIT) {
+                t = lane * R + r;
+                valid = t < tn;
+                order = (unsigned)(r * 32 + lane);
+            } else {
+                int idx = r * 32 + lane;
+                t = tn - 1 - idx;
+                valid = idx < tn;
+                order = 0;
+            }
+            float qi[GPRM_MAX_FRAMES];
+            if (valid) {
+                edge_step_config(qs, qe, e, offset, sc.ndof, t, tn, qi);
+                forward_kinematics<PF32>(sc, qi, F);
+            }
+            const unsigned valid_mask = __ballot_sync(FULL_MASK, valid);
+            if (lane == 0) exec += __popc(valid_mask);
+            bool active = valid;
+            int code = 0;
+            float mmin = PF32::inf(), mdec = 0.0f;
+            int cut = 32;   /* lanes above the highest-priority colliding lane no longer matter */
+            int jend = 0;   /* pairs processed by the warp */
+#pragma unroll 1
+            for (int j = 0; j < sc.npairs; ++j) {
+                if (!__any_sync(FULL_MASK, active)) break;
+                if (active) {
+                    float m;
+                    int rr = pair_test<PF32>(sc, S.verts, S.dest, S.pairs[j], F, &m);
+                    if (rr != 0) { code = rr; mdec = m; active = false; }
+                    else mmin = min_nan(mmin, m);
+                }
+                jend = j + 1;
+                bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
+                unsigned hits = __ballot_sync(FULL_MASK, oobj);
+                if (hits) {
+                    int Lj = __ffs(hits) - 1;
+                    if (Lj < cut) cut = Lj;
+                    if (POLICY == EDGE_EARLY_EXIT) break;
+                    if (lane > cut) active = false;
+                }
+            }
+            /* settle the round */
+            const bool oob = code != 0 && !(band_on && in_band(code, mdec, band));
+            const unsigned hits = __ballot_sync(FULL_MASK, oob && lane <= cut);
+            const int L = hits ? __ffs(hits) - 1 : 32;
+            const bool free_done = valid && code == 0 && active && jend == sc.npairs;
+            const bool inb = band_on && ((code != 0 && !oob) || (free_done && in_band(0, mmin, band)));
+            /* in-band steps earlier in order (early exit) or higher t (all steps)
+               than the deciding step go to the FP64 queue */
+            const bool want = inb && lane < L;
+            warp_append(want, make_uint2((unsigned)e, (unsigned)t | ((unsigned)(code + 1) << 27)),
+                        queue, qcap, ctl);
+            if (hits) {
+                if (lane == L)
+                    key[e] = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
+                decided = true;
+            }
+        }
+    }
+    exec = warp_sum(exec);
+    nominal = warp_sum(nominal);
+    if (lane == 0) {
+        if (exec) atomicAdd(&ctl->steps_exec, exec);
+        if (nominal) atomicAdd(&ctl->steps_nominal, nominal);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* FP64 recheck and finalisation                                        */
+/* ------------------------------------------------------------------ */
+
+__global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const float* __restrict__ q,
+                                                 const float* __restrict__ qs, const float* __restrict__ qe,
+                                                 long long offset, float dq, int policy,
+                                                 int* __restrict__ res, unsigned* __restrict__ key,
+                                                 const uint2* __restrict__ queue, unsigned qcap,
+                                                 Control* ctl)
+{
+    unsigned cnt = ctl->qcount;
+    if (cnt > qcap) cnt = qcap;
+    unsigned long long checks = 0, flips = 0;
+    Frame<double> F[GPRM_MAX_FRAMES];
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
+        const uint2 it = queue[idx];
+        const int code32 = (int)(it.y >> 27) - 1;
+        float qi[GPRM_MAX_FRAMES];
+        int t = 0, tn = 0;
+        if (kind == 0) {
+            for (int j = 0; j < sc.ndof; ++j) qi[j] = q[(long long)it.x + offset * j];
+        } else {
+            t = (int)(it.y & ((1u << 27) - 1));
+            tn = edge_testnum(qs, qe, (long long)it.x, offset, sc.ndof, dq);
+            edge_step_config(qs, qe, (long long)it.x, offset, sc.ndof, t, tn, qi);
+        }
+        forward_kinematics<PF64>(sc, qi, F);
+        int code = 0;
+#pragma unroll 1
+        for (int j = 0; j < sc.npairs; ++j) {
+            double m;
+            int r = pair_test<PF64>(sc, sc.verts, sc.dest, sc.pairs[j], F, &m);
+            if (r != 0) { code = r; break; }
+        }
+        ++checks;
+        flips += ((code != 0) != (code32 != 0));
+        if (kind == 0) {
+            res[it.x] = code;
+        } else if (code != 0) {
+            if (policy == EDGE_EARLY_EXIT) {
+                int R = (tn + 31) >> 5;
+                unsigned order = (unsigned)((t % R) * 32 + t / R);
+                atomicMin(&key[it.x], early_key(order, code));
+            } else {
+                atomicMax(&key[it.x], all_key(t, code));
+            }
+        }
+    }
+    if (checks) atomicAdd(&ctl->band_checks, checks);
+    if (flips) atomicAdd(&ctl->band_flips, flips);
+}
+
+__global__ void k_finalize_edges(long long n, int policy, const unsigned* __restrict__ key,
+                                 int* __restrict__ res)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        unsigned k = key[e];
+        bool none = (policy == EDGE_EARLY_EXIT) ? (k == 0xffffffffu) : (k == 0u);
+        res[e] = none ? 0 : (int)(k & 15u) - 1;
+    }
+}
+
+__global__ void k_fk_probe(DevScene sc, const float* q, float* out)
+{
+    Frame<float> F[GPRM_MAX_FRAMES];
+    float qi[GPRM_MAX_FRAMES];
+    for (int j = 0; j < sc.ndof; ++j) qi[j] = q[j];
+    forward_kinematics<PF32>(sc, qi, F);
+    for (int f = 0; f <= sc.ndof; ++f)
+        for (int c = 0; c < 12; ++c) out[f * 12 + c] = F[f].m[c];
+}
+
+/* ------------------------------------------------------------------ */
+/* launchers                                                            */
+/* ------------------------------------------------------------------ */
+
+cudaError_t plan_launch(const DevScene& sc, int vertex_kernel, int threads, LaunchCfg* cfg)
+{
+    int dev = 0, sms = 0, optin = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    size_t need = scene_smem_bytes(sc);
+    bool smem = need <= (size_t)optin / 2;   /* leave room for two blocks per SM */
+    const void* fn;
+    if (vertex_kernel) fn = smem ? (const void*)k_check_configs<true> : (const void*)k_check_configs<false>;
+    else fn = smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT>;
+    cfg->smem_bytes = smem ? need : 0;
+    cfg->threads = threads;
+    if (smem) {
+        const void* fns[4] = {(const void*)k_check_configs<true>, (const void*)k_check_edges<true, EDGE_EARLY_EXIT>,
+                              (const void*)k_check_edges<true, EDGE_ALL_STEPS>, nullptr};
+        for (int i = 0; i < 3; ++i) {
+            err = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+            if (err != cudaSuccess) return err;
+        }
+    }
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, cfg->smem_bytes);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    cfg->blocks = sms * per_sm;
+    return cudaSuccess;
+}
+
+cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q, long long n,
+                                 long long offset, int* res, int band_on, float band, uint2* queue,
+                                 unsigned qcap, Control* ctl, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    if (cfg.smem_bytes)
+        k_check_configs<true><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on,
+                                                                              band, queue, qcap, ctl);
+    else
+        k_check_configs<false><<<cfg.blocks, cfg.threads, 0, st>>>(sc, q, n, offset, res, band_on, band,
+                                                                  queue, qcap, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs, const float* qe,
+                               long long n, long long offset, float dq, int policy, unsigned* key,
+                               int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
+                               cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    size_t sm = cfg.smem_bytes;
+    if (policy == EDGE_EARLY_EXIT) {
+        if (sm) k_check_edges<true, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+        else k_check_edges<false, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, 0, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+    } else {
+        if (sm) k_check_edges<true, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+        else k_check_edges<false, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, 0, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_recheck(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,
+                           const float* qe, long long offset, float dq, int policy, int* res, unsigned* key,
+                           const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
+{
+    k_recheck<<<blocks, 128, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, res, key, queue, qcap, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_edges(long long n, int policy, const unsigned* key, int* res, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    long long b = (n + 255) / 256;
+    if (b > 4096) b = 4096;
+    k_finalize_edges<<<(int)b, 256, 0, st>>>(n, policy, key, res);
+    return cudaGetLastError();
+}
+
+__global__ void k_fma_probe(int iters, float* out)
+{
+    float x[GPRM_FMA_PROBE_CHAINS];
+    const float a = 1.0000001f, b = -0.9999999f;
+#pragma unroll
+    for (int c = 0; c < GPRM_FMA_PROBE_CHAINS; ++c) x[c] = (float)(threadIdx.x + c);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int c = 0; c < GPRM_FMA_PROBE_CHAINS; ++c) x[c] = __fmaf_rn(x[c], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < GPRM_FMA_PROBE_CHAINS; ++c) s += x[c];
+    out[(blockIdx.x * blockDim.x + threadIdx.x) & (1024 * 1024 - 1)] = s;
+}
+
+cudaError_t launch_fma_probe(int blocks, int threads, int iters, float* out, cudaStream_t st)
+{
+    k_fma_probe<<<blocks, threads, 0, st>>>(iters, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fk_probe(const DevScene& sc, const float* q, float* out, cudaStream_t st)
+{
+    k_fk_probe<<<1, 1, 0, st>>>(sc, q, out);
+    return cudaGetLastError();
+}
+
+}  // namespace gprm

@@ -1,0 +1,206 @@
+/*
+ * gprm_b200.h - C ABI of the B200 configuration-space collision checker.
+ *
+ * This library replaces the collision-checking half of GPUPRM's
+ * RobotConfigspace<ndof> (prm/src/lib/robotspace/robotconfigspace.{h,cpp})
+ * behind the planner-facing interface Configspace<ndof>
+ * (prm/src/lib/prm/configspace.hpp:10-50).  Every entry point takes plain
+ * pointers and sizes, returns an int status (GPRM_OK == 0, negative on
+ * error, never aborts) and leaves a message for gprm_last_error().
+ *
+ * Verdict codes are the reference's (collision4.h:226-332,
+ * robotconfigspace.cpp:313-346): 0 = free, > 0 = the Chung-Wang iteration
+ * that found "no separating half plane", -1 = iteration cap reached,
+ * 1 = outside the joint bounds (vertex checks only).  Any nonzero code means
+ * "not free".
+ *
+ * Layouts follow the reference:
+ *   configurations  q[i + offset*j]  (component j of configuration i; SoA
+ *                   with row stride `offset`, as in indicator(q,res,N,offset)
+ *                   and indicator2, configspace.hpp:262,268)
+ *   single config   q[j]             (indicator(q), configspace.hpp:264)
+ *
+ * Threading: one host thread per handle, like the reference
+ * (robotconfigspace.h:116,166); different handles may be used concurrently.
+ */
+#ifndef GPRM_B200_H
+#define GPRM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define GPRM_OK               0
+#define GPRM_ERR_ARG         -1   /* bad argument (null pointer, size, ...) */
+#define GPRM_ERR_SCENE       -2   /* scene failed validation */
+#define GPRM_ERR_IO          -3   /* config directory unreadable */
+#define GPRM_ERR_CUDA        -4   /* CUDA runtime error */
+#define GPRM_ERR_NOMEM       -5   /* device or host allocation failed */
+#define GPRM_ERR_STATE       -6   /* call out of order (e.g. not initialised) */
+#define GPRM_ERR_REQUEST     -7   /* unknown async request id */
+#define GPRM_ERR_DEVICE      -8   /* device-side watchdog or bounds flag */
+#define GPRM_ERR_UNSUPPORTED -9
+
+/* ---- limits (the reference asserts n <= 100, robotconfigspace.cpp:50) -- */
+#define GPRM_MAX_VERTICES 100
+#define GPRM_MAX_DOF      7
+
+/* ---- check modes (gprm_set_mode) ------------------------------------- */
+/* FP32 only: verdicts bit-identical to the reference CPU path. */
+#define GPRM_MODE_FP32        0
+/* FP32, then every check whose separation margin is inside the band is
+ * recomputed in FP64 and the FP64 verdict is returned for it. */
+#define GPRM_MODE_FP64_BAND   1
+
+/* Edge evaluation (gprm_set_edge_policy). */
+/* Stop an edge at its first colliding step; res[e] is that step's code. */
+#define GPRM_EDGES_EARLY_EXIT 0
+/* Check every step; res[e] is the code of the last colliding step, exactly
+ * what the reference CPU path writes (robotconfigspace.cpp:458,694-705). */
+#define GPRM_EDGES_ALL_STEPS  1
+
+/* ---- scene description --------------------------------------------- */
+/* The arrays of a config directory (robotconfigspace.cpp:101-208) and of
+ * RobotConfigspace's array constructor (robotconfigspace.cpp:75-82, with
+ * Robot<ndof> from robot.h:10-22 and polytope from polytope.h:5-16).
+ * Polytopes must be sorted by sys and pairs by `pair_from`, as
+ * polytope4data::build requires (polytope4data.h:224-291). */
+typedef struct gprm_scene_desc {
+    int ndof;                 /* 1..GPRM_MAX_DOF */
+    const float* dh_a;        /* [ndof] modified-DH a */
+    const float* dh_alpha;    /* [ndof] modified-DH alpha */
+    const float* dh_q;        /* [ndof] theta of prismatic joints */
+    const float* dh_d;        /* [ndof] d of revolute joints */
+    const int*   dh_types;    /* [ndof] 0 revolute, 1 prismatic */
+    const float* mins;        /* [ndof] joint lower bounds */
+    const float* maxs;        /* [ndof] joint upper bounds */
+    int num_polytopes;        /* N */
+    const int*   poly_n;      /* [N] vertices per polytope */
+    const int*   poly_m;      /* [N] CRS entries per polytope */
+    const float* vertices;    /* [3*sum(n)] xyz, body frame, concatenated */
+    const int*   dsp;         /* [sum(n)] CRS offsets, local to the polytope */
+    const int*   cnt;         /* [sum(n)] neighbour counts, all > 0 */
+    const int*   dest;        /* [sum(m)] neighbour indices, local */
+    const int*   sys;         /* [N] frame index 0..ndof (0 = world) */
+    int num_pairs;            /* M */
+    const int*   pair_from;   /* [M] sorted ascending */
+    const int*   pair_to;     /* [M] */
+} gprm_scene_desc;
+
+typedef struct gprm_space gprm_space;   /* one scene on one device */
+
+/* Counters since creation (numthreads_all, robotconfigspace.h:169, plus
+ * the FP64 band statistics). */
+typedef struct gprm_stats {
+    int64_t vertex_checks;        /* configurations checked */
+    int64_t edge_steps_nominal;   /* sum of testnum over checked edges */
+    int64_t edge_steps_executed;  /* steps actually evaluated */
+    int64_t band_rechecks;        /* checks recomputed in FP64 */
+    int64_t band_flips;           /* of those, verdict changed free<->not free */
+    int64_t launches;             /* kernels launched */
+} gprm_stats;
+
+/* ---- lifetime --------------------------------------------------------- */
+
+/* RobotConfigspace(robot, polys, sys, N, from, to, M, mins, maxs, dq, nbuf)
+ * (robotconfigspace.cpp:75-82).  `nbuf` bounds N of every edge request like
+ * the reference's nbuf (robotconfigspace.cpp:618-619); 0 means unbounded. */
+int gprm_create(const gprm_scene_desc* desc, float dq, int nbuf, gprm_space** out);
+
+/* RobotConfigspace(path, dq, nbuf) (robotconfigspace.cpp:84-98): reads the
+ * reference's config directory; `ndof` must match ndof.bin. */
+int gprm_create_from_dir(const char* path, int ndof, float dq, int nbuf, gprm_space** out);
+
+/* init(rank, size) (configspace.hpp:13, robotconfigspace.cpp:213-287):
+ * selects device rank*devcount/size, uploads the scene, creates a stream. */
+int gprm_init(gprm_space* h, int rank, int size);
+
+/* Frees device and host state (the reference's clear() is a stub,
+ * robotconfigspace.cpp:289-295). Safe on NULL. */
+void gprm_destroy(gprm_space* h);
+
+/* Message of the last failed call on `h` (or of the last failed create
+ * when h == NULL).  Never NULL. */
+const char* gprm_last_error(const gprm_space* h);
+
+int gprm_set_mode(gprm_space* h, int mode);
+int gprm_set_edge_policy(gprm_space* h, int policy);
+/* FP64 band half-width in metres (default 1e-5). */
+int gprm_set_band(gprm_space* h, float band_m);
+int gprm_get_stats(const gprm_space* h, gprm_stats* out);
+
+/* ---- queries (host buffers) ------------------------------------------ */
+
+/* indicator(q) (configspace.hpp:264, robotconfigspace.cpp:313-346):
+ * bounds check (code 1), then the pair loop; *code gets the first nonzero
+ * pair result or 0. */
+int gprm_indicator(gprm_space* h, const float* q, int* code);
+
+/* indicator(q, res, N, offset) (configspace.hpp:262): batched vertex check,
+ * q[i + offset*j]; res[i] gets the code of configuration i.  The reference
+ * leaves this unimplemented (robotconfigspace.cpp:304-309). */
+int gprm_indicator_batch(gprm_space* h, const float* q, int* res, int n, int offset);
+
+/* indicator2(qs, qe, res, N, offset) (configspace.hpp:268,
+ * robotconfigspace.cpp:745-752): edge i runs from qs[i+offset*j] to
+ * qe[i+offset*j] in testnum = (int)(|qe-qs|/dq)+1 steps; res[i] = 0 if every
+ * step is free, else nonzero (see the edge policies above). */
+int gprm_indicator2(gprm_space* h, const float* qs, const float* qe, int* res, int n, int offset);
+
+/* indicator2_async / indicator2_async_wait (configspace.hpp:269-270,
+ * robotconfigspace.cpp:617-742).  `qs`, `qe` are read before the call
+ * returns; `res` must stay valid until gprm_indicator2_wait returns, which
+ * synchronises the request's stream. */
+int gprm_indicator2_async(gprm_space* h, const float* qs, const float* qe, int* res,
+                          int n, int offset, int* request);
+int gprm_indicator2_wait(gprm_space* h, int request);
+
+/* check_boundaries(q, res, N, offset) and check_boundaries(q)
+ * (configspace.hpp:277-279, robotconfigspace.cpp:780-802): 1 outside. */
+int gprm_check_boundaries(gprm_space* h, const float* q, int* res, int n, int offset);
+int gprm_check_boundaries1(gprm_space* h, const float* q, int* inside_violation);
+
+/* min(i), max(i), deltaq(), dim() (configspace.hpp:282-289). */
+float gprm_min(const gprm_space* h, int i);
+float gprm_max(const gprm_space* h, int i);
+float gprm_deltaq(const gprm_space* h);
+int   gprm_dim(const gprm_space* h);
+
+/* ---- queries (device buffers, caller's stream; no host sync) ----------
+ * Pointers are device pointers; `stream` is a cudaStream_t (NULL = the
+ * handle's stream).  These never synchronise and are safe to capture in a
+ * CUDA graph after one warm-up call with the same sizes. */
+int gprm_indicator_batch_device(gprm_space* h, const float* q, int* res, int n,
+                                int offset, void* stream);
+int gprm_indicator2_device(gprm_space* h, const float* qs, const float* qe, int* res,
+                           int n, int offset, void* stream);
+
+/* ---- diagnostics (no counterpart in the reference) -------------------- */
+
+/* The FP32 frames the kernels compute for one configuration q[ndof]:
+ * out[(ndof+1)*12], frame f column c row r at out[f*12 + c*3 + r], in the
+ * column layout of trafo4 (geo4.h:24). */
+int gprm_debug_fk(gprm_space* h, const float* q, float* out);
+
+/* Streaming multiprocessors of the handle's device (0 before init). */
+int gprm_device_sm_count(const gprm_space* h);
+
+/* Kernel timing: while enabled, every request records CUDA events around
+ * its FP32 check kernel and its FP64 recheck kernel on the stream they run
+ * on; gprm_profile_read synchronises the device and returns the summed
+ * durations (ms) and the number of timed FP32 launches since enabling. */
+int gprm_profile_enable(gprm_space* h, int on);
+int gprm_profile_read(gprm_space* h, double* fp32_ms, double* fp64_ms, int64_t* fp32_launches);
+
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (2 flops
+ * per FMA), from a register-resident FMA loop on every SM. */
+int gprm_measure_fp32_peak(double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPRM_B200_H */
