@@ -178,7 +178,8 @@ def run_ours(args, rank, world, local_rank):
     qs, qe = ws["qs"], ws["qe"]
     E = qs.shape[1]
     res = torch.empty(E, dtype=torch.int32, device=dev)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
 
     def barrier():
         if world > 1:
@@ -269,7 +270,7 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(WORKLOAD, edges_per_gpu=E, free_samples=ws["n_free"], policy=args.policy,
                        l2="inputs (qs,qe: %.0f MB) larger than L2" % (2 * qs.numel() * 4 / 1e6)),
         "executed_steps_per_s": executed_all / t_max,
-        "nominal_steps_per_step": nominal, "executed_steps_per_step_": executed / args.steps,
+        "nominal_steps_per_step": nominal // args.steps, "executed_steps_per_step": executed // args.steps,
         "colliding_edges": colliding, "band_rechecks_per_step": band / args.steps,
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},

@@ -50,6 +50,8 @@ class Stats(C.Structure):
         ("band_rechecks", C.c_int64),
         ("band_flips", C.c_int64),
         ("launches", C.c_int64),
+        ("pairs_certified", C.c_int64),
+        ("pairs_tested", C.c_int64),
     ]
 
 
@@ -118,6 +120,8 @@ SIGNATURES = [
     ("gprm_indicator2_device", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     ("gprm_debug_fk", C.c_int, [_P, _F, _F]),
     ("gprm_device_sm_count", C.c_int, [_P]),
+    ("gprm_set_launch", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    ("gprm_get_launch", C.c_int, [_P, C.c_int, _I, _I, _I]),
     ("gprm_profile_enable", C.c_int, [_P, C.c_int]),
     ("gprm_profile_read", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("gprm_measure_fp32_peak", C.c_int, [C.POINTER(C.c_double)]),

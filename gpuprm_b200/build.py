@@ -38,11 +38,12 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
-    if not force and not needs_build():
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, out: str = OUT,
+          defines=()) -> str:
+    if not force and out == OUT and not needs_build():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + [
-        "-o", OUT] + [os.path.join(CSRC, f) for f in SOURCES]
+    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + [f"-D{d}" for d in defines] + [
+        "-o", out] + [os.path.join(CSRC, f) for f in SOURCES]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -51,7 +52,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         raise RuntimeError("nvcc failed building libgprm_b200.so")
     if verbose or ptxas_info:
         sys.stderr.write(r.stderr)
-    return OUT
+    return out
 
 
 if __name__ == "__main__":

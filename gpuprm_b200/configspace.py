@@ -177,6 +177,14 @@ class RobotConfigspace:
             self.h, C.c_void_p(qs_soa.data_ptr()), C.c_void_p(qe_soa.data_ptr()), C.c_void_p(res.data_ptr()),
             n, n, C.c_void_p(st)))
 
+    def set_launch(self, vertex_kernel: bool, threads: int, scene_in_smem: bool) -> None:
+        _check(self.lib, self.h, self.lib.gprm_set_launch(self.h, int(vertex_kernel), threads, int(scene_in_smem)))
+
+    def get_launch(self, vertex_kernel: bool) -> dict:
+        t, s, w = C.c_int(0), C.c_int(0), C.c_int(0)
+        _check(self.lib, self.h, self.lib.gprm_get_launch(self.h, int(vertex_kernel), C.byref(t), C.byref(s), C.byref(w)))
+        return {"threads": t.value, "scene_in_smem": bool(s.value), "warps_per_sm": w.value}
+
     def profile_enable(self, on: bool = True) -> None:
         _check(self.lib, self.h, self.lib.gprm_profile_enable(self.h, 1 if on else 0))
 

@@ -69,9 +69,15 @@ struct gprm_space {
     float mins[GPRM_MAX_DOF], maxs[GPRM_MAX_DOF];
     int types[GPRM_MAX_DOF];
     int npoly = 0, npairs = 0, sumn = 0, summ = 0;
-    std::vector<float4> verts;
-    std::vector<uint8_t> dest;
+    std::vector<float4> tab;       /* per-polytope blocks, see gprm_device.cuh */
     std::vector<int4> pairs;
+    std::vector<float4> pairs_b;   /* certificate data per pair */
+    std::vector<double> rad;       /* inflated ball radius per polytope */
+    std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
+    std::vector<int> slot_sys, slot_block;
+    std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */
+    double extent = 1.0;           /* length scale of the scene (m) */
+    float thr_dir = 0, eps_dir = 0;
 
     bool inited = false;
     int device = 0;
@@ -130,6 +136,39 @@ float float_ceil(double x)
     return f;
 }
 
+/* Certificate thresholds (see pair_certified in gprm_device.cuh).
+ * eps_pos bounds, per coordinate, both the rounding of the reference's
+ * world vertices (float transforms) and of the kernel's FMA ball centres;
+ * radii are inflated by 2*eps_pos and by 1e-5 relative for the deviation
+ * of the float rotation from orthogonality.  The slack added to the band
+ * covers the rounding of the reference's dp and h (a few ulps of metres). */
+void compute_certificates(gprm_space* h, const int* from, const int* to)
+{
+    const double eps_pos = 1e-6 * h->extent;
+    const double slack = 1e-4 + 1e-5 * h->extent;
+    const double thr = (double)h->band + slack;
+    (void)from;
+    (void)to;
+    h->pairs_b.resize(h->npairs);
+    for (int j = 0; j < h->npairs; ++j) {
+        int a = h->pair_poly[2 * j], b = h->pair_poly[2 * j + 1];
+        bool ok = (h->pair_sys[2 * j] == 0 || h->slot[a] >= 0) && (h->pair_sys[2 * j + 1] == 0 || h->slot[b] >= 0);
+        double R = h->rad[a] * (1 + 1e-5) + h->rad[b] * (1 + 1e-5) + 4 * eps_pos;
+        double x = 0.5 * ((2 * R + thr) + sqrt((2 * R + thr) * (2 * R + thr) + 4 * R * (R + thr)));
+        float Rf = nextafterf((float)R, INFINITY);
+        float T2 = nextafterf((float)(x * x * (1 + 1e-5)), INFINITY);
+        if (!ok) { Rf = INFINITY; T2 = INFINITY; }
+        int sa = h->pair_sys[2 * j] == 0 ? -1 : h->slot[a];
+        int sb = h->pair_sys[2 * j + 1] == 0 ? -1 : h->slot[b];
+        float fa, fb;
+        memcpy(&fa, &sa, 4);
+        memcpy(&fb, &sb, 4);
+        h->pairs_b[j] = make_float4(Rf, T2, fa, fb);
+    }
+    h->thr_dir = (float)thr;
+    h->eps_dir = (float)(7.0 * eps_pos);
+}
+
 int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
 {
     if (!d || !out) return fail(nullptr, GPRM_ERR_ARG, "null argument");
@@ -176,20 +215,39 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
         voff[k] = (int)sn; moff[k] = (int)sm;
         sn += n; sm += m;
     }
-    if (sm >= (1LL << 27) || sn >= (1LL << 30)) {
+    if (sm >= (1LL << 17) * 64 || sn >= (1LL << 30)) {
         delete h;
         return fail(nullptr, GPRM_ERR_SCENE, "scene too large (sum n=%lld, sum m=%lld)", sn, sm);
     }
     h->sumn = (int)sn;
     h->summ = (int)sm;
-    h->verts.resize(h->sumn);
-    h->dest.assign(((size_t)h->summ + 15) & ~(size_t)15, 0);
+    /* validate the CRS, then lay out one table block per polytope:
+       [vertex 0][entries of dest in CRS order], each entry the neighbour's
+       coordinates with (index | degree << 7 | offset << 15) in w */
+    std::vector<int> boff(h->npoly);
+    size_t ntab = 0;
+    for (int k = 0; k < h->npoly; ++k) { boff[k] = (int)ntab; ntab += 2 + (size_t)d->poly_m[k]; }
+    h->tab.resize(ntab);
+    h->rad.assign(h->npoly, 0.0);
+    h->slot.assign(h->npoly, -1);
     for (int k = 0; k < h->npoly; ++k) {
         int n = d->poly_n[k], m = d->poly_m[k];
+        if (m >= (1 << 17)) {
+            delete h;
+            return fail(nullptr, GPRM_ERR_SCENE, "polytope %d: m=%d >= 131072", k, m);
+        }
+        auto entry = [&](int v) {
+            int g = voff[k] + v;
+            int packed = v | (d->cnt[g] << 7) | (d->dsp[g] << 15);
+            float w;
+            memcpy(&w, &packed, 4);
+            return make_float4(d->vertices[3 * (size_t)g], d->vertices[3 * (size_t)g + 1],
+                               d->vertices[3 * (size_t)g + 2], w);
+        };
         for (int i = 0; i < n; ++i) {
             int g = voff[k] + i;
             int ds = d->dsp[g], c = d->cnt[g];
-            if (c < 1 || c > 255 || ds < 0 || ds + c > m || ds >= (1 << 23)) {
+            if (c < 1 || c > 255 || ds < 0 || ds + c > m) {
                 delete h;
                 return fail(nullptr, GPRM_ERR_SCENE,
                             "polytope %d vertex %d: dsp=%d cnt=%d (need cnt in 1..255, dsp+cnt<=m=%d)", k, i, ds, c, m);
@@ -199,10 +257,6 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
                 delete h;
                 return fail(nullptr, GPRM_ERR_SCENE, "polytope %d vertex %d is not finite", k, i);
             }
-            int packed = (ds << 8) | c;
-            float w;
-            memcpy(&w, &packed, 4);
-            h->verts[g] = make_float4(x, y, z, w);
         }
         for (int j = 0; j < m; ++j) {
             int v = d->dest[moff[k] + j];
@@ -210,8 +264,55 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
                 delete h;
                 return fail(nullptr, GPRM_ERR_SCENE, "polytope %d: dest[%d]=%d outside 0..%d", k, j, v, n - 1);
             }
-            h->dest[moff[k] + j] = (uint8_t)v;
+            h->tab[boff[k] + 2 + j] = entry(v);
         }
+        h->tab[boff[k] + 1] = entry(0);
+        /* bounding ball: centre of the bounding box, radius to the farthest
+           vertex (inflated in compute_certificates) */
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) {
+                double x = d->vertices[3 * (size_t)(voff[k] + i) + c];
+                lo[c] = x < lo[c] ? x : lo[c];
+                hi[c] = x > hi[c] ? x : hi[c];
+            }
+        double cc[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
+        float cf[3] = {(float)cc[0], (float)cc[1], (float)cc[2]};
+        double r = 0;
+        for (int i = 0; i < n; ++i) {
+            double dd = 0;
+            for (int c = 0; c < 3; ++c) {
+                double x = d->vertices[3 * (size_t)(voff[k] + i) + c] - (double)cf[c];
+                dd += x * x;
+            }
+            r = dd > r ? dd : r;
+        }
+        h->rad[k] = sqrt(r);
+        h->tab[boff[k]] = make_float4(cf[0], cf[1], cf[2], (float)h->rad[k]);
+    }
+    /* slots: moving polytopes in frame order */
+    for (int f = 1; f <= h->ndof; ++f)
+        for (int k = 0; k < h->npoly; ++k)
+            if (d->sys[k] == f && (int)h->slot_sys.size() < GPRM_MAX_SLOTS) {
+                h->slot[k] = (int)h->slot_sys.size();
+                h->slot_sys.push_back(f);
+                h->slot_block.push_back(boff[k]);
+            }
+    /* length scale: farthest static ball, plus the arm's reach */
+    {
+        double reach = 0, world = 0, link = 0;
+        for (int i = 0; i < h->ndof; ++i) {
+            double dm = fabs((double)h->d0[i]);
+            if (h->types[i] == 1) dm = fmax(fabs((double)h->mins[i]), fabs((double)h->maxs[i]));
+            reach += fabs((double)h->a[i]) + dm;
+        }
+        for (int k = 0; k < h->npoly; ++k) {
+            float4 b = h->tab[boff[k]];
+            double c = sqrt((double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z) + h->rad[k];
+            if (d->sys[k] == 0) world = fmax(world, c);
+            else link = fmax(link, c);
+        }
+        h->extent = fmax(1.0, fmax(world, reach + link));
     }
     h->npairs = d->num_pairs;
     h->pairs.resize(h->npairs);
@@ -226,8 +327,11 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
             delete h;
             return fail(nullptr, GPRM_ERR_SCENE, "pairs must be sorted by from (pair %d)", j);
         }
-        h->pairs[j] = make_int4(voff[f], moff[f] | (d->sys[f] << 28), voff[t], moff[t] | (d->sys[t] << 28));
+        h->pairs[j] = make_int4(boff[f], boff[t], d->sys[f], d->sys[t]);
+        h->pair_poly.push_back(f); h->pair_poly.push_back(t);
+        h->pair_sys.push_back(d->sys[f]); h->pair_sys.push_back(d->sys[t]);
     }
+    compute_certificates(h, d->pair_from, d->pair_to);
     *out = h;
     return GPRM_OK;
 }
@@ -312,6 +416,10 @@ __global__ void k_accumulate(const Control* c, Control* total)
     total->steps_exec += c->steps_exec;
     total->band_checks += c->band_checks;
     total->band_flips += c->band_flips;
+    total->configs_exec += c->configs_exec;
+    total->cert_far += c->cert_far;
+    total->cert_dir += c->cert_dir;
+    total->full_tests += c->full_tests;
     total->flags |= c->flags;
     total->next += 1;  /* requests completed */
 }
@@ -511,12 +619,12 @@ int gprm_init(gprm_space* h, int rank, int size)
     CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
 
-    size_t vb = (size_t)h->sumn * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4), db = h->dest.size();
-    CUDA_TRY(h, cudaMalloc(&h->d_scene, vb + pb + db + 64));
+    size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
+    CUDA_TRY(h, cudaMalloc(&h->d_scene, tb + 2 * pb + 64));
     char* base = (char*)h->d_scene;
-    CUDA_TRY(h, cudaMemcpy(base, h->verts.data(), vb, cudaMemcpyHostToDevice));
-    if (pb) CUDA_TRY(h, cudaMemcpy(base + vb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
-    if (db) CUDA_TRY(h, cudaMemcpy(base + vb + pb, h->dest.data(), db, cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpy(base, h->tab.data(), tb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
 
     DevScene& s = h->dsc;
     memset(&s, 0, sizeof(s));
@@ -532,9 +640,14 @@ int gprm_init(gprm_space* h, int rank, int size)
     }
     s.sep_thr = float_ceil(-0.000001);
     s.tiny_thr = float_ceil(0.000001);
-    s.verts = (const float4*)base;
-    s.pairs = (const int4*)(base + vb);
-    s.dest = (const uint8_t*)(base + vb + pb);
+    s.ntab = (int)h->tab.size();
+    s.tab = (const float4*)base;
+    s.pairs = (const int4*)(base + tb);
+    s.pairs_b = (const float4*)(base + tb + pb);
+    s.thr_dir = h->thr_dir;
+    s.eps_dir = h->eps_dir;
+    s.nslots = (int)h->slot_sys.size();
+    for (int i = 0; i < s.nslots; ++i) { s.slot_sys[i] = h->slot_sys[i]; s.slot_block[i] = h->slot_block[i]; }
 
     CUDA_TRY(h, plan_launch(s, 1, 128, &h->cfg_v));
     CUDA_TRY(h, plan_launch(s, 0, 128, &h->cfg_e));
@@ -590,6 +703,15 @@ int gprm_set_band(gprm_space* h, float band_m)
     if (!h) return GPRM_ERR_ARG;
     if (!(band_m >= 0.0f) || !isfinite(band_m)) return fail(h, GPRM_ERR_ARG, "band must be finite and >= 0");
     h->band = band_m;
+    compute_certificates(h, nullptr, nullptr);
+    if (h->inited) {
+        CUDA_TRY(h, cudaSetDevice(h->device));
+        CUDA_TRY(h, cudaDeviceSynchronize());
+        size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
+        if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
+        h->dsc.thr_dir = h->thr_dir;
+        h->dsc.eps_dir = h->eps_dir;
+    }
     return GPRM_OK;
 }
 
@@ -609,6 +731,8 @@ int gprm_get_stats(const gprm_space* hc, gprm_stats* out)
     out->edge_steps_executed = (int64_t)tot.steps_exec;
     out->band_rechecks = (int64_t)tot.band_checks;
     out->band_flips = (int64_t)tot.band_flips;
+    out->pairs_certified = (int64_t)(tot.cert_far + tot.cert_dir);
+    out->pairs_tested = (int64_t)tot.full_tests;
     if (tot.flags & GPRM_DEVFLAG_QUEUE_FULL)
         return fail(h, GPRM_ERR_DEVICE, "a device-pointer request overflowed the FP64 queue; its band results are incomplete");
     if (tot.flags & GPRM_DEVFLAG_BAD_EDGE)
@@ -702,7 +826,7 @@ int gprm_indicator_batch_device(gprm_space* h, const float* q, int* res, int n, 
     if (n == 0) return GPRM_OK;
     rc = ensure_request(h, h->dev, 0, (size_t)n, false, false);
     if (rc) return rc;
-    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    cudaStream_t st = (cudaStream_t)stream;
     h->host_stats.vertex_checks += n;
     return enqueue(h, h->dev, 0, q, nullptr, res, n, offset, st);
 }
@@ -715,7 +839,7 @@ int gprm_indicator2_device(gprm_space* h, const float* qs, const float* qe, int*
     if (n == 0) return GPRM_OK;
     rc = ensure_request(h, h->dev, 1, (size_t)n, false, false);
     if (rc) return rc;
-    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    cudaStream_t st = (cudaStream_t)stream;
     return enqueue(h, h->dev, 1, qs, qe, res, n, offset, st);
 }
 
@@ -739,6 +863,36 @@ int gprm_debug_fk(gprm_space* h, const float* q, float* out)
 }
 
 int gprm_device_sm_count(const gprm_space* h) { return h ? h->sms : 0; }
+
+int gprm_set_launch(gprm_space* h, int vertex_kernel, int threads, int scene_in_smem)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (threads < 32 || threads > 512 || threads % 32) return fail(h, GPRM_ERR_ARG, "threads must be 32..512, a multiple of 32");
+    LaunchCfg c{};
+    cudaError_t e = configure_launch(h->dsc, vertex_kernel ? 1 : 0, threads, scene_in_smem ? 1 : 0, &c);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        /* restore the attribute of the current shape */
+        LaunchCfg& cur = vertex_kernel ? h->cfg_v : h->cfg_e;
+        configure_launch(h->dsc, vertex_kernel ? 1 : 0, cur.threads, cur.scene_in_smem, &cur);
+        return fail(h, GPRM_ERR_UNSUPPORTED, "launch shape %d threads / scene_in_smem=%d does not fit: %s",
+                    threads, scene_in_smem, cudaGetErrorString(e));
+    }
+    (vertex_kernel ? h->cfg_v : h->cfg_e) = c;
+    return GPRM_OK;
+}
+
+int gprm_get_launch(const gprm_space* h, int vertex_kernel, int* threads, int* scene_in_smem, int* warps_per_sm)
+{
+    if (!h || !threads || !scene_in_smem || !warps_per_sm) return GPRM_ERR_ARG;
+    if (!h->inited) return GPRM_ERR_STATE;
+    const LaunchCfg& c = vertex_kernel ? h->cfg_v : h->cfg_e;
+    *threads = c.threads;
+    *scene_in_smem = c.scene_in_smem;
+    *warps_per_sm = c.warps_per_sm;
+    return GPRM_OK;
+}
 
 int gprm_profile_enable(gprm_space* h, int on)
 {

@@ -11,11 +11,22 @@
  * policy runs the same steps in double for the near-contact recheck.
  *
  * Scene layout in memory (global, or copied to shared memory per block):
- *   float4 verts[sumn]   xyz in the body frame; w holds the adjacency of
- *                        the vertex as int bits: (dsp_local << 8) | cnt
- *   uint8  dest[summ]    neighbour indices, local to the polytope
- *   int4   pairs[M]      (voffA, moffA | sysA << 28, voffB, moffB | sysB << 28)
- *                        in the reference's pair order (CRS by `from`)
+ *   float4 tab[2N + sum(m)] one block per polytope: entry 0 is its bounding
+ *                           ball (centre xyz in the body frame, radius),
+ *                           entry 1 is vertex 0, then the polytope's CRS
+ *                           adjacency in order, each entry holding the
+ *                           NEIGHBOUR's body-frame xyz and, in w (int
+ *                           bits), the neighbour's index | its degree << 7 |
+ *                           its CRS offset << 15.  A support climb reads one
+ *                           16-byte entry per candidate, no indirection.
+ *   int4   pairs[M]         (blockA, blockB, sysA, sysB) in the reference's
+ *                           pair order (CRS by `from`)
+ *   float4 pairs_b[M]       (R = rA + rB, T2, slotA, slotB) for the
+ *                           separation certificates (see pair_certified)
+ * A polytope in frame 0 (the world) is used untransformed: the reference
+ * multiplies it by trafos[0], whose entries are exactly 1 and +-0, which
+ * changes at most the sign of a zero coordinate; no comparison or nonzero
+ * result depends on that sign.
  */
 #ifndef GPRM_DEVICE_CUH
 #define GPRM_DEVICE_CUH
@@ -25,6 +36,11 @@
 #include "gprm_sincos64.h"
 
 #define GPRM_MAX_FRAMES 8   /* ndof + 1 */
+#define GPRM_MAX_SLOTS 16   /* moving polytopes whose ball centre is tracked per lane */
+/* neighbours evaluated together by the support climb (1 or 4) */
+#ifndef GPRM_CLIMB_CHUNK
+#define GPRM_CLIMB_CHUNK 1
+#endif
 #define GPRM_MAX_ITERS 10   /* max_for_loop, max_for_loop_whole (collision4.h:17-18) */
 
 namespace gprm {
@@ -39,10 +55,24 @@ struct DevScene {
     float mins[GPRM_MAX_FRAMES], maxs[GPRM_MAX_FRAMES];
     /* (double)dp >= -1e-6  <=>  dp >= sep_thr ; (double)n < 1e-6 <=> n < tiny_thr */
     float sep_thr, tiny_thr;
-    const float4* verts;
-    const uint8_t* dest;
+    int ntab;               /* entries of tab */
+    const float4* tab;
     const int4* pairs;
+    const float4* pairs_b;
+    /* certificates: a pair whose guaranteed separation along the first
+       search direction exceeds thr_dir is reported free without the test;
+       eps_dir bounds the direction error of the approximate first direction
+       times its distance (see pair_certified) */
+    float thr_dir, eps_dir;
+    int nslots;                          /* moving polytopes with a ball slot */
+    int slot_sys[GPRM_MAX_SLOTS];        /* frame of each slot */
+    int slot_block[GPRM_MAX_SLOTS];      /* its table block (entry 0 = ball) */
 };
+
+/* fields of a table entry's w word */
+__device__ __forceinline__ int ent_idx(float4 e) { return __float_as_int(e.w) & 127; }
+__device__ __forceinline__ int ent_cnt(float4 e) { return (__float_as_int(e.w) >> 7) & 255; }
+__device__ __forceinline__ int ent_dsp(float4 e) { return (int)((unsigned)__float_as_int(e.w) >> 15); }
 
 /* ---------------------------------------------------------------- */
 /* precision policies                                                 */
@@ -145,6 +175,61 @@ __device__ __forceinline__ void forward_kinematics(const DevScene& sc, const flo
     }
 }
 
+/* The same chain for the FP32 kernels, storing frames 1..ndof to a
+ * lane-interleaved shared-memory array: entry e of frame f at
+ * out[((f-1)*12 + e) * 32] (out already offset by the lane).  The world
+ * centre of every slot's bounding ball follows at
+ * cen[(slot*3 + c) * 32] (computed with FMA: it only feeds the
+ * certificates, whose slack covers its rounding). */
+__device__ __forceinline__ void forward_kinematics_smem(const DevScene& sc, const float4* __restrict__ tab,
+                                                        const float* q, float* out, float* cen)
+{
+    Frame<float> T;
+    {
+        float c0, s0;
+        PF32::trig(0.0f, c0, s0);
+        dh_frame<PF32>(T, c0, s0, c0, s0, 0.0f, 0.0f);
+    }
+    int slot = 0;
+#pragma unroll 1
+    for (int i = 0; i < sc.ndof; ++i) {
+        float th = sc.q0[i], d = sc.d0[i];
+        if (sc.types[i] == 0) th = q[i];
+        else d = q[i];
+        float cq, sq, ca, sa;
+        PF32::trig(th, cq, sq);
+        PF32::trig_alpha(sc, i, ca, sa);
+        Frame<float> L;
+        dh_frame<PF32>(L, cq, sq, ca, sa, sc.a[i], d);
+        Frame<float> O;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float ux = L.m[3 * c], uy = L.m[3 * c + 1], uz = L.m[3 * c + 2];
+            float ox = T.m[0] * ux + T.m[3] * uy + T.m[6] * uz;
+            float oy = T.m[1] * ux + T.m[4] * uy + T.m[7] * uz;
+            float oz = T.m[2] * ux + T.m[5] * uy + T.m[8] * uz;
+            if (c == 3) { ox = ox + T.m[9]; oy = oy + T.m[10]; oz = oz + T.m[11]; }
+            O.m[3 * c] = ox; O.m[3 * c + 1] = oy; O.m[3 * c + 2] = oz;
+        }
+#pragma unroll
+        for (int e = 0; e < 12; ++e) out[(i * 12 + e) * 32] = O.m[e];
+        for (; slot < sc.nslots && sc.slot_sys[slot] == i + 1; ++slot) {
+            float4 b = tab[sc.slot_block[slot]];
+            cen[(slot * 3 + 0) * 32] = __fmaf_rn(O.m[0], b.x, __fmaf_rn(O.m[3], b.y, __fmaf_rn(O.m[6], b.z, O.m[9])));
+            cen[(slot * 3 + 1) * 32] = __fmaf_rn(O.m[1], b.x, __fmaf_rn(O.m[4], b.y, __fmaf_rn(O.m[7], b.z, O.m[10])));
+            cen[(slot * 3 + 2) * 32] = __fmaf_rn(O.m[2], b.x, __fmaf_rn(O.m[5], b.y, __fmaf_rn(O.m[8], b.z, O.m[11])));
+        }
+        T = O;
+    }
+}
+
+/* Loads frame f (1..ndof) of the lane from the array written above. */
+__device__ __forceinline__ void load_frame(const float* fr, int f, Frame<float>& T)
+{
+#pragma unroll
+    for (int e = 0; e < 12; ++e) T.m[e] = fr[((f - 1) * 12 + e) * 32];
+}
+
 /* T*v (geo4.h:215-221) */
 template <class R>
 __device__ __forceinline__ V3<R> xform(const Frame<R>& T, R x, R y, R z)
@@ -180,31 +265,52 @@ __device__ __forceinline__ typename P::R normalize3(V3<typename P::R>& u)
 }
 
 /* support_vertex_searcher::search_support_vertex (collision4.h:66-103):
- * first-improvement climb over the vertex adjacency.  The maximum rises
- * strictly, so there are at most n-1 moves; the loop bound is never hit on
- * validated scenes and only guards corrupt data. */
+ * first-improvement climb over the vertex adjacency, starting at `cur`
+ * (an entry of the polytope's block B).  The neighbours of the current
+ * vertex are evaluated four at a time (independent loads and dot
+ * products); the move goes to the first of them, in CRS order, whose dot
+ * product exceeds the current maximum, which is the vertex the reference's
+ * one-at-a-time scan moves to.  The maximum rises strictly, so there are at
+ * most n-1 moves; the loop bound only guards corrupt data. */
 template <class P>
-__device__ __forceinline__ int climb(const float4* __restrict__ V, const uint8_t* __restrict__ D,
-                                     int p, typename P::R dx, typename P::R dy, typename P::R dz)
+__device__ __forceinline__ float4 climb(const float4* __restrict__ B, float4 cur, typename P::R dx,
+                                        typename P::R dy, typename P::R dz)
 {
     typedef typename P::R R;
-    float4 v = V[p];
-    R best = dot3<R>((R)v.x, (R)v.y, (R)v.z, dx, dy, dz);
+    R best = dot3<R>((R)cur.x, (R)cur.y, (R)cur.z, dx, dy, dz);
 #pragma unroll 1
     for (int guard = 0; guard < 128; ++guard) {
-        int adj = __float_as_int(v.w);
-        int b = adj >> 8, c = adj & 255;
+        const float4* e = B + 2 + ent_dsp(cur);
+        const int c = ent_cnt(cur);
         bool moved = false;
+#if GPRM_CLIMB_CHUNK == 4
+#pragma unroll 1
+        for (int i = 0; i < c && !moved; i += 4) {
+            const int left = c - i;
+            float4 u0 = e[i], u1 = u0, u2 = u0, u3 = u0;
+            if (left > 1) u1 = e[i + 1];
+            if (left > 2) u2 = e[i + 2];
+            if (left > 3) u3 = e[i + 3];
+            R d0 = dot3<R>((R)u0.x, (R)u0.y, (R)u0.z, dx, dy, dz);
+            R d1 = dot3<R>((R)u1.x, (R)u1.y, (R)u1.z, dx, dy, dz);
+            R d2 = dot3<R>((R)u2.x, (R)u2.y, (R)u2.z, dx, dy, dz);
+            R d3 = dot3<R>((R)u3.x, (R)u3.y, (R)u3.z, dx, dy, dz);
+            if (d0 > best) { best = d0; cur = u0; moved = true; }
+            else if (left > 1 && d1 > best) { best = d1; cur = u1; moved = true; }
+            else if (left > 2 && d2 > best) { best = d2; cur = u2; moved = true; }
+            else if (left > 3 && d3 > best) { best = d3; cur = u3; moved = true; }
+        }
+#else
 #pragma unroll 1
         for (int i = 0; i < c; ++i) {
-            int u = D[b + i];
-            float4 vu = V[u];
-            R d = dot3<R>((R)vu.x, (R)vu.y, (R)vu.z, dx, dy, dz);
-            if (d > best) { best = d; p = u; v = vu; moved = true; break; }
+            float4 u = e[i];
+            R d = dot3<R>((R)u.x, (R)u.y, (R)u.z, dx, dy, dz);
+            if (d > best) { best = d; cur = u; moved = true; break; }
         }
+#endif
         if (!moved) break;
     }
-    return p;
+    return cur;
 }
 
 template <class R> struct V2 { R x, y; };
@@ -260,26 +366,26 @@ __device__ __forceinline__ bool half_plane(const V3<typename P::R>* hist, int k,
     return true;
 }
 
-/* seperating_vector_algorithm (collision4.h:226-332) for pair `pr`.
+/* seperating_vector_algorithm (collision4.h:226-332) for pair `pr`, with
+ * frames tp, tq (ignored for a polytope in frame 0).
  * Returns 0 (separated), l+1 (no separating half plane) or -1 (cap).
  * *margin: h = dp*|q0-p0| at the deciding iteration if separated, else the
  * largest h seen. */
 template <class P>
-__device__ __forceinline__ int pair_test(const DevScene& sc, const float4* __restrict__ verts,
-                                         const uint8_t* __restrict__ dest, int4 pr,
-                                         const Frame<typename P::R>* F, typename P::R* margin)
+__device__ __forceinline__ int pair_test(const DevScene& sc, const float4* __restrict__ tab, int4 pr,
+                                         const Frame<typename P::R>& tp, const Frame<typename P::R>& tq,
+                                         typename P::R* margin)
 {
     typedef typename P::R R;
-    const float4* VP = verts + pr.x;
-    const uint8_t* DP = dest + (pr.y & 0x0fffffff);
-    const float4* VQ = verts + pr.z;
-    const uint8_t* DQ = dest + (pr.w & 0x0fffffff);
-    const Frame<R>& tp = F[(unsigned)pr.y >> 28];
-    const Frame<R>& tq = F[(unsigned)pr.w >> 28];
-
-    float4 vq0 = VQ[0], vp0 = VP[0];
-    V3<R> Sa = xform<R>(tq, (R)vq0.x, (R)vq0.y, (R)vq0.z);
-    V3<R> Sb = xform<R>(tp, (R)vp0.x, (R)vp0.y, (R)vp0.z);
+    const float4* BP = tab + pr.x;
+    const float4* BQ = tab + pr.y;
+    const bool idP = pr.z == 0, idQ = pr.w == 0;
+    float4 ep = BP[1], eq = BQ[1];
+    V3<R> Sa, Sb;
+    if (idQ) { Sa.x = (R)eq.x; Sa.y = (R)eq.y; Sa.z = (R)eq.z; }
+    else Sa = xform<R>(tq, (R)eq.x, (R)eq.y, (R)eq.z);
+    if (idP) { Sb.x = (R)ep.x; Sb.y = (R)ep.y; Sb.z = (R)ep.z; }
+    else Sb = xform<R>(tp, (R)ep.x, (R)ep.y, (R)ep.z);
     V3<R> S;
     S.x = Sa.x - Sb.x; S.y = Sa.y - Sb.y; S.z = Sa.z - Sb.z;
     R norm = normalize3<P>(S);
@@ -288,16 +394,21 @@ __device__ __forceinline__ int pair_test(const DevScene& sc, const float4* __res
     V3<R> hist[GPRM_MAX_ITERS];
     int combs[GPRM_MAX_ITERS];
     R best = R(0.0f);
-    int p = 0, q = 0, k = 0, l = 0;
+    int k = 0, l = 0;
 #pragma unroll 1
     for (; k < GPRM_MAX_ITERS && l < GPRM_MAX_ITERS; ++l) {
-        V3<R> Sp = rot_t<R>(tp, S.x, S.y, S.z);
-        V3<R> Sq = rot_t<R>(tq, -S.x, -S.y, -S.z);
-        p = climb<P>(VP, DP, p, Sp.x, Sp.y, Sp.z);
-        q = climb<P>(VQ, DQ, q, Sq.x, Sq.y, Sq.z);
-        float4 vp = VP[p], vq = VQ[q];
-        V3<R> p0 = xform<R>(tp, (R)vp.x, (R)vp.y, (R)vp.z);
-        V3<R> q0 = xform<R>(tq, (R)vq.x, (R)vq.y, (R)vq.z);
+        V3<R> Sp, Sq;
+        if (idP) Sp = S;
+        else Sp = rot_t<R>(tp, S.x, S.y, S.z);
+        if (idQ) { Sq.x = -S.x; Sq.y = -S.y; Sq.z = -S.z; }
+        else Sq = rot_t<R>(tq, -S.x, -S.y, -S.z);
+        ep = climb<P>(BP, ep, Sp.x, Sp.y, Sp.z);
+        eq = climb<P>(BQ, eq, Sq.x, Sq.y, Sq.z);
+        V3<R> p0, q0;
+        if (idP) { p0.x = (R)ep.x; p0.y = (R)ep.y; p0.z = (R)ep.z; }
+        else p0 = xform<R>(tp, (R)ep.x, (R)ep.y, (R)ep.z);
+        if (idQ) { q0.x = (R)eq.x; q0.y = (R)eq.y; q0.z = (R)eq.z; }
+        else q0 = xform<R>(tq, (R)eq.x, (R)eq.y, (R)eq.z);
         V3<R> r;
         r.x = q0.x - p0.x; r.y = q0.y - p0.y; r.z = q0.z - p0.z;
         R rn = normalize3<P>(r);
@@ -309,7 +420,7 @@ __device__ __forceinline__ int pair_test(const DevScene& sc, const float4* __res
             return 0;
         }
         hist[k] = r;
-        int comb = p | (q << 8);
+        int comb = ent_idx(ep) | (ent_idx(eq) << 8);
         combs[k] = comb;
         bool rep = false;
 #pragma unroll 1
@@ -333,6 +444,70 @@ __device__ __forceinline__ int pair_test(const DevScene& sc, const float4* __res
     }
     *margin = best;
     return -1;
+}
+
+/* Separation certificate for pair `pr` (FP32 kernels).
+ *
+ * Balls: every world vertex the reference computes for polytope X lies in
+ * the ball (c_X, r_X) (radii are inflated on the host by the rounding of
+ * the reference's transforms and of the centre computed here).  For ANY
+ * vertices p*, q* the first Chung-Wang iteration may reach,
+ *     <S0, q0 - p0> >= G := <S0, c_Q - c_P> - (r_P + r_Q)
+ * with S0 the algorithm's unit first direction.  If G > band + slack, the
+ * reference's first iteration has dp > 0 >= -1e-6 (returns 0) and its
+ * margin h = dp*|q0-p0| exceeds the band, so the pair contributes code 0
+ * and no band-relevant margin: it can be skipped with identical output.
+ *   far test   without S0: S0 = (D + e)/|D + e| with |e| <= R (e = the
+ *              vertex-0 offsets from the centres) gives
+ *              <S0, D> >= (|D|^2 - R|D|)/(|D| + R); pairs_b.y holds the
+ *              squared distance T2 beyond which that bound passes.
+ *   direction  S0 from vertex 0 of each polytope (FMA, rsqrt); its error
+ *              against the reference's S0 is at most eps_dir/|s| (s the
+ *              vertex-0 offset), charged against G with |D| + R.
+ * NaN never passes (every test is a '>' comparison). */
+__device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4* __restrict__ tab,
+                                               int4 pr, float4 pb, const float* cen,
+                                               const float* frames, bool* used_dir)
+{
+    *used_dir = false;
+    const int sa = __float_as_int(pb.z), sb = __float_as_int(pb.w);
+    float px, py, pz, qx, qy, qz;
+    if (sa >= 0) { px = cen[(sa * 3) * 32]; py = cen[(sa * 3 + 1) * 32]; pz = cen[(sa * 3 + 2) * 32]; }
+    else { float4 b = tab[pr.x]; px = b.x; py = b.y; pz = b.z; }
+    if (sb >= 0) { qx = cen[(sb * 3) * 32]; qy = cen[(sb * 3 + 1) * 32]; qz = cen[(sb * 3 + 2) * 32]; }
+    else { float4 b = tab[pr.y]; qx = b.x; qy = b.y; qz = b.z; }
+    const float dx = qx - px, dy = qy - py, dz = qz - pz;
+    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+    if (d2 > pb.y) return true;
+    /* direction test: approximate first direction from vertex 0 of each */
+    *used_dir = true;
+    float4 v0p = tab[pr.x + 1], v0q = tab[pr.y + 1];
+    float ax = v0p.x, ay = v0p.y, az = v0p.z, bx = v0q.x, by = v0q.y, bz = v0q.z;
+    if (pr.z) {
+        Frame<float> T;
+        load_frame(frames, pr.z, T);
+        float x = __fmaf_rn(T.m[0], ax, __fmaf_rn(T.m[3], ay, __fmaf_rn(T.m[6], az, T.m[9])));
+        float y = __fmaf_rn(T.m[1], ax, __fmaf_rn(T.m[4], ay, __fmaf_rn(T.m[7], az, T.m[10])));
+        float z = __fmaf_rn(T.m[2], ax, __fmaf_rn(T.m[5], ay, __fmaf_rn(T.m[8], az, T.m[11])));
+        ax = x; ay = y; az = z;
+    }
+    if (pr.w) {
+        Frame<float> T;
+        load_frame(frames, pr.w, T);
+        float x = __fmaf_rn(T.m[0], bx, __fmaf_rn(T.m[3], by, __fmaf_rn(T.m[6], bz, T.m[9])));
+        float y = __fmaf_rn(T.m[1], bx, __fmaf_rn(T.m[4], by, __fmaf_rn(T.m[7], bz, T.m[10])));
+        float z = __fmaf_rn(T.m[2], bx, __fmaf_rn(T.m[5], by, __fmaf_rn(T.m[8], bz, T.m[11])));
+        bx = x; by = y; bz = z;
+    }
+    const float sx = bx - ax, sy = by - ay, sz = bz - az;
+    const float n2 = __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, sz * sz));
+    if (!(n2 > 1e-6f)) return false;           /* |s| < 1e-3: leave it to the test */
+    const float inv = rsqrtf(n2);
+    const float G = __fmaf_rn(sx, dx, __fmaf_rn(sy, dy, sz * dz)) * inv - pb.x;
+    const float dn = sqrtf(d2);
+    /* direction error <= eps_dir*inv (+ rsqrt and rounding, 1e-6) */
+    const float err = (dn + pb.x) * __fmaf_rn(sc.eps_dir, inv, 1e-6f);
+    return G - err > sc.thr_dir;
 }
 
 /* FP32 check band test: the check's result is decided within `band` of

@@ -20,6 +20,10 @@ struct Control {
     unsigned long long steps_exec;    /* steps evaluated in FP32 */
     unsigned long long band_checks;   /* checks recomputed in FP64 */
     unsigned long long band_flips;    /* FP64 verdict differs from FP32 verdict */
+    unsigned long long configs_exec;  /* vertex checks that ran the pair loop */
+    unsigned long long cert_far;      /* pair tests settled by the distance certificate */
+    unsigned long long cert_dir;      /* ... by the first-direction certificate */
+    unsigned long long full_tests;    /* pair tests that ran the Chung-Wang iteration */
 };
 
 #define GPRM_DEVFLAG_BAD_EDGE    1u   /* non-finite or oversized edge length */
@@ -29,13 +33,21 @@ struct Control {
 struct LaunchCfg {
     int blocks;          /* persistent grid size */
     int threads;         /* threads per block (multiple of 32) */
-    size_t smem_bytes;   /* dynamic shared memory (scene copy), 0 = global */
+    size_t smem_bytes;   /* dynamic shared memory: per-lane frames (+ scene copy) */
+    int scene_in_smem;   /* the scene table is copied into shared memory */
+    int warps_per_sm;    /* resident warps per SM at this configuration */
 };
 
 enum EdgePolicy { EDGE_EARLY_EXIT = 0, EDGE_ALL_STEPS = 1 };
 
-/* Scene bytes when staged in shared memory. */
+/* Scene bytes when staged in shared memory; per-lane frame bytes of a block. */
 size_t scene_smem_bytes(const DevScene& sc);
+size_t frame_smem_bytes(const DevScene& sc, int threads);
+
+/* Sets up one launch variant (threads per block, scene in shared memory or
+ * read through L1) and its persistent grid; fails if it does not fit. */
+cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads, int scene_in_smem,
+                             LaunchCfg* cfg);
 
 /* Vertex checks: res[i] = code of configuration q[i + offset*j]. */
 cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q,

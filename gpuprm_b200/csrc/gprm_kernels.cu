@@ -29,41 +29,120 @@ namespace gprm {
 
 #define FULL_MASK 0xffffffffu
 
+/* minimum resident blocks of 128 threads the FP32 kernels are compiled for
+ * (caps registers per thread; 0 = no cap) */
+#ifndef GPRM_MIN_BLOCKS
+#define GPRM_MIN_BLOCKS 0
+#endif
+#if GPRM_MIN_BLOCKS > 0
+#define GPRM_BOUNDS __launch_bounds__(128, GPRM_MIN_BLOCKS)
+#else
+#define GPRM_BOUNDS __launch_bounds__(512)
+#endif
+
 size_t scene_smem_bytes(const DevScene& sc)
 {
-    size_t v = (size_t)sc.sumn * 16, p = (size_t)sc.npairs * 16;
-    size_t d = ((size_t)sc.summ + 15) & ~(size_t)15;
-    return v + p + d;
+    return (size_t)sc.ntab * 16 + (size_t)sc.npairs * 32;
+}
+
+/* per warp: frames 1..ndof (12 floats each) and the ball centres of the
+ * slots (3 floats each), lane-interleaved */
+__host__ __device__ __forceinline__ size_t lane_floats(const DevScene& sc)
+{
+    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 3;
+}
+
+size_t frame_smem_bytes(const DevScene& sc, int threads)
+{
+    return (size_t)(threads / 32) * lane_floats(sc) * 32 * sizeof(float);
 }
 
 struct SceneView {
-    const float4* verts;
-    const uint8_t* dest;
+    const float4* tab;
     const int4* pairs;
+    const float4* pairs_b;
+    float* frames;   /* this lane's frames (lane-interleaved, stride 32) */
+    float* cen;      /* this lane's slot ball centres */
 };
 
+/* Copies the scene into shared memory (SMEM) and returns the pointers the
+ * warp uses, including its lane's slice of the frame array. */
 template <bool SMEM>
 __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned char* smem)
 {
     SceneView s;
-    if (!SMEM) {
-        s.verts = sc.verts;
-        s.dest = sc.dest;
+    size_t off = 0;
+    if (SMEM) {
+        float4* t = reinterpret_cast<float4*>(smem);
+        int4* p = reinterpret_cast<int4*>(smem + (size_t)sc.ntab * 16);
+        float4* pb = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + (size_t)sc.npairs * 16);
+        for (int i = threadIdx.x; i < sc.ntab; i += blockDim.x) t[i] = sc.tab[i];
+        for (int i = threadIdx.x; i < sc.npairs; i += blockDim.x) { p[i] = sc.pairs[i]; pb[i] = sc.pairs_b[i]; }
+        s.tab = t;
+        s.pairs = p;
+        s.pairs_b = pb;
+        off = (size_t)sc.ntab * 16 + (size_t)sc.npairs * 32;
+    } else {
+        s.tab = sc.tab;
         s.pairs = sc.pairs;
-        return s;
+        s.pairs_b = sc.pairs_b;
     }
-    float4* v = reinterpret_cast<float4*>(smem);
-    int4* p = reinterpret_cast<int4*>(smem + (size_t)sc.sumn * 16);
-    uint32_t* d = reinterpret_cast<uint32_t*>(smem + (size_t)sc.sumn * 16 + (size_t)sc.npairs * 16);
-    for (int i = threadIdx.x; i < sc.sumn; i += blockDim.x) v[i] = sc.verts[i];
-    for (int i = threadIdx.x; i < sc.npairs; i += blockDim.x) p[i] = sc.pairs[i];
-    const uint32_t* dsrc = reinterpret_cast<const uint32_t*>(sc.dest);
-    for (int i = threadIdx.x; i < (sc.summ + 3) / 4; i += blockDim.x) d[i] = dsrc[i];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    s.frames = reinterpret_cast<float*>(smem + off) + (size_t)warp * lane_floats(sc) * 32 + lane;
+    s.cen = s.frames + (size_t)sc.ndof * 12 * 32;
     __syncthreads();
-    s.verts = v;
-    s.dest = reinterpret_cast<const uint8_t*>(d);
-    s.pairs = p;
     return s;
+}
+
+/* Per-lane counts of how pair tests were settled. */
+struct PairCounts {
+    unsigned long long far, dir, full;
+};
+
+/* One pair of the reference's pair loop for this lane: the certificate
+ * first, the exact test otherwise.  Returns the pair's code; *margin is set
+ * (and *has_margin true) only when the exact test ran. */
+__device__ __forceinline__ int eval_pair(const DevScene& sc, const SceneView& S, int j, float* margin,
+                                         bool* has_margin, PairCounts& pc);
+
+/* The frames of a pair, from the lane's frame array (frame 0 is unused). */
+__device__ __forceinline__ void pair_frames(const float* fr, int4 pr, Frame<float>& tp, Frame<float>& tq)
+{
+    if (pr.z) load_frame(fr, pr.z, tp);
+    if (pr.w) load_frame(fr, pr.w, tq);
+}
+
+__device__ __forceinline__ int eval_pair(const DevScene& sc, const SceneView& S, int j, float* margin,
+                                         bool* has_margin, PairCounts& pc)
+{
+    const int4 pr = S.pairs[j];
+    const float4 pb = S.pairs_b[j];
+    bool used_dir;
+    if (pair_certified(sc, S.tab, pr, pb, S.cen, S.frames, &used_dir)) {
+        if (used_dir) ++pc.dir;
+        else ++pc.far;
+        *has_margin = false;
+        return 0;
+    }
+    ++pc.full;
+    Frame<float> tp, tq;
+    pair_frames(S.frames, pr, tp, tq);
+    *has_margin = true;
+    return pair_test<PF32>(sc, S.tab, pr, tp, tq, margin);
+}
+
+__device__ __forceinline__ void flush_counts(PairCounts pc, Control* ctl)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        pc.far += __shfl_xor_sync(0xffffffffu, pc.far, o);
+        pc.dir += __shfl_xor_sync(0xffffffffu, pc.dir, o);
+        pc.full += __shfl_xor_sync(0xffffffffu, pc.full, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (pc.far) atomicAdd(&ctl->cert_far, pc.far);
+        if (pc.dir) atomicAdd(&ctl->cert_dir, pc.dir);
+        if (pc.full) atomicAdd(&ctl->full_tests, pc.full);
+    }
 }
 
 /* Appends the items of the lanes with `want` set, one atomic per warp. */
@@ -94,7 +173,7 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
 /* ------------------------------------------------------------------ */
 
 template <bool SMEM>
-__global__ void __launch_bounds__(128) k_check_configs(DevScene sc, const float* __restrict__ q,
+__global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict__ q,
                                                        long long n, long long offset,
                                                        int* __restrict__ res, int band_on, float band,
                                                        uint2* __restrict__ queue, unsigned qcap,
@@ -104,7 +183,7 @@ __global__ void __launch_bounds__(128) k_check_configs(DevScene sc, const float*
     const SceneView S = stage_scene<SMEM>(sc, smem);
     const int lane = threadIdx.x & 31;
     unsigned long long exec = 0;
-    Frame<float> F[GPRM_MAX_FRAMES];
+    PairCounts pc = {0, 0, 0};
     for (;;) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(&ctl->next, 32ull);
@@ -121,16 +200,17 @@ __global__ void __launch_bounds__(128) k_check_configs(DevScene sc, const float*
             for (int j = 0; j < sc.ndof; ++j)
                 if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
         }
-        if (active) forward_kinematics<PF32>(sc, qi, F);
+        if (active) forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
         float mmin = PF32::inf(), mdec = 0.0f;
 #pragma unroll 1
         for (int j = 0; j < sc.npairs; ++j) {
             if (!__any_sync(FULL_MASK, active)) break;
             if (active) {
                 float m;
-                int r = pair_test<PF32>(sc, S.verts, S.dest, S.pairs[j], F, &m);
+                bool hm;
+                int r = eval_pair(sc, S, j, &m, &hm, pc);
                 if (r != 0) { code = r; mdec = m; active = false; }
-                else mmin = min_nan(mmin, m);
+                else if (hm) mmin = min_nan(mmin, m);
             }
         }
         if (valid) {
@@ -141,7 +221,8 @@ __global__ void __launch_bounds__(128) k_check_configs(DevScene sc, const float*
         warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), queue, qcap, ctl);
     }
     exec = warp_sum(exec);
-    if (lane == 0 && exec) atomicAdd(&ctl->steps_exec, exec);
+    if (lane == 0 && exec) atomicAdd(&ctl->configs_exec, exec);
+    flush_counts(pc, ctl);
 }
 
 /* ------------------------------------------------------------------ */
@@ -157,7 +238,7 @@ __device__ __forceinline__ unsigned early_key(unsigned order, int code) { return
 __device__ __forceinline__ unsigned all_key(int t, int code) { return ((unsigned)(t + 1) << 4) | (unsigned)(code + 1); }
 
 template <bool SMEM, int POLICY>
-__global__ void __launch_bounds__(128) k_check_edges(DevScene sc, const float* __restrict__ qs,
+__global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__ qs,
                                                      const float* __restrict__ qe, long long n,
                                                      long long offset, float dq, unsigned* __restrict__ key,
                                                      int band_on, float band, uint2* __restrict__ queue,
@@ -167,7 +248,7 @@ __global__ void __launch_bounds__(128) k_check_edges(DevScene sc, const float* _
     const SceneView S = stage_scene<SMEM>(sc, smem);
     const int lane = threadIdx.x & 31;
     unsigned long long exec = 0, nominal = 0;
-    Frame<float> F[GPRM_MAX_FRAMES];
+    PairCounts pc = {0, 0, 0};
     for (;;) {
         unsigned long long eu = 0;
         if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
@@ -200,7 +281,7 @@ __global__ void __launch_bounds__(128) k_check_edges(DevScene sc, const float* _
             float qi[GPRM_MAX_FRAMES];
             if (valid) {
                 edge_step_config(qs, qe, e, offset, sc.ndof, t, tn, qi);
-                forward_kinematics<PF32>(sc, qi, F);
+                forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
             }
             const unsigned valid_mask = __ballot_sync(FULL_MASK, valid);
             if (lane == 0) exec += __popc(valid_mask);
@@ -214,9 +295,10 @@ __global__ void __launch_bounds__(128) k_check_edges(DevScene sc, const float* _
                 if (!__any_sync(FULL_MASK, active)) break;
                 if (active) {
                     float m;
-                    int rr = pair_test<PF32>(sc, S.verts, S.dest, S.pairs[j], F, &m);
+                    bool hm;
+                    int rr = eval_pair(sc, S, j, &m, &hm, pc);
                     if (rr != 0) { code = rr; mdec = m; active = false; }
-                    else mmin = min_nan(mmin, m);
+                    else if (hm) mmin = min_nan(mmin, m);
                 }
                 jend = j + 1;
                 bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
@@ -252,6 +334,7 @@ __global__ void __launch_bounds__(128) k_check_edges(DevScene sc, const float* _
         if (exec) atomicAdd(&ctl->steps_exec, exec);
         if (nominal) atomicAdd(&ctl->steps_nominal, nominal);
     }
+    flush_counts(pc, ctl);
 }
 
 /* ------------------------------------------------------------------ */
@@ -286,7 +369,8 @@ __global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const fl
 #pragma unroll 1
         for (int j = 0; j < sc.npairs; ++j) {
             double m;
-            int r = pair_test<PF64>(sc, sc.verts, sc.dest, sc.pairs[j], F, &m);
+            const int4 pr = sc.pairs[j];
+            int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
             if (r != 0) { code = r; break; }
         }
         ++checks;
@@ -332,34 +416,70 @@ __global__ void k_fk_probe(DevScene sc, const float* q, float* out)
 /* launchers                                                            */
 /* ------------------------------------------------------------------ */
 
-cudaError_t plan_launch(const DevScene& sc, int vertex_kernel, int threads, LaunchCfg* cfg)
+/* Occupancy of one FP32 kernel variant, in resident warps per SM. */
+static cudaError_t variant_warps(const void* fn, int threads, size_t smem, int* warps_per_sm)
+{
+    int per_sm = 0;
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    *warps_per_sm = per_sm * (threads / 32);
+    return err;
+}
+
+static const void* kernel_fn(int vertex_kernel, bool smem, int policy)
+{
+    if (vertex_kernel) return smem ? (const void*)k_check_configs<true> : (const void*)k_check_configs<false>;
+    if (policy == EDGE_EARLY_EXIT)
+        return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT>;
+    return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS> : (const void*)k_check_edges<false, EDGE_ALL_STEPS>;
+}
+
+cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads, int scene_in_smem,
+                             LaunchCfg* cfg)
 {
     int dev = 0, sms = 0, optin = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    size_t need = scene_smem_bytes(sc);
-    bool smem = need <= (size_t)optin / 2;   /* leave room for two blocks per SM */
-    const void* fn;
-    if (vertex_kernel) fn = smem ? (const void*)k_check_configs<true> : (const void*)k_check_configs<false>;
-    else fn = smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT>;
-    cfg->smem_bytes = smem ? need : 0;
-    cfg->threads = threads;
-    if (smem) {
-        const void* fns[4] = {(const void*)k_check_configs<true>, (const void*)k_check_edges<true, EDGE_EARLY_EXIT>,
-                              (const void*)k_check_edges<true, EDGE_ALL_STEPS>, nullptr};
-        for (int i = 0; i < 3; ++i) {
-            err = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
-            if (err != cudaSuccess) return err;
-        }
+    size_t smem = frame_smem_bytes(sc, threads) + (scene_in_smem ? scene_smem_bytes(sc) : 0);
+    if (smem > (size_t)optin) return cudaErrorInvalidValue;
+    for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol) {
+        err = cudaFuncSetAttribute(kernel_fn(vertex_kernel, scene_in_smem != 0, pol),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err != cudaSuccess) return err;
     }
-    int per_sm = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, cfg->smem_bytes);
+    int warps = 0;
+    err = variant_warps(kernel_fn(vertex_kernel, scene_in_smem != 0, 0), threads, smem, &warps);
     if (err != cudaSuccess) return err;
-    if (per_sm < 1) per_sm = 1;
-    cfg->blocks = sms * per_sm;
+    if (warps < 1) return cudaErrorInvalidConfiguration;
+    cfg->threads = threads;
+    cfg->smem_bytes = smem;
+    cfg->scene_in_smem = scene_in_smem;
+    cfg->blocks = sms * (warps / (threads / 32));
+    cfg->warps_per_sm = warps;
     return cudaSuccess;
+}
+
+cudaError_t plan_launch(const DevScene& sc, int vertex_kernel, int threads, LaunchCfg* cfg)
+{
+    /* default: the variant with the most resident warps, the scene in shared
+       memory on ties (the autotuner times the candidates instead) */
+    LaunchCfg best{};
+    int best_w = -1;
+    const int cand_threads[4] = {threads, 256, 384, 512};
+    for (int ci = 0; ci < 4; ++ci)
+        for (int sm = 1; sm >= 0; --sm) {
+            LaunchCfg c{};
+            if (configure_launch(sc, vertex_kernel, cand_threads[ci], sm, &c) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            if (c.warps_per_sm > best_w) { best = c; best_w = c.warps_per_sm; }
+        }
+    if (best_w < 0) return cudaErrorInvalidConfiguration;
+    /* re-apply the chosen variant's shared-memory attribute */
+    cudaError_t err = configure_launch(sc, vertex_kernel, best.threads, best.scene_in_smem, cfg);
+    return err;
 }
 
 cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q, long long n,
@@ -367,12 +487,12 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
                                  unsigned qcap, Control* ctl, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    if (cfg.smem_bytes)
+    if (cfg.scene_in_smem)
         k_check_configs<true><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on,
                                                                               band, queue, qcap, ctl);
     else
-        k_check_configs<false><<<cfg.blocks, cfg.threads, 0, st>>>(sc, q, n, offset, res, band_on, band,
-                                                                  queue, qcap, ctl);
+        k_check_configs<false><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on,
+                                                                               band, queue, qcap, ctl);
     return cudaGetLastError();
 }
 
@@ -384,11 +504,11 @@ cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const f
     if (n <= 0) return cudaSuccess;
     size_t sm = cfg.smem_bytes;
     if (policy == EDGE_EARLY_EXIT) {
-        if (sm) k_check_edges<true, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
-        else k_check_edges<false, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, 0, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+        if (cfg.scene_in_smem) k_check_edges<true, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+        else k_check_edges<false, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
     } else {
-        if (sm) k_check_edges<true, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
-        else k_check_edges<false, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, 0, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+        if (cfg.scene_in_smem) k_check_edges<true, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+        else k_check_edges<false, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
     }
     return cudaGetLastError();
 }

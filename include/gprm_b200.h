@@ -102,6 +102,8 @@ typedef struct gprm_stats {
     int64_t band_rechecks;        /* checks recomputed in FP64 */
     int64_t band_flips;           /* of those, verdict changed free<->not free */
     int64_t launches;             /* kernels launched */
+    int64_t pairs_certified;      /* FP32 pair tests settled by a separation certificate */
+    int64_t pairs_tested;         /* FP32 pair tests that ran the full iteration */
 } gprm_stats;
 
 /* ---- lifetime --------------------------------------------------------- */
@@ -171,9 +173,11 @@ float gprm_deltaq(const gprm_space* h);
 int   gprm_dim(const gprm_space* h);
 
 /* ---- queries (device buffers, caller's stream; no host sync) ----------
- * Pointers are device pointers; `stream` is a cudaStream_t (NULL = the
- * handle's stream).  These never synchronise and are safe to capture in a
- * CUDA graph after one warm-up call with the same sizes. */
+ * Pointers are device pointers; `stream` is the cudaStream_t to launch on
+ * (NULL is the legacy default stream).  These never synchronise; after one
+ * call with a given n they allocate nothing for calls with n no larger, so
+ * they can be captured in a CUDA graph.  Calls on one handle share its
+ * device scratch: do not overlap two of them on different streams. */
 int gprm_indicator_batch_device(gprm_space* h, const float* q, int* res, int n,
                                 int offset, void* stream);
 int gprm_indicator2_device(gprm_space* h, const float* qs, const float* qe, int* res,
@@ -188,6 +192,15 @@ int gprm_debug_fk(gprm_space* h, const float* q, float* out);
 
 /* Streaming multiprocessors of the handle's device (0 before init). */
 int gprm_device_sm_count(const gprm_space* h);
+
+/* Launch shape of the FP32 kernels (vertex_kernel = 1: vertex checks,
+ * 0: edge checks): threads per block (a multiple of 32, <= 512) and
+ * whether the scene table is copied into shared memory (1) or read through
+ * L1 (0).  Fails without changing anything if the shape does not fit.
+ * gprm_init picks the shape with the most resident warps. */
+int gprm_set_launch(gprm_space* h, int vertex_kernel, int threads, int scene_in_smem);
+int gprm_get_launch(const gprm_space* h, int vertex_kernel, int* threads, int* scene_in_smem,
+                    int* warps_per_sm);
 
 /* Kernel timing: while enabled, every request records CUDA events around
  * its FP32 check kernel and its FP64 recheck kernel on the stream they run

@@ -185,3 +185,26 @@ def test_device_pointer_api_matches_host_api():
     torch.cuda.synchronize()
     np.testing.assert_array_equal(res.cpu().numpy(), host_res)
     np.testing.assert_array_equal(codes.cpu().numpy(), host_codes)
+
+
+@pytest.mark.parametrize("band", [0.0, 1e-3, 2e-2])
+def test_band_width_changes_nothing_but_the_band(band):
+    """The separation certificates depend on the band; results must equal
+    the oracle's for every band width."""
+    sc, z = load_golden("hull6")
+    dq = float(z["dq"])
+    cs = space(sc, dq, mode=GPRM_MODE_FP64_BAND)
+    cs.set_band(band)
+    orc = O.Oracle(sc)
+    want, _, _ = orc.check_configs(z["q"], O.FP32_BAND | O.DEVICE_TRIG, band=band)
+    np.testing.assert_array_equal(cs.check_configs(z["q"]), want)
+    want_e, _ = orc.check_edges(z["qs"], z["qe"], dq, O.FP32_BAND | O.DEVICE_TRIG, band=band)
+    np.testing.assert_array_equal(cs.check_edges(z["qs"], z["qe"]), want_e)
+
+
+def test_certificates_settle_most_pairs():
+    sc, z = load_golden("hull6")
+    cs = space(sc, float(z["dq"]))
+    cs.check_configs(z["q"])
+    st = cs.stats()
+    assert st["pairs_certified"] > 4 * st["pairs_tested"]
