@@ -148,3 +148,31 @@ def test_queries_without_gpu_fail_cleanly():
     with pytest.raises(GprmError) as e:
         cs.indicator(np.zeros(4, np.float32))
     assert e.value.status == -6   # not initialised
+
+
+REF_LIB_DIR = "/root/reference/prm/src/lib"
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_LIB_DIR, "prm", "configspace.hpp")),
+                    reason="the reference's Configspace header is only present where the reference is")
+def test_cpp_shim_implements_reference_interface(tmp_path):
+    """include/gprm_configspace.hpp compiles against the reference's own
+    Configspace<ndof> (every pure virtual overridden) and links against
+    libgprm_b200.so."""
+    import subprocess
+    src = tmp_path / "shim.cpp"
+    src.write_text(
+        '#include <prm/configspace.hpp>\n#include "gprm_configspace.hpp"\n'
+        "int main(int argc, char** argv) {\n"
+        "  if (argc < 2) return 0;\n"
+        "  B200RobotConfigspace<4> s(argv[1], 0.01f, 64);\n"
+        "  Configspace<4>* cs = &s;\n"
+        "  return cs->dim() == 4 ? 0 : 1;\n}\n")
+    lib_dir = os.path.join(ROOT, "gpuprm_b200")
+    r = subprocess.run(["g++", "-std=c++14", "-I", REF_LIB_DIR, "-I", os.path.join(ROOT, "include"), str(src),
+                        "-L", lib_dir, "-lgprm_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(tmp_path / "shim")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    sc = scenes.make_box4(1)
+    d = scenes.write_config_dir(sc, str(tmp_path / "scene"))
+    assert subprocess.run([str(tmp_path / "shim"), d]).returncode == 0
