@@ -16,6 +16,7 @@ GPRM_EDGES_EARLY_EXIT = 0
 GPRM_EDGES_ALL_STEPS = 1
 GPRM_MAX_DOF = 7
 GPRM_MAX_VERTICES = 100
+GPRM_NOALLOC_MAX_CONFIGS = 65536
 
 
 class SceneDesc(C.Structure):
@@ -118,6 +119,8 @@ SIGNATURES = [
     ("gprm_dim", C.c_int, [_P]),
     ("gprm_indicator_batch_device", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     ("gprm_indicator2_device", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    ("gprm_indicator_batch_device_noalloc", C.c_int,
+     [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     ("gprm_debug_fk", C.c_int, [_P, _F, _F]),
     ("gprm_device_sm_count", C.c_int, [_P]),
     ("gprm_set_launch", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),

@@ -23,6 +23,7 @@
 
 #include <fstream>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -956,3 +957,72 @@ int gprm_measure_fp32_peak(double* tflops)
 }
 
 }  /* extern "C" */
+
+/* ====================================================================== */
+/* vertex checks without allocation                                        */
+/* ====================================================================== */
+
+namespace {
+
+/* Work buffers of gprm_indicator_batch_device_noalloc: the control block
+ * (zeroed by every call) at offset 0, the FP64 queue (at most one entry per
+ * configuration, so it cannot overflow) at NOALLOC_QUEUE_OFFSET.  The name is
+ * a host-side stand-in; kernels get the device address looked up below. */
+constexpr size_t NOALLOC_QUEUE_OFFSET = 256;
+static_assert(sizeof(Control) <= NOALLOC_QUEUE_OFFSET, "control block outgrew its slot");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_QUEUE_OFFSET +
+                                                                 (size_t)GPRM_NOALLOC_MAX_CONFIGS * sizeof(uint2)];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+/* Device address of the scratch array on the current device (`dev`),
+ * looked up once per device. */
+int noalloc_scratch(gprm_space* h, int dev, unsigned char** out)
+{
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(h, GPRM_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, NOALLOC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(h, GPRM_ERR_CUDA, "cudaGetSymbolAddress(no-allocation scratch): %s", cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = (unsigned char*)g_noalloc_addr[dev];
+    return GPRM_OK;
+}
+
+}  // namespace
+
+extern "C" int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q, int* res, int n, int offset,
+                                                   void* stream)
+{
+    int rc = check_ready(h);   /* makes the handle's device current */
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!q || !res)) || offset < n) return fail(h, GPRM_ERR_ARG, "bad q/res/n/offset");
+    if (n > GPRM_NOALLOC_MAX_CONFIGS)
+        return fail(h, GPRM_ERR_ARG, "n=%d exceeds the no-allocation limit of %d configurations per call",
+                    n, GPRM_NOALLOC_MAX_CONFIGS);
+    if (n == 0) return GPRM_OK;
+    unsigned char* base = nullptr;
+    rc = noalloc_scratch(h, h->device, &base);
+    if (rc) return rc;
+    Control* ctl = (Control*)base;
+    uint2* queue = (uint2*)(base + NOALLOC_QUEUE_OFFSET);
+    const unsigned qcap = (unsigned)GPRM_NOALLOC_MAX_CONFIGS;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int band_on = h->mode == GPRM_MODE_FP64_BAND;
+    CUDA_TRY(h, cudaMemsetAsync(ctl, 0, sizeof(Control), st));
+    CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, q, n, offset, res, band_on, h->band, queue, qcap, ctl, st));
+    if (band_on)
+        CUDA_TRY(h, launch_recheck(h->dsc, h->sms * 4, 0, q, nullptr, nullptr, offset, h->dq, h->policy, res,
+                                   nullptr, queue, qcap, ctl, st));
+    k_accumulate<<<1, 1, 0, st>>>(ctl, h->d_total);
+    CUDA_TRY(h, cudaGetLastError());
+    h->host_stats.vertex_checks += n;
+    h->host_stats.launches += 2 + (band_on ? 1 : 0);
+    return GPRM_OK;
+}

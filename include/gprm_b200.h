@@ -183,6 +183,26 @@ int gprm_indicator_batch_device(gprm_space* h, const float* q, int* res, int n,
 int gprm_indicator2_device(gprm_space* h, const float* qs, const float* qe, int* res,
                            int n, int offset, void* stream);
 
+/* ---- vertex checks without allocation (no counterpart in the reference) --
+ * For callers that must not allocate device memory while they run: a
+ * planner inside a real-time control loop (cudaMalloc and cudaFree can
+ * block and synchronise the whole device), or a host whose device memory is
+ * owned by another allocator and cannot hand out raw allocations.  Same
+ * result as gprm_indicator_batch_device, but the work buffers (a control
+ * block and the FP64 recheck queue) live in a fixed device array inside the
+ * library, sized for GPRM_NOALLOC_MAX_CONFIGS configurations
+ * (about 0.5 MB, held by every GPU that loads the library until the process
+ * exits).  Larger n is rejected with GPRM_ERR_ARG.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other handles, other host
+ * threads) race and must be serialised by the caller.  q and res are
+ * device pointers as in gprm_indicator_batch_device; `stream` NULL is the
+ * legacy default stream.  Nothing is allocated by this call. */
+#define GPRM_NOALLOC_MAX_CONFIGS 65536
+int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q, int* res, int n, int offset,
+                                        void* stream);
+
 /* ---- diagnostics (no counterpart in the reference) -------------------- */
 
 /* The FP32 frames the kernels compute for one configuration q[ndof]:
