@@ -510,6 +510,36 @@ __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4*
     return G - err > sc.thr_dir;
 }
 
+/* The same certificate for the FP64 recheck, in double from the FP64
+ * frames: the balls bound the FP64 world vertices as well (their inflation
+ * covers float rounding, which exceeds double rounding), and the first
+ * direction is computed in double, so its error term only needs the
+ * 1e-6 relative allowance. */
+__device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float4* __restrict__ tab, int4 pr,
+                                                 float4 pb, const Frame<double>* F)
+{
+    const float4 bp = tab[pr.x], bq = tab[pr.y];
+    double px = bp.x, py = bp.y, pz = bp.z, qx = bq.x, qy = bq.y, qz = bq.z;
+    if (pr.z) { V3<double> c = xform<double>(F[pr.z], px, py, pz); px = c.x; py = c.y; pz = c.z; }
+    if (pr.w) { V3<double> c = xform<double>(F[pr.w], qx, qy, qz); qx = c.x; qy = c.y; qz = c.z; }
+    const double dx = qx - px, dy = qy - py, dz = qz - pz;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 > (double)pb.y) return true;
+    const float4 vp = tab[pr.x + 1], vq = tab[pr.y + 1];
+    V3<double> a, b;
+    if (pr.z) a = xform<double>(F[pr.z], (double)vp.x, (double)vp.y, (double)vp.z);
+    else { a.x = vp.x; a.y = vp.y; a.z = vp.z; }
+    if (pr.w) b = xform<double>(F[pr.w], (double)vq.x, (double)vq.y, (double)vq.z);
+    else { b.x = vq.x; b.y = vq.y; b.z = vq.z; }
+    const double sx = b.x - a.x, sy = b.y - a.y, sz = b.z - a.z;
+    const double n2 = sx * sx + sy * sy + sz * sz;
+    if (!(n2 > 1e-6)) return false;
+    const double inv = 1.0 / sqrt(n2);
+    const double G = (sx * dx + sy * dy + sz * dz) * inv - (double)pb.x;
+    const double err = (sqrt(d2) + (double)pb.x) * 1e-6;
+    return G - err > (double)sc.thr_dir;
+}
+
 /* FP32 check band test: the check's result is decided within `band` of
  * contact (free with minimum margin below band, colliding with the deciding
  * pair's best margin above -band) or by the iteration cap. */

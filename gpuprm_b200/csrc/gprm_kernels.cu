@@ -368,8 +368,9 @@ __global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const fl
         int code = 0;
 #pragma unroll 1
         for (int j = 0; j < sc.npairs; ++j) {
-            double m;
             const int4 pr = sc.pairs[j];
+            if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F)) continue;
+            double m;
             int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
             if (r != 0) { code = r; break; }
         }
