@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--policy", default="early", choices=["early", "all"])
+    ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
+    ap.add_argument("--prm-samples", type=int, default=1 << 16)
     return ap.parse_args()
 
 
@@ -274,6 +276,20 @@ def run_ours(args, rank, world, local_rank):
                 "reference_equivalent_tflops": work["ref_flops_per_step"] * exec_pl / (k_ms * 1e-3) / 1e12,
                 "kernel_ms": k_ms, "pairs_certified_frac": cert_pl / max(1.0, cert_pl + full_pl),
                 "fp64_recheck_ms_per_launch": prof["fp64_ms"] / max(1, prof["fp32_launches"])}
+    prm = None
+    if not args.no_prm and world == 1:
+        from gpuprm_b200 import planner, scenes as _sc
+        psc = _sc.make_scene("hull6", args.seed)
+        from gpuprm_b200.configspace import RobotConfigspace as _RC
+        pcs = _RC(psc, dq=WORKLOAD["dq"])
+        pcs.init()
+        pcs.set_mode(GPRM_MODE_FP64_BAND)
+        mlp, losses, t_lab, t_train = planner.train_predictor(pcs, psc, n_labels=1 << 20, epochs=10, batch=4096,
+                                                              lr=1e-3, seed=args.seed)
+        prm = planner.compare_planners(pcs, psc, n_samples=args.prm_samples, n_queries=1000, k=10, seed=args.seed,
+                                       mlp=mlp, repeats=3)
+        prm["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
+                            "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
     line = {
         "metric": METRIC, "value": nominal_all / t_max, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
@@ -287,6 +303,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+        "prm": prm,
     }
     return line
 

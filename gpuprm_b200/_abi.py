@@ -121,6 +121,17 @@ SIGNATURES = [
     ("gprm_indicator2_device", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     ("gprm_indicator_batch_device_noalloc", C.c_int,
      [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    ("gprm_mlp_create", C.c_int, [C.c_int, C.c_ulonglong, C.POINTER(_P)]),
+    ("gprm_mlp_destroy", None, [_P]),
+    ("gprm_mlp_last_error", C.c_char_p, [_P]),
+    ("gprm_mlp_num_params", C.c_longlong, [_P]),
+    ("gprm_mlp_get_params", C.c_int, [_P, _F]),
+    ("gprm_mlp_set_params", C.c_int, [_P, _F]),
+    ("gprm_mlp_predict", C.c_int, [_P, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    ("gprm_mlp_gradients", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, _F, _F]),
+    ("gprm_mlp_adam_step", C.c_int, [_P, C.c_float]),
+    ("gprm_mlp_train", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                 C.c_float, _F]),
     ("gprm_debug_fk", C.c_int, [_P, _F, _F]),
     ("gprm_device_sm_count", C.c_int, [_P]),
     ("gprm_set_launch", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),

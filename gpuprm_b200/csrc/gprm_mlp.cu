@@ -1,0 +1,604 @@
+/*
+ * gprm_mlp.cu - the learned collision-probability predictor.
+ *
+ * No counterpart in GPUPRM.  A multilayer perceptron
+ *     x (sin/cos of the joints, padded to 16) -> 256 -> 256 -> 256 -> 256 -> 1
+ * with GELU (erf form) on the hidden layers and a sigmoid output, trained
+ * with binary cross-entropy and Adam.  Weights are kept in FP32 (master)
+ * and BF16 (the GEMM operands); activations are stored in BF16; every GEMM
+ * accumulates in FP32 on the tensor cores (warp-level BF16 MMA, m16n8k16).
+ *
+ * Layout (row-major): W_l is [out x in] like a Linear layer; activations
+ * are [batch x features].  Forward:  Z_l = H_{l-1} W_l^T + b_l,
+ * H_l = gelu(Z_l).  Backward:  dZ_l = dH_l * gelu'(Z_l),
+ * dW_l = dZ_l^T H_{l-1},  db_l = colsum(dZ_l),  dH_{l-1} = dZ_l W_l.
+ */
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gprm_b200.h"
+
+namespace {
+
+constexpr int IN_PAD = 16;     /* input features padded to one MMA k-step */
+constexpr int HID = 256;
+constexpr int NLAYER = 4;      /* hidden layers */
+
+/* ------------------------------------------------------------------ */
+/* GEMM: C[M x N] = sum_k A(m,k) B(k,n), BF16 in, FP32 accumulate        */
+/*   A(m,k) = TA ? A[k*lda + m] : A[m*lda + k]                            */
+/*   B(k,n) = TB ? B[n*ldb + k] : B[k*ldb + n]                            */
+/* 64x64 block tile, 32-deep k tile, 4 warps of 32x32, mma m16n8k16.     */
+/* ------------------------------------------------------------------ */
+
+constexpr int BM = 64, BN = 64, BK = 32, KPAD = 8;
+
+enum Epi {
+    EPI_FWD_HIDDEN = 0,   /* Z = acc + bias (fp32 out), H = gelu(Z) (bf16 out) */
+    EPI_BWD_DH = 1,       /* dZ = acc * gelu'(Z) (bf16 out) */
+    EPI_GRAD_W = 2        /* dW = acc (fp32 out) */
+};
+
+struct EpiArgs {
+    const float* bias;        /* [N] (FWD) */
+    float* zout;              /* [M x N] fp32 (FWD) */
+    __nv_bfloat16* hout;      /* [M x N] bf16 (FWD: H, BWD: dZ) */
+    const float* zin;         /* [M x N] fp32 pre-activation (BWD) */
+    float* gout;              /* [M x N] fp32 (GRAD) */
+    int ldc;
+};
+
+__device__ __forceinline__ float gelu_f(float z)
+{
+    return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+
+__device__ __forceinline__ float gelu_grad(float z)
+{
+    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+    return cdf + z * pdf;
+}
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
+                                              const __nv_bfloat16* __restrict__ B, int ldb, EpiArgs ep)
+{
+    __shared__ __align__(16) __nv_bfloat16 As[BM][BK + KPAD];
+    __shared__ __align__(16) __nv_bfloat16 Bs[BN][BK + KPAD];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int g = lane >> 2, t = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    for (int k0 = 0; k0 < K; k0 += BK) {
+        /* stage the tiles, k contiguous in shared memory */
+        for (int idx = tid; idx < BM * BK; idx += 128) {
+            int mm, kk;
+            if (TA) { mm = idx % BM; kk = idx / BM; }   /* global m contiguous */
+            else { kk = idx % BK; mm = idx / BK; }       /* global k contiguous */
+            int gm = m0 + mm, gk = k0 + kk;
+            __nv_bfloat16 v = zero;
+            if (gm < M && gk < K) v = TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
+            As[mm][kk] = v;
+        }
+        for (int idx = tid; idx < BN * BK; idx += 128) {
+            int nn, kk;
+            if (TB) { kk = idx % BK; nn = idx / BK; }   /* global k contiguous */
+            else { nn = idx % BN; kk = idx / BN; }       /* global n contiguous */
+            int gn = n0 + nn, gk = k0 + kk;
+            __nv_bfloat16 v = zero;
+            if (gn < N && gk < K) v = TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
+            Bs[nn][kk] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < BK; ks += 16) {
+            uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + i * 16 + g;
+                af[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][ks + 2 * t]);
+                af[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][ks + 2 * t]);
+                af[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][ks + 2 * t + 8]);
+                af[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][ks + 2 * t + 8]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = wn + j * 8 + g;
+                bfr[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[c][ks + 2 * t]);
+                bfr[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[c][ks + 2 * t + 8]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
+        }
+        __syncthreads();
+    }
+    /* epilogue: accumulator element (row g / g+8, cols 2t, 2t+1) */
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int gm = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
+                const int gn = n0 + wn + j * 8 + 2 * t + (r & 1);
+                if (gm >= M || gn >= N) continue;
+                const size_t o = (size_t)gm * ep.ldc + gn;
+                const float a = acc[i][j][r];
+                if (EPI == EPI_FWD_HIDDEN) {
+                    const float z = a + ep.bias[gn];
+                    ep.zout[o] = z;
+                    ep.hout[o] = __float2bfloat16(gelu_f(z));
+                } else if (EPI == EPI_BWD_DH) {
+                    ep.hout[o] = __float2bfloat16(a * gelu_grad(ep.zin[o]));
+                } else {
+                    ep.gout[o] = a;
+                }
+            }
+}
+
+/* ------------------------------------------------------------------ */
+/* small kernels                                                        */
+/* ------------------------------------------------------------------ */
+
+/* features: (sin q_j, cos q_j) for j < ndof, zero padded to IN_PAD;
+ * q is SoA q[i + offset*j]; rows are optionally gathered through idx */
+__global__ void k_features(const float* __restrict__ q, long long offset, int ndof, int n,
+                           const int* __restrict__ idx, __nv_bfloat16* __restrict__ X)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const long long src = idx ? idx[i] : i;
+        __nv_bfloat16* row = X + (size_t)i * IN_PAD;
+        for (int j = 0; j < IN_PAD / 2; ++j) {
+            float s = 0.0f, c = 0.0f;
+            if (j < ndof) sincosf(q[src + offset * j], &s, &c);
+            row[2 * j] = __float2bfloat16(j < ndof ? s : 0.0f);
+            row[2 * j + 1] = __float2bfloat16(j < ndof ? c : 0.0f);
+        }
+    }
+}
+
+/* output layer (256 -> 1) and the loss: one warp per row.
+ * p = sigmoid(H4 . w5 + b5); with labels: loss += BCE, dlogit = (p - y)/B */
+__global__ void k_out(int n, const __nv_bfloat16* __restrict__ H, const __nv_bfloat16* __restrict__ w5,
+                      const float* __restrict__ b5, float* __restrict__ p, const float* __restrict__ y,
+                      const int* __restrict__ yidx, float* __restrict__ dlogit, float* __restrict__ loss, float inv_b)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int r = warp; r < n; r += nw) {
+        float s = 0.0f;
+        for (int k = lane; k < HID; k += 32)
+            s += __bfloat162float(H[(size_t)r * HID + k]) * __bfloat162float(w5[k]);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            const float logit = s + b5[0];
+            const float pr = 1.0f / (1.0f + expf(-logit));
+            if (p) p[r] = pr;
+            if (y) {
+                const float yy = y[yidx ? yidx[r] : r];
+                /* BCE with logits, stable form */
+                const float l = fmaxf(logit, 0.0f) - logit * yy + log1pf(expf(-fabsf(logit)));
+                atomicAdd(loss, l * inv_b);
+                dlogit[r] = (pr - yy) * inv_b;
+            }
+        }
+    }
+}
+
+/* output-layer backward: dw5 = H4^T dlogit, db5 = sum dlogit,
+ * dZ4 = (dlogit w5) * gelu'(Z4) */
+__global__ void k_out_back(int n, const __nv_bfloat16* __restrict__ H, const float* __restrict__ Z,
+                           const __nv_bfloat16* __restrict__ w5, const float* __restrict__ dlogit,
+                           float* __restrict__ dw5, float* __restrict__ db5, __nv_bfloat16* __restrict__ dZ)
+{
+    /* block per column chunk: column k = threadIdx.x (HID threads) */
+    const int k = threadIdx.x;
+    float acc = 0.0f, accb = 0.0f;
+    for (int r = blockIdx.x; r < n; r += gridDim.x) {
+        const float d = dlogit[r];
+        acc += d * __bfloat162float(H[(size_t)r * HID + k]);
+        accb += d;
+        dZ[(size_t)r * HID + k] = __float2bfloat16(d * __bfloat162float(w5[k]) * gelu_grad(Z[(size_t)r * HID + k]));
+    }
+    atomicAdd(&dw5[k], acc);
+    if (k == 0) atomicAdd(db5, accb);
+}
+
+/* db[c] = sum_r dZ[r][c] */
+__global__ void k_colsum(int n, int cols, const __nv_bfloat16* __restrict__ dZ, float* __restrict__ db)
+{
+    const int c = threadIdx.x;
+    if (c >= cols) return;
+    float acc = 0.0f;
+    for (int r = blockIdx.x; r < n; r += gridDim.x) acc += __bfloat162float(dZ[(size_t)r * cols + c]);
+    atomicAdd(&db[c], acc);
+}
+
+/* Adam on the FP32 master parameters, refreshing their BF16 copies.
+ * bf_map[i] = index into the bf16 array or -1. */
+__global__ void k_adam(long long n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, const int* __restrict__ bf_map, __nv_bfloat16* __restrict__ wbf,
+                       float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        const int b = bf_map[i];
+        if (b >= 0) wbf[b] = __float2bfloat16(wi);
+    }
+}
+
+__global__ void k_to_bf16(long long n, const float* __restrict__ w, const int* __restrict__ bf_map,
+                          __nv_bfloat16* __restrict__ wbf)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int b = bf_map[i];
+        if (b >= 0) wbf[b] = __float2bfloat16(w[i]);
+    }
+}
+
+/* shuffled batch indices for step s: perm[s*B .. s*B+B) */
+__global__ void k_gather_labels(int n, const int* __restrict__ idx, const float* __restrict__ y, float* __restrict__ yb)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) yb[i] = y[idx[i]];
+}
+
+}  // namespace
+
+/* ====================================================================== */
+/* host side                                                              */
+/* ====================================================================== */
+
+struct gprm_mlp {
+    int ndof = 6;
+    int max_batch = 0;
+    /* parameter vector (fp32 master): W1[HID x IN_PAD] b1 W2 b2 W3 b3 W4 b4 w5[HID] b5[1] */
+    long long nparam = 0;
+    long long offW[NLAYER + 1], offB[NLAYER + 1];
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    int* bf_map = nullptr;
+    __nv_bfloat16* wbf = nullptr;       /* bf16 copies of W1..W4, w5 */
+    long long offWbf[NLAYER + 1];
+    long long nbf = 0;
+    /* activations for max_batch rows */
+    __nv_bfloat16* X = nullptr;
+    __nv_bfloat16* H[NLAYER] = {nullptr};
+    float* Z[NLAYER] = {nullptr};
+    __nv_bfloat16* dZ[NLAYER] = {nullptr};
+    float *p = nullptr, *dlogit = nullptr, *loss = nullptr, *ybatch = nullptr;
+    int* idx = nullptr;
+    long long adam_t = 0;
+    cudaStream_t st = nullptr;
+    std::string err = "no error";
+};
+
+namespace {
+
+int mfail(gprm_mlp* h, int code, const char* msg, cudaError_t e = cudaSuccess)
+{
+    if (h) h->err = std::string(msg) + (e != cudaSuccess ? std::string(": ") + cudaGetErrorString(e) : "");
+    return code;
+}
+
+#define MLP_TRY(h, call)                                                         \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) return mfail((h), GPRM_ERR_CUDA, #call, e_);      \
+    } while (0)
+
+int alloc_batch(gprm_mlp* h, int rows)
+{
+    if (rows <= h->max_batch) return GPRM_OK;
+    cudaFree(h->X);
+    for (int l = 0; l < NLAYER; ++l) { cudaFree(h->H[l]); cudaFree(h->Z[l]); cudaFree(h->dZ[l]); }
+    cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
+    size_t R = (size_t)rows;
+    MLP_TRY(h, cudaMalloc((void**)&h->X, R * IN_PAD * sizeof(__nv_bfloat16)));
+    for (int l = 0; l < NLAYER; ++l) {
+        MLP_TRY(h, cudaMalloc((void**)&h->H[l], R * HID * sizeof(__nv_bfloat16)));
+        MLP_TRY(h, cudaMalloc((void**)&h->Z[l], R * HID * sizeof(float)));
+        MLP_TRY(h, cudaMalloc((void**)&h->dZ[l], R * HID * sizeof(__nv_bfloat16)));
+    }
+    MLP_TRY(h, cudaMalloc((void**)&h->p, R * sizeof(float)));
+    MLP_TRY(h, cudaMalloc((void**)&h->dlogit, R * sizeof(float)));
+    MLP_TRY(h, cudaMalloc((void**)&h->ybatch, R * sizeof(float)));
+    MLP_TRY(h, cudaMalloc((void**)&h->idx, R * sizeof(int)));
+    h->max_batch = rows;
+    return GPRM_OK;
+}
+
+dim3 ggrid(int M, int N) { return dim3((N + BN - 1) / BN, (M + BM - 1) / BM); }
+
+/* Forward on rows already featurised in h->X; p written to `p`. */
+int forward(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, float inv_b, cudaStream_t st)
+{
+    const __nv_bfloat16* in = h->X;
+    int kin = IN_PAD;
+    for (int l = 0; l < NLAYER; ++l) {
+        EpiArgs ep{};
+        ep.bias = h->w + h->offB[l];
+        ep.zout = h->Z[l];
+        ep.hout = h->H[l];
+        ep.ldc = HID;
+        k_gemm<false, true, EPI_FWD_HIDDEN><<<ggrid(n, HID), 128, 0, st>>>(n, HID, kin, in, kin,
+                                                                           h->wbf + h->offWbf[l], kin, ep);
+        in = h->H[l];
+        kin = HID;
+    }
+    int blocks = (n * 32 + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    k_out<<<blocks, 256, 0, st>>>(n, h->H[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->w + h->offB[NLAYER], p, y,
+                                  yidx, h->dlogit, h->loss, inv_b);
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+/* Backward for a batch of n rows whose forward pass just ran; gradients
+ * accumulate into h->g (zeroed here). */
+int backward(gprm_mlp* h, int n, cudaStream_t st)
+{
+    MLP_TRY(h, cudaMemsetAsync(h->g, 0, (size_t)h->nparam * sizeof(float), st));
+    int blocks = n < 1024 ? n : 1024;
+    k_out_back<<<blocks, HID, 0, st>>>(n, h->H[NLAYER - 1], h->Z[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->dlogit,
+                                       h->g + h->offW[NLAYER], h->g + h->offB[NLAYER], h->dZ[NLAYER - 1]);
+    for (int l = NLAYER - 1; l >= 0; --l) {
+        const int kin = l == 0 ? IN_PAD : HID;
+        const __nv_bfloat16* hin = l == 0 ? h->X : h->H[l - 1];
+        /* dW_l = dZ_l^T H_{l-1}: M = HID, N = kin, K = n */
+        EpiArgs eg{};
+        eg.gout = h->g + h->offW[l];
+        eg.ldc = kin;
+        k_gemm<true, false, EPI_GRAD_W><<<ggrid(HID, kin), 128, 0, st>>>(HID, kin, n, h->dZ[l], HID, hin, kin, eg);
+        k_colsum<<<blocks, HID, 0, st>>>(n, HID, h->dZ[l], h->g + h->offB[l]);
+        if (l > 0) {
+            /* dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}): M = n, N = HID, K = HID */
+            EpiArgs ed{};
+            ed.hout = h->dZ[l - 1];
+            ed.zin = h->Z[l - 1];
+            ed.ldc = HID;
+            k_gemm<false, false, EPI_BWD_DH><<<ggrid(n, HID), 128, 0, st>>>(n, HID, HID, h->dZ[l], HID,
+                                                                            h->wbf + h->offWbf[l], HID, ed);
+        }
+    }
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+int adam(gprm_mlp* h, float lr, cudaStream_t st)
+{
+    h->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = (float)(1.0 - pow(0.9, (double)h->adam_t)), c2 = (float)(1.0 - pow(0.999, (double)h->adam_t));
+    k_adam<<<1024, 256, 0, st>>>(h->nparam, h->w, h->g, h->m, h->v, h->bf_map, h->wbf, lr, b1, b2, eps, c1, c2);
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+/* deterministic uniform init in [-1/sqrt(in), 1/sqrt(in)] (Linear's default
+ * range) from a 64-bit LCG */
+double lcg_uniform(uint64_t& s)
+{
+    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+    return (double)(s >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gprm_mlp_create(int ndof, unsigned long long seed, gprm_mlp** out)
+{
+    if (!out || ndof < 1 || ndof > IN_PAD / 2) return GPRM_ERR_ARG;
+    gprm_mlp* h = new gprm_mlp();
+    h->ndof = ndof;
+    long long off = 0, offbf = 0;
+    for (int l = 0; l <= NLAYER; ++l) {
+        const int nin = l == 0 ? IN_PAD : HID, nout = l == NLAYER ? 1 : HID;
+        h->offW[l] = off; off += (long long)nout * nin;
+        h->offB[l] = off; off += nout;
+        h->offWbf[l] = offbf; offbf += (long long)nout * nin;
+    }
+    h->nparam = off;
+    h->nbf = offbf;
+    std::vector<float> w(off, 0.0f);
+    std::vector<int> map(off, -1);
+    uint64_t s = seed * 0x9E3779B97F4A7C15ULL + 12345;
+    for (int l = 0; l <= NLAYER; ++l) {
+        const int nin = l == 0 ? IN_PAD : HID, nout = l == NLAYER ? 1 : HID;
+        const int fan_in = l == 0 ? 2 * ndof : nin;
+        const double bound = 1.0 / sqrt((double)fan_in);
+        for (int o = 0; o < nout; ++o) {
+            for (int i = 0; i < nin; ++i) {
+                long long k = h->offW[l] + (long long)o * nin + i;
+                bool pad = (l == 0 && i >= 2 * ndof);
+                w[k] = pad ? 0.0f : (float)((2.0 * lcg_uniform(s) - 1.0) * bound);
+                map[k] = (int)(h->offWbf[l] + (long long)o * nin + i);
+            }
+            w[h->offB[l] + o] = (float)((2.0 * lcg_uniform(s) - 1.0) * bound);
+        }
+    }
+    cudaError_t e;
+    if ((e = cudaMalloc((void**)&h->w, off * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->g, off * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->m, off * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->v, off * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->bf_map, off * sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->wbf, offbf * sizeof(__nv_bfloat16))) != cudaSuccess ||
+        (e = cudaMalloc((void**)&h->loss, sizeof(float))) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking)) != cudaSuccess) {
+        gprm_mlp_destroy(h);
+        return GPRM_ERR_CUDA;
+    }
+    cudaMemcpy(h->w, w.data(), off * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->bf_map, map.data(), off * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemset(h->m, 0, off * sizeof(float));
+    cudaMemset(h->v, 0, off * sizeof(float));
+    k_to_bf16<<<256, 256>>>(off, h->w, h->bf_map, h->wbf);
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+        gprm_mlp_destroy(h);
+        return GPRM_ERR_CUDA;
+    }
+    *out = h;
+    return GPRM_OK;
+}
+
+void gprm_mlp_destroy(gprm_mlp* h)
+{
+    if (!h) return;
+    if (h->st) cudaStreamSynchronize(h->st);
+    cudaFree(h->w); cudaFree(h->g); cudaFree(h->m); cudaFree(h->v); cudaFree(h->bf_map); cudaFree(h->wbf);
+    cudaFree(h->loss); cudaFree(h->X);
+    for (int l = 0; l < NLAYER; ++l) { cudaFree(h->H[l]); cudaFree(h->Z[l]); cudaFree(h->dZ[l]); }
+    cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+const char* gprm_mlp_last_error(const gprm_mlp* h) { return h ? h->err.c_str() : "null handle"; }
+
+long long gprm_mlp_num_params(const gprm_mlp* h) { return h ? h->nparam : 0; }
+
+int gprm_mlp_get_params(gprm_mlp* h, float* out)
+{
+    if (!h || !out) return GPRM_ERR_ARG;
+    MLP_TRY(h, cudaStreamSynchronize(h->st));
+    MLP_TRY(h, cudaMemcpy(out, h->w, h->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+    return GPRM_OK;
+}
+
+int gprm_mlp_set_params(gprm_mlp* h, const float* in)
+{
+    if (!h || !in) return GPRM_ERR_ARG;
+    MLP_TRY(h, cudaStreamSynchronize(h->st));
+    MLP_TRY(h, cudaMemcpy(h->w, in, h->nparam * sizeof(float), cudaMemcpyHostToDevice));
+    k_to_bf16<<<256, 256, 0, h->st>>>(h->nparam, h->w, h->bf_map, h->wbf);
+    MLP_TRY(h, cudaStreamSynchronize(h->st));
+    return GPRM_OK;
+}
+
+/* p[i] = P(collision) for configurations q (device SoA, q[i + offset*j]). */
+int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, void* stream)
+{
+    if (!h || n < 0 || (n > 0 && (!q || !p)) || offset < n) return mfail(h, GPRM_ERR_ARG, "bad arguments");
+    if (n == 0) return GPRM_OK;
+    cudaStream_t st = (cudaStream_t)stream;   /* NULL: the legacy default stream */
+    const int chunk = 1 << 16;
+    int rc = alloc_batch(h, n < chunk ? n : chunk);
+    if (rc) return rc;
+    for (int s = 0; s < n; s += chunk) {
+        int c = n - s < chunk ? n - s : chunk;
+        k_features<<<(c + 255) / 256, 256, 0, st>>>(q + s, offset, h->ndof, c, nullptr, h->X);
+        rc = forward(h, c, p + s, nullptr, nullptr, 0.0f, st);
+        if (rc) return rc;
+    }
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+/* Gradients of the mean BCE over the n labelled configurations (one
+ * forward/backward, no update): grads[nparam] and *loss on the host. */
+int gprm_mlp_gradients(gprm_mlp* h, const float* q, const float* y, int n, int offset, float* grads, float* loss)
+{
+    if (!h || n < 1 || !q || !y || !grads || !loss || offset < n) return mfail(h, GPRM_ERR_ARG, "bad arguments");
+    int rc = alloc_batch(h, n);
+    if (rc) return rc;
+    MLP_TRY(h, cudaMemsetAsync(h->loss, 0, sizeof(float), h->st));
+    k_features<<<(n + 255) / 256, 256, 0, h->st>>>(q, offset, h->ndof, n, nullptr, h->X);
+    if ((rc = forward(h, n, h->p, y, nullptr, 1.0f / n, h->st))) return rc;
+    if ((rc = backward(h, n, h->st))) return rc;
+    MLP_TRY(h, cudaStreamSynchronize(h->st));
+    MLP_TRY(h, cudaMemcpy(grads, h->g, h->nparam * sizeof(float), cudaMemcpyDeviceToHost));
+    MLP_TRY(h, cudaMemcpy(loss, h->loss, sizeof(float), cudaMemcpyDeviceToHost));
+    return GPRM_OK;
+}
+
+/* One Adam step (lr, beta 0.9/0.999, eps 1e-8) with the current gradients. */
+int gprm_mlp_adam_step(gprm_mlp* h, float lr)
+{
+    if (!h) return GPRM_ERR_ARG;
+    int rc = adam(h, lr, h->st);
+    if (rc) return rc;
+    MLP_TRY(h, cudaStreamSynchronize(h->st));
+    return GPRM_OK;
+}
+
+/* Trains on n labelled configurations (device SoA q, labels y in {0,1}):
+ * `epochs` passes in shuffled order (perm: device array of epochs*n
+ * indices, each epoch a permutation), batches of `batch`, Adam at `lr`.
+ * Every step runs features, forward, loss, backward and Adam on the
+ * device; each epoch's launches are captured into one CUDA graph.
+ * losses[epoch] gets the mean batch loss of each epoch (host array). */
+int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offset, const int* perm, int epochs,
+                   int batch, float lr, float* losses)
+{
+    if (!h || !q || !y || !perm || n < batch || batch < 1 || epochs < 1 || offset < n)
+        return mfail(h, GPRM_ERR_ARG, "bad arguments");
+    int rc = alloc_batch(h, batch);
+    if (rc) return rc;
+    const int steps = n / batch;
+    std::vector<float> ep_loss(epochs, 0.0f);
+    for (int e = 0; e < epochs; ++e) {
+        /* the epoch's launches are captured into one graph and replayed */
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        MLP_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        int crc = GPRM_OK;
+        cudaMemsetAsync(h->loss, 0, sizeof(float), h->st);
+        for (int s = 0; s < steps && !crc; ++s) {
+            const int* idx = perm + (size_t)e * n + (size_t)s * batch;
+            k_features<<<(batch + 255) / 256, 256, 0, h->st>>>(q, offset, h->ndof, batch, idx, h->X);
+            if (!crc) crc = forward(h, batch, h->p, y, idx, 1.0f / batch, h->st);
+            if (!crc) crc = backward(h, batch, h->st);
+            if (!crc) crc = adam(h, lr, h->st);
+        }
+        cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
+        if (crc) { if (graph) cudaGraphDestroy(graph); return crc; }
+        if (ce != cudaSuccess) return mfail(h, GPRM_ERR_CUDA, "capturing the training epoch", ce);
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, h->st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return mfail(h, GPRM_ERR_CUDA, "running the training epoch", ce);
+        float l = 0;
+        MLP_TRY(h, cudaMemcpy(&l, h->loss, sizeof(float), cudaMemcpyDeviceToHost));
+        ep_loss[e] = l / steps;
+    }
+    if (losses) memcpy(losses, ep_loss.data(), epochs * sizeof(float));
+    return GPRM_OK;
+}
+
+}  /* extern "C" */

@@ -183,6 +183,34 @@ int gprm_indicator_batch_device(gprm_space* h, const float* q, int* res, int n,
 int gprm_indicator2_device(gprm_space* h, const float* qs, const float* qe, int* res,
                            int n, int offset, void* stream);
 
+/* ---- learned collision predictor (no counterpart in the reference) -------
+ * An MLP (sin/cos of the joints -> 256 -> 256 -> 256 -> 256 -> 1, GELU,
+ * sigmoid) estimating P(collision) of a configuration, trained on the exact
+ * checker's verdicts; BF16 operands with FP32 accumulation on the tensor
+ * cores, FP32 master weights, Adam.  The planner uses it to order lazy
+ * edge checks and to prune samples; the exact checker still decides. */
+typedef struct gprm_mlp gprm_mlp;
+int  gprm_mlp_create(int ndof, unsigned long long seed, gprm_mlp** out);
+void gprm_mlp_destroy(gprm_mlp* h);
+const char* gprm_mlp_last_error(const gprm_mlp* h);
+/* parameter count; parameters as one FP32 vector
+ * [W1 (256x16, inputs padded) b1 W2 b2 W3 b3 W4 b4 w5 (1x256) b5] */
+long long gprm_mlp_num_params(const gprm_mlp* h);
+int gprm_mlp_get_params(gprm_mlp* h, float* out);
+int gprm_mlp_set_params(gprm_mlp* h, const float* in);
+/* p[i] = P(collision) of device configurations q[i + offset*j], launched on
+ * `stream` (NULL: the legacy default stream) */
+int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, void* stream);
+/* one forward/backward on n device configurations with labels y (device):
+ * mean BCE loss and its gradient (host arrays) */
+int gprm_mlp_gradients(gprm_mlp* h, const float* q, const float* y, int n, int offset, float* grads,
+                       float* loss);
+/* one Adam step (beta 0.9/0.999, eps 1e-8) with the last gradients */
+int gprm_mlp_adam_step(gprm_mlp* h, float lr);
+/* training: perm (device) holds `epochs` permutations of 0..n-1 */
+int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offset, const int* perm,
+                   int epochs, int batch, float lr, float* losses);
+
 /* ---- vertex checks without allocation (no counterpart in the reference) --
  * For callers that must not allocate device memory while they run: a
  * planner inside a real-time control loop (cudaMalloc and cudaFree can

@@ -1,0 +1,127 @@
+"""The learned collision predictor: FP64 oracle (CPU) and CUDA kernels (B200).
+
+Tolerances: the CUDA network stores inputs, weights, activations and
+backpropagated dZ in BF16 and accumulates in FP32.  The oracle emulates the
+BF16 storage, so gradients agree to FP32 summation-order error: per-tensor
+relative L2 error <= 2e-2, loss relative error <= 1e-3, probabilities within
+2e-3.  Adam is compared on the same gradient to 1e-6 absolute.
+"""
+import numpy as np
+import pytest
+
+import mlp_oracle as MO
+
+
+def _rand_params(rng, n_params, scale=0.2):
+    return (rng.standard_normal(n_params) * scale).astype(np.float64)
+
+
+def _n_params():
+    n = 0
+    for l in range(MO.LAYERS + 1):
+        nin = MO.IN_PAD if l == 0 else MO.HID
+        nout = 1 if l == MO.LAYERS else MO.HID
+        n += nout * nin + nout
+    return n
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    params = _rand_params(rng, _n_params(), 0.1)
+    X = MO.features(rng.uniform(-np.pi, np.pi, (6, 6)))
+    y = (rng.random(6) < 0.5).astype(np.float64)
+    loss, g, _ = MO.forward_backward(params, X, y, emulate_bf16=False)
+    idx = rng.choice(len(params), 40, replace=False)
+    # include a bias of every layer and the output layer
+    idx = np.concatenate([idx, [len(params) - 1, len(params) - 2]])
+    for i in idx:
+        e = np.zeros_like(params)
+        e[i] = 1e-6
+        lp, _, _ = MO.forward_backward(params + e, X, y, emulate_bf16=False)
+        lm, _, _ = MO.forward_backward(params - e, X, y, emulate_bf16=False)
+        fd = (lp - lm) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding_is_round_to_nearest_even():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 2 ** -9, 1.0 + 3 * 2 ** -9, -2.5], np.float32)
+    r = MO.bf16(x)
+    assert r[0] == 1.0
+    assert r[1] == 1.0            # exactly half an ulp: tie -> even
+    assert r[2] == 1.0            # below the tie
+    assert r[3] == 1.0 + 2 ** -7  # above the tie
+    assert r[4] == -2.5
+
+
+def _gpu_setup(n=512, seed=1):
+    import torch
+    from gpuprm_b200.mlp import CollisionMLP
+    rng = np.random.default_rng(seed)
+    q = rng.uniform(-np.pi, np.pi, (n, 6)).astype(np.float32)
+    y = (rng.random(n) < 0.4).astype(np.float32)
+    mlp = CollisionMLP(6, seed=seed)
+    q_soa = torch.tensor(np.ascontiguousarray(q.T), device="cuda:0")
+    y_t = torch.tensor(y, device="cuda:0")
+    return mlp, q, y, q_soa, y_t
+
+
+@pytest.mark.gpu
+def test_gpu_gradients_match_oracle():
+    mlp, q, y, q_soa, y_t = _gpu_setup()
+    params = mlp.get_params().astype(np.float64)
+    g_gpu, loss_gpu = mlp.gradients(q_soa, y_t)
+    loss, g, _ = MO.forward_backward(params, MO.features(q), y.astype(np.float64), emulate_bf16=True)
+    assert abs(loss_gpu - loss) <= 1e-3 * abs(loss)
+    G, Gg = MO.unpack(g), MO.unpack(g_gpu.astype(np.float64))
+    for k in G:
+        num = np.linalg.norm(Gg[k] - G[k])
+        den = np.linalg.norm(G[k]) + 1e-12
+        assert num / den <= 2e-2, (k, num / den)
+
+
+@pytest.mark.gpu
+def test_gpu_adam_matches_oracle():
+    mlp, q, y, q_soa, y_t = _gpu_setup(seed=2)
+    w0 = mlp.get_params().astype(np.float64)
+    g, _ = mlp.gradients(q_soa, y_t)
+    mlp.adam_step(1e-3)
+    w1 = mlp.get_params().astype(np.float64)
+    want, _, _ = MO.adam(w0, g.astype(np.float64), np.zeros_like(w0), np.zeros_like(w0), 1, lr=1e-3)
+    assert np.max(np.abs(w1 - want)) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_gpu_predict_matches_oracle():
+    mlp, q, y, q_soa, y_t = _gpu_setup(n=3000, seed=3)
+    p_gpu = mlp.predict(q_soa).cpu().numpy()
+    _, _, p = MO.forward_backward(mlp.get_params().astype(np.float64), MO.features(q), y.astype(np.float64))
+    assert np.max(np.abs(p_gpu - p)) <= 2e-3
+
+
+@pytest.mark.gpu
+def test_training_learns_exact_checker_labels():
+    """A short training run on exact-checker labels of the hull6 scene
+    lowers the loss and beats the constant predictor."""
+    import torch
+    from gpuprm_b200 import scenes
+    from gpuprm_b200.configspace import RobotConfigspace
+    from gpuprm_b200.mlp import CollisionMLP
+    sc = scenes.make_hull6(0)
+    cs = RobotConfigspace(sc, dq=0.01)
+    cs.init()
+    n = 1 << 16
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, n, 7).T), device="cuda:0")
+    codes = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+    cs.check_configs_device(q, codes)
+    y = (codes != 0).float()
+    mlp = CollisionMLP(6, seed=4)
+    losses = mlp.train(q, y, epochs=4, batch=4096, lr=1e-3, seed=5)
+    assert losses[-1] < losses[0]
+    qt = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, 8192, 8).T), device="cuda:0")
+    ct = torch.zeros(8192, dtype=torch.int32, device="cuda:0")
+    cs.check_configs_device(qt, ct)
+    p = mlp.predict(qt)
+    torch.cuda.synchronize()
+    acc = ((p > 0.5) == (ct != 0)).float().mean().item()
+    base = max((ct != 0).float().mean().item(), 1 - (ct != 0).float().mean().item())
+    assert acc > base + 0.05, (acc, base)

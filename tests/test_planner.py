@@ -1,0 +1,74 @@
+"""Roadmap planners: graph helpers (CPU) and plain vs lazy vs learned (B200)."""
+import numpy as np
+import pytest
+
+from gpuprm_b200 import planner
+
+
+def test_bfs_forest_paths_follow_edges():
+    rng = np.random.default_rng(0)
+    V = 300
+    ei = rng.integers(0, V, 700)
+    ej = rng.integers(0, V, 700)
+    keep = ei != ej
+    ei, ej = ei[keep], ej[keep]
+    comp = planner._components(V, ei, ej)
+    parent = planner._bfs_parents(V, ei, ej, comp)
+    edges = set(zip(ei.tolist(), ej.tolist())) | set(zip(ej.tolist(), ei.tolist()))
+    for v in range(V):
+        if parent[v] >= 0:
+            assert (v, int(parent[v])) in edges
+            assert comp[parent[v]] == comp[v]
+        else:
+            assert parent[v] == -1      # every vertex reached: a root
+    for _ in range(200):
+        s, t = rng.integers(0, V, 2)
+        p = planner._tree_path(parent, int(s), int(t))
+        if comp[s] != comp[t]:
+            assert p is None
+            continue
+        assert p[0] == s and p[-1] == t
+        for a, b in zip(p[:-1], p[1:]):
+            assert (a, b) in edges
+
+
+@pytest.mark.gpu
+def test_lazy_prm_has_the_connectivity_of_the_eager_prm():
+    """Two-round lazy checking solves exactly the queries the eager PRM
+    solves on the same samples, checking fewer edges; every path verifies."""
+    from gpuprm_b200 import scenes
+    from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
+    from gpuprm_b200.configspace import RobotConfigspace
+    sc = scenes.make_hull6(0)
+    cs = RobotConfigspace(sc, dq=0.01)
+    cs.init()
+    cs.set_mode(GPRM_MODE_FP64_BAND)
+    starts, goals = planner.make_queries(cs, sc, 200, seed=3)
+    plain = planner.plain_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=4)
+    lazy = planner.lazy_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=4)
+    np.testing.assert_array_equal(plain.success, lazy.success)
+    assert plain.info["verified"] and lazy.info["verified"]
+    assert lazy.edge_checks < plain.edge_checks
+    assert plain.success.mean() > 0.2
+
+
+@pytest.mark.gpu
+def test_learned_guidance_prunes_and_keeps_paths_verified():
+    from gpuprm_b200 import scenes
+    from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
+    from gpuprm_b200.configspace import RobotConfigspace
+    sc = scenes.make_hull6(0)
+    cs = RobotConfigspace(sc, dq=0.01)
+    cs.init()
+    cs.set_mode(GPRM_MODE_FP64_BAND)
+    mlp, losses, _, _ = planner.train_predictor(cs, sc, n_labels=1 << 17, epochs=3)
+    starts, goals = planner.make_queries(cs, sc, 200, seed=5)
+    plain = planner.plain_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=6)
+    learned = planner.lazy_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=6, mlp=mlp)
+    assert learned.info["verified"]
+    assert learned.info["pruned"] > 0
+    assert learned.edge_steps < plain.edge_steps
+    # every reported path connects its own start and goal
+    for i, p in enumerate(learned.paths):
+        if p is not None:
+            assert np.array_equal(p[0], starts[i]) and np.array_equal(p[-1], goals[i])
