@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--policy", default="early", choices=["early", "all"])
     ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
     ap.add_argument("--prm-samples", type=int, default=1 << 16)
+    ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
+    ap.add_argument("--batch-problems", type=int, default=256)
     return ap.parse_args()
 
 
@@ -290,6 +292,9 @@ def run_ours(args, rank, world, local_rank):
                                        mlp=mlp, repeats=3)
         prm["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
                             "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
+    batch = None
+    if not args.no_batch and world == 1:
+        batch = batch_leg(args, dev, policy)
     line = {
         "metric": METRIC, "value": nominal_all / t_max, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
@@ -303,9 +308,92 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-        "prm": prm,
+        "prm": prm, "batch": batch,
     }
     return line
+
+
+def batch_leg(args, dev, policy):
+    """Many independent problems: one graph-captured batched launch per kind
+    against a loop of per-problem launches (same stream, same inputs);
+    results must agree bit for bit."""
+    import torch
+    from gpuprm_b200 import workloads
+    from gpuprm_b200.batch import CONFIGS, EDGES, ProblemBatch
+    t_build = time.perf_counter()
+    ws = workloads.batch_workload(seed=args.seed, problems=args.batch_problems, device=str(dev))
+    t_build = time.perf_counter() - t_build
+    spaces = ws["spaces"]
+    for cs in spaces:
+        cs.set_edge_policy(policy)
+    B = ProblemBatch(spaces)
+    Q, A, Bq = ws["q"], ws["qs"], ws["qe"]
+    nv, ne = Q.shape[1], A.shape[1]
+    rv = torch.zeros(nv, dtype=torch.int32, device=dev)
+    re = torch.zeros(ne, dtype=torch.int32, device=dev)
+    B.set_layout(CONFIGS, ws["offs_v"])
+    B.set_layout(EDGES, ws["offs_e"])
+    tune_v = B.autotune(CONFIGS, Q, None, rv, reps=2)
+    tune_e = B.autotune(EDGES, A, Bq, re, reps=2)
+    B.capture(CONFIGS, Q, None, rv)
+    B.capture(EDGES, A, Bq, re)
+    # per-problem inputs for the launch loop
+    pv = [torch.tensor(np.ascontiguousarray(q.T), device=dev) for q in ws["q_host"]]
+    pa = [torch.tensor(np.ascontiguousarray(a.T), device=dev) for a in ws["qs_host"]]
+    pb = [torch.tensor(np.ascontiguousarray(b.T), device=dev) for b in ws["qe_host"]]
+    lv = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pv]
+    le = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pa]
+    stream = torch.cuda.current_stream()
+
+    def loop(kind):
+        for p, cs in enumerate(spaces):
+            if kind == CONFIGS and lv[p].numel():
+                cs.check_configs_device(pv[p], lv[p])
+            elif kind == EDGES and le[p].numel():
+                cs.check_edges_device(pa[p], pb[p], le[p])
+
+    def timed(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / steps
+
+    s0 = B.stats()
+    t_bv = timed(lambda: B.replay(CONFIGS), args.steps)
+    s1 = B.stats()
+    t_be = timed(lambda: B.replay(EDGES), args.steps)
+    s2 = B.stats()
+    t_lv = timed(lambda: loop(CONFIGS), args.steps)
+    t_le = timed(lambda: loop(EDGES), args.steps)
+    reps = max(3, args.warmup) + args.steps
+    nominal = (s2["edge_steps_nominal"] - s1["edge_steps_nominal"]) // reps
+    got_v, got_e = rv.cpu().numpy(), re.cpu().numpy()
+    ov, oe = ws["offs_v"], ws["offs_e"]
+    same_v = all(np.array_equal(got_v[ov[p]:ov[p + 1]], lv[p].cpu().numpy()) for p in range(len(spaces)))
+    same_e = all(np.array_equal(got_e[oe[p]:oe[p + 1]], le[p].cpu().numpy()) for p in range(len(spaces)))
+    dofs = [sc.ndof for sc in ws["scenes"]]
+    return {
+        "workload": "many problems: %d mixed scenes (DOF 4-7, 8-128 hull obstacles), 2^14-2^18 samples each, "
+                    "kNN k=%d of the first %d free samples, edges cut to a radius U[0.4,0.8], dq=%g"
+                    % (len(spaces), workloads.MANY["k"], workloads.MANY["edge_sources"], workloads.MANY["dq"]),
+        "problems": len(spaces), "dof_counts": {str(d): dofs.count(d) for d in sorted(set(dofs))},
+        "configs": int(nv), "edges": int(ne), "edge_steps_nominal": int(nominal),
+        "batched": {"configs_per_s": nv / t_bv, "edge_steps_per_s": nominal / t_be,
+                    "configs_ms": 1e3 * t_bv, "edges_ms": 1e3 * t_be, "graph_launches_per_step": 2,
+                    "threads": {"configs": tune_v["threads"], "edges": tune_e["threads"]}},
+        "per_problem_loop": {"configs_per_s": nv / t_lv, "edge_steps_per_s": nominal / t_le,
+                             "configs_ms": 1e3 * t_lv, "edges_ms": 1e3 * t_le},
+        "speedup": {"configs": t_lv / t_bv, "edges": t_le / t_be},
+        "results_identical": bool(same_v and same_e),
+        "vertex_checks_per_step": int((s1["vertex_checks"] - s0["vertex_checks"]) // reps),
+        "setup_seconds": t_build,
+    }
 
 
 # --------------------------------------------------------------------------

@@ -139,6 +139,20 @@ SIGNATURES = [
     ("gprm_profile_enable", C.c_int, [_P, C.c_int]),
     ("gprm_profile_read", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("gprm_measure_fp32_peak", C.c_int, [C.POINTER(C.c_double)]),
+    ("gprm_batch_create", C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
+    ("gprm_batch_destroy", None, [_P]),
+    ("gprm_batch_last_error", C.c_char_p, [_P]),
+    ("gprm_batch_set_layout", C.c_int, [_P, C.c_int, C.POINTER(C.c_longlong), C.c_longlong]),
+    ("gprm_batch_indicator_device", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]),
+    ("gprm_batch_indicator2_device", C.c_int,
+     [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]),
+    ("gprm_batch_capture", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("gprm_batch_replay", C.c_int, [_P, C.c_int, C.c_void_p]),
+    ("gprm_batch_set_launch", C.c_int, [_P, C.c_int, C.c_int]),
+    ("gprm_batch_get_launch", C.c_int, [_P, C.c_int, _I, _I]),
+    ("gprm_batch_autotune", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
+                                      _I, _F]),
+    ("gprm_batch_get_stats", C.c_int, [_P, C.POINTER(Stats)]),
 ]
 
 _lib = None

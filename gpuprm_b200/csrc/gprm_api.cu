@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/gprm_b200.h"
+#include "gprm_host.h"
 #include "gprm_internal.h"
 
 using namespace gprm;
@@ -36,75 +37,7 @@ namespace {
 
 thread_local std::string g_create_error = "no error";
 
-struct Request {
-    cudaStream_t st = nullptr;
-    Control* ctl = nullptr;       /* device */
-    Control* ctl_host = nullptr;  /* pinned copy read after the request */
-    float* d_a = nullptr;         /* q or qs (contiguous SoA, offset = n) */
-    float* d_b = nullptr;         /* qe */
-    int* d_res = nullptr;
-    unsigned* d_key = nullptr;
-    uint2* d_queue = nullptr;
-    float* h_a = nullptr;         /* pinned staging */
-    float* h_b = nullptr;
-    int* h_res = nullptr;
-    size_t cap_items = 0;         /* edges or configurations */
-    size_t cap_queue = 0;
-    bool busy = false;
-    /* the request in flight */
-    int kind = 0;                 /* 0 vertices, 1 edges */
-    int* user_res = nullptr;
-    int n = 0;
-    const float* user_a = nullptr;
-    const float* user_b = nullptr;
-    int user_offset = 0;
-};
-
 }  // namespace
-
-struct gprm_space {
-    int ndof = 0;
-    float dq = 0.01f;
-    int nbuf = 0;
-    float a[GPRM_MAX_DOF], alpha[GPRM_MAX_DOF], q0[GPRM_MAX_DOF], d0[GPRM_MAX_DOF];
-    float mins[GPRM_MAX_DOF], maxs[GPRM_MAX_DOF];
-    int types[GPRM_MAX_DOF];
-    int npoly = 0, npairs = 0, sumn = 0, summ = 0;
-    std::vector<float4> tab;       /* per-polytope blocks, see gprm_device.cuh */
-    std::vector<int4> pairs;
-    std::vector<float4> pairs_b;   /* certificate data per pair */
-    std::vector<double> rad;       /* inflated ball radius per polytope */
-    std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
-    std::vector<int> slot_sys, slot_block;
-    std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */
-    double extent = 1.0;           /* length scale of the scene (m) */
-    float thr_dir = 0, eps_dir = 0;
-
-    bool inited = false;
-    int device = 0;
-    int sms = 0;
-    cudaStream_t stream = nullptr;
-    void* d_scene = nullptr;
-    DevScene dsc;
-    LaunchCfg cfg_v, cfg_e;
-
-    int mode = GPRM_MODE_FP64_BAND;
-    int policy = GPRM_EDGES_EARLY_EXIT;
-    float band = 1e-5f;
-
-    std::vector<Request> reqs;
-    std::map<int, int> live;       /* request id -> slot */
-    int next_id = 0;
-    Request dev;                   /* scratch of the device-pointer entry points */
-    Control* d_total = nullptr;    /* cumulative counters of all requests */
-    gprm_stats host_stats;         /* host-side counters */
-
-    bool profiling = false;
-    std::vector<cudaEvent_t> ev32, ev64;   /* start/stop pairs */
-    size_t ev32_used = 0, ev64_used = 0;
-
-    std::string err = "no error";
-};
 
 namespace {
 
@@ -411,20 +344,6 @@ int event_pair(gprm_space* h, std::vector<cudaEvent_t>& pool, size_t& used, cuda
     return GPRM_OK;
 }
 
-__global__ void k_accumulate(const Control* c, Control* total)
-{
-    total->steps_nominal += c->steps_nominal;
-    total->steps_exec += c->steps_exec;
-    total->band_checks += c->band_checks;
-    total->band_flips += c->band_flips;
-    total->configs_exec += c->configs_exec;
-    total->cert_far += c->cert_far;
-    total->cert_dir += c->cert_dir;
-    total->full_tests += c->full_tests;
-    total->flags |= c->flags;
-    total->next += 1;  /* requests completed */
-}
-
 /* Enqueues one request on stream `st` with device inputs/outputs.
  * kind 0: q -> res.  kind 1: (qs, qe) -> res. */
 int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
@@ -463,8 +382,7 @@ int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b,
     if (kind == 1) CUDA_TRY(h, launch_finalize_edges(n, h->policy, r.d_key, res, st));
     /* check + accumulate, plus recheck and finalize where they run */
     h->host_stats.launches += 2 + (band_on ? 1 : 0) + (kind == 1 ? 1 : 0);
-    k_accumulate<<<1, 1, 0, st>>>(r.ctl, h->d_total);
-    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, launch_accumulate(r.ctl, h->d_total, st));
     return GPRM_OK;
 }
 
@@ -629,7 +547,7 @@ int gprm_init(gprm_space* h, int rank, int size)
 
     DevScene& s = h->dsc;
     memset(&s, 0, sizeof(s));
-    s.ndof = h->ndof; s.npoly = h->npoly; s.npairs = h->npairs; s.sumn = h->sumn; s.summ = h->summ;
+    s.ndof = h->ndof; s.dq = h->dq; s.npoly = h->npoly; s.npairs = h->npairs; s.sumn = h->sumn; s.summ = h->summ;
     for (int i = 0; i < h->ndof; ++i) {
         s.a[i] = h->a[i]; s.q0[i] = h->q0[i]; s.d0[i] = h->d0[i]; s.types[i] = h->types[i];
         s.mins[i] = h->mins[i]; s.maxs[i] = h->maxs[i];
@@ -1020,8 +938,7 @@ extern "C" int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q
     if (band_on)
         CUDA_TRY(h, launch_recheck(h->dsc, h->sms * 4, 0, q, nullptr, nullptr, offset, h->dq, h->policy, res,
                                    nullptr, queue, qcap, ctl, st));
-    k_accumulate<<<1, 1, 0, st>>>(ctl, h->d_total);
-    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, launch_accumulate(ctl, h->d_total, st));
     h->host_stats.vertex_checks += n;
     h->host_stats.launches += 2 + (band_on ? 1 : 0);
     return GPRM_OK;

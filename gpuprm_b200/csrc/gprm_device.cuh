@@ -64,6 +64,7 @@ struct DevScene {
        eps_dir bounds the direction error of the approximate first direction
        times its distance (see pair_certified) */
     float thr_dir, eps_dir;
+    float dq;                            /* edge resolution (batched problems) */
     int nslots;                          /* moving polytopes with a ball slot */
     int slot_sys[GPRM_MAX_SLOTS];        /* frame of each slot */
     int slot_block[GPRM_MAX_SLOTS];      /* its table block (entry 0 = ball) */

@@ -1,0 +1,88 @@
+/*
+ * gprm_host.h - host-side state of a gprm_space handle, shared by the
+ * library's host sources (gprm_api.cu, gprm_batch.cu).  Not installed.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/gprm_b200.h"
+#include "gprm_internal.h"
+
+namespace gprm {
+
+/* One request of the pool: stream, control block, device buffers and
+ * pinned staging. */
+struct Request {
+    cudaStream_t st = nullptr;
+    Control* ctl = nullptr;       /* device */
+    Control* ctl_host = nullptr;  /* pinned copy read after the request */
+    float* d_a = nullptr;         /* q or qs (contiguous SoA, offset = n) */
+    float* d_b = nullptr;         /* qe */
+    int* d_res = nullptr;
+    unsigned* d_key = nullptr;
+    uint2* d_queue = nullptr;
+    float* h_a = nullptr;         /* pinned staging */
+    float* h_b = nullptr;
+    int* h_res = nullptr;
+    size_t cap_items = 0;         /* edges or configurations */
+    size_t cap_queue = 0;
+    bool busy = false;
+    /* the request in flight */
+    int kind = 0;                 /* 0 vertices, 1 edges */
+    int* user_res = nullptr;
+    int n = 0;
+    const float* user_a = nullptr;
+    const float* user_b = nullptr;
+    int user_offset = 0;
+};
+
+}  // namespace gprm
+
+struct gprm_space {
+    int ndof = 0;
+    float dq = 0.01f;
+    int nbuf = 0;
+    float a[GPRM_MAX_DOF], alpha[GPRM_MAX_DOF], q0[GPRM_MAX_DOF], d0[GPRM_MAX_DOF];
+    float mins[GPRM_MAX_DOF], maxs[GPRM_MAX_DOF];
+    int types[GPRM_MAX_DOF];
+    int npoly = 0, npairs = 0, sumn = 0, summ = 0;
+    std::vector<float4> tab;       /* per-polytope blocks, see gprm_device.cuh */
+    std::vector<int4> pairs;
+    std::vector<float4> pairs_b;   /* certificate data per pair */
+    std::vector<double> rad;       /* inflated ball radius per polytope */
+    std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
+    std::vector<int> slot_sys, slot_block;
+    std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */
+    double extent = 1.0;           /* length scale of the scene (m) */
+    float thr_dir = 0, eps_dir = 0;
+
+    bool inited = false;
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    void* d_scene = nullptr;
+    gprm::DevScene dsc;
+    gprm::LaunchCfg cfg_v, cfg_e;
+
+    int mode = GPRM_MODE_FP64_BAND;
+    int policy = GPRM_EDGES_EARLY_EXIT;
+    float band = 1e-5f;
+
+    std::vector<gprm::Request> reqs;
+    std::map<int, int> live;       /* request id -> slot */
+    int next_id = 0;
+    gprm::Request dev;             /* scratch of the device-pointer entry points */
+    gprm::Control* d_total = nullptr;  /* cumulative counters of all requests */
+    gprm_stats host_stats;         /* host-side counters */
+
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev32, ev64;   /* start/stop pairs */
+    size_t ev32_used = 0, ev64_used = 0;
+
+    std::string err = "no error";
+};

@@ -40,6 +40,35 @@ struct LaunchCfg {
 
 enum EdgePolicy { EDGE_EARLY_EXIT = 0, EDGE_ALL_STEPS = 1 };
 
+/* Adds the counters of request control block c to `total` (one thread). */
+cudaError_t launch_accumulate(const Control* c, Control* total, cudaStream_t st);
+
+/* Many independent problems in one launch.  Items (configurations or
+ * edges) of problem p are offs[p] .. offs[p+1]-1 of the input arrays, which
+ * hold GPRM_MAX_DOF rows (rows >= the problem's ndof are ignored).  Vertex
+ * work is handed out in chunks of at most 32 configurations of one problem
+ * (problem, first item, count). */
+struct BatchView {
+    const DevScene* scenes;   /* [S], device */
+    const long long* offs;    /* [S+1], device */
+    const int4* chunks;       /* vertex chunks, device */
+    long long nwork;          /* chunks (vertex) or edges (edge) */
+    int S;
+    int lane_floats;          /* per-lane shared floats: max over the problems */
+};
+
+/* Launch shape of the batched kernels. */
+cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg);
+cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg, const float* q, long long offset,
+                                       int* res, int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
+                                       cudaStream_t st);
+cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, const float* qs, const float* qe,
+                                     long long offset, int policy, unsigned* key, int band_on, float band,
+                                     uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
+cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,
+                                 const float* qe, long long offset, int policy, int* res, unsigned* key,
+                                 const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
+
 /* Scene bytes when staged in shared memory; per-lane frame bytes of a block. */
 size_t scene_smem_bytes(const DevScene& sc);
 size_t frame_smem_bytes(const DevScene& sc, int threads);

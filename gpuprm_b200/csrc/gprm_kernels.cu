@@ -172,12 +172,51 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
 /* vertex checks                                                        */
 /* ------------------------------------------------------------------ */
 
+/* Configurations i0 .. i0+count-1 (count <= 32), one per lane. */
+__device__ __forceinline__ void check_config_chunk(const DevScene& sc, const SceneView& S, const float* __restrict__ q,
+                                                   long long offset, long long i0, int count, int* __restrict__ res,
+                                                   int band_on, float band, uint2* __restrict__ queue, unsigned qcap,
+                                                   Control* ctl, PairCounts& pc, unsigned long long& exec)
+{
+    const int lane = threadIdx.x & 31;
+    const long long i = i0 + lane;
+    const bool valid = lane < count;
+    float qi[GPRM_MAX_FRAMES];
+    int code = 0;
+    bool active = valid;
+    if (valid) {
+        for (int j = 0; j < sc.ndof; ++j) qi[j] = q[i + offset * j];
+        /* check_boundaries(q) (robotconfigspace.cpp:795-802) */
+        for (int j = 0; j < sc.ndof; ++j)
+            if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
+    }
+    if (active) forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
+    float mmin = PF32::inf(), mdec = 0.0f;
+#pragma unroll 1
+    for (int j = 0; j < sc.npairs; ++j) {
+        if (!__any_sync(FULL_MASK, active)) break;
+        if (active) {
+            float m;
+            bool hm;
+            int r = eval_pair(sc, S, j, &m, &hm, pc);
+            if (r != 0) { code = r; mdec = m; active = false; }
+            else if (hm) mmin = min_nan(mmin, m);
+        }
+    }
+    if (valid) {
+        exec += (code != 1);
+        res[i] = code;
+    }
+    bool want = valid && band_on && code != 1 && in_band(code, code == 0 ? mmin : mdec, band);
+    warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), queue, qcap, ctl);
+}
+
 template <bool SMEM>
 __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict__ q,
-                                                       long long n, long long offset,
-                                                       int* __restrict__ res, int band_on, float band,
-                                                       uint2* __restrict__ queue, unsigned qcap,
-                                                       Control* ctl)
+                                            long long n, long long offset,
+                                            int* __restrict__ res, int band_on, float band,
+                                            uint2* __restrict__ queue, unsigned qcap,
+                                            Control* ctl)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const SceneView S = stage_scene<SMEM>(sc, smem);
@@ -189,36 +228,9 @@ __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict
         if (lane == 0) base = atomicAdd(&ctl->next, 32ull);
         base = __shfl_sync(FULL_MASK, base, 0);
         if (base >= (unsigned long long)n) break;
-        const long long i = (long long)base + lane;
-        const bool valid = i < n;
-        float qi[GPRM_MAX_FRAMES];
-        int code = 0;
-        bool active = valid;
-        if (valid) {
-            for (int j = 0; j < sc.ndof; ++j) qi[j] = q[i + offset * j];
-            /* check_boundaries(q) (robotconfigspace.cpp:795-802) */
-            for (int j = 0; j < sc.ndof; ++j)
-                if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
-        }
-        if (active) forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
-        float mmin = PF32::inf(), mdec = 0.0f;
-#pragma unroll 1
-        for (int j = 0; j < sc.npairs; ++j) {
-            if (!__any_sync(FULL_MASK, active)) break;
-            if (active) {
-                float m;
-                bool hm;
-                int r = eval_pair(sc, S, j, &m, &hm, pc);
-                if (r != 0) { code = r; mdec = m; active = false; }
-                else if (hm) mmin = min_nan(mmin, m);
-            }
-        }
-        if (valid) {
-            exec += (code != 1);
-            res[i] = code;
-        }
-        bool want = valid && band_on && code != 1 && in_band(code, code == 0 ? mmin : mdec, band);
-        warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), queue, qcap, ctl);
+        const long long left = n - (long long)base;
+        check_config_chunk(sc, S, q, offset, (long long)base, left < 32 ? (int)left : 32, res, band_on, band,
+                           queue, qcap, ctl, pc, exec);
     }
     exec = warp_sum(exec);
     if (lane == 0 && exec) atomicAdd(&ctl->configs_exec, exec);
@@ -237,12 +249,107 @@ __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict
 __device__ __forceinline__ unsigned early_key(unsigned order, int code) { return (order << 4) | (unsigned)(code + 1); }
 __device__ __forceinline__ unsigned all_key(int t, int code) { return ((unsigned)(t + 1) << 4) | (unsigned)(code + 1); }
 
+/* One edge e (testnum steps, rounds of 32 steps over the lanes). */
+template <int POLICY>
+__device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& S, const float* __restrict__ qs,
+                                           const float* __restrict__ qe, long long e, long long offset, float dq,
+                                           unsigned* __restrict__ key, int band_on, float band,
+                                           uint2* __restrict__ queue, unsigned qcap, Control* ctl, PairCounts& pc,
+                                           unsigned long long& exec, unsigned long long& nominal)
+{
+    const int lane = threadIdx.x & 31;
+    const int tn = edge_testnum(qs, qe, e, offset, sc.ndof, dq);
+    if (tn < 0) {
+        if (lane == 0) atomicOr(&ctl->flags, GPRM_DEVFLAG_BAD_EDGE);
+        return;
+    }
+    if (lane == 0) nominal += tn;
+    const int R = (tn + 31) >> 5;
+    bool decided = false;
+#pragma unroll 1
+    for (int r = 0; r < R && !decided; ++r) {
+        int t;
+        unsigned order;
+        bool valid;
+        if (POLICY == EDGE_EARLY_EXIT) {
+            t = lane * R + r;
+            valid = t < tn;
+            order = (unsigned)(r * 32 + lane);
+        } else {
+            int idx = r * 32 + lane;
+            t = tn - 1 - idx;
+            valid = idx < tn;
+            order = 0;
+        }
+        float qi[GPRM_MAX_FRAMES];
+        if (valid) {
+            edge_step_config(qs, qe, e, offset, sc.ndof, t, tn, qi);
+            forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
+        }
+        const unsigned valid_mask = __ballot_sync(FULL_MASK, valid);
+        if (lane == 0) exec += __popc(valid_mask);
+        bool active = valid;
+        int code = 0;
+        float mmin = PF32::inf(), mdec = 0.0f;
+        int cut = 32;   /* lanes above the highest-priority colliding lane no longer matter */
+        int jend = 0;   /* pairs processed by the warp */
+#pragma unroll 1
+        for (int j = 0; j < sc.npairs; ++j) {
+            if (!__any_sync(FULL_MASK, active)) break;
+            if (active) {
+                float m;
+                bool hm;
+                int rr = eval_pair(sc, S, j, &m, &hm, pc);
+                if (rr != 0) { code = rr; mdec = m; active = false; }
+                else if (hm) mmin = min_nan(mmin, m);
+            }
+            jend = j + 1;
+            bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
+            unsigned hits = __ballot_sync(FULL_MASK, oobj);
+            if (hits) {
+                int Lj = __ffs(hits) - 1;
+                if (Lj < cut) cut = Lj;
+                if (POLICY == EDGE_EARLY_EXIT) break;
+                if (lane > cut) active = false;
+            }
+        }
+        /* settle the round */
+        const bool oob = code != 0 && !(band_on && in_band(code, mdec, band));
+        const unsigned hits = __ballot_sync(FULL_MASK, oob && lane <= cut);
+        const int L = hits ? __ffs(hits) - 1 : 32;
+        const bool free_done = valid && code == 0 && active && jend == sc.npairs;
+        const bool inb = band_on && ((code != 0 && !oob) || (free_done && in_band(0, mmin, band)));
+        /* in-band steps earlier in order (early exit) or higher t (all steps)
+           than the deciding step go to the FP64 queue */
+        const bool want = inb && lane < L;
+        warp_append(want, make_uint2((unsigned)e, (unsigned)t | ((unsigned)(code + 1) << 27)),
+                    queue, qcap, ctl);
+        if (hits) {
+            if (lane == L)
+                key[e] = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
+            decided = true;
+        }
+    }
+}
+
+__device__ __forceinline__ void flush_edge_counts(unsigned long long exec, unsigned long long nominal, PairCounts pc,
+                                                  Control* ctl)
+{
+    exec = warp_sum(exec);
+    nominal = warp_sum(nominal);
+    if ((threadIdx.x & 31) == 0) {
+        if (exec) atomicAdd(&ctl->steps_exec, exec);
+        if (nominal) atomicAdd(&ctl->steps_nominal, nominal);
+    }
+    flush_counts(pc, ctl);
+}
+
 template <bool SMEM, int POLICY>
 __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__ qs,
-                                                     const float* __restrict__ qe, long long n,
-                                                     long long offset, float dq, unsigned* __restrict__ key,
-                                                     int band_on, float band, uint2* __restrict__ queue,
-                                                     unsigned qcap, Control* ctl)
+                                          const float* __restrict__ qe, long long n,
+                                          long long offset, float dq, unsigned* __restrict__ key,
+                                          int band_on, float band, uint2* __restrict__ queue,
+                                          unsigned qcap, Control* ctl)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const SceneView S = stage_scene<SMEM>(sc, smem);
@@ -254,92 +361,58 @@ __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__
         if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
         eu = __shfl_sync(FULL_MASK, eu, 0);
         if (eu >= (unsigned long long)n) break;
-        const long long e = (long long)eu;
-        const int tn = edge_testnum(qs, qe, e, offset, sc.ndof, dq);
-        if (tn < 0) {
-            if (lane == 0) atomicOr(&ctl->flags, GPRM_DEVFLAG_BAD_EDGE);
-            continue;
-        }
-        if (lane == 0) nominal += tn;
-        const int R = (tn + 31) >> 5;
-        bool decided = false;
-#pragma unroll 1
-        for (int r = 0; r < R && !decided; ++r) {
-            int t;
-            unsigned order;
-            bool valid;
-            if (POLICY == EDGE_EARLY_EXIT) {
-                t = lane * R + r;
-                valid = t < tn;
-                order = (unsigned)(r * 32 + lane);
-            } else {
-                int idx = r * 32 + lane;
-                t = tn - 1 - idx;
-                valid = idx < tn;
-                order = 0;
-            }
-            float qi[GPRM_MAX_FRAMES];
-            if (valid) {
-                edge_step_config(qs, qe, e, offset, sc.ndof, t, tn, qi);
-                forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
-            }
-            const unsigned valid_mask = __ballot_sync(FULL_MASK, valid);
-            if (lane == 0) exec += __popc(valid_mask);
-            bool active = valid;
-            int code = 0;
-            float mmin = PF32::inf(), mdec = 0.0f;
-            int cut = 32;   /* lanes above the highest-priority colliding lane no longer matter */
-            int jend = 0;   /* pairs processed by the warp */
-#pragma unroll 1
-            for (int j = 0; j < sc.npairs; ++j) {
-                if (!__any_sync(FULL_MASK, active)) break;
-                if (active) {
-                    float m;
-                    bool hm;
-                    int rr = eval_pair(sc, S, j, &m, &hm, pc);
-                    if (rr != 0) { code = rr; mdec = m; active = false; }
-                    else if (hm) mmin = min_nan(mmin, m);
-                }
-                jend = j + 1;
-                bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
-                unsigned hits = __ballot_sync(FULL_MASK, oobj);
-                if (hits) {
-                    int Lj = __ffs(hits) - 1;
-                    if (Lj < cut) cut = Lj;
-                    if (POLICY == EDGE_EARLY_EXIT) break;
-                    if (lane > cut) active = false;
-                }
-            }
-            /* settle the round */
-            const bool oob = code != 0 && !(band_on && in_band(code, mdec, band));
-            const unsigned hits = __ballot_sync(FULL_MASK, oob && lane <= cut);
-            const int L = hits ? __ffs(hits) - 1 : 32;
-            const bool free_done = valid && code == 0 && active && jend == sc.npairs;
-            const bool inb = band_on && ((code != 0 && !oob) || (free_done && in_band(0, mmin, band)));
-            /* in-band steps earlier in order (early exit) or higher t (all steps)
-               than the deciding step go to the FP64 queue */
-            const bool want = inb && lane < L;
-            warp_append(want, make_uint2((unsigned)e, (unsigned)t | ((unsigned)(code + 1) << 27)),
-                        queue, qcap, ctl);
-            if (hits) {
-                if (lane == L)
-                    key[e] = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
-                decided = true;
-            }
-        }
+        check_edge<POLICY>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, queue, qcap, ctl, pc, exec,
+                           nominal);
     }
-    exec = warp_sum(exec);
-    nominal = warp_sum(nominal);
-    if (lane == 0) {
-        if (exec) atomicAdd(&ctl->steps_exec, exec);
-        if (nominal) atomicAdd(&ctl->steps_nominal, nominal);
-    }
-    flush_counts(pc, ctl);
+    flush_edge_counts(exec, nominal, pc, ctl);
 }
 
 /* ------------------------------------------------------------------ */
 /* FP64 recheck and finalisation                                        */
 /* ------------------------------------------------------------------ */
+
+/* FP64 recheck of one queued item (vertex kind 0, edge step kind 1). */
+__device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2 it, const float* __restrict__ q,
+                                             const float* __restrict__ qs, const float* __restrict__ qe,
+                                             long long offset, float dq, int policy, int* __restrict__ res,
+                                             unsigned* __restrict__ key, unsigned long long& checks,
+                                             unsigned long long& flips)
+{
+    Frame<double> F[GPRM_MAX_FRAMES];
+    const int code32 = (int)(it.y >> 27) - 1;
+    float qi[GPRM_MAX_FRAMES];
+    int t = 0, tn = 0;
+    if (kind == 0) {
+        for (int j = 0; j < sc.ndof; ++j) qi[j] = q[(long long)it.x + offset * j];
+    } else {
+        t = (int)(it.y & ((1u << 27) - 1));
+        tn = edge_testnum(qs, qe, (long long)it.x, offset, sc.ndof, dq);
+        edge_step_config(qs, qe, (long long)it.x, offset, sc.ndof, t, tn, qi);
+    }
+    forward_kinematics<PF64>(sc, qi, F);
+    int code = 0;
+#pragma unroll 1
+    for (int j = 0; j < sc.npairs; ++j) {
+        const int4 pr = sc.pairs[j];
+        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F)) continue;
+        double m;
+        int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
+        if (r != 0) { code = r; break; }
+    }
+    ++checks;
+    flips += ((code != 0) != (code32 != 0));
+    if (kind == 0) {
+        res[it.x] = code;
+    } else if (code != 0) {
+        if (policy == EDGE_EARLY_EXIT) {
+            int R = (tn + 31) >> 5;
+            unsigned order = (unsigned)((t % R) * 32 + t / R);
+            atomicMin(&key[it.x], early_key(order, code));
+        } else {
+            atomicMax(&key[it.x], all_key(t, code));
+        }
+    }
+}
 
 __global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const float* __restrict__ q,
                                                  const float* __restrict__ qs, const float* __restrict__ qe,
@@ -351,43 +424,8 @@ __global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const fl
     unsigned cnt = ctl->qcount;
     if (cnt > qcap) cnt = qcap;
     unsigned long long checks = 0, flips = 0;
-    Frame<double> F[GPRM_MAX_FRAMES];
-    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
-        const uint2 it = queue[idx];
-        const int code32 = (int)(it.y >> 27) - 1;
-        float qi[GPRM_MAX_FRAMES];
-        int t = 0, tn = 0;
-        if (kind == 0) {
-            for (int j = 0; j < sc.ndof; ++j) qi[j] = q[(long long)it.x + offset * j];
-        } else {
-            t = (int)(it.y & ((1u << 27) - 1));
-            tn = edge_testnum(qs, qe, (long long)it.x, offset, sc.ndof, dq);
-            edge_step_config(qs, qe, (long long)it.x, offset, sc.ndof, t, tn, qi);
-        }
-        forward_kinematics<PF64>(sc, qi, F);
-        int code = 0;
-#pragma unroll 1
-        for (int j = 0; j < sc.npairs; ++j) {
-            const int4 pr = sc.pairs[j];
-            if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F)) continue;
-            double m;
-            int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
-            if (r != 0) { code = r; break; }
-        }
-        ++checks;
-        flips += ((code != 0) != (code32 != 0));
-        if (kind == 0) {
-            res[it.x] = code;
-        } else if (code != 0) {
-            if (policy == EDGE_EARLY_EXIT) {
-                int R = (tn + 31) >> 5;
-                unsigned order = (unsigned)((t % R) * 32 + t / R);
-                atomicMin(&key[it.x], early_key(order, code));
-            } else {
-                atomicMax(&key[it.x], all_key(t, code));
-            }
-        }
-    }
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x)
+        recheck_item(sc, kind, queue[idx], q, qs, qe, offset, dq, policy, res, key, checks, flips);
     if (checks) atomicAdd(&ctl->band_checks, checks);
     if (flips) atomicAdd(&ctl->band_flips, flips);
 }
@@ -417,6 +455,21 @@ __global__ void k_fk_probe(DevScene sc, const float* q, float* out)
 /* launchers                                                            */
 /* ------------------------------------------------------------------ */
 
+/* The dynamic shared-memory cap is an attribute of the kernel, shared by
+ * every handle in the process: it is opened to the device's opt-in limit
+ * (less the kernel's static shared memory), so that configuring one handle
+ * never shrinks what another handle launches with.  Fails when `need`
+ * bytes do not fit. */
+static cudaError_t open_smem_cap(const void* fn, int optin, size_t need)
+{
+    cudaFuncAttributes fa;
+    cudaError_t err = cudaFuncGetAttributes(&fa, fn);
+    if (err != cudaSuccess) return err;
+    const int cap = optin - (int)fa.sharedSizeBytes;
+    if (cap < 0 || need > (size_t)cap) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+}
+
 /* Occupancy of one FP32 kernel variant, in resident warps per SM. */
 static cudaError_t variant_warps(const void* fn, int threads, size_t smem, int* warps_per_sm)
 {
@@ -443,10 +496,8 @@ cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads,
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     size_t smem = frame_smem_bytes(sc, threads) + (scene_in_smem ? scene_smem_bytes(sc) : 0);
-    if (smem > (size_t)optin) return cudaErrorInvalidValue;
     for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol) {
-        err = cudaFuncSetAttribute(kernel_fn(vertex_kernel, scene_in_smem != 0, pol),
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        err = open_smem_cap(kernel_fn(vertex_kernel, scene_in_smem != 0, pol), optin, smem);
         if (err != cudaSuccess) return err;
     }
     int warps = 0;
@@ -528,6 +579,196 @@ cudaError_t launch_finalize_edges(long long n, int policy, const unsigned* key, 
     long long b = (n + 255) / 256;
     if (b > 4096) b = 4096;
     k_finalize_edges<<<(int)b, 256, 0, st>>>(n, policy, key, res);
+    return cudaGetLastError();
+}
+
+
+/* ------------------------------------------------------------------ */
+/* many problems in one launch                                          */
+/* ------------------------------------------------------------------ */
+
+/* shared bytes of one warp's cached scene descriptor */
+constexpr int SCENE_CACHE_BYTES = (int)((sizeof(DevScene) + 15) / 16 * 16);
+
+/* Problem of item `it`: the p with offs[p] <= it < offs[p+1]. */
+__device__ __forceinline__ int problem_of(const BatchView& B, long long it)
+{
+    int lo = 0, hi = B.S;   /* offs[lo] <= it < offs[hi] */
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (B.offs[mid] <= it) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+/* Makes problem p's descriptor the warp's current scene (warp-uniform p). */
+__device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene* wsc, float* frames, SceneView& S)
+{
+    __syncwarp();
+    const unsigned* src = reinterpret_cast<const unsigned*>(B.scenes + p);
+    unsigned* dst = reinterpret_cast<unsigned*>(wsc);
+    for (int k = threadIdx.x & 31; k < (int)(sizeof(DevScene) / 4); k += 32) dst[k] = src[k];
+    __syncwarp();
+    S.tab = wsc->tab;
+    S.pairs = wsc->pairs;
+    S.pairs_b = wsc->pairs_b;
+    S.frames = frames;
+    S.cen = frames + (size_t)wsc->ndof * 12 * 32;
+}
+
+__global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __restrict__ q, long long offset,
+                                                  int* __restrict__ res, int band_on, float band,
+                                                  uint2* __restrict__ queue, unsigned qcap, Control* ctl)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    DevScene* wsc = reinterpret_cast<DevScene*>(smem + warp * SCENE_CACHE_BYTES);
+    float* frames = reinterpret_cast<float*>(smem + nw * SCENE_CACHE_BYTES) + (size_t)warp * B.lane_floats * 32 + lane;
+    SceneView S;
+    int cur = -1;
+    unsigned long long exec = 0;
+    PairCounts pc = {0, 0, 0};
+    for (;;) {
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(&ctl->next, 1ull);
+        c = __shfl_sync(FULL_MASK, c, 0);
+        if (c >= (unsigned long long)B.nwork) break;
+        const int4 ch = B.chunks[c];
+        if (ch.x != cur) { switch_scene(B, ch.x, wsc, frames, S); cur = ch.x; }
+        check_config_chunk(*wsc, S, q, offset, (long long)ch.y, ch.z, res, band_on, band, queue, qcap, ctl, pc, exec);
+    }
+    exec = warp_sum(exec);
+    if (lane == 0 && exec) atomicAdd(&ctl->configs_exec, exec);
+    flush_counts(pc, ctl);
+}
+
+template <int POLICY>
+__global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __restrict__ qs, const float* __restrict__ qe,
+                                                long long offset, unsigned* __restrict__ key, int band_on, float band,
+                                                uint2* __restrict__ queue, unsigned qcap, Control* ctl)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    DevScene* wsc = reinterpret_cast<DevScene*>(smem + warp * SCENE_CACHE_BYTES);
+    float* frames = reinterpret_cast<float*>(smem + nw * SCENE_CACHE_BYTES) + (size_t)warp * B.lane_floats * 32 + lane;
+    SceneView S;
+    int cur = -1;
+    unsigned long long exec = 0, nominal = 0;
+    PairCounts pc = {0, 0, 0};
+    for (;;) {
+        unsigned long long eu = 0;
+        if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
+        eu = __shfl_sync(FULL_MASK, eu, 0);
+        if (eu >= (unsigned long long)B.nwork) break;
+        const int p = problem_of(B, (long long)eu);
+        if (p != cur) { switch_scene(B, p, wsc, frames, S); cur = p; }
+        check_edge<POLICY>(*wsc, S, qs, qe, (long long)eu, offset, wsc->dq, key, band_on, band, queue, qcap, ctl,
+                           pc, exec, nominal);
+    }
+    flush_edge_counts(exec, nominal, pc, ctl);
+}
+
+__global__ void __launch_bounds__(128) k_recheck_multi(BatchView B, int kind, const float* __restrict__ q,
+                                                       const float* __restrict__ qs, const float* __restrict__ qe,
+                                                       long long offset, int policy, int* __restrict__ res,
+                                                       unsigned* __restrict__ key, const uint2* __restrict__ queue,
+                                                       unsigned qcap, Control* ctl)
+{
+    unsigned cnt = ctl->qcount;
+    if (cnt > qcap) cnt = qcap;
+    unsigned long long checks = 0, flips = 0;
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
+        const uint2 it = queue[idx];
+        const DevScene& sc = B.scenes[problem_of(B, (long long)it.x)];
+        recheck_item(sc, kind, it, q, qs, qe, offset, sc.dq, policy, res, key, checks, flips);
+    }
+    if (checks) atomicAdd(&ctl->band_checks, checks);
+    if (flips) atomicAdd(&ctl->band_flips, flips);
+}
+
+static const void* batch_kernel_fn(int vertex_kernel, int policy)
+{
+    if (vertex_kernel) return (const void*)k_check_configs_multi;
+    return policy == EDGE_EARLY_EXIT ? (const void*)k_check_edges_multi<EDGE_EARLY_EXIT>
+                                     : (const void*)k_check_edges_multi<EDGE_ALL_STEPS>;
+}
+
+cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg)
+{
+    int dev = 0, sms = 0, optin = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int nw = threads / 32;
+    size_t smem = (size_t)nw * SCENE_CACHE_BYTES + (size_t)nw * B.lane_floats * 32 * sizeof(float);
+    for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol) {
+        err = open_smem_cap(batch_kernel_fn(vertex_kernel, pol), optin, smem);
+        if (err != cudaSuccess) return err;
+    }
+    int warps = 0;
+    err = variant_warps(batch_kernel_fn(vertex_kernel, 0), threads, smem, &warps);
+    if (err != cudaSuccess) return err;
+    if (warps < 1) return cudaErrorInvalidConfiguration;
+    cfg->threads = threads;
+    cfg->smem_bytes = smem;
+    cfg->scene_in_smem = 0;
+    cfg->blocks = sms * (warps / nw);
+    cfg->warps_per_sm = warps;
+    return cudaSuccess;
+}
+
+cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg, const float* q, long long offset,
+                                       int* res, int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
+                                       cudaStream_t st)
+{
+    if (B.nwork <= 0) return cudaSuccess;
+    k_check_configs_multi<<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on, band, queue,
+                                                                          qcap, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, const float* qs, const float* qe,
+                                     long long offset, int policy, unsigned* key, int band_on, float band,
+                                     uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
+{
+    if (B.nwork <= 0) return cudaSuccess;
+    if (policy == EDGE_EARLY_EXIT)
+        k_check_edges_multi<EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(
+            B, qs, qe, offset, key, band_on, band, queue, qcap, ctl);
+    else
+        k_check_edges_multi<EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(
+            B, qs, qe, offset, key, band_on, band, queue, qcap, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,
+                                 const float* qe, long long offset, int policy, int* res, unsigned* key,
+                                 const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
+{
+    k_recheck_multi<<<blocks, 128, 0, st>>>(B, kind, q, qs, qe, offset, policy, res, key, queue, qcap, ctl);
+    return cudaGetLastError();
+}
+
+/* Adds a request's counters to the handle's running totals. */
+__global__ void k_accumulate(const Control* c, Control* total)
+{
+    total->steps_nominal += c->steps_nominal;
+    total->steps_exec += c->steps_exec;
+    total->band_checks += c->band_checks;
+    total->band_flips += c->band_flips;
+    total->configs_exec += c->configs_exec;
+    total->cert_far += c->cert_far;
+    total->cert_dir += c->cert_dir;
+    total->full_tests += c->full_tests;
+    total->flags |= c->flags;
+    total->next += 1;  /* requests completed */
+}
+
+cudaError_t launch_accumulate(const Control* c, Control* total, cudaStream_t st)
+{
+    k_accumulate<<<1, 1, 0, st>>>(c, total);
     return cudaGetLastError();
 }
 

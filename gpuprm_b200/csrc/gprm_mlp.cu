@@ -270,12 +270,6 @@ __global__ void k_to_bf16(long long n, const float* __restrict__ w, const int* _
     }
 }
 
-/* shuffled batch indices for step s: perm[s*B .. s*B+B) */
-__global__ void k_gather_labels(int n, const int* __restrict__ idx, const float* __restrict__ y, float* __restrict__ yb)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) yb[i] = y[idx[i]];
-}
-
 }  // namespace
 
 /* ====================================================================== */
@@ -460,7 +454,7 @@ int gprm_mlp_create(int ndof, unsigned long long seed, gprm_mlp** out)
         (e = cudaMalloc((void**)&h->loss, sizeof(float))) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking)) != cudaSuccess) {
         gprm_mlp_destroy(h);
-        return GPRM_ERR_CUDA;
+        return e == cudaErrorMemoryAllocation ? GPRM_ERR_NOMEM : GPRM_ERR_CUDA;
     }
     cudaMemcpy(h->w, w.data(), off * sizeof(float), cudaMemcpyHostToDevice);
     cudaMemcpy(h->bf_map, map.data(), off * sizeof(int), cudaMemcpyHostToDevice);

@@ -61,3 +61,56 @@ def edge_workload(kind: str = "hull6", seed: int = 0, n_samples: int = 1 << 20, 
     qe = qf[j].T.contiguous()
     return dict(scene=sc, space=cs, qs=qs, qe=qe, n_free=int(free.numel()), n_samples=n_samples,
                 q_soa=q_soa, codes=codes)
+
+
+MANY = dict(problems=256, dof=(4, 7), obstacles=(8, 128), samples_log2=(14, 18), radius=(0.4, 0.8),
+            edge_sources=1024, k=10, dq=0.01)
+
+
+def batch_workload(seed: int = 0, problems: int = MANY["problems"], samples_log2=MANY["samples_log2"],
+                   radius=MANY["radius"], edge_sources: int = MANY["edge_sources"], k: int = MANY["k"],
+                   dq: float = MANY["dq"], device: str = "cuda:0"):
+    """Many independent problems (``scenes.make_mixed``: DOF 4-7, 8-128
+    obstacles), each with 2^U[lo,hi] uniform samples and a connection
+    radius U[0.4, 0.8].  Edges: the k nearest free neighbours of the first
+    ``edge_sources`` free samples of each problem, every edge longer than
+    the radius cut back to the radius along its direction (the planner
+    connects within the radius).  Returns dict(spaces, scenes, q, qs, qe
+    (7, total) float32 CUDA SoA, offs_v, offs_e (numpy), n_free)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    spaces, scs, qv, qa, qb, n_free = [], [], [], [], [], []
+    for p in range(problems):
+        sc = scenes.make_mixed(seed * 100003 + p)
+        cs = RobotConfigspace(sc, dq=dq)
+        cs.init()
+        n = int(round(2.0 ** rng.uniform(*samples_log2)))
+        r = float(rng.uniform(*radius))
+        q = scenes.uniform_configs(sc, n, seed * 7 + p)
+        qd = torch.tensor(np.ascontiguousarray(q.T), device=device)
+        codes = torch.zeros(n, dtype=torch.int32, device=device)
+        cs.check_configs_device(qd, codes)
+        free = torch.nonzero(codes == 0).squeeze(1)[:edge_sources]
+        qf = qd[:, free].T.contiguous()
+        if qf.shape[0] >= 2:
+            i, j = knn_pairs(qf, k)
+            a, b = qf[i], qf[j]
+            d = b - a
+            L = torch.linalg.vector_norm(d, dim=1, keepdim=True)
+            scale = torch.clamp(r / torch.clamp(L, min=1e-30), max=1.0)
+            b = a + d * scale
+        else:
+            a = b = qf[:0]
+        spaces.append(cs)
+        scs.append(sc)
+        qv.append(q)
+        qa.append(a.cpu().numpy())
+        qb.append(b.cpu().numpy())
+        n_free.append(int((codes == 0).sum().item()))
+    from .batch import pack_items
+    Q, offs_v = pack_items(qv)
+    A, offs_e = pack_items(qa)
+    B, _ = pack_items(qb)
+    return dict(spaces=spaces, scenes=scs, q=torch.tensor(Q, device=device), qs=torch.tensor(A, device=device),
+                qe=torch.tensor(B, device=device), offs_v=offs_v, offs_e=offs_e, n_free=n_free,
+                q_host=qv, qs_host=qa, qe_host=qb)

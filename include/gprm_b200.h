@@ -231,6 +231,53 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
 int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q, int* res, int n, int offset,
                                         void* stream);
 
+/* ---- many problems per launch (no counterpart in the reference) --------
+ * The reference holds one scene per RobotConfigspace and launches once per
+ * request (robotconfigspace.cpp:687-693).  A batch groups `count`
+ * initialised handles on one device - different robots, DOF, obstacle
+ * sets, dq - and checks the configurations or edges of all of them in one
+ * persistent launch.  Mode, edge policy and FP64 band are taken from
+ * spaces[0] at creation; every space must share its mode and band.  The
+ * batch reads the spaces' device tables: set their mode, policy and band
+ * before creating it, and destroy it before them.
+ *
+ * Item layout: problem p owns items offsets[p] .. offsets[p+1]-1 (host
+ * array of count+1 entries, offsets[0] = 0, non-decreasing, total at most
+ * INT_MAX).  Inputs are device arrays with one row per joint and row
+ * stride `stride` >= total: joint j of item i at q[i + stride*j]; problem
+ * p reads rows 0 .. ndof_p-1.  res[i] is the code gprm_indicator_batch /
+ * gprm_indicator2 would give item i on its own handle.  set_layout
+ * allocates (and synchronises); the check calls allocate nothing and never
+ * synchronise.  queue_capacity: FP64 recheck queue entries, 0 = total for
+ * configurations (cannot overflow), 4*total + 65536 for edges; an
+ * overflow is reported by gprm_batch_get_stats.  Calls on one batch share
+ * its control block: do not overlap them on different streams. */
+typedef struct gprm_batch gprm_batch;
+int  gprm_batch_create(gprm_space* const* spaces, int count, gprm_batch** out);
+void gprm_batch_destroy(gprm_batch* b);
+const char* gprm_batch_last_error(const gprm_batch* b);
+int  gprm_batch_set_layout(gprm_batch* b, int vertex_kernel, const long long* offsets,
+                           long long queue_capacity);
+int  gprm_batch_indicator_device(gprm_batch* b, const float* q, int* res, long long stride,
+                                 void* stream);
+int  gprm_batch_indicator2_device(gprm_batch* b, const float* qs, const float* qe, int* res,
+                                  long long stride, void* stream);
+/* Captures one check call (those pointers, the current launch shape) into
+ * a CUDA graph held by the batch; replay launches it on `stream` as one
+ * graph launch.  Re-capture after changing the layout or launch shape. */
+int  gprm_batch_capture(gprm_batch* b, int vertex_kernel, const float* qa, const float* qb,
+                        int* res, long long stride);
+int  gprm_batch_replay(gprm_batch* b, int vertex_kernel, void* stream);
+/* Launch shape: threads per block (32..512); blocks fill every SM. */
+int  gprm_batch_set_launch(gprm_batch* b, int vertex_kernel, int threads);
+int  gprm_batch_get_launch(const gprm_batch* b, int vertex_kernel, int* threads, int* warps_per_sm);
+/* Times every launch shape (64, 128, 256, 512 threads) on this input,
+ * `reps` runs each after one untimed run, and keeps the fastest.
+ * Synchronous; the runs' counters are discarded. */
+int  gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, const float* qb,
+                         int* res, long long stride, int reps, int* best_threads, float* best_ms);
+int  gprm_batch_get_stats(const gprm_batch* b, gprm_stats* out);
+
 /* ---- diagnostics (no counterpart in the reference) -------------------- */
 
 /* The FP32 frames the kernels compute for one configuration q[ndof]:

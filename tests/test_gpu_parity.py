@@ -208,3 +208,16 @@ def test_certificates_settle_most_pairs():
     cs.check_configs(z["q"])
     st = cs.stats()
     assert st["pairs_certified"] > 4 * st["pairs_tested"]
+
+
+def test_handles_keep_their_launch_shapes():
+    """Launch shapes are per handle: configuring a second handle with a
+    smaller shared-memory footprint must not break the first one."""
+    sc, z = load_golden("hull6")
+    a = space(sc, float(z["dq"]), mode=GPRM_MODE_FP64_BAND)
+    want = a.check_configs(z["q"])
+    a.set_launch(True, 256, True)
+    assert a.get_launch(True)["scene_in_smem"]
+    b = space(scenes.make_box4(3), 0.02, mode=GPRM_MODE_FP64_BAND)
+    b.check_configs(scenes.uniform_configs(scenes.make_box4(3), 100, 1))
+    np.testing.assert_array_equal(a.check_configs(z["q"]), want)
