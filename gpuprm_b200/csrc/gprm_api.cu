@@ -84,6 +84,8 @@ void compute_certificates(gprm_space* h, const int* from, const int* to)
     (void)from;
     (void)to;
     h->pairs_b.resize(h->npairs);
+    h->far.resize(h->npairs);
+    h->far_slot.resize(h->npairs);
     for (int j = 0; j < h->npairs; ++j) {
         int a = h->pair_poly[2 * j], b = h->pair_poly[2 * j + 1];
         bool ok = (h->pair_sys[2 * j] == 0 || h->slot[a] >= 0) && (h->pair_sys[2 * j + 1] == 0 || h->slot[b] >= 0);
@@ -98,6 +100,21 @@ void compute_certificates(gprm_space* h, const int* from, const int* to)
         memcpy(&fa, &sa, 4);
         memcpy(&fb, &sb, 4);
         h->pairs_b[j] = make_float4(Rf, T2, fa, fb);
+        /* distance-test record: the moving ball's slot first, the static
+         * partner's ball centre inline; no slot -> never certified here */
+        float4 fr = make_float4(0.0f, 0.0f, 0.0f, INFINITY);
+        int2 fs = make_int2(-1, -1);
+        if (T2 < INFINITY && (sa >= 0 || sb >= 0)) {
+            fs = sa >= 0 ? make_int2(sa, sb) : make_int2(sb, -1);
+            if (sa < 0 || sb < 0) {
+                const float4 c = h->tab[sa < 0 ? h->pairs[j].x : h->pairs[j].y];
+                fr = make_float4(c.x, c.y, c.z, T2);
+            } else {
+                fr.w = T2;
+            }
+        }
+        h->far[j] = fr;
+        h->far_slot[j] = fs;
     }
     h->thr_dir = (float)thr;
     h->eps_dir = (float)(7.0 * eps_pos);
@@ -538,12 +555,16 @@ int gprm_init(gprm_space* h, int rank, int size)
     CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
 
+    /* d_scene: tab | pairs | pairs_b | far | far_slot */
     size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
-    CUDA_TRY(h, cudaMalloc(&h->d_scene, tb + 2 * pb + 64));
+    size_t fsb = (size_t)h->npairs * sizeof(int2);
+    CUDA_TRY(h, cudaMalloc(&h->d_scene, tb + 3 * pb + fsb + 64));
     char* base = (char*)h->d_scene;
     CUDA_TRY(h, cudaMemcpy(base, h->tab.data(), tb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 2 * pb, h->far.data(), pb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 3 * pb, h->far_slot.data(), fsb, cudaMemcpyHostToDevice));
 
     DevScene& s = h->dsc;
     memset(&s, 0, sizeof(s));
@@ -563,6 +584,8 @@ int gprm_init(gprm_space* h, int rank, int size)
     s.tab = (const float4*)base;
     s.pairs = (const int4*)(base + tb);
     s.pairs_b = (const float4*)(base + tb + pb);
+    s.far = (const float4*)(base + tb + 2 * pb);
+    s.far_slot = (const int2*)(base + tb + 3 * pb);
     s.thr_dir = h->thr_dir;
     s.eps_dir = h->eps_dir;
     s.nslots = (int)h->slot_sys.size();
@@ -628,6 +651,7 @@ int gprm_set_band(gprm_space* h, float band_m)
         CUDA_TRY(h, cudaDeviceSynchronize());
         size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
         if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
+        if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + 2 * pb, h->far.data(), pb, cudaMemcpyHostToDevice));
         h->dsc.thr_dir = h->thr_dir;
         h->dsc.eps_dir = h->eps_dir;
     }

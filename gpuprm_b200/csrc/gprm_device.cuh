@@ -59,6 +59,11 @@ struct DevScene {
     const float4* tab;
     const int4* pairs;
     const float4* pairs_b;
+    /* distance test per pair: (static partner's ball centre, T2) and the
+       moving ball slot(s) (x: moving slot, y: second moving slot or -1;
+       x = -1: the pair is never settled by the distance test) */
+    const float4* far;
+    const int2* far_slot;
     /* certificates: a pair whose guaranteed separation along the first
        search direction exceeds thr_dir is reported free without the test;
        eps_dir bounds the direction error of the approximate first direction

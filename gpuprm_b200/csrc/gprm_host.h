@@ -54,6 +54,8 @@ struct gprm_space {
     std::vector<float4> tab;       /* per-polytope blocks, see gprm_device.cuh */
     std::vector<int4> pairs;
     std::vector<float4> pairs_b;   /* certificate data per pair */
+    std::vector<float4> far;       /* distance test: static ball centre, T2 */
+    std::vector<int2> far_slot;    /* distance test: moving slot(s), -1 none */
     std::vector<double> rad;       /* inflated ball radius per polytope */
     std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
     std::vector<int> slot_sys, slot_block;

@@ -42,7 +42,7 @@ namespace gprm {
 
 size_t scene_smem_bytes(const DevScene& sc)
 {
-    return (size_t)sc.ntab * 16 + (size_t)sc.npairs * 32;
+    return (size_t)sc.ntab * 16 + (size_t)sc.npairs * 56;
 }
 
 /* per warp: frames 1..ndof (12 floats each) and the ball centres of the
@@ -61,6 +61,8 @@ struct SceneView {
     const float4* tab;
     const int4* pairs;
     const float4* pairs_b;
+    const float4* far;
+    const int2* far_slot;
     float* frames;   /* this lane's frames (lane-interleaved, stride 32) */
     float* cen;      /* this lane's slot ball centres */
 };
@@ -73,25 +75,67 @@ __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned ch
     SceneView s;
     size_t off = 0;
     if (SMEM) {
+        const size_t np = (size_t)sc.npairs;
         float4* t = reinterpret_cast<float4*>(smem);
         int4* p = reinterpret_cast<int4*>(smem + (size_t)sc.ntab * 16);
-        float4* pb = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + (size_t)sc.npairs * 16);
+        float4* pb = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + np * 16);
+        float4* fr = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + np * 32);
+        int2* fs = reinterpret_cast<int2*>(smem + (size_t)sc.ntab * 16 + np * 48);
         for (int i = threadIdx.x; i < sc.ntab; i += blockDim.x) t[i] = sc.tab[i];
-        for (int i = threadIdx.x; i < sc.npairs; i += blockDim.x) { p[i] = sc.pairs[i]; pb[i] = sc.pairs_b[i]; }
+        for (int i = threadIdx.x; i < sc.npairs; i += blockDim.x) {
+            p[i] = sc.pairs[i];
+            pb[i] = sc.pairs_b[i];
+            fr[i] = sc.far[i];
+            fs[i] = sc.far_slot[i];
+        }
         s.tab = t;
         s.pairs = p;
         s.pairs_b = pb;
-        off = (size_t)sc.ntab * 16 + (size_t)sc.npairs * 32;
+        s.far = fr;
+        s.far_slot = fs;
+        off = (size_t)sc.ntab * 16 + np * 56;
     } else {
         s.tab = sc.tab;
         s.pairs = sc.pairs;
         s.pairs_b = sc.pairs_b;
+        s.far = sc.far;
+        s.far_slot = sc.far_slot;
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     s.frames = reinterpret_cast<float*>(smem + off) + (size_t)warp * lane_floats(sc) * 32 + lane;
     s.cen = s.frames + (size_t)sc.ndof * 12 * 32;
     __syncthreads();
     return s;
+}
+
+/* Distance-test scan of pairs j0 .. j0+jn-1 (jn <= 32) for this lane: bit
+ * k of the result is set when pair j0+k is NOT settled by the distance
+ * certificate (the same test as the first half of pair_certified, on the
+ * same values).  Order-free: a settled pair is free with its margin above
+ * the band, so it changes neither a code nor a band decision. */
+__device__ __forceinline__ unsigned far_scan(const SceneView& S, int j0, int jn)
+{
+    unsigned need = 0;
+#pragma unroll 4
+    for (int k = 0; k < jn; ++k) {
+        const float4 f = S.far[j0 + k];
+        const int2 fs = S.far_slot[j0 + k];
+        bool cert = false;
+        if (fs.x >= 0) {
+            const float px = S.cen[(fs.x * 3) * 32], py = S.cen[(fs.x * 3 + 1) * 32], pz = S.cen[(fs.x * 3 + 2) * 32];
+            float qx = f.x, qy = f.y, qz = f.z;
+            if (fs.y >= 0) {
+                qx = S.cen[(fs.y * 3) * 32];
+                qy = S.cen[(fs.y * 3 + 1) * 32];
+                qz = S.cen[(fs.y * 3 + 2) * 32];
+            }
+            const float dx = qx - px, dy = qy - py, dz = qz - pz;
+            const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            cert = d2 > f.w;
+        }
+        need |= (cert ? 0u : 1u) << k;
+    }
+    return need;
 }
 
 /* Per-lane counts of how pair tests were settled. */
@@ -192,15 +236,26 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
     }
     if (active) forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
     float mmin = PF32::inf(), mdec = 0.0f;
+    /* pairs in chunks of 32: the order-free distance scan, then the
+       remaining pairs of the chunk in the reference's order */
 #pragma unroll 1
-    for (int j = 0; j < sc.npairs; ++j) {
+    for (int j0 = 0; j0 < sc.npairs; j0 += 32) {
         if (!__any_sync(FULL_MASK, active)) break;
-        if (active) {
-            float m;
-            bool hm;
-            int r = eval_pair(sc, S, j, &m, &hm, pc);
-            if (r != 0) { code = r; mdec = m; active = false; }
-            else if (hm) mmin = min_nan(mmin, m);
+        const int jn = min(32, sc.npairs - j0);
+        unsigned need = far_scan(S, j0, jn);
+        if (!active) need = 0u;
+        else pc.far += (unsigned)(jn - __popc(need));
+        unsigned todo = __reduce_or_sync(FULL_MASK, need);
+        while (todo) {
+            const int k = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            if (active && ((need >> k) & 1u)) {
+                float m;
+                bool hm;
+                int r = eval_pair(sc, S, j0 + k, &m, &hm, pc);
+                if (r != 0) { code = r; mdec = m; active = false; }
+                else if (hm) mmin = min_nan(mmin, m);
+            }
         }
     }
     if (valid) {
@@ -293,25 +348,39 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         float mmin = PF32::inf(), mdec = 0.0f;
         int cut = 32;   /* lanes above the highest-priority colliding lane no longer matter */
         int jend = 0;   /* pairs processed by the warp */
+        bool stop = false;
+        /* pairs in chunks of 32: the order-free distance scan, then the
+           remaining pairs of the chunk in the reference's order; a code can
+           only change at a remaining pair, so the vote runs only there */
 #pragma unroll 1
-        for (int j = 0; j < sc.npairs; ++j) {
+        for (int j0 = 0; j0 < sc.npairs && !stop; j0 += 32) {
             if (!__any_sync(FULL_MASK, active)) break;
-            if (active) {
-                float m;
-                bool hm;
-                int rr = eval_pair(sc, S, j, &m, &hm, pc);
-                if (rr != 0) { code = rr; mdec = m; active = false; }
-                else if (hm) mmin = min_nan(mmin, m);
+            const int jn = min(32, sc.npairs - j0);
+            unsigned need = far_scan(S, j0, jn);
+            if (!active) need = 0u;
+            else pc.far += (unsigned)(jn - __popc(need));
+            unsigned todo = __reduce_or_sync(FULL_MASK, need);
+            while (todo) {
+                const int k = __ffs(todo) - 1;
+                todo &= todo - 1u;
+                if (active && ((need >> k) & 1u)) {
+                    float m;
+                    bool hm;
+                    int rr = eval_pair(sc, S, j0 + k, &m, &hm, pc);
+                    if (rr != 0) { code = rr; mdec = m; active = false; }
+                    else if (hm) mmin = min_nan(mmin, m);
+                }
+                jend = j0 + k + 1;
+                bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
+                unsigned hits = __ballot_sync(FULL_MASK, oobj);
+                if (hits) {
+                    int Lj = __ffs(hits) - 1;
+                    if (Lj < cut) cut = Lj;
+                    if (POLICY == EDGE_EARLY_EXIT) { stop = true; break; }
+                    if (lane > cut) active = false;
+                }
             }
-            jend = j + 1;
-            bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
-            unsigned hits = __ballot_sync(FULL_MASK, oobj);
-            if (hits) {
-                int Lj = __ffs(hits) - 1;
-                if (Lj < cut) cut = Lj;
-                if (POLICY == EDGE_EARLY_EXIT) break;
-                if (lane > cut) active = false;
-            }
+            if (!stop) jend = j0 + jn;
         }
         /* settle the round */
         const bool oob = code != 0 && !(band_on && in_band(code, mdec, band));
@@ -613,6 +682,8 @@ __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene
     S.tab = wsc->tab;
     S.pairs = wsc->pairs;
     S.pairs_b = wsc->pairs_b;
+    S.far = wsc->far;
+    S.far_slot = wsc->far_slot;
     S.frames = frames;
     S.cen = frames + (size_t)wsc->ndof * 12 * 32;
 }
