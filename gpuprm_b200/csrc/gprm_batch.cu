@@ -191,7 +191,7 @@ int gprm_batch_create(gprm_space* const* spaces, int count, gprm_batch** out)
     std::vector<DevScene> sc(count);
     for (int i = 0; i < count; ++i) {
         sc[i] = spaces[i]->dsc;
-        int lf = sc[i].ndof * 12 + sc[i].nslots * 3;
+        int lf = (int)lane_floats(sc[i]);
         if (lf > b->lane_floats) b->lane_floats = lf;
     }
     auto bad = [&](int rc) {

@@ -69,6 +69,17 @@ cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const
                                  const float* qe, long long offset, int policy, int* res, unsigned* key,
                                  const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
 
+/* Per-lane shared floats of a warp's block: frames 1..ndof (12 floats
+ * each), the ball centres of the slots (3 floats each), lane-interleaved,
+ * then SWEEP_LANE_FLOATS per lane that together hold the warp's per-slot
+ * sweep balls (GPRM_MAX_SLOTS float4). */
+#define SWEEP_LANE_FLOATS 2
+static_assert(SWEEP_LANE_FLOATS * 32 >= GPRM_MAX_SLOTS * 4, "sweep area too small");
+__host__ __device__ __forceinline__ size_t lane_floats(const DevScene& sc)
+{
+    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 3 + SWEEP_LANE_FLOATS;
+}
+
 /* Scene bytes when staged in shared memory; per-lane frame bytes of a block. */
 size_t scene_smem_bytes(const DevScene& sc);
 size_t frame_smem_bytes(const DevScene& sc, int threads);

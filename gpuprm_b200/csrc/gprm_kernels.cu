@@ -42,14 +42,8 @@ namespace gprm {
 
 size_t scene_smem_bytes(const DevScene& sc)
 {
-    return (size_t)sc.ntab * 16 + (size_t)sc.npairs * 56;
-}
-
-/* per warp: frames 1..ndof (12 floats each) and the ball centres of the
- * slots (3 floats each), lane-interleaved */
-__host__ __device__ __forceinline__ size_t lane_floats(const DevScene& sc)
-{
-    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 3;
+    /* tab | pairs | pairs_b | far | far_slot, padded to 16 bytes */
+    return ((size_t)sc.ntab * 16 + (size_t)sc.npairs * 56 + 15) & ~(size_t)15;
 }
 
 size_t frame_smem_bytes(const DevScene& sc, int threads)
@@ -65,7 +59,15 @@ struct SceneView {
     const int2* far_slot;
     float* frames;   /* this lane's frames (lane-interleaved, stride 32) */
     float* cen;      /* this lane's slot ball centres */
+    float4* sweep;   /* the warp's per-slot sweep balls (GPRM_MAX_SLOTS) */
 };
+
+/* The warp's sweep area: the last SWEEP_LANE_FLOATS entries of its block. */
+__device__ __forceinline__ float4* sweep_area(const DevScene& sc, float* lane_frames)
+{
+    const int lane = threadIdx.x & 31;
+    return reinterpret_cast<float4*>(lane_frames - lane + (lane_floats(sc) - SWEEP_LANE_FLOATS) * 32);
+}
 
 /* Copies the scene into shared memory (SMEM) and returns the pointers the
  * warp uses, including its lane's slice of the frame array. */
@@ -93,7 +95,7 @@ __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned ch
         s.pairs_b = pb;
         s.far = fr;
         s.far_slot = fs;
-        off = (size_t)sc.ntab * 16 + np * 56;
+        off = ((size_t)sc.ntab * 16 + np * 56 + 15) & ~(size_t)15;   /* frames stay 16-byte aligned */
     } else {
         s.tab = sc.tab;
         s.pairs = sc.pairs;
@@ -104,6 +106,7 @@ __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned ch
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     s.frames = reinterpret_cast<float*>(smem + off) + (size_t)warp * lane_floats(sc) * 32 + lane;
     s.cen = s.frames + (size_t)sc.ndof * 12 * 32;
+    s.sweep = sweep_area(sc, s.frames);
     __syncthreads();
     return s;
 }
@@ -118,6 +121,90 @@ __device__ __forceinline__ unsigned far_scan(const SceneView& S, int j0, int jn)
     unsigned need = 0;
 #pragma unroll 4
     for (int k = 0; k < jn; ++k) {
+        const float4 f = S.far[j0 + k];
+        const int2 fs = S.far_slot[j0 + k];
+        bool cert = false;
+        if (fs.x >= 0) {
+            const float px = S.cen[(fs.x * 3) * 32], py = S.cen[(fs.x * 3 + 1) * 32], pz = S.cen[(fs.x * 3 + 2) * 32];
+            float qx = f.x, qy = f.y, qz = f.z;
+            if (fs.y >= 0) {
+                qx = S.cen[(fs.y * 3) * 32];
+                qy = S.cen[(fs.y * 3 + 1) * 32];
+                qz = S.cen[(fs.y * 3 + 2) * 32];
+            }
+            const float dx = qx - px, dy = qy - py, dz = qz - pz;
+            const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            cert = d2 > f.w;
+        }
+        need |= (cert ? 0u : 1u) << k;
+    }
+    return need;
+}
+
+/* Per slot, a ball holding that slot's ball centre in every lane of `mask`
+ * (lanes whose frames are current): centre m = the midpoint of the lanes'
+ * bounding box, radius rho >= max |c_lane - m| (the box half-diagonal from
+ * m, rounded up).  Lanes with a non-finite centre make rho infinite, which
+ * disables the sweep test for the slot.  One lane per slot. */
+__device__ __forceinline__ void sweep_bounds(const DevScene& sc, const SceneView& S, unsigned mask)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();   /* the lanes' centres are written */
+    if (lane < sc.nslots) {
+        const float* c0 = S.cen - lane;   /* lane 0's centres; lane i at +i */
+        float lo[3], hi[3];
+        bool bad = false;
+        for (int c = 0; c < 3; ++c) { lo[c] = PF32::inf(); hi[c] = -PF32::inf(); }
+        for (unsigned m = mask; m; m &= m - 1u) {
+            const int i = __ffs(m) - 1;
+            for (int c = 0; c < 3; ++c) {
+                const float v = c0[(lane * 3 + c) * 32 + i];
+                bad |= !isfinite(v);
+                lo[c] = fminf(lo[c], v);
+                hi[c] = fmaxf(hi[c], v);
+            }
+        }
+        float mc[3], e2 = 0.0f;
+        for (int c = 0; c < 3; ++c) {
+            mc[c] = 0.5f * (lo[c] + hi[c]);
+            const float e = fmaxf(hi[c] - mc[c], mc[c] - lo[c]);
+            e2 = __fmaf_rn(e, e, e2);
+        }
+        float rho = __fsqrt_ru(e2) * (1.0f + 4e-6f) + 1e-30f;
+        if (bad || !mask || !isfinite(rho)) rho = PF32::inf();
+        S.sweep[lane] = make_float4(mc[0], mc[1], mc[2], rho);
+    }
+    __syncwarp();
+}
+
+/* far_scan for a warp whose lanes hold nearby configurations: lane k first
+ * tests pair j0+k against the sweep ball of its moving slot; a pair whose
+ * static partner lies farther than rho + sqrt(T2) from the sweep centre is
+ * settled for every lane at once (each lane's exact distance then exceeds
+ * sqrt(T2), the per-lane test's threshold).  The other pairs get the
+ * per-lane test of far_scan. */
+__device__ __forceinline__ unsigned far_scan_swept(const SceneView& S, int j0, int jn)
+{
+    const int lane = threadIdx.x & 31;
+    bool maybe = false;
+    if (lane < jn) {
+        maybe = true;
+        const int2 fs = S.far_slot[j0 + lane];
+        if (fs.x >= 0 && fs.y < 0) {
+            const float4 f = S.far[j0 + lane];
+            const float4 b = S.sweep[fs.x];
+            const float dx = f.x - b.x, dy = f.y - b.y, dz = f.z - b.z;
+            const float dd2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+            const float A = (__fsqrt_ru(f.w) + b.w) * (1.0f + 1e-6f);
+            /* |m - c|^2 >= dd2 (1 - 1e-6) > A^2 >= (rho + sqrt(T2))^2 */
+            if (dd2 * (1.0f - 1e-6f) > A * A) maybe = false;
+        }
+    }
+    unsigned cand = __ballot_sync(FULL_MASK, maybe);
+    unsigned need = 0;
+    while (cand) {
+        const int k = __ffs(cand) - 1;
+        cand &= cand - 1u;
         const float4 f = S.far[j0 + k];
         const int2 fs = S.far_slot[j0 + k];
         bool cert = false;
@@ -343,6 +430,7 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         }
         const unsigned valid_mask = __ballot_sync(FULL_MASK, valid);
         if (lane == 0) exec += __popc(valid_mask);
+        sweep_bounds(sc, S, valid_mask);
         bool active = valid;
         int code = 0;
         float mmin = PF32::inf(), mdec = 0.0f;
@@ -356,7 +444,7 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         for (int j0 = 0; j0 < sc.npairs && !stop; j0 += 32) {
             if (!__any_sync(FULL_MASK, active)) break;
             const int jn = min(32, sc.npairs - j0);
-            unsigned need = far_scan(S, j0, jn);
+            unsigned need = far_scan_swept(S, j0, jn);
             if (!active) need = 0u;
             else pc.far += (unsigned)(jn - __popc(need));
             unsigned todo = __reduce_or_sync(FULL_MASK, need);
@@ -686,6 +774,7 @@ __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene
     S.far_slot = wsc->far_slot;
     S.frames = frames;
     S.cen = frames + (size_t)wsc->ndof * 12 * 32;
+    S.sweep = sweep_area(*wsc, frames);
 }
 
 __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __restrict__ q, long long offset,
