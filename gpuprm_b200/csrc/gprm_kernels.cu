@@ -914,16 +914,17 @@ cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const
 /* Adds a request's counters to the handle's running totals. */
 __global__ void k_accumulate(const Control* c, Control* total)
 {
-    total->steps_nominal += c->steps_nominal;
-    total->steps_exec += c->steps_exec;
-    total->band_checks += c->band_checks;
-    total->band_flips += c->band_flips;
-    total->configs_exec += c->configs_exec;
-    total->cert_far += c->cert_far;
-    total->cert_dir += c->cert_dir;
-    total->full_tests += c->full_tests;
-    total->flags |= c->flags;
-    total->next += 1;  /* requests completed */
+    /* atomics: requests on different streams accumulate concurrently */
+    atomicAdd(&total->steps_nominal, c->steps_nominal);
+    atomicAdd(&total->steps_exec, c->steps_exec);
+    atomicAdd(&total->band_checks, c->band_checks);
+    atomicAdd(&total->band_flips, c->band_flips);
+    atomicAdd(&total->configs_exec, c->configs_exec);
+    atomicAdd(&total->cert_far, c->cert_far);
+    atomicAdd(&total->cert_dir, c->cert_dir);
+    atomicAdd(&total->full_tests, c->full_tests);
+    atomicOr(&total->flags, c->flags);
+    atomicAdd(&total->next, 1ull);  /* requests completed */
 }
 
 cudaError_t launch_accumulate(const Control* c, Control* total, cudaStream_t st)

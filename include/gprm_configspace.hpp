@@ -33,49 +33,49 @@ public:
     /* RobotConfigspace(path, dq, nbuf) (robotconfigspace.cpp:84-98) */
     B200RobotConfigspace(const std::string& path, float dq, int nbuf) : h_(nullptr)
     {
-        check(gprm_create_from_dir(path.c_str(), ndof, dq, nbuf, &h_), nullptr);
+        throw_on_error(gprm_create_from_dir(path.c_str(), ndof, dq, nbuf, &h_), nullptr);
     }
     /* RobotConfigspace(robot, polys, ...) (robotconfigspace.cpp:75-82) */
     B200RobotConfigspace(const gprm_scene_desc& desc, float dq, int nbuf) : h_(nullptr)
     {
-        check(gprm_create(&desc, dq, nbuf, &h_), nullptr);
+        throw_on_error(gprm_create(&desc, dq, nbuf, &h_), nullptr);
     }
     ~B200RobotConfigspace() { gprm_destroy(h_); }
     B200RobotConfigspace(const B200RobotConfigspace&) = delete;
     B200RobotConfigspace& operator=(const B200RobotConfigspace&) = delete;
 
-    int init(const int rank = 0, const int size = 1) { return check(gprm_init(h_, rank, size)); }
+    int init(const int rank = 0, const int size = 1) { return throw_on_error(gprm_init(h_, rank, size)); }
 
     int indicator(const float* q, int* res, const int N, const int offset)
     {
-        return check(gprm_indicator_batch(h_, q, res, N, offset));
+        return throw_on_error(gprm_indicator_batch(h_, q, res, N, offset));
     }
     int indicator(const float* q)
     {
         int code = 0;
-        check(gprm_indicator(h_, q, &code));
+        throw_on_error(gprm_indicator(h_, q, &code));
         return code;
     }
     int indicator2(const float* qs, const float* qe, int* res, const int N, const int offset)
     {
-        return check(gprm_indicator2(h_, qs, qe, res, N, offset));
+        return throw_on_error(gprm_indicator2(h_, qs, qe, res, N, offset));
     }
     int indicator2_async(const float* qs, const float* qe, int* res, const int N, const int offset, int& request)
     {
-        return check(gprm_indicator2_async(h_, qs, qe, res, N, offset, &request));
+        return throw_on_error(gprm_indicator2_async(h_, qs, qe, res, N, offset, &request));
     }
-    int indicator2_async_wait(int request) { return check(gprm_indicator2_wait(h_, request)); }
+    int indicator2_async_wait(int request) { return throw_on_error(gprm_indicator2_wait(h_, request)); }
     /* the compressed form is declared but unimplemented in the reference
        too (robotconfigspace.cpp:765-772) */
     int indicator2(const float*, const int, const float*, int*, const int*, const int*, const int) { return -1; }
     int check_boundaries(const float* q, int* res, const int N, const int offset)
     {
-        return check(gprm_check_boundaries(h_, q, res, N, offset));
+        return throw_on_error(gprm_check_boundaries(h_, q, res, N, offset));
     }
     int check_boundaries(const float* q)
     {
         int out = 0;
-        check(gprm_check_boundaries1(h_, q, &out));
+        throw_on_error(gprm_check_boundaries1(h_, q, &out));
         return out;
     }
     float min(int i) { return gprm_min(h_, i); }
@@ -86,8 +86,8 @@ public:
     gprm_space* handle() { return h_; }
 
 private:
-    int check(int rc) { return check(rc, h_); }
-    static int check(int rc, gprm_space* h)
+    int throw_on_error(int rc) { return throw_on_error(rc, h_); }
+    static int throw_on_error(int rc, gprm_space* h)
     {
         if (rc != GPRM_OK) throw std::runtime_error(std::string("gprm: ") + gprm_last_error(h));
         return 0;

@@ -1,0 +1,50 @@
+"""GPUPRM's own planner with the B200 checker dropped in.
+
+oracle/_ref/prm_dropin compiles the reference's PRMSolver (prmsolver.cpp,
+unmodified, single-rank MPI stand-in) and runs it on the reference scene
+with either checker behind Configspace<4>.  The reference run's stored
+roadmap (store_results, prmsolver.cpp:2947-3055) is pinned in
+tests/golden/prm_dropin_config1.json by make_prm_golden.py.  With the B200
+checker in FP32 mode the planner must draw the same random numbers and
+store byte-identical results: every verdict it asked for was the same.
+"""
+import json
+import os
+import sys
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import make_prm_golden as G  # noqa: E402
+
+FIX = json.load(open(G.FIXTURE))
+needs_bin = pytest.mark.skipif(not os.path.exists(G.BIN), reason="oracle/_ref/prm_dropin not built")
+
+
+def test_fixture_is_complete():
+    assert FIX["counters"]["num_nodes"] > 0
+    assert FIX["files"]["connection.bin"] == "01"          # the planner connected start and goal
+    for g in ("graphl", "graphr"):
+        for f in ("qstorage.bin", "edgesfrom.bin", "edgesto.bin", "edgesweight.bin", "path.bin", "pathc.bin"):
+            assert f"{g}/{f}" in FIX["files"]
+
+
+@needs_bin
+@pytest.mark.skipif(not os.path.isdir("/root/reference/prm"), reason="reference tree absent")
+def test_reference_run_reproduces_fixture(tmp_path):
+    line, files = G.run_planner("ref", str(tmp_path))
+    assert files == FIX["files"]
+    for k, v in FIX["counters"].items():
+        assert line[k] == v, k
+
+
+@needs_bin
+@pytest.mark.gpu
+def test_b200_checker_builds_the_same_roadmap(tmp_path):
+    line, files = G.run_planner("b200", str(tmp_path), ["--mode", "fp32"])
+    print("reference checker plan s:", FIX["reference_plan_seconds"], " B200 checker plan s:", line["plan_seconds"])
+    for k, v in FIX["counters"].items():
+        assert line[k] == v, k
+    assert files == FIX["files"]
