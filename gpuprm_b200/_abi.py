@@ -153,6 +153,15 @@ SIGNATURES = [
     ("gprm_batch_autotune", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                                       _I, _F]),
     ("gprm_batch_get_stats", C.c_int, [_P, C.POINTER(Stats)]),
+    ("gprm_nbr_create", C.c_int, [C.c_int, C.POINTER(_P)]),
+    ("gprm_nbr_destroy", None, [_P]),
+    ("gprm_nbr_last_error", C.c_char_p, [_P]),
+    ("gprm_nbr_build", C.c_int, [_P, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    ("gprm_nbr_radius", C.c_int, [_P, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+    ("gprm_nbr_knn", C.c_int, [_P, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                               C.c_void_p]),
+    ("gprm_nbr_redo_count", C.c_int, [_P, _I]),
 ]
 
 _lib = None

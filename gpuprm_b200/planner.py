@@ -40,6 +40,7 @@ import numpy as np
 
 from . import scenes, workloads
 from ._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT
+from .neighbours import NeighbourIndex
 
 
 @dataclass
@@ -129,7 +130,9 @@ def _answer_queries(cs, verts, comp, parent, starts, goals, k):
     gl = torch.as_tensor(goals, device=verts.device)
     ends = torch.cat([st, gl])
     kk = min(k, verts.shape[0])
-    nb = torch.topk(torch.cdist(ends, verts), kk, dim=1, largest=False).indices
+    index = NeighbourIndex(verts.shape[1])
+    index.build(verts.T.contiguous())
+    nb = index.knn(kk, q=ends.T.contiguous())[0].long()
     qa = ends[:, None, :].expand(-1, kk, -1).reshape(-1, ends.shape[1])
     res = _check_edges(cs, qa, verts[nb.reshape(-1)]).reshape(2 * Q, kk)
     ok = (res == 0).cpu().numpy()

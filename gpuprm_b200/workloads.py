@@ -4,8 +4,8 @@
 uniform samples in the joint box, the vertex check on the GPU, then the k
 nearest free neighbours of every free sample (L2 in configuration space,
 the metric the reference's planner connects by, prmsolver.cpp:2533-2574),
-each undirected edge once.  The neighbour search runs on the GPU through
-torch (chunked distance matrix + top-k); it prepares inputs and is not part
+each undirected edge once.  The neighbour search runs on the GPU in the
+library's own kNN kernel (gprm_nbr_knn); it prepares inputs and is not part
 of any timed region.
 """
 from __future__ import annotations
@@ -18,28 +18,12 @@ from .configspace import RobotConfigspace
 HEADLINE = dict(kind="hull6", seed=0, n_samples=1 << 20, k=10, dq=0.01)
 
 
-def knn_pairs(q, k: int, chunk: int = 2048):
+def knn_pairs(q, k: int):
     """Undirected k-nearest-neighbour pairs (i < j) of the rows of q, a
-    (n, d) float32 CUDA tensor.  Returns two int64 CUDA tensors."""
-    import torch
-    n = q.shape[0]
-    sq = (q * q).sum(1)
-    out_i, out_j = [], []
-    for s in range(0, n, chunk):
-        e = min(n, s + chunk)
-        d2 = sq[s:e, None] + sq[None, :] - 2.0 * (q[s:e] @ q.T)
-        d2[torch.arange(e - s, device=q.device), torch.arange(s, e, device=q.device)] = float("inf")
-        kk = min(k, n - 1)
-        idx = torch.topk(d2, kk, dim=1, largest=False).indices
-        rows = torch.arange(s, e, device=q.device)[:, None].expand(-1, kk)
-        out_i.append(rows.reshape(-1))
-        out_j.append(idx.reshape(-1))
-    i = torch.cat(out_i)
-    j = torch.cat(out_j)
-    a = torch.minimum(i, j)
-    b = torch.maximum(i, j)
-    key = torch.unique(a * n + b)
-    return key // n, key % n
+    (n, d) float32 CUDA tensor, by the library's exact grid kNN kernel
+    (gprm_nbr_knn).  Returns two int64 CUDA tensors."""
+    from .neighbours import knn_pairs as _knn
+    return _knn(q.T.contiguous(), k)
 
 
 def edge_workload(kind: str = "hull6", seed: int = 0, n_samples: int = 1 << 20, k: int = 10,

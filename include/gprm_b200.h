@@ -278,6 +278,35 @@ int  gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, cons
                          int* res, long long stride, int reps, int* best_threads, float* best_ms);
 int  gprm_batch_get_stats(const gprm_batch* b, gprm_stats* out);
 
+/* ---- neighbour search on the device -------------------------------------
+ * get_near_vertices (prmsolver.cpp:2533-2574) keeps the nodes whose squared
+ * distance, accumulated over the joints in order in float, is below D*D.
+ * A gprm_nbr indexes n device nodes x[i + stride*j] (the array must stay
+ * valid and unchanged until the next build); queries are device arrays
+ * q[t + qstride*j].  build synchronises its stream (it reads the nodes'
+ * extent); radius and knn never synchronise.
+ *   radius: counts[t] <= cap neighbours of query t in ascending node index,
+ *           idx/dist[t*cap + r] (the first cap in index order, like the
+ *           reference's full buffer);
+ *   knn:    the k <= 32 nearest nodes by the same distance, ties by lower
+ *           index, idx/dist[t*k + r] in ascending order (-1 / inf where
+ *           fewer exist); queries_are_nodes = 1 queries every node against
+ *           the others (q, m, qstride ignored).
+ * `cell` is the grid cell edge used by knn (0: chosen from the extent so
+ * that a cell holds about the 16-neighbour radius). */
+typedef struct gprm_nbr gprm_nbr;
+int  gprm_nbr_create(int ndof, gprm_nbr** out);
+void gprm_nbr_destroy(gprm_nbr* h);
+const char* gprm_nbr_last_error(const gprm_nbr* h);
+int  gprm_nbr_build(gprm_nbr* h, const float* x, int n, int stride, float cell, void* stream);
+int  gprm_nbr_radius(gprm_nbr* h, const float* q, int m, int qstride, float D, int cap, int* counts,
+                     int* idx, float* dist, void* stream);
+int  gprm_nbr_knn(gprm_nbr* h, const float* q, int m, int qstride, int k, int queries_are_nodes,
+                  int* idx, float* dist, void* stream);
+/* queries of the last knn call that the grid could not settle and a full
+ * scan answered (synchronises) */
+int  gprm_nbr_redo_count(gprm_nbr* h, int* out);
+
 /* ---- diagnostics (no counterpart in the reference) -------------------- */
 
 /* The FP32 frames the kernels compute for one configuration q[ndof]:

@@ -1,0 +1,76 @@
+/*
+ * nbr_ref_probe.cpp - C ABI over the reference planner's own radius search,
+ * PRMSolver<ndof>::get_near_vertices (prm/src/lib/prm/prmsolver.cpp:
+ * 2533-2574), compiled from the reference sources.
+ *
+ * TEST INFRASTRUCTURE ONLY: pins oracle/nbr_oracle.py.  The nodes are
+ * inserted into the solver's left graph with its own insert()
+ * (prmsolver.cpp:2408-2469, key blocks of width H over joint 0); a query
+ * returns the neighbours within D in the solver's block order, mapped back
+ * to the caller's node indices.  The members are private in the reference
+ * header, so this translation unit opens them.
+ */
+#include <mpi.h>
+
+/* standard headers first, so that only the planner's classes are opened */
+#include <assert.h>
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <queue>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#define private public
+#define protected public
+#include "prm/prmsolver.cpp"
+#undef private
+#undef protected
+
+template class PRMSolver<6>;
+
+template <int ndof>
+static int near_impl(const float* x, int n, const float* q, int m, float D, float H, int nbuf, int* counts,
+                     int* idx, float* dist)
+{
+    PRMSolver<ndof>* s = new PRMSolver<ndof>(nullptr, H, D, n + 1024, 256);
+    std::vector<int> node_of(n + 1024 * 256, -1);
+    for (int i = 0; i < n; ++i) {
+        float v[ndof];
+        for (int j = 0; j < ndof; ++j) v[j] = x[(size_t)i * ndof + j];
+        int pos = s->insert(v, 1, s->graphl);
+        if (pos < 0 || pos >= (int)node_of.size()) { delete s; return -1; }
+        node_of[pos] = i;
+    }
+    std::vector<float> qlist((size_t)ndof * nbuf);
+    std::vector<int> posq(nbuf);
+    std::vector<float> dl(nbuf);
+    for (int t = 0; t < m; ++t) {
+        int w = s->get_near_vertices(&q[(size_t)t * ndof], 1, qlist.data(), posq.data(), dl.data(), nbuf, nbuf,
+                                     s->graphl);
+        counts[t] = w;
+        for (int r = 0; r < w; ++r) {
+            idx[(size_t)t * nbuf + r] = node_of[posq[r]];
+            dist[(size_t)t * nbuf + r] = dl[r];
+        }
+    }
+    delete s;
+    return 0;
+}
+
+/* x: (n, ndof) and q: (m, ndof) row-major; outputs (m, nbuf). */
+extern "C" int ref_near_vertices(int ndof, const float* x, int n, const float* q, int m, float D, float H, int nbuf,
+                                 int* counts, int* idx, float* dist)
+{
+    if (ndof == 4) return near_impl<4>(x, n, q, m, D, H, nbuf, counts, idx, dist);
+    if (ndof == 6) return near_impl<6>(x, n, q, m, D, H, nbuf, counts, idx, dist);
+    return -2;
+}
