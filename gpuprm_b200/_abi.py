@@ -162,6 +162,19 @@ SIGNATURES = [
     ("gprm_nbr_knn", C.c_int, [_P, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                C.c_void_p]),
     ("gprm_nbr_redo_count", C.c_int, [_P, _I]),
+    ("gprm_graph_create", C.c_int, [C.POINTER(_P)]),
+    ("gprm_graph_destroy", None, [_P]),
+    ("gprm_graph_last_error", C.c_char_p, [_P]),
+    ("gprm_graph_components", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    ("gprm_graph_forest", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, _I, C.c_void_p]),
+    ("gprm_graph_path_lengths", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gprm_graph_path_write", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("gprm_graph_sssp", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                  C.c_void_p, C.c_void_p, _I, C.c_void_p]),
 ]
 
 _lib = None

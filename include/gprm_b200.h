@@ -307,6 +307,48 @@ int  gprm_nbr_knn(gprm_nbr* h, const float* q, int m, int qstride, int k, int qu
  * scan answered (synchronises) */
 int  gprm_nbr_redo_count(gprm_nbr* h, int* out);
 
+/* ---- roadmap graphs on the device ----------------------------------------
+ * The reference keeps roadmaps as host adjacency lists and runs Dijkstra
+ * once start and goal connect (do_dijkstra, prmsolver.cpp:2805-2846).  Here a
+ * roadmap is an undirected edge list in device memory: eu[e], ev[e] in
+ * 0..V-1, an optional mask (nonzero = usable edge, NULL = all) and, for
+ * shortest paths, float weights w[e] >= 0.  All pointers are device
+ * pointers; calls run on `stream`.
+ *   components: label[i] = smallest vertex of i's component (asynchronous);
+ *   forest:     breadth-first forest from each component's label vertex:
+ *               parent[i] (-1 at roots and unreached), depth[i] (INT_MAX when
+ *               unreached); the parent is the smallest vertex of the
+ *               previous level adjacent to i.  Synchronises every 16 levels;
+ *               *levels (may be NULL) gets the number of levels run;
+ *   path_lengths / path_write: the forest path from qs[t] to qt[t]
+ *               (vertex ids, both ends included) when they share a
+ *               component, else length 0; write it at out[offsets[t]..]
+ *               with offsets the caller's exclusive prefix sum of len
+ *               (path_write only follows queries path_lengths measured);
+ * Edges or query vertices outside 0..V-1 are skipped (length 0).
+ *   sssp:       distances from src under float path sums accumulated from
+ *               the source (those of Dijkstra with the same arithmetic),
+ *               dist = inf where unreachable; parent[v] = the smallest u with
+ *               dist[u] + w == dist[v] (parent[src] = src, -1 unreached).
+ *               Synchronises every 8 relaxation rounds. */
+typedef struct gprm_graph gprm_graph;
+int  gprm_graph_create(gprm_graph** out);
+void gprm_graph_destroy(gprm_graph* h);
+const char* gprm_graph_last_error(const gprm_graph* h);
+int  gprm_graph_components(gprm_graph* h, int V, int E, const int* eu, const int* ev,
+                           const unsigned char* mask, int* label, void* stream);
+int  gprm_graph_forest(gprm_graph* h, int V, int E, const int* eu, const int* ev,
+                       const unsigned char* mask, const int* label, int* parent, int* depth,
+                       int* levels, void* stream);
+int  gprm_graph_path_lengths(gprm_graph* h, int V, int Q, const int* qs, const int* qt, const int* label,
+                             const int* parent, const int* depth, int* len, void* stream);
+int  gprm_graph_path_write(gprm_graph* h, int Q, const int* qs, const int* qt, const int* parent,
+                           const int* depth, const int* len, const long long* offsets, int* out,
+                           void* stream);
+int  gprm_graph_sssp(gprm_graph* h, int V, int E, const int* eu, const int* ev,
+                     const unsigned char* mask, const float* w, int src, float* dist, int* parent,
+                     int* rounds, void* stream);
+
 /* ---- diagnostics (no counterpart in the reference) -------------------- */
 
 /* The FP32 frames the kernels compute for one configuration q[ndof]:

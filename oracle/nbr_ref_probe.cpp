@@ -41,7 +41,7 @@ template <int ndof>
 static int near_impl(const float* x, int n, const float* q, int m, float D, float H, int nbuf, int* counts,
                      int* idx, float* dist)
 {
-    PRMSolver<ndof>* s = new PRMSolver<ndof>(nullptr, H, D, n + 1024, 256);
+    PRMSolver<ndof>* s = new PRMSolver<ndof>(nullptr, H, D, n + 256 * 64, 256);
     std::vector<int> node_of(n + 1024 * 256, -1);
     for (int i = 0; i < n; ++i) {
         float v[ndof];
@@ -73,4 +73,55 @@ extern "C" int ref_near_vertices(int ndof, const float* x, int n, const float* q
     if (ndof == 4) return near_impl<4>(x, n, q, m, D, H, nbuf, counts, idx, dist);
     if (ndof == 6) return near_impl<6>(x, n, q, m, D, H, nbuf, counts, idx, dist);
     return -2;
+}
+
+/* do_dijkstra (prmsolver.cpp:2805-2846) on a graph of n nodes x (n, ndof)
+ * and m undirected edges (eu[e], ev[e], weight w[e]), entered the way
+ * processing_step_part3a stores them (prmsolver.cpp:2111-2126: both
+ * directions, in edge order).  Writes the path (node indices, goal first, as
+ * the reference builds it) and returns its length, 0 when there is none,
+ * <0 on error; *dist_to gets the goal's distance. */
+template <int ndof>
+static int dijkstra_impl(const float* x, int n, const int* eu, const int* ev, const float* w, int m, int from,
+                         int to, int* path, int path_cap, float* dist_to)
+{
+    PRMSolver<ndof>* s = new PRMSolver<ndof>(nullptr, 1.0f, 1.0f, n + 256 * 64, 256);
+    auto& g = s->graphl;   /* its type is private to the class: name it through the member */
+    g.edgelists.resize(n + 256 * 1024);
+    g.edgeweights.resize(n + 256 * 1024);
+    std::vector<int> pos_of(n), node_of(n + 256 * 1024, -1);
+    for (int i = 0; i < n; ++i) {
+        float v[ndof];
+        for (int j = 0; j < ndof; ++j) v[j] = x[(size_t)i * ndof + j];
+        int p = s->insert(v, 1, g);
+        if (p < 0 || p >= (int)node_of.size()) { delete s; return -1; }
+        pos_of[i] = p;
+        node_of[p] = i;
+    }
+    for (int e = 0; e < m; ++e) {
+        const int a = pos_of[eu[e]], b = pos_of[ev[e]];
+        g.edgelists[a].push_back(b);
+        g.edgeweights[a].push_back(w[e]);
+        g.edgelists[b].push_back(a);
+        g.edgeweights[b].push_back(w[e]);
+    }
+    decltype(s->dijkstral) d;
+    const int found = s->do_dijkstra(g, d, pos_of[from], pos_of[to]);
+    int len = 0;
+    if (found) {
+        len = (int)d.path.size();
+        if (len > path_cap) { delete s; return -2; }
+        for (int k = 0; k < len; ++k) path[k] = node_of[d.path[k]];
+        *dist_to = d.dist[pos_of[to]];
+    }
+    delete s;
+    return len;
+}
+
+extern "C" int ref_dijkstra(int ndof, const float* x, int n, const int* eu, const int* ev, const float* w, int m,
+                            int from, int to, int* path, int path_cap, float* dist_to)
+{
+    if (ndof == 4) return dijkstra_impl<4>(x, n, eu, ev, w, m, from, to, path, path_cap, dist_to);
+    if (ndof == 6) return dijkstra_impl<6>(x, n, eu, ev, w, m, from, to, path, path_cap, dist_to);
+    return -3;
 }
