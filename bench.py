@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--policy", default="early", choices=["early", "all"])
     ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
     ap.add_argument("--prm-samples", type=int, default=1 << 16)
+    ap.add_argument("--no-stress", action="store_true", help="skip the 7-DOF wall planner comparison")
+    ap.add_argument("--stress-samples", type=int, default=1 << 17)
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
     ap.add_argument("--batch-problems", type=int, default=256)
     return ap.parse_args()
@@ -292,20 +294,11 @@ def run_ours(args, rank, world, local_rank):
                 "ref_flops_per_step": work["ref_flops_per_step"],
                 "kernel_ms": k_ms, "pairs_certified_frac": cert_pl / max(1.0, cert_pl + full_pl),
                 "fp64_recheck_ms_per_launch": prof["fp64_ms"] / max(1, prof["fp32_launches"])}
-    prm = None
+    prm = prm_stress = None
     if not args.no_prm and world == 1:
-        from gpuprm_b200 import planner, scenes as _sc
-        psc = _sc.make_scene("hull6", args.seed)
-        from gpuprm_b200.configspace import RobotConfigspace as _RC
-        pcs = _RC(psc, dq=WORKLOAD["dq"])
-        pcs.init()
-        pcs.set_mode(GPRM_MODE_FP64_BAND)
-        mlp, losses, t_lab, t_train = planner.train_predictor(pcs, psc, n_labels=1 << 20, epochs=10, batch=4096,
-                                                              lr=1e-3, seed=args.seed)
-        prm = planner.compare_planners(pcs, psc, n_samples=args.prm_samples, n_queries=1000, k=10, seed=args.seed,
-                                       mlp=mlp, repeats=3)
-        prm["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
-                            "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
+        prm = prm_leg(args, "hull6", WORKLOAD["dq"], args.prm_samples, 10)
+        if not args.no_stress:
+            prm_stress = prm_leg(args, "wall7", 0.005, args.stress_samples, 16)
     batch = None
     if not args.no_batch and world == 1:
         batch = batch_leg(args, dev, policy)
@@ -322,9 +315,30 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-        "prm": prm, "batch": batch,
+        "prm": prm, "prm_stress": prm_stress, "batch": batch,
     }
     return line
+
+
+def prm_leg(args, kind, dq, n_samples, k):
+    """Learned-guided vs plain GPU PRM on one scene: the predictor is trained
+    on 2^20 exact-checker labels (10 epochs, batch 4096, lr 1e-3) by the
+    library's BF16 kernels, then the planners answer 1000 seeded queries."""
+    from gpuprm_b200 import planner, scenes as _sc
+    from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
+    from gpuprm_b200.configspace import RobotConfigspace as _RC
+    psc = _sc.make_scene(kind, args.seed)
+    pcs = _RC(psc, dq=dq)
+    pcs.init()
+    pcs.set_mode(GPRM_MODE_FP64_BAND)
+    mlp, losses, t_lab, t_train = planner.train_predictor(pcs, psc, n_labels=1 << 20, epochs=10, batch=4096,
+                                                          lr=1e-3, seed=args.seed)
+    out = planner.compare_planners(pcs, psc, n_samples=n_samples, n_queries=1000, k=k, seed=args.seed, mlp=mlp,
+                                   repeats=3)
+    out["scene"] = {"kind": kind, "ndof": psc.ndof, "polytopes": len(psc.polys), "pairs": len(psc.pair_from)}
+    out["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
+                        "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
+    return out
 
 
 def batch_leg(args, dev, policy):

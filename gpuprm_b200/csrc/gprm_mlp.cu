@@ -270,6 +270,225 @@ __global__ void k_to_bf16(long long n, const float* __restrict__ w, const int* _
     }
 }
 
+
+/* ------------------------------------------------------------------ */
+/* inference layers on the 5th-generation tensor cores (tcgen05)         */
+/* ------------------------------------------------------------------ */
+/*
+ * One persistent CTA per SM (256 threads) holds a layer's weights W
+ * [256 x K] in shared memory and runs 128-row tiles through it:
+ *   1. all threads stage the tile's inputs A [128 x K] in shared memory
+ *      (for the first layer: sin/cos features computed on the fly);
+ *   2. one thread issues K/16 tcgen05.mma (M=128, N=256, K=16, BF16 in,
+ *      FP32 accumulate) into a 256-column TMEM accumulator and commits
+ *      them to an mbarrier;
+ *   3. the eight warps read the accumulator back (tcgen05.ld, warp w owns
+ *      TMEM lanes 32*(w%4).. and columns 128*(w/4)..), add the bias,
+ *      apply GELU and store BF16 activations - or, for the last hidden
+ *      layer, reduce them against the output weights to P(collision).
+ * Operands use the no-swizzle K-major layout of 8-row x 16-byte core
+ * matrices: byte offset of (row r, k) = (r/8)*SBO + (k/8)*128 + (r%8)*16 +
+ * (k%8)*2 with SBO = 16*K, LBO = 128.  Waits on the mbarrier are bounded;
+ * on expiry the kernel sets *err, stops, and frees its TMEM.
+ */
+constexpr int TC_ROWS = 128;
+constexpr int TC_COLS = HID;                 /* 256 accumulator columns */
+constexpr long long TC_WAIT_LIMIT = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+/* shared-memory matrix descriptor: no swizzle, K-major (version 1) */
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+/* instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, M=128, N=256 */
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_COLS >> 3) << 17) |
+                              ((uint32_t)(TC_ROWS >> 4) << 24);
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase)
+{
+    for (long long i = 0; i < TC_WAIT_LIMIT; ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P1;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                     : "=r"(done) : "r"(mbar), "r"(phase) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v)
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                   "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+                   "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+                   "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+/* shared memory of k_mlp_tc<K>: W | A | mbarrier | TMEM address | row partials */
+template <int K>
+struct TcSmem {
+    static constexpr size_t W = (size_t)HID * K * 2;
+    static constexpr size_t A = (size_t)TC_ROWS * K * 2;
+    static constexpr size_t MBAR = W + A;
+    static constexpr size_t TADDR = MBAR + 8;
+    static constexpr size_t RED = TADDR + 8;                       /* 2 x 128 floats */
+    static constexpr size_t BYTES = RED + 2 * TC_ROWS * 4;
+    /* at least half of the SM's shared memory: one CTA per SM, so that the
+       256 TMEM columns this CTA allocates are always available */
+    static constexpr size_t LAUNCH = BYTES > 120 * 1024 ? BYTES : 120 * 1024;
+};
+
+template <int K, bool FEAT, bool LAST>
+__global__ void __launch_bounds__(256, 1)
+k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __nv_bfloat16* __restrict__ Hin,
+         const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias, __nv_bfloat16* __restrict__ Hout,
+         const __nv_bfloat16* __restrict__ w5, const float* __restrict__ b5, float* __restrict__ p,
+         unsigned* err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    using L = TcSmem<K>;
+    constexpr uint32_t SBO = 16u * K, LBO = 128u;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    unsigned char* Ws = sm;
+    unsigned char* As = sm + L::W;
+    const uint32_t mbar = smem_u32(sm + L::MBAR);
+    uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(sm + L::TADDR);
+    float* red = reinterpret_cast<float*>(sm + L::RED);
+
+    /* weights -> shared memory, core-matrix layout */
+    for (int idx = tid; idx < HID * (K / 8); idx += blockDim.x) {
+        const int nrow = idx % HID, c = idx / HID;
+        const uint4 v = *reinterpret_cast<const uint4*>(W + (size_t)nrow * K + c * 8);
+        *reinterpret_cast<uint4*>(Ws + (nrow / 8) * SBO + c * LBO + (nrow % 8) * 16) = v;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     :: "r"(smem_u32(taddr_slot)), "r"(TC_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *taddr_slot;
+    const int ntiles = (n + TC_ROWS - 1) / TC_ROWS;
+    uint32_t phase = 0;
+    bool failed = false;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int row0 = tile * TC_ROWS;
+        /* 1. inputs of the tile -> shared memory */
+        if (FEAT) {
+            if (tid < TC_ROWS) {
+                const int r = row0 + tid;
+                __align__(16) __nv_bfloat16 x[16];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float sv = 0.0f, cv = 0.0f;
+                    if (j < ndof && r < n) sincosf(q[r + qoff * j], &sv, &cv);
+                    x[2 * j] = __float2bfloat16(j < ndof ? sv : 0.0f);
+                    x[2 * j + 1] = __float2bfloat16(j < ndof ? cv : 0.0f);
+                }
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    *reinterpret_cast<uint4*>(As + (tid / 8) * SBO + c * LBO + (tid % 8) * 16) =
+                        *reinterpret_cast<const uint4*>(x + 8 * c);
+            }
+        } else {
+            for (int idx = tid; idx < TC_ROWS * (K / 8); idx += blockDim.x) {
+                const int r = idx % TC_ROWS, c = idx / TC_ROWS;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (row0 + r < n) v = *reinterpret_cast<const uint4*>(Hin + (size_t)(row0 + r) * K + c * 8);
+                *reinterpret_cast<uint4*>(As + (r / 8) * SBO + c * LBO + (r % 8) * 16) = v;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        /* 2. the MMAs */
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t a0 = smem_u32(As), b0 = smem_u32(Ws);
+#pragma unroll
+            for (int s = 0; s < K / 16; ++s) {
+                const uint64_t ad = tc_sdesc(a0 + s * 2 * LBO, LBO, SBO);
+                const uint64_t bd = tc_sdesc(b0 + s * 2 * LBO, LBO, SBO);
+                const uint32_t acc = s > 0 ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                             :: "r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc),
+                                "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         :: "r"(mbar) : "memory");
+        }
+        /* 3. accumulator -> bias, GELU -> out */
+        const bool ok = tc_wait(mbar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(err, 1u);
+            failed = true;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const int rl = 32 * (warp & 3) + lane;          /* this thread's row in the tile */
+        const int r = row0 + rl;
+        const int colbase = 128 * (warp >> 2);
+        float part = 0.0f;
+#pragma unroll 1
+        for (int cc = 0; cc < 4; ++cc) {
+            const int col = colbase + 32 * cc;
+            float v[32];
+            tc_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col, v);
+            __align__(16) __nv_bfloat16 hb[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) hb[j] = __float2bfloat16(gelu_f(v[j] + bias[col + j]));
+            if (LAST) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) part += __bfloat162float(hb[j]) * __bfloat162float(w5[col + j]);
+            } else if (r < n) {
+#pragma unroll
+                for (int c4 = 0; c4 < 4; ++c4)
+                    *reinterpret_cast<uint4*>(Hout + (size_t)r * HID + col + 8 * c4) =
+                        *reinterpret_cast<const uint4*>(hb + 8 * c4);
+            }
+        }
+        if (LAST) red[(warp >> 2) * TC_ROWS + rl] = part;
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        if (LAST && tid < TC_ROWS && row0 + tid < n) {
+            const float logit = red[tid] + red[TC_ROWS + tid] + b5[0];
+            p[row0 + tid] = 1.0f / (1.0f + expf(-logit));
+        }
+    }
+    if (failed) {
+        /* let an outstanding commit land before the accumulator is freed */
+        tc_wait(mbar, phase ^ 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(TC_COLS) : "memory");
+}
+
 }  // namespace
 
 /* ====================================================================== */
@@ -296,6 +515,12 @@ struct gprm_mlp {
     int* idx = nullptr;
     long long adam_t = 0;
     cudaStream_t st = nullptr;
+    /* inference on the tensor-core layers (k_mlp_tc) */
+    int infer_path = GPRM_MLP_INFER_TCGEN05;
+    __nv_bfloat16 *Ha = nullptr, *Hb = nullptr;
+    int infer_rows = 0;
+    unsigned* dev_err = nullptr;
+    int sms = 0;
     std::string err = "no error";
 };
 
@@ -411,6 +636,58 @@ double lcg_uniform(uint64_t& s)
 
 }  // namespace
 
+namespace {
+
+/* Predictions of n rows (q[i + offset*j]) through the tensor-core layers. */
+int predict_tc(gprm_mlp* h, const float* q, int n, int offset, float* p, cudaStream_t st)
+{
+    const int chunk = 1 << 18;
+    const int rows = n < chunk ? n : chunk;
+    if (rows > h->infer_rows) {
+        cudaFree(h->Ha);
+        cudaFree(h->Hb);
+        h->Ha = h->Hb = nullptr;
+        h->infer_rows = 0;
+        MLP_TRY(h, cudaMalloc((void**)&h->Ha, (size_t)rows * HID * sizeof(__nv_bfloat16)));
+        MLP_TRY(h, cudaMalloc((void**)&h->Hb, (size_t)rows * HID * sizeof(__nv_bfloat16)));
+        h->infer_rows = rows;
+    }
+    if (!h->dev_err) {
+        MLP_TRY(h, cudaMalloc((void**)&h->dev_err, sizeof(unsigned)));
+        MLP_TRY(h, cudaMemset(h->dev_err, 0, sizeof(unsigned)));
+        int dev = 0;
+        MLP_TRY(h, cudaGetDevice(&dev));
+        MLP_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev));
+        MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<IN_PAD, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TcSmem<IN_PAD>::LAUNCH));
+        MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<HID, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TcSmem<HID>::LAUNCH));
+        MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<HID, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TcSmem<HID>::LAUNCH));
+    }
+    const __nv_bfloat16* wb = h->wbf;
+    const float* w = h->w;
+    for (int s = 0; s < n; s += chunk) {
+        const int c = n - s < chunk ? n - s : chunk;
+        const int tiles = (c + TC_ROWS - 1) / TC_ROWS;
+        const int grid = tiles < h->sms ? tiles : h->sms;
+        k_mlp_tc<IN_PAD, true, false><<<grid, 256, TcSmem<IN_PAD>::LAUNCH, st>>>(
+            c, q + s, offset, h->ndof, nullptr, wb + h->offWbf[0], w + h->offB[0], h->Ha, nullptr, nullptr, nullptr,
+            h->dev_err);
+        k_mlp_tc<HID, false, false><<<grid, 256, TcSmem<HID>::LAUNCH, st>>>(
+            c, nullptr, 0, 0, h->Ha, wb + h->offWbf[1], w + h->offB[1], h->Hb, nullptr, nullptr, nullptr, h->dev_err);
+        k_mlp_tc<HID, false, false><<<grid, 256, TcSmem<HID>::LAUNCH, st>>>(
+            c, nullptr, 0, 0, h->Hb, wb + h->offWbf[2], w + h->offB[2], h->Ha, nullptr, nullptr, nullptr, h->dev_err);
+        k_mlp_tc<HID, false, true><<<grid, 256, TcSmem<HID>::LAUNCH, st>>>(
+            c, nullptr, 0, 0, h->Ha, wb + h->offWbf[3], w + h->offB[3], nullptr, wb + h->offWbf[NLAYER],
+            w + h->offB[NLAYER], p + s, h->dev_err);
+        MLP_TRY(h, cudaGetLastError());
+    }
+    return GPRM_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int gprm_mlp_create(int ndof, unsigned long long seed, gprm_mlp** out)
@@ -477,6 +754,7 @@ void gprm_mlp_destroy(gprm_mlp* h)
     cudaFree(h->loss); cudaFree(h->X);
     for (int l = 0; l < NLAYER; ++l) { cudaFree(h->H[l]); cudaFree(h->Z[l]); cudaFree(h->dZ[l]); }
     cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
+    cudaFree(h->Ha); cudaFree(h->Hb); cudaFree(h->dev_err);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -509,6 +787,7 @@ int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, v
     if (!h || n < 0 || (n > 0 && (!q || !p)) || offset < n) return mfail(h, GPRM_ERR_ARG, "bad arguments");
     if (n == 0) return GPRM_OK;
     cudaStream_t st = (cudaStream_t)stream;   /* NULL: the legacy default stream */
+    if (h->infer_path == GPRM_MLP_INFER_TCGEN05) return predict_tc(h, q, n, offset, p, st);
     const int chunk = 1 << 16;
     int rc = alloc_batch(h, n < chunk ? n : chunk);
     if (rc) return rc;
@@ -592,6 +871,25 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
         ep_loss[e] = l / steps;
     }
     if (losses) memcpy(losses, ep_loss.data(), epochs * sizeof(float));
+    return GPRM_OK;
+}
+
+int gprm_mlp_set_inference(gprm_mlp* h, int path)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (path != GPRM_MLP_INFER_TCGEN05 && path != GPRM_MLP_INFER_TRAINING_GEMM)
+        return mfail(h, GPRM_ERR_ARG, "unknown inference path");
+    h->infer_path = path;
+    return GPRM_OK;
+}
+
+int gprm_mlp_device_status(gprm_mlp* h, unsigned* flags)
+{
+    if (!h || !flags) return GPRM_ERR_ARG;
+    *flags = 0;
+    MLP_TRY(h, cudaDeviceSynchronize());
+    if (h->dev_err) MLP_TRY(h, cudaMemcpy(flags, h->dev_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (*flags) return mfail(h, GPRM_ERR_DEVICE, "a tensor-core layer timed out waiting for its MMAs");
     return GPRM_OK;
 }
 

@@ -82,6 +82,18 @@ class CollisionMLP:
                                               C.c_void_p(out.data_ptr()), C.c_void_p(st)))
         return out
 
+    def set_inference(self, path: str) -> None:
+        """'tcgen05' (default): tensor-core layers with TMEM accumulators;
+        'training': the training GEMMs."""
+        code = {"tcgen05": _abi.GPRM_MLP_INFER_TCGEN05, "training": _abi.GPRM_MLP_INFER_TRAINING_GEMM}[path]
+        self._check(self.lib.gprm_mlp_set_inference(self.h, code))
+
+    def device_status(self) -> int:
+        """Synchronises; 0 unless a tensor-core layer gave up waiting for its MMAs."""
+        f = C.c_uint(0)
+        self.lib.gprm_mlp_device_status(self.h, C.byref(f))
+        return int(f.value)
+
     def gradients(self, q_soa, y):
         import torch
         n = int(q_soa.shape[1])

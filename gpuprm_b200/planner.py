@@ -9,9 +9,8 @@ start/goal queries; every collision verdict comes from the exact checker.
 
 * ``plain_prm``: check every candidate edge, take connected components.
 * ``lazy_prm``: batched lazy Kruskal, exact connectivity with fewer checks.
-    round 1: each vertex's ``first`` lowest-weight candidate edges (or,
-             with first="mst", a minimum spanning forest) are checked; their
-             free edges define components.
+    round 1: each vertex's ``first`` lowest-weight candidate edges are
+             checked; their free edges define components.
     round r: the unchecked edges that join two different components, in
              weight order, are checked in one batch (the first
              ``batch_frac`` of them, all of them in the last round); the
@@ -28,6 +27,10 @@ start/goal queries; every collision verdict comes from the exact checker.
 * Every returned path is re-checked edge by edge with the all-steps policy
   (``verify_paths``).
 
+The roadmap stays on the device: kNN candidates (gprm_nbr_knn), component
+labels, the breadth-first forest the query paths follow and the paths
+themselves (gprm_graph_*); the host only sees the final paths.
+
 Time-to-path: wall time from sampling to verified paths for the whole
 query batch, divided by the number of queries.
 """
@@ -40,6 +43,7 @@ import numpy as np
 
 from . import scenes, workloads
 from ._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT
+from .graph import RoadmapGraph
 from .neighbours import NeighbourIndex
 
 
@@ -78,82 +82,50 @@ def _check_vertices(cs, q):
     return res
 
 
-def _components(V, ei, ej):
-    from scipy.sparse import coo_matrix
-    from scipy.sparse.csgraph import connected_components
-    return connected_components(coo_matrix((np.ones(len(ei)), (ei, ej)), shape=(V, V)), directed=False)[1]
+def _components(graph, V, i, j, good):
+    """Component labels (smallest vertex) of the free-edge graph, on the device."""
+    return graph.components(V, i, j, good)
 
 
-def _bfs_parents(V, ei, ej, comp):
-    """Parent pointers of a BFS forest of the graph (ei, ej), one root per
-    component (its smallest vertex); level-synchronous, vectorised."""
-    from scipy.sparse import coo_matrix
-    A = coo_matrix((np.ones(len(ei), np.int8), (ei, ej)), shape=(V, V)).tocsr()
-    A = (A + A.T).tocsr()
-    parent = np.full(V, -2, np.int64)
-    _, roots = np.unique(comp, return_index=True)
-    parent[roots] = -1
-    frontier = roots
-    while len(frontier):
-        starts = A.indptr[frontier]
-        cnt = A.indptr[frontier + 1] - starts
-        src = np.repeat(frontier, cnt)
-        idx = np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt) + np.repeat(starts, cnt)
-        nb = A.indices[idx]
-        new = parent[nb] == -2
-        nb, src = nb[new], src[new]
-        nb, first = np.unique(nb, return_index=True)
-        parent[nb] = src[first]
-        frontier = nb
-    return parent
-
-
-def _tree_path(parent, s, t):
-    a, b = [s], [t]
-    seen = {s: 0}
-    while parent[a[-1]] >= 0:
-        a.append(int(parent[a[-1]]))
-        seen[a[-1]] = len(a) - 1
-    while b[-1] not in seen:
-        if parent[b[-1]] < 0:
-            return None
-        b.append(int(parent[b[-1]]))
-    return a[:seen[b[-1]]] + b[::-1]
-
-
-def _answer_queries(cs, verts, comp, parent, starts, goals, k):
-    """Attaches starts and goals to up to k nearest roadmap vertices with
-    exactly checked edges and returns the paths through the BFS forest."""
+def _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k):
+    """Attaches every start and goal to its k nearest roadmap vertices by
+    exactly checked edges, picks the first (start, goal) attachment pair in
+    nearest-first order whose vertices share a component, and returns the
+    forest paths through the roadmap (all on the device).  Returns
+    (paths as host arrays or None, attachment edges checked)."""
     import torch
+    dev = verts.device
     Q = starts.shape[0]
-    st = torch.as_tensor(starts, device=verts.device)
-    gl = torch.as_tensor(goals, device=verts.device)
-    ends = torch.cat([st, gl])
-    kk = min(k, verts.shape[0])
+    V = verts.shape[0]
+    if V == 0:
+        return [None] * Q, 0
+    ends = torch.cat([torch.as_tensor(starts, device=dev), torch.as_tensor(goals, device=dev)])
+    kk = min(k, V)
     index = NeighbourIndex(verts.shape[1])
     index.build(verts.T.contiguous())
-    nb = index.knn(kk, q=ends.T.contiguous())[0].long()
+    nb = index.knn(kk, q=ends.T.contiguous())[0].long()                       # (2Q, kk)
     qa = ends[:, None, :].expand(-1, kk, -1).reshape(-1, ends.shape[1])
-    res = _check_edges(cs, qa, verts[nb.reshape(-1)]).reshape(2 * Q, kk)
-    ok = (res == 0).cpu().numpy()
-    nbn = nb.cpu().numpy()
-    c = np.where(ok, comp[nbn], -1)
-    cs_, cg_ = c[:Q], c[Q:]
-    # first start attachment whose component some goal attachment shares
-    match = (cs_[:, :, None] == cg_[:, None, :]) & (cs_[:, :, None] >= 0)
-    has = match.any(axis=(1, 2))
-    verts_np = verts.cpu().numpy()
+    ok = (_check_edges(cs, qa, verts[nb.reshape(-1)]) == 0).reshape(2 * Q, kk)
+    lab = torch.where(ok, label[nb].long(), torch.full_like(nb, -1))
+    ls, lg = lab[:Q], lab[Q:]
+    match = (ls[:, :, None] == lg[:, None, :]) & (ls[:, :, None] >= 0)       # (Q, kk, kk)
+    flat = match.reshape(Q, -1)
+    has = flat.any(1)
+    first = torch.argmax(flat.to(torch.int8), dim=1)                         # lexicographic first (a, b)
+    a, b = first // kk, first % kk
+    rows = torch.arange(Q, device=dev)
+    vs = torch.where(has, nb[:Q][rows, a], torch.full_like(a, -1)).to(torch.int32)
+    vt = torch.where(has, nb[Q:][rows, b], torch.full_like(b, -1)).to(torch.int32)
+    parent, depth, _ = graph.forest(V, i, j, label, good)
+    length, off, flat_path = graph.paths(vs, vt, label, parent, depth)
+    pts = verts[flat_path.long()].cpu().numpy()
+    length, off = length.cpu().numpy(), off.cpu().numpy()
     paths = []
-    for i in range(Q):
-        if not has[i]:
+    for t in range(Q):
+        if length[t] == 0:
             paths.append(None)
             continue
-        a, b = np.argwhere(match[i])[0]
-        p = _tree_path(parent, int(nbn[i, a]), int(nbn[Q + i, b]))
-        if p is None:
-            paths.append(None)
-            continue
-        paths.append(np.concatenate([starts[i:i + 1], verts_np[p], goals[i:i + 1]]))
+        paths.append(np.concatenate([starts[t:t + 1], pts[off[t]:off[t] + length[t]], goals[t:t + 1]]))
     return paths, 2 * Q * kk
 
 
@@ -185,32 +157,32 @@ def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0) -> PlanResult:
     """Eager GPU PRM: every vertex and every candidate edge checked."""
     import torch
     s0 = cs.stats()["edge_steps_nominal"]
+    graph = RoadmapGraph()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     q = _sample(scene, n_samples, seed)
     verts = q[_check_vertices(cs, q) == 0]
     i, j = workloads.knn_pairs(verts, k)
-    good = (_check_edges(cs, verts[i], verts[j]) == 0).cpu().numpy()
-    ei, ej = i.cpu().numpy()[good], j.cpu().numpy()[good]
+    i, j = i.to(torch.int32), j.to(torch.int32)
+    good = (_check_edges(cs, verts[i.long()], verts[j.long()]) == 0).to(torch.uint8)
     V = verts.shape[0]
-    comp = _components(V, ei, ej)
-    parent = _bfs_parents(V, ei, ej, comp)
-    paths, nconn = _answer_queries(cs, verts, comp, parent, starts, goals, k)
+    label = _components(graph, V, i, j, good)
+    paths, nconn = _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k)
     ok = verify_paths(cs, paths)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return PlanResult(np.array([p is not None for p in paths]), paths, dt, int(len(good)) + nconn,
+    return PlanResult(np.array([p is not None for p in paths]), paths, dt, int(i.numel()) + nconn,
                       int(cs.stats()["edge_steps_nominal"] - s0), n_samples,
-                      {"verified": ok, "free_vertices": V, "candidate_edges": int(len(good))})
+                      {"verified": ok, "free_vertices": V, "candidate_edges": int(i.numel())})
 
 
 def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=0.9, beta=4.0,
              batch_frac=1.0, min_batch=4096, max_rounds=2, first=2) -> PlanResult:
-    """Batched lazy-Kruskal PRM (exact connectivity), optionally MLP-guided."""
+    """Batched lazy-Kruskal PRM (exact connectivity), optionally MLP-guided;
+    the roadmap and its bookkeeping stay on the device."""
     import torch
-    from scipy.sparse import coo_matrix
-    from scipy.sparse.csgraph import minimum_spanning_tree
     s0 = cs.stats()["edge_steps_nominal"]
+    graph = RoadmapGraph()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     q = _sample(scene, n_samples, seed)
@@ -221,70 +193,60 @@ def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=
         q = q[keep]
     verts = q[_check_vertices(cs, q) == 0]
     vchecks = int(q.shape[0])
-    i, j = workloads.knn_pairs(verts, k)
-    V, E = verts.shape[0], int(i.shape[0])
-    length = torch.linalg.norm(verts[i] - verts[j], dim=1)
-    if mlp is not None:
-        pts = torch.cat([verts[i] + t * (verts[j] - verts[i]) for t in (0.25, 0.5, 0.75)])
+    i64, j64 = workloads.knn_pairs(verts, k)
+    i, j = i64.to(torch.int32), j64.to(torch.int32)
+    V, E = verts.shape[0], int(i.numel())
+    dev = verts.device
+    length = torch.linalg.norm(verts[i64] - verts[j64], dim=1)
+    if mlp is not None and E:
+        pts = torch.cat([verts[i64] + t * (verts[j64] - verts[i64]) for t in (0.25, 0.5, 0.75)])
         pe = mlp.predict(pts.T.contiguous()).reshape(3, -1).max(0).values
         cost = length * (1.0 + beta * pe)
     else:
         cost = length
-    ii, jj = i.cpu().numpy(), j.cpu().numpy()
-    w = cost.cpu().numpy().astype(np.float64) + 1e-9
-    good = np.zeros(E, bool)
-    checked = np.zeros(E, bool)
+    good = torch.zeros(E, dtype=torch.uint8, device=dev)
+    checked = torch.zeros(E, dtype=torch.bool, device=dev)
 
     def run(sel):
-        t = torch.as_tensor(sel, device="cuda:0")
-        ok_ = (_check_edges(cs, verts[i[t]], verts[j[t]]) == 0).cpu().numpy()
+        if sel.numel() == 0:
+            return 0
+        ok_ = _check_edges(cs, verts[i64[sel]], verts[j64[sel]]) == 0
         checked[sel] = True
-        good[sel[ok_]] = True
-        return int(ok_.sum())
+        good[sel] = ok_.to(torch.uint8)
+        return int(ok_.sum().item())
 
-    if first == "mst":
-        # round 1: the minimum spanning forest
-        T = minimum_spanning_tree(coo_matrix((w, (ii, jj)), shape=(V, V))).tocoo()
-        key = ii.astype(np.int64) * V + jj
-        korder = np.argsort(key)
-        tk = np.minimum(T.row, T.col).astype(np.int64) * V + np.maximum(T.row, T.col)
-        r1 = korder[np.searchsorted(key[korder], tk)]
-    else:
-        # round 1: every vertex's `first` cheapest candidate edges (on the GPU)
-        m = int(first)
-        ends = torch.cat([i, j])
-        eid = torch.arange(E, device="cuda:0").repeat(2)
-        c2 = cost.repeat(2)
-        o = torch.argsort(c2, stable=True)
-        o = o[torch.argsort(ends[o], stable=True)]          # by vertex, then cost
-        ev = ends[o]
-        startpos = torch.searchsorted(ev, torch.arange(V, device="cuda:0"))
-        rank = torch.arange(2 * E, device="cuda:0") - startpos[ev]
-        r1 = torch.unique(eid[o][rank < m]).cpu().numpy()
+    # round 1: every vertex's `first` cheapest candidate edges
+    m = int(first)
+    ends = torch.cat([i64, j64])
+    eid = torch.arange(E, device=dev).repeat(2)
+    o = torch.argsort(cost.repeat(2), stable=True)
+    o = o[torch.argsort(ends[o], stable=True)]          # by vertex, then cost
+    ev = ends[o]
+    startpos = torch.searchsorted(ev, torch.arange(V, device=dev))
+    rank = torch.arange(2 * E, device=dev) - startpos[ev]
+    r1 = torch.unique(eid[o][rank < m])
     free1 = run(r1)
-    rounds = [len(r1)]
-    order = np.argsort(w, kind="stable")
+    rounds = [int(r1.numel())]
+    order = torch.argsort(cost, stable=True)
     for rnd in range(max_rounds):
-        comp_r = _components(V, ii[good], jj[good])
+        label = _components(graph, V, i, j, good)
         rest = order[~checked[order]]
-        cross = rest[comp_r[ii[rest]] != comp_r[jj[rest]]]
-        if len(cross) == 0:
+        cross = rest[label[i64[rest]] != label[j64[rest]]]
+        if cross.numel() == 0:
             break
-        take = cross if rnd == max_rounds - 1 else cross[:max(min_batch, int(len(cross) * batch_frac))]
+        take = cross if rnd == max_rounds - 1 else cross[:max(min_batch, int(cross.numel() * batch_frac))]
         run(take)
-        rounds.append(len(take))
-    r2n = int(sum(rounds[1:]))
-    ei, ej = ii[good], jj[good]
-    comp = _components(V, ei, ej)
-    parent = _bfs_parents(V, ei, ej, comp)
-    paths, nconn = _answer_queries(cs, verts, comp, parent, starts, goals, k)
+        rounds.append(int(take.numel()))
+    label = _components(graph, V, i, j, good)
+    paths, nconn = _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k)
     ok = verify_paths(cs, paths)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return PlanResult(np.array([p is not None for p in paths]), paths, dt, int(checked.sum()) + nconn,
+    return PlanResult(np.array([p is not None for p in paths]), paths, dt, int(checked.sum().item()) + nconn,
                       int(cs.stats()["edge_steps_nominal"] - s0), vchecks,
-                      {"verified": ok, "free_vertices": V, "candidate_edges": E, "round1_edges": int(len(r1)),
-                       "round1_free": free1, "later_edges": r2n, "rounds": len(rounds), "pruned": pruned})
+                      {"verified": ok, "free_vertices": V, "candidate_edges": E, "round1_edges": rounds[0],
+                       "round1_free": free1, "later_edges": int(sum(rounds[1:])), "rounds": len(rounds),
+                       "pruned": pruned})
 
 
 def make_queries(cs, scene, n_queries, seed):
@@ -318,27 +280,73 @@ def train_predictor(cs, scene, n_labels=1 << 20, epochs=10, batch=4096, lr=1e-3,
     return mlp, losses, t1 - t0, time.perf_counter() - t1
 
 
-def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0, mlp=None, repeats=3):
-    """Plain (eager) PRM against the learned-guided lazy PRM (and the lazy PRM
-    without guidance) on the same seeded samples and queries.  Each method
-    runs once untimed, then `repeats` times; the median is reported."""
+def predictor_errors(cs, scene, mlp, n=1 << 16, seed=0, prune=0.9):
+    """The exact checker as the judge of the predictor on held-out uniform
+    configurations: false-free rate (colliding, predicted p < 0.5),
+    false-colliding rate (free, predicted p >= 0.5), and the share of free
+    configurations the planner would prune (p > prune)."""
+    import torch
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(scene, n, seed + 999).T), device="cuda:0")
+    codes = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+    cs.check_configs_device(q, codes)
+    p = mlp.predict(q)
+    coll = codes != 0
+    free = ~coll
+    ncoll, nfree = max(1, int(coll.sum().item())), max(1, int(free.sum().item()))
+    return {"held_out": n,
+            "false_free_rate": int((coll & (p < 0.5)).sum().item()) / ncoll,
+            "false_colliding_rate": int((free & (p >= 0.5)).sum().item()) / nfree,
+            "free_pruned_rate": int((free & (p > prune)).sum().item()) / nfree,
+            "accuracy": float(((p >= 0.5) == coll).float().mean().item())}
+
+
+def _summary(r):
+    return {"success_rate": float(r.success.mean()), "time_to_path_ms": 1e3 * r.time_to_path,
+            "batch_seconds": r.seconds, "edge_checks": r.edge_checks, "edge_steps": r.edge_steps,
+            "vertex_checks": r.vertex_checks, "paths_verified": bool(r.info["verified"]),
+            **{k_: (v.item() if isinstance(v, np.generic) else v) for k_, v in r.info.items() if k_ != "verified"}}
+
+
+def _median_run(fn, repeats):
+    fn()
+    rs = [fn() for _ in range(repeats)]
+    return sorted(rs, key=lambda x: x.seconds)[len(rs) // 2]
+
+
+def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0, mlp=None, repeats=3,
+                     first=2, max_rounds=2):
+    """Plain (eager) PRM against the lazy PRM without guidance and the
+    learned-guided lazy PRM, on the same seeded queries.  Each run is
+    repeated (`repeats` timed runs after one untimed) and the median is
+    reported.  The lazy PRM has the eager PRM's connectivity on the same
+    samples, so its success rate is the same by construction.  The learned
+    PRM prunes samples, which can change the roadmap: it runs on
+    n_samples, then on 1.125x, 1.25x, ... samples until its success rate
+    reaches the plain planner's, and the time of that run is the one
+    compared ("equal success rate")."""
     starts, goals = make_queries(cs, scene, n_queries, seed + 17)
     out = {}
-    runs = {"plain": lambda: plain_prm(cs, scene, starts, goals, n_samples, k, seed),
-            "lazy": lambda: lazy_prm(cs, scene, starts, goals, n_samples, k, seed),
-            "learned": lambda: lazy_prm(cs, scene, starts, goals, n_samples, k, seed, mlp=mlp)}
-    for name, fn in runs.items():
-        if name == "learned" and mlp is None:
-            continue
-        fn()
-        rs = [fn() for _ in range(repeats)]
-        r = sorted(rs, key=lambda x: x.seconds)[len(rs) // 2]
-        out[name] = {"success_rate": float(r.success.mean()), "time_to_path_ms": 1e3 * r.time_to_path,
-                     "batch_seconds": r.seconds, "edge_checks": r.edge_checks, "edge_steps": r.edge_steps,
-                     "vertex_checks": r.vertex_checks, "paths_verified": bool(r.info["verified"]),
-                     **{k_: (v.item() if isinstance(v, np.generic) else v) for k_, v in r.info.items()
-                        if k_ != "verified"}}
-    if "learned" in out:
+    plain = _median_run(lambda: plain_prm(cs, scene, starts, goals, n_samples, k, seed), repeats)
+    out["plain"] = _summary(plain)
+    lazy = _median_run(lambda: lazy_prm(cs, scene, starts, goals, n_samples, k, seed, first=first,
+                                        max_rounds=max_rounds), repeats)
+    out["lazy"] = _summary(lazy)
+    if mlp is not None:
+        target = float(plain.success.mean())
+        n, tries = n_samples, []
+        for _ in range(8):
+            r = _median_run(lambda: lazy_prm(cs, scene, starts, goals, n, k, seed, mlp=mlp, first=first,
+                                             max_rounds=max_rounds), repeats)
+            tries.append({"samples": n, "success_rate": float(r.success.mean()), "time_to_path_ms": 1e3 * r.time_to_path})
+            if r.success.mean() >= target:
+                break
+            n = int(n * 1.125)
+        out["learned"] = dict(_summary(r), samples=n, sample_search=tries,
+                              success_matched=bool(r.success.mean() >= target))
         out["learned_over_plain_time"] = out["learned"]["time_to_path_ms"] / out["plain"]["time_to_path_ms"]
-    out["config"] = {"samples": n_samples, "queries": n_queries, "k": k, "seed": seed}
+        out["learned_over_lazy_time"] = out["learned"]["time_to_path_ms"] / out["lazy"]["time_to_path_ms"]
+        out["predictor_errors"] = predictor_errors(cs, scene, mlp, seed=seed)
+    out["lazy_over_plain_time"] = out["lazy"]["time_to_path_ms"] / out["plain"]["time_to_path_ms"]
+    out["config"] = {"samples": n_samples, "queries": n_queries, "k": k, "seed": seed, "dq": float(cs.deltaq()),
+                     "lazy_first": first, "lazy_rounds": max_rounds}
     return out

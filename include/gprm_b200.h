@@ -201,6 +201,16 @@ int gprm_mlp_set_params(gprm_mlp* h, const float* in);
 /* p[i] = P(collision) of device configurations q[i + offset*j], launched on
  * `stream` (NULL: the legacy default stream) */
 int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, void* stream);
+/* Inference path of gprm_mlp_predict: the tcgen05 layers (default; BF16
+ * tensor-core MMAs into TMEM, one persistent CTA per SM per layer) or the
+ * training GEMMs.  Both compute the same function (BF16 operands and
+ * activations, FP32 accumulation) up to FP32 summation order. */
+#define GPRM_MLP_INFER_TCGEN05        0
+#define GPRM_MLP_INFER_TRAINING_GEMM  1
+int gprm_mlp_set_inference(gprm_mlp* h, int path);
+/* Synchronises the device; *flags != 0 (and GPRM_ERR_DEVICE) when a
+ * tensor-core layer gave up waiting for its MMAs. */
+int gprm_mlp_device_status(gprm_mlp* h, unsigned* flags);
 /* one forward/backward on n device configurations with labels y (device):
  * mean BCE loss and its gradient (host arrays) */
 int gprm_mlp_gradients(gprm_mlp* h, const float* q, const float* y, int n, int offset, float* grads,

@@ -125,3 +125,30 @@ def test_training_learns_exact_checker_labels():
     acc = ((p > 0.5) == (ct != 0)).float().mean().item()
     base = max((ct != 0).float().mean().item(), 1 - (ct != 0).float().mean().item())
     assert acc > base + 0.05, (acc, base)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,ndof", [(5000, 6), (131, 7), (1, 4)])
+def test_gpu_tensor_core_inference_matches_training_path_and_oracle(n, ndof):
+    """The tcgen05 inference layers compute the training forward's function
+    (same BF16 roundings, FP32 accumulation in another order)."""
+    import torch
+    from gpuprm_b200.mlp import CollisionMLP
+    rng = np.random.default_rng(7)
+    q = rng.uniform(-np.pi, np.pi, (n, ndof)).astype(np.float32)
+    mlp = CollisionMLP(ndof, seed=9)
+    mlp.set_params(mlp.get_params() * 3.0)      # larger weights: outputs away from 0.5
+    q_soa = torch.tensor(np.ascontiguousarray(q.T), device="cuda:0")
+    mlp.set_inference("training")
+    p_ref = mlp.predict(q_soa).cpu().numpy()
+    mlp.set_inference("tcgen05")
+    p_tc = mlp.predict(q_soa).cpu().numpy()
+    assert mlp.device_status() == 0
+    assert np.max(np.abs(p_tc - p_ref)) <= 2e-3
+    _, _, p = MO.forward_backward(mlp.get_params().astype(np.float64), MO.features(q), np.zeros(n))
+    # the tripled weights amplify a one-ulp BF16 difference of an activation
+    # (FP32 summation order decides a rounding) up to the output: bound the
+    # worst case loosely and the typical error tightly
+    assert np.max(np.abs(p_tc - p)) <= 1e-2
+    if n >= 100:
+        assert np.median(np.abs(p_tc - p)) <= 1e-5

@@ -1,35 +1,8 @@
-"""Roadmap planners: graph helpers (CPU) and plain vs lazy vs learned (B200)."""
+"""Roadmap planners: plain vs lazy vs learned (B200)."""
 import numpy as np
 import pytest
 
 from gpuprm_b200 import planner
-
-
-def test_bfs_forest_paths_follow_edges():
-    rng = np.random.default_rng(0)
-    V = 300
-    ei = rng.integers(0, V, 700)
-    ej = rng.integers(0, V, 700)
-    keep = ei != ej
-    ei, ej = ei[keep], ej[keep]
-    comp = planner._components(V, ei, ej)
-    parent = planner._bfs_parents(V, ei, ej, comp)
-    edges = set(zip(ei.tolist(), ej.tolist())) | set(zip(ej.tolist(), ei.tolist()))
-    for v in range(V):
-        if parent[v] >= 0:
-            assert (v, int(parent[v])) in edges
-            assert comp[parent[v]] == comp[v]
-        else:
-            assert parent[v] == -1      # every vertex reached: a root
-    for _ in range(200):
-        s, t = rng.integers(0, V, 2)
-        p = planner._tree_path(parent, int(s), int(t))
-        if comp[s] != comp[t]:
-            assert p is None
-            continue
-        assert p[0] == s and p[-1] == t
-        for a, b in zip(p[:-1], p[1:]):
-            assert (a, b) in edges
 
 
 @pytest.mark.gpu
