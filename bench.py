@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--policy", default="early", choices=["early", "all"])
     ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
-    ap.add_argument("--prm-samples", type=int, default=1 << 16)
+    ap.add_argument("--prm-samples", type=int, default=1 << 20)
     ap.add_argument("--no-stress", action="store_true", help="skip the 7-DOF wall planner comparison")
     ap.add_argument("--stress-samples", type=int, default=1 << 17)
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")

@@ -14,8 +14,10 @@
  *            (the reference's "terminate if buffer full");
  *   knn      the k nearest nodes under the same distance, ties broken by
  *            the lower index.  Nodes are bucketed into a uniform grid over
- *            the first min(3, ndof) joints (counting sort by cell); a query
- *            scans the 3^G cells around its own and keeps a sorted top-k; a
+ *            the first min(4, ndof) joints (counting sort by cell); a query
+ *            scans the 3^G cells around its own and keeps a sorted top-k
+ *            (a thread per query for the nodes themselves, a warp per query
+ *            for outside queries); a
  *            result is accepted only when its k-th distance is below the
  *            distance to the scanned block's boundary (with slack for float
  *            rounding), otherwise the query is redone by a warp that scans
@@ -36,7 +38,7 @@
 
 namespace {
 
-constexpr int NBR_MAX_GRID = 3;
+constexpr int NBR_MAX_GRID = 4;
 constexpr int NBR_MAX_K = 32;
 constexpr int NBR_MAX_CELLS = 1 << 21;
 
@@ -198,64 +200,159 @@ __device__ __forceinline__ void topk_insert(float* ts, int* ti, int& len, int k,
     if (len < k) ++len;
 }
 
-/* Query t (or the node at sorted position t when `self_sorted`): grid scan
- * of the 3^G cells around the query's cell.  Queries whose result cannot be
- * proven exact are appended to `redo`. */
-__global__ void k_knn_grid(GridView g, const float* __restrict__ q, int m, long long qstride, int k, int exclude_self,
-                           int self_sorted, int* out_idx, float* out_dist, int* redo, int* nredo)
+/* The block of cells a query scans: cells c-1..c+1 in each gridded joint
+ * (clipped to the grid); guard = the distance from q to the block's faces
+ * that have cells beyond them (infinite when none).  Returns false when a
+ * gridded coordinate is not finite. */
+__device__ __forceinline__ bool query_block(const GridView& g, const float* qv, int* lo, int* hi, float* guard)
+{
+    bool finite = true;
+    float gd = INFINITY;
+    for (int d = 0; d < g.G; ++d) {
+        finite &= isfinite(qv[d]);
+        const int c = cell_coord(qv[d], g.lo[d], g.inv_cell, g.nc[d]);
+        lo[d] = max(c - 1, 0);
+        hi[d] = min(c + 1, g.nc[d] - 1);
+        if (lo[d] > 0) gd = fminf(gd, qv[d] - (g.lo[d] + (float)lo[d] * g.cell));
+        if (hi[d] < g.nc[d] - 1) gd = fminf(gd, (g.lo[d] + (float)(hi[d] + 1) * g.cell) - qv[d]);
+    }
+    for (int j = g.G; j < g.ndof; ++j) finite &= isfinite(qv[j]);
+    *guard = gd;
+    return finite;
+}
+
+/* Number of rows of the block (cells varying in joints 1..G-1) and the
+ * sorted-node range of row r (joint 0 runs lo[0]..hi[0], contiguous). */
+__device__ __forceinline__ int block_rows(const GridView& g, const int* lo, const int* hi)
+{
+    int r = 1;
+    for (int d = 1; d < g.G; ++d) r *= hi[d] - lo[d] + 1;
+    return r;
+}
+
+__device__ __forceinline__ void block_row_range(const GridView& g, const int* lo, const int* hi, int r, int* b, int* e)
+{
+    int cell = 0;
+    int rest = r;
+    int coord[NBR_MAX_GRID];
+    for (int d = 1; d < g.G; ++d) {
+        const int span = hi[d] - lo[d] + 1;
+        coord[d] = lo[d] + rest % span;
+        rest /= span;
+    }
+    for (int d = g.G - 1; d >= 1; --d) cell = cell * g.nc[d] + coord[d];
+    const int row = cell * g.nc[0];
+    *b = g.start[row + lo[0]];
+    *e = g.start[row + hi[0] + 1];
+}
+
+/* The exactness test: k results strictly inside the guard ball, with slack
+ * for the rounding of the cell assignment and of s. */
+__device__ __forceinline__ bool knn_exact(const GridView& g, bool finite, int len, int k, float kth, float guard)
+{
+    const float gs = guard - g.slack;
+    return finite && len == k && (!isfinite(gs) || (gs > 0.0f && kth < gs * gs * 0.99999f));
+}
+
+/* Thread per query: the node at sorted position t (queries are the nodes;
+ * neighbouring threads hold neighbouring nodes). */
+__global__ void k_knn_grid(GridView g, int m, int k, int* out_idx, float* out_dist, int* redo, int* nredo)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
         float qv[GPRM_MAX_DOF];
-        int qid;
-        if (self_sorted) {
-            qid = g.id[t];
-            for (int j = 0; j < g.ndof; ++j) qv[j] = g.xs[t + (long long)g.n * j];
-        } else {
-            qid = t;
-            for (int j = 0; j < g.ndof; ++j) qv[j] = q[t + qstride * j];
-        }
+        const int qid = g.id[t];
+        for (int j = 0; j < g.ndof; ++j) qv[j] = g.xs[t + (long long)g.n * j];
         float ts[NBR_MAX_K];
         int ti[NBR_MAX_K];
         int len = 0;
-        int c[NBR_MAX_GRID], lo[NBR_MAX_GRID], hi[NBR_MAX_GRID];
-        float guard = INFINITY;
-        bool finite = true;
-        for (int d = 0; d < g.G; ++d) {
-            finite &= isfinite(qv[d]);
-            c[d] = cell_coord(qv[d], g.lo[d], g.inv_cell, g.nc[d]);
-            lo[d] = max(c[d] - 1, 0);
-            hi[d] = min(c[d] + 1, g.nc[d] - 1);
-            /* distance from q to the scanned block's faces that have cells beyond */
-            if (lo[d] > 0) guard = fminf(guard, qv[d] - (g.lo[d] + (float)lo[d] * g.cell));
-            if (hi[d] < g.nc[d] - 1) guard = fminf(guard, (g.lo[d] + (float)(hi[d] + 1) * g.cell) - qv[d]);
-        }
-        for (int j = g.G; j < g.ndof; ++j) finite &= isfinite(qv[j]);
-        const int c1lo = g.G > 1 ? lo[1] : 0, c1hi = g.G > 1 ? hi[1] : 0;
-        const int c2lo = g.G > 2 ? lo[2] : 0, c2hi = g.G > 2 ? hi[2] : 0;
-        for (int z = c2lo; z <= c2hi; ++z)
-            for (int y = c1lo; y <= c1hi; ++y) {
-                const int row = (z * (g.G > 1 ? g.nc[1] : 1) + y) * g.nc[0];
-                const int b = g.start[row + lo[0]], e = g.start[row + hi[0] + 1];
-                for (int p = b; p < e; ++p) {
-                    const int nid = g.id[p];
-                    if (exclude_self && nid == qid) continue;
-                    float s = dist2(g.xs, g.n, p, qv, g.ndof);
-                    if (s != s) s = INFINITY;   /* NaN sorts last */
-                    topk_insert(ts, ti, len, k, s, nid);
-                }
+        int lo[NBR_MAX_GRID], hi[NBR_MAX_GRID];
+        float guard;
+        const bool finite = query_block(g, qv, lo, hi, &guard);
+        const int rows = block_rows(g, lo, hi);
+        for (int r = 0; r < rows; ++r) {
+            int b, e;
+            block_row_range(g, lo, hi, r, &b, &e);
+            for (int p = b; p < e; ++p) {
+                const int nid = g.id[p];
+                if (nid == qid) continue;
+                float sd = dist2(g.xs, g.n, p, qv, g.ndof);
+                if (sd != sd) sd = INFINITY;   /* NaN sorts last */
+                topk_insert(ts, ti, len, k, sd, nid);
             }
-        /* exact when k results lie strictly inside the guard ball: any node
-           outside the block is at least `guard` away in one joint.  The
-           slack covers the rounding of the cell assignment and of s. */
-        const float gs = guard - g.slack;
-        const bool exact = finite && len == k && (!isfinite(gs) || (gs > 0.0f && ts[k - 1] < gs * gs * 0.99999f));
-        if (exact) {
+        }
+        if (knn_exact(g, finite, len, k, len ? ts[len - 1] : INFINITY, guard)) {
             for (int r = 0; r < k; ++r) {
                 out_idx[(long long)qid * k + r] = ti[r];
                 out_dist[(long long)qid * k + r] = sqrtf(ts[r]);
             }
         } else {
             redo[atomicAdd(nredo, 1)] = qid;
+        }
+    }
+}
+
+/* Merges the lanes' sorted top lists into the warp's k smallest (k rounds
+ * of a warp argmin); every lane gets round r's winner in (ws, wi) when
+ * r == its lane. */
+__device__ __forceinline__ void warp_topk_merge(const float* ts, const int* ti, int len, int k, float* my_s, int* my_i,
+                                                float* kth, int* found)
+{
+    const int lane = threadIdx.x & 31;
+    int head = 0, cnt = 0;
+    float last = INFINITY;
+    *my_s = INFINITY;
+    *my_i = -1;
+    for (int r = 0; r < k; ++r) {
+        float bs = head < len ? ts[head] : INFINITY;
+        int bi = head < len ? ti[head] : 0x7fffffff;
+        for (int o = 16; o > 0; o >>= 1) {
+            const float os = __shfl_xor_sync(0xffffffffu, bs, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (less_pair(os, oi, bs, bi)) { bs = os; bi = oi; }
+        }
+        if (head < len && ti[head] == bi && ts[head] == bs) ++head;
+        if (bi != 0x7fffffff) { ++cnt; last = bs; }
+        if (lane == r) { *my_s = bs; *my_i = bi != 0x7fffffff ? bi : -1; }
+    }
+    *kth = last;
+    *found = cnt;
+}
+
+/* Warp per query (outside queries q): lanes split the block's nodes. */
+__global__ void k_knn_grid_warp(GridView g, const float* __restrict__ q, int m, long long qstride, int k,
+                                int* out_idx, float* out_dist, int* redo, int* nredo)
+{
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (int t = blockIdx.x * wpb + (threadIdx.x >> 5); t < m; t += gridDim.x * wpb) {
+        float qv[GPRM_MAX_DOF];
+        for (int j = 0; j < g.ndof; ++j) qv[j] = q[t + qstride * j];
+        float ts[NBR_MAX_K];
+        int ti[NBR_MAX_K];
+        int len = 0;
+        int lo[NBR_MAX_GRID], hi[NBR_MAX_GRID];
+        float guard;
+        const bool finite = query_block(g, qv, lo, hi, &guard);
+        const int rows = block_rows(g, lo, hi);
+        for (int r = 0; r < rows; ++r) {
+            int b, e;
+            block_row_range(g, lo, hi, r, &b, &e);
+            for (int p = b + lane; p < e; p += 32) {
+                float sd = dist2(g.xs, g.n, p, qv, g.ndof);
+                if (sd != sd) sd = INFINITY;
+                topk_insert(ts, ti, len, k, sd, g.id[p]);
+            }
+        }
+        float my_s, kth;
+        int my_i, found;
+        warp_topk_merge(ts, ti, len, k, &my_s, &my_i, &kth, &found);
+        if (knn_exact(g, finite, found, k, kth, guard)) {
+            if (lane < k) {
+                out_idx[(long long)t * k + lane] = my_i;
+                out_dist[(long long)t * k + lane] = sqrtf(my_s);
+            }
+        } else if (lane == 0) {
+            redo[atomicAdd(nredo, 1)] = t;
         }
     }
 }
@@ -323,7 +420,7 @@ struct gprm_nbr {
     float* mm = nullptr;
     int* redo = nullptr;
     int* nredo = nullptr;
-    size_t cap_n = 0, cap_redo = 0;
+    size_t cap_xs = 0, cap_id = 0, cap_key = 0, cap_start = 0, cap_count = 0, cap_cursor = 0, cap_redo = 0;
     std::string err = "no error";
 };
 
@@ -467,16 +564,13 @@ int gprm_nbr_build(gprm_nbr* h, const float* x, int n, int stride, float cell, v
     double mag = 0.0;
     for (int d = 0; d < G; ++d) mag = fmax(mag, fabs((double)g.lo[d]) + g.nc[d] * c);
     g.slack = (float)(1e-5 * c + 1e-6 * mag);
-    if ((rc = grow(h, &h->xs, h->cap_n, (size_t)n * nd + 1)) != GPRM_OK) return rc;
-    cudaFree(h->id); h->id = nullptr;
-    cudaFree(h->key); h->key = nullptr;
-    NBR_TRY(h, cudaMalloc((void**)&h->id, ((size_t)n + 1) * sizeof(int)));
-    NBR_TRY(h, cudaMalloc((void**)&h->key, ((size_t)n + 1) * sizeof(int)));
-    cudaFree(h->start); cudaFree(h->count); cudaFree(h->cursor);
-    h->start = h->count = h->cursor = nullptr;
-    NBR_TRY(h, cudaMalloc((void**)&h->start, ((size_t)ncells + 1) * sizeof(int)));
-    NBR_TRY(h, cudaMalloc((void**)&h->count, (size_t)ncells * sizeof(int)));
-    NBR_TRY(h, cudaMalloc((void**)&h->cursor, (size_t)ncells * sizeof(int)));
+    /* buffers only grow, so rebuilding an index allocates nothing */
+    if ((rc = grow(h, &h->xs, h->cap_xs, (size_t)n * nd + 1)) != GPRM_OK) return rc;
+    if ((rc = grow(h, &h->id, h->cap_id, (size_t)n + 1)) != GPRM_OK) return rc;
+    if ((rc = grow(h, &h->key, h->cap_key, (size_t)n + 1)) != GPRM_OK) return rc;
+    if ((rc = grow(h, &h->start, h->cap_start, (size_t)ncells + 1)) != GPRM_OK) return rc;
+    if ((rc = grow(h, &h->count, h->cap_count, (size_t)ncells)) != GPRM_OK) return rc;
+    if ((rc = grow(h, &h->cursor, h->cap_cursor, (size_t)ncells)) != GPRM_OK) return rc;
     NBR_TRY(h, cudaMemsetAsync(h->count, 0, (size_t)ncells * sizeof(int), st));
     NBR_TRY(h, cudaMemsetAsync(h->cursor, 0, (size_t)ncells * sizeof(int), st));
     if (n > 0) k_cell_keys<<<h->sms * 8, 256, 0, st>>>(x, n, stride, g, h->key, h->count);
@@ -522,10 +616,16 @@ int gprm_nbr_knn(gprm_nbr* h, const float* q, int m, int qstride, int k, int que
     int rc = grow(h, &h->redo, h->cap_redo, (size_t)m);
     if (rc) return rc;
     NBR_TRY(h, cudaMemsetAsync(h->nredo, 0, sizeof(int), st));
-    const int threads = 128;
-    const int blocks = (int)((m + threads - 1) / threads);
-    k_knn_grid<<<blocks, threads, 0, st>>>(h->g, q, m, qstride, k, queries_are_nodes ? 1 : 0,
-                                           queries_are_nodes ? 1 : 0, idx, dist, h->redo, h->nredo);
+    if (queries_are_nodes) {
+        const int threads = 128;
+        const int blocks = (int)((m + threads - 1) / threads);
+        k_knn_grid<<<blocks, threads, 0, st>>>(h->g, m, k, idx, dist, h->redo, h->nredo);
+    } else {
+        const int wpb = 8;
+        const long long wblocks = ((long long)m + wpb - 1) / wpb;
+        const int blocks = (int)(wblocks < (long long)h->sms * 16 ? wblocks : (long long)h->sms * 16);
+        k_knn_grid_warp<<<blocks, 32 * wpb, 0, st>>>(h->g, q, m, qstride, k, idx, dist, h->redo, h->nredo);
+    }
     NBR_TRY(h, cudaGetLastError());
     k_knn_full<<<h->sms * 4, 256, 0, st>>>(h->x, h->n, h->xstride, q, qstride, h->ndof, k, queries_are_nodes ? 1 : 0,
                                            h->redo, h->nredo, idx, dist);

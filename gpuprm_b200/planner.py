@@ -20,8 +20,8 @@ start/goal queries; every collision verdict comes from the exact checker.
   components are exactly those of the fully checked graph: the same
   queries succeed.  With a trained ``CollisionMLP`` the samples with
   predicted P(collision) > ``prune`` are dropped before the vertex check
-  and edges are weighted by length * (1 + beta * p_edge) (p_edge: largest
-  prediction at three interior points), so likely-free edges are checked
+  and edges are weighted by length * (1 + beta * p_edge) (p_edge: the
+  prediction at the edge's midpoint), so likely-free edges are checked
   first and likely-colliding ones tend to become internal before their
   turn.  Without one, edges are weighted by length.
 * Every returned path is re-checked edge by edge with the all-steps policy
@@ -41,16 +41,47 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import scenes, workloads
+from . import scenes
 from ._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT
 from .graph import RoadmapGraph
 from .neighbours import NeighbourIndex
 
 
+class DevicePaths:
+    """The planner's answer kept on the device: for query t, the path is
+    start[t], verts[flat[off[t] : off[t] + length[t]]], goal[t] (length 0:
+    no path).  Host arrays are built on first access."""
+
+    def __init__(self, verts, length, off, flat, starts, goals):
+        self.verts, self.length, self.off, self.flat = verts, length, off, flat
+        self.starts, self.goals = starts, goals
+        self._host = None
+
+    def __len__(self):
+        return int(self.length.numel())
+
+    def found(self) -> np.ndarray:
+        return (self.length > 0).cpu().numpy()
+
+    def to_list(self):
+        if self._host is None:
+            pts = self.verts[self.flat.long()].cpu().numpy()
+            length, off = self.length.cpu().numpy(), self.off.cpu().numpy()
+            out = []
+            for t in range(len(length)):
+                if length[t] == 0:
+                    out.append(None)
+                    continue
+                out.append(np.concatenate([self.starts[t:t + 1], pts[off[t]:off[t] + length[t]],
+                                           self.goals[t:t + 1]]))
+            self._host = out
+        return self._host
+
+
 @dataclass
 class PlanResult:
     success: np.ndarray            # (Q,) bool
-    paths: list                    # list of (L, ndof) arrays or None
+    device_paths: DevicePaths      # paths on the device
     seconds: float                 # wall time for the whole query batch
     edge_checks: int               # edges sent to the exact checker
     edge_steps: int                # nominal edge steps checked
@@ -58,8 +89,32 @@ class PlanResult:
     info: dict = field(default_factory=dict)
 
     @property
+    def paths(self):
+        """list of (L, ndof) arrays (start ... goal) or None per query."""
+        return self.device_paths.to_list()
+
+    @property
     def time_to_path(self) -> float:
         return self.seconds / max(1, len(self.success))
+
+
+class _Phases:
+    """Wall time per planner phase (synchronising at each mark) when enabled."""
+
+    def __init__(self, on: bool):
+        self.on = on
+        self.t = {}
+        self.last = None
+
+    def mark(self, name):
+        if not self.on:
+            return
+        import torch
+        torch.cuda.synchronize()
+        now = time.perf_counter()
+        if self.last is not None:
+            self.t[name] = self.t.get(name, 0.0) + 1e3 * (now - self.last)
+        self.last = now
 
 
 def _check_edges(cs, qa, qb, policy=GPRM_EDGES_EARLY_EXIT):
@@ -87,25 +142,29 @@ def _components(graph, V, i, j, good):
     return graph.components(V, i, j, good)
 
 
-def _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k):
+def _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph=None):
     """Attaches every start and goal to its k nearest roadmap vertices by
     exactly checked edges, picks the first (start, goal) attachment pair in
     nearest-first order whose vertices share a component, and returns the
-    forest paths through the roadmap (all on the device).  Returns
-    (paths as host arrays or None, attachment edges checked)."""
+    forest paths through the roadmap, all on the device.  Returns
+    (DevicePaths, attachment edges checked)."""
     import torch
     dev = verts.device
     Q = starts.shape[0]
     V = verts.shape[0]
+    st = torch.as_tensor(starts, device=dev)
+    gl = torch.as_tensor(goals, device=dev)
     if V == 0:
-        return [None] * Q, 0
-    ends = torch.cat([torch.as_tensor(starts, device=dev), torch.as_tensor(goals, device=dev)])
+        z = torch.zeros(Q, dtype=torch.int32, device=dev)
+        return DevicePaths(verts, z, z.long(), z[:0], starts, goals), 0
+    ends = torch.cat([st, gl])
     kk = min(k, V)
-    index = NeighbourIndex(verts.shape[1])
-    index.build(verts.T.contiguous())
+    ph = ph or _Phases(False)
     nb = index.knn(kk, q=ends.T.contiguous())[0].long()                       # (2Q, kk)
+    ph.mark("attach_knn")
     qa = ends[:, None, :].expand(-1, kk, -1).reshape(-1, ends.shape[1])
     ok = (_check_edges(cs, qa, verts[nb.reshape(-1)]) == 0).reshape(2 * Q, kk)
+    ph.mark("attach_edges")
     lab = torch.where(ok, label[nb].long(), torch.full_like(nb, -1))
     ls, lg = lab[:Q], lab[Q:]
     match = (ls[:, :, None] == lg[:, None, :]) & (ls[:, :, None] >= 0)       # (Q, kk, kk)
@@ -116,31 +175,77 @@ def _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k):
     rows = torch.arange(Q, device=dev)
     vs = torch.where(has, nb[:Q][rows, a], torch.full_like(a, -1)).to(torch.int32)
     vt = torch.where(has, nb[Q:][rows, b], torch.full_like(b, -1)).to(torch.int32)
-    parent, depth, _ = graph.forest(V, i, j, label, good)
+    ph.mark("attach_match")
+    parent, depth, levels = graph.forest(V, i, j, label, good)
+    ph.mark("forest")
     length, off, flat_path = graph.paths(vs, vt, label, parent, depth)
-    pts = verts[flat_path.long()].cpu().numpy()
-    length, off = length.cpu().numpy(), off.cpu().numpy()
-    paths = []
-    for t in range(Q):
-        if length[t] == 0:
-            paths.append(None)
-            continue
-        paths.append(np.concatenate([starts[t:t + 1], pts[off[t]:off[t] + length[t]], goals[t:t + 1]]))
-    return paths, 2 * Q * kk
+    ph.mark("paths")
+    if ph.on:
+        ph.t["forest_levels"] = levels
+    return DevicePaths(verts, length, off, flat_path, starts, goals), 2 * Q * kk
 
 
-def verify_paths(cs, paths):
-    """Re-checks every edge of every path (all-steps policy); True if all free."""
+def verify_paths(cs, dp: DevicePaths):
+    """Re-checks every edge of every path with the all-steps policy (each
+    roadmap edge once, plus each path's start and goal segments); True if
+    all are free."""
     import torch
-    segs_a = [p[:-1] for p in paths if p is not None and len(p) > 1]
-    segs_b = [p[1:] for p in paths if p is not None and len(p) > 1]
-    if not segs_a:
+    if len(dp) == 0:
         return True
-    seg = np.unique(np.concatenate([np.concatenate(segs_a), np.concatenate(segs_b)], axis=1), axis=0)
-    d = seg.shape[1] // 2
-    qa = torch.tensor(seg[:, :d], device="cuda:0", dtype=torch.float32)
-    qb = torch.tensor(seg[:, d:], device="cuda:0", dtype=torch.float32)
+    length, off, flat, verts = dp.length.long(), dp.off, dp.flat.long(), dp.verts
+    dev = verts.device
+    found = length > 0
+    # roadmap segments: consecutive entries of the same path
+    if flat.numel() > 1:
+        owner = torch.repeat_interleave(torch.arange(len(dp), device=dev), length)
+        same = owner[1:] == owner[:-1]
+        u, v = flat[:-1][same], flat[1:][same]
+        V = verts.shape[0]
+        key = torch.unique(torch.minimum(u, v) * V + torch.maximum(u, v))
+        ra, rb = verts[key // V], verts[key % V]
+    else:
+        ra = rb = verts[:0]
+    st = torch.as_tensor(dp.starts, device=dev)[found]
+    gl = torch.as_tensor(dp.goals, device=dev)[found]
+    head = verts[flat[off[found]]]
+    tail = verts[flat[off[found] + length[found] - 1]]
+    qa = torch.cat([ra, st, tail])
+    qb = torch.cat([rb, head, gl])
     return bool((_check_edges(cs, qa, qb, GPRM_EDGES_ALL_STEPS) == 0).all().item())
+
+
+
+_WORKSPACES = {}
+
+
+def _workspace(ndof: int):
+    """The graph-operation and neighbour-index handles of a DOF, kept across
+    planner calls so that their device buffers are allocated once."""
+    ws = _WORKSPACES.get(ndof)
+    if ws is None:
+        ws = (RoadmapGraph(), NeighbourIndex(ndof))
+        _WORKSPACES[ndof] = ws
+    return ws
+
+
+def _index_and_pairs(index, verts, k):
+    """Indexes the roadmap vertices (the index is reused for the queries)
+    and returns the undirected k-nearest-neighbour candidate edges (i < j,
+    int64)."""
+    import torch
+    V = verts.shape[0]
+    if V < 2:
+        e = torch.empty(0, dtype=torch.int64, device=verts.device)
+        if V:
+            index.build(verts.T.contiguous())
+        return e, e
+    index.build(verts.T.contiguous())
+    idx, _ = index.knn(min(k, V - 1))
+    rows = torch.arange(V, device=verts.device)[:, None].expand_as(idx)
+    valid = idx >= 0
+    a, b = rows[valid].long(), idx[valid].long()
+    key = torch.unique(torch.minimum(a, b) * V + torch.maximum(a, b))
+    return key // V, key % V
 
 
 def _sample(scene, n, seed):
@@ -153,55 +258,71 @@ def _sample(scene, n, seed):
     return lo + (hi - lo) * torch.rand((n, scene.ndof), device="cuda:0", generator=g)
 
 
-def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0) -> PlanResult:
+def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False) -> PlanResult:
     """Eager GPU PRM: every vertex and every candidate edge checked."""
     import torch
     s0 = cs.stats()["edge_steps_nominal"]
-    graph = RoadmapGraph()
+    graph, index = _workspace(scene.ndof)
+    ph = _Phases(profile)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    ph.mark(None)
     q = _sample(scene, n_samples, seed)
     verts = q[_check_vertices(cs, q) == 0]
-    i, j = workloads.knn_pairs(verts, k)
+    ph.mark("vertices")
+    i, j = _index_and_pairs(index, verts, k)
     i, j = i.to(torch.int32), j.to(torch.int32)
+    ph.mark("knn")
     good = (_check_edges(cs, verts[i.long()], verts[j.long()]) == 0).to(torch.uint8)
+    ph.mark("edges")
     V = verts.shape[0]
     label = _components(graph, V, i, j, good)
-    paths, nconn = _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k)
-    ok = verify_paths(cs, paths)
+    ph.mark("components")
+    dp, nconn = _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph)
+    ph.mark("queries")
+    ok = verify_paths(cs, dp)
+    ph.mark("verify")
+    found = dp.found()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return PlanResult(np.array([p is not None for p in paths]), paths, dt, int(i.numel()) + nconn,
+    return PlanResult(found, dp, dt, int(i.numel()) + nconn,
                       int(cs.stats()["edge_steps_nominal"] - s0), n_samples,
-                      {"verified": ok, "free_vertices": V, "candidate_edges": int(i.numel())})
+                      {"verified": ok, "free_vertices": V, "candidate_edges": int(i.numel()),
+                       **({"phases_ms": ph.t} if profile else {})})
 
 
 def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=0.9, beta=4.0,
-             batch_frac=1.0, min_batch=4096, max_rounds=2, first=2) -> PlanResult:
+             batch_frac=1.0, min_batch=4096, max_rounds=2, first=2, profile=False) -> PlanResult:
     """Batched lazy-Kruskal PRM (exact connectivity), optionally MLP-guided;
     the roadmap and its bookkeeping stay on the device."""
     import torch
     s0 = cs.stats()["edge_steps_nominal"]
-    graph = RoadmapGraph()
+    graph, index = _workspace(scene.ndof)
+    ph = _Phases(profile)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    ph.mark(None)
     q = _sample(scene, n_samples, seed)
     pruned = 0
     if mlp is not None:
         keep = mlp.predict(q.T.contiguous()) <= prune
         pruned = int((~keep).sum().item())
         q = q[keep]
+        ph.mark("predict_samples")
     verts = q[_check_vertices(cs, q) == 0]
     vchecks = int(q.shape[0])
-    i64, j64 = workloads.knn_pairs(verts, k)
+    ph.mark("vertices")
+    i64, j64 = _index_and_pairs(index, verts, k)
+    ph.mark("knn")
     i, j = i64.to(torch.int32), j64.to(torch.int32)
     V, E = verts.shape[0], int(i.numel())
     dev = verts.device
     length = torch.linalg.norm(verts[i64] - verts[j64], dim=1)
     if mlp is not None and E:
-        pts = torch.cat([verts[i64] + t * (verts[j64] - verts[i64]) for t in (0.25, 0.5, 0.75)])
-        pe = mlp.predict(pts.T.contiguous()).reshape(3, -1).max(0).values
+        mid = 0.5 * (verts[i64] + verts[j64])
+        pe = mlp.predict(mid.T.contiguous())
         cost = length * (1.0 + beta * pe)
+        ph.mark("predict_edges")
     else:
         cost = length
     good = torch.zeros(E, dtype=torch.uint8, device=dev)
@@ -225,7 +346,9 @@ def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=
     startpos = torch.searchsorted(ev, torch.arange(V, device=dev))
     rank = torch.arange(2 * E, device=dev) - startpos[ev]
     r1 = torch.unique(eid[o][rank < m])
+    ph.mark("round1_select")
     free1 = run(r1)
+    ph.mark("round1_edges")
     rounds = [int(r1.numel())]
     order = torch.argsort(cost, stable=True)
     for rnd in range(max_rounds):
@@ -235,18 +358,24 @@ def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=
         if cross.numel() == 0:
             break
         take = cross if rnd == max_rounds - 1 else cross[:max(min_batch, int(cross.numel() * batch_frac))]
+        ph.mark("round_select")
         run(take)
         rounds.append(int(take.numel()))
+        ph.mark("round_edges")
     label = _components(graph, V, i, j, good)
-    paths, nconn = _answer_queries(cs, graph, verts, i, j, good, label, starts, goals, k)
-    ok = verify_paths(cs, paths)
+    ph.mark("components")
+    dp, nconn = _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph)
+    ph.mark("queries")
+    ok = verify_paths(cs, dp)
+    ph.mark("verify")
+    found = dp.found()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return PlanResult(np.array([p is not None for p in paths]), paths, dt, int(checked.sum().item()) + nconn,
+    return PlanResult(found, dp, dt, int(checked.sum().item()) + nconn,
                       int(cs.stats()["edge_steps_nominal"] - s0), vchecks,
                       {"verified": ok, "free_vertices": V, "candidate_edges": E, "round1_edges": rounds[0],
                        "round1_free": free1, "later_edges": int(sum(rounds[1:])), "rounds": len(rounds),
-                       "pruned": pruned})
+                       "pruned": pruned, **({"phases_ms": ph.t} if profile else {})})
 
 
 def make_queries(cs, scene, n_queries, seed):
