@@ -22,6 +22,15 @@ One step = one pass of the edge checker over the whole edge batch.
          reference sources) on a bounded sample of the same edges, all host
          cores, one checker instance per thread.
 
+Extra legs in the same line (not part of `value`):
+  prm        learned-guided vs plain GPU PRM time-to-path on the same scene
+             (2^20 samples, 1000 seeded queries; the predictor is trained on
+             2^20 exact-checker labels by the library's BF16 kernels);
+  prm_stress the same on the 7-DOF wall scene (512 obstacles, two walls with
+             a 0.12 m gap, dq 0.005, k 16, 2^17 samples);
+  batch      256 independent problems in one graph-captured launch per kind
+             against a loop of per-problem launches.
+
 --impl reference times only that CPU checker (same metric/config).
 """
 from __future__ import annotations

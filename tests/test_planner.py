@@ -38,9 +38,14 @@ def test_learned_guidance_prunes_and_keeps_paths_verified():
     starts, goals = planner.make_queries(cs, sc, 200, seed=5)
     plain = planner.plain_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=6)
     learned = planner.lazy_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=6, mlp=mlp)
+    lazy = planner.lazy_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=6)
     assert learned.info["verified"]
     assert learned.info["pruned"] > 0
     assert learned.edge_steps < plain.edge_steps
+    # what the network adds to the same lazy planner on the same samples:
+    # fewer vertex checks (pruning) and fewer cross-component checks (ordering)
+    assert learned.vertex_checks < lazy.vertex_checks
+    assert learned.info["later_edges"] < lazy.info["later_edges"]
     # every reported path connects its own start and goal
     for i, p in enumerate(learned.paths):
         if p is not None:
