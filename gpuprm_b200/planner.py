@@ -258,8 +258,10 @@ def _sample(scene, n, seed):
     return lo + (hi - lo) * torch.rand((n, scene.ndof), device="cuda:0", generator=g)
 
 
-def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False) -> PlanResult:
-    """Eager GPU PRM: every vertex and every candidate edge checked."""
+def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, keep_roadmap=False) -> PlanResult:
+    """Eager GPU PRM: every vertex and every candidate edge checked.  With
+    keep_roadmap, info["roadmap"] = (vertices, free-edge ends i, j) as host
+    arrays (copied after the timed region), e.g. for results.store_plan."""
     import torch
     s0 = cs.stats()["edge_steps_nominal"]
     graph, index = _workspace(scene.ndof)
@@ -285,10 +287,13 @@ def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False) 
     found = dp.found()
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    info = {"verified": ok, "free_vertices": V, "candidate_edges": int(i.numel()),
+            **({"phases_ms": ph.t} if profile else {})}
+    if keep_roadmap:
+        g = good.bool()
+        info["roadmap"] = (verts.cpu().numpy(), i[g].cpu().numpy(), j[g].cpu().numpy())
     return PlanResult(found, dp, dt, int(i.numel()) + nconn,
-                      int(cs.stats()["edge_steps_nominal"] - s0), n_samples,
-                      {"verified": ok, "free_vertices": V, "candidate_edges": int(i.numel()),
-                       **({"phases_ms": ph.t} if profile else {})})
+                      int(cs.stats()["edge_steps_nominal"] - s0), n_samples, info)
 
 
 def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=0.9, beta=4.0,

@@ -23,17 +23,44 @@
  * into a loop running past its bound at -O1 and above, and into a trap at
  * -O0 unless unreachable traps are off.
  *
+ * --dump DIR writes the planner's final roadmaps as raw arrays (blocks,
+ * node storage, adjacency with float weights, start/end positions, the
+ * Dijkstra path) so that a test can feed them to another store_results
+ * writer and compare its files with the planner's own.
+ *
  * --mode fp32 (default) runs the B200 checker in FP32 mode, whose verdicts
  * equal the reference's, so both runs draw the same random numbers and
  * build the same roadmap; --mode band enables the FP64 near-contact recheck.
  */
 #include <mpi.h>
 
+/* standard headers first: the planner's members are opened for --dump only */
+#include <assert.h>
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <queue>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#define private public
+#define protected public
 #include "prm/prmsolver.h"
+#undef private
+#undef protected
 #include "robotspace/robotconfigspace.cpp"
 #include "gprm_configspace.hpp"
 
 #include <fcntl.h>
+#include <sys/stat.h>
 #include <unistd.h>
 
 #include <chrono>
@@ -116,9 +143,44 @@ private:
     std::map<int, Pending> pending_;
 };
 
+template <class T>
+static void dump_array(const std::string& path, const T* p, size_t n)
+{
+    FILE* f = fopen(path.c_str(), "wb");
+    if (!f) return;
+    if (n) fwrite(p, sizeof(T), n, f);
+    fclose(f);
+}
+
+/* One roadmap as raw arrays: meta = [ndof, blocknum, newblockpos, start,
+ * end, path length]; blocks = (pos, num) per block; qstorage; surrnum;
+ * adjacency in CSR over positions with float weights; path positions. */
+template <class G, class D>
+static void dump_graph(const std::string& dir, const G& g, const D& d, int start, int end, bool with_path)
+{
+    const int n = g.newblockpos;
+    std::vector<int> meta = {4, g.blocknum, n, start, end, with_path ? (int)d.path.size() : 0};
+    dump_array(dir + "/meta.bin", meta.data(), meta.size());
+    std::vector<int> blocks;
+    for (int l = 0; l < g.blocknum; ++l) { blocks.push_back(g.blocks[l].pos); blocks.push_back(g.blocks[l].num); }
+    dump_array(dir + "/blocks.bin", blocks.data(), blocks.size());
+    dump_array(dir + "/qstorage.bin", g.qstorage.data(), (size_t)4 * n);
+    dump_array(dir + "/surrnum.bin", g.surrnum.data(), (size_t)n);
+    std::vector<int> off(1, 0), dest;
+    std::vector<float> w;
+    for (int p = 0; p < n; ++p) {
+        for (size_t i = 0; i < g.edgelists[p].size(); ++i) { dest.push_back(g.edgelists[p][i]); w.push_back(g.edgeweights[p][i]); }
+        off.push_back((int)dest.size());
+    }
+    dump_array(dir + "/adj_off.bin", off.data(), off.size());
+    dump_array(dir + "/adj_dest.bin", dest.data(), dest.size());
+    dump_array(dir + "/adj_w.bin", w.data(), w.size());
+    if (with_path) dump_array(dir + "/path.bin", d.path.data(), d.path.size());
+}
+
 int main(int argc, char** argv)
 {
-    std::string checker = "ref", config, out, mode = "fp32", trace;
+    std::string checker = "ref", config, out, mode = "fp32", trace, dump;
     int num = 32, nbuf = 2048, seed = 0, blocksize = 256, workerversion = 1, maxsteps = 10000;
     int maxstorage = 1024 * 1024;
     float dq = 0.01f, distD = 1.0f, distH = 1.0f;
@@ -138,6 +200,7 @@ int main(int argc, char** argv)
         else if (k == "--blocksize") blocksize = atoi(v.c_str());
         else if (k == "--mode") mode = v;
         else if (k == "--trace") trace = v;
+        else if (k == "--dump") dump = v;
         else { fprintf(stderr, "unknown argument %s\n", k.c_str()); return 2; }
     }
     if (config.empty() || out.empty() || (checker != "ref" && checker != "b200")) {
@@ -191,6 +254,18 @@ int main(int argc, char** argv)
     const int found = prm.process_mpi5(num, nbuf, maxsteps, seed, workerversion);
     auto t3 = std::chrono::steady_clock::now();
     prm.store_results(out);
+    if (!dump.empty()) {
+        /* the arguments store_results gives store_graph (prmsolver.cpp:2965-2976) */
+        mkdir(dump.c_str(), 0755);
+        mkdir((dump + "/graphl").c_str(), 0755);
+        mkdir((dump + "/graphr").c_str(), 0755);
+        dump_graph(dump + "/graphl", prm.graphl, prm.dijkstral, prm.i0l, prm.connection.index_left,
+                   prm.connection_found);
+        dump_graph(dump + "/graphr", prm.graphr, prm.dijkstrar, prm.connection.index_right, prm.i0r,
+                   prm.connection_found);
+        int cf = prm.connection_found ? 1 : 0;
+        dump_array(dump + "/connection.bin", &cf, 1);
+    }
     MPI_Finalize();
     if (tf) fclose(tf);
 

@@ -33,11 +33,22 @@ def test_fixture_is_complete():
 
 @needs_bin
 @pytest.mark.skipif(not os.path.isdir("/root/reference/prm"), reason="reference tree absent")
-def test_reference_run_reproduces_fixture(tmp_path):
-    line, files = G.run_planner("ref", str(tmp_path))
+def test_reference_run_reproduces_fixture_and_writer_matches_store_results(tmp_path):
+    """The reference run still gives the fixture, and gpuprm_b200.results,
+    fed the planner's final roadmaps (raw arrays dumped by the harness),
+    writes the same 33 files byte for byte as the planner's own
+    store_results (prmsolver.cpp:2947-3055)."""
+    from gpuprm_b200 import results as R
+    dump = str(tmp_path / "dump")
+    line, files = G.run_planner("ref", str(tmp_path), ["--dump", dump])
     assert files == FIX["files"]
     for k, v in FIX["counters"].items():
         assert line[k] == v, k
+    connected = open(os.path.join(dump, "connection.bin"), "rb").read()[0] == 1
+    mine = str(tmp_path / "mine")
+    R.store_results(mine, R.load_dump(os.path.join(dump, "graphl")), R.load_dump(os.path.join(dump, "graphr")),
+                    connected)
+    assert G.digest_outputs(mine) == FIX["files"]
 
 
 @needs_bin
