@@ -79,6 +79,7 @@ def parse():
     ap.add_argument("--no-stress", action="store_true", help="skip the 7-DOF wall planner comparison")
     ap.add_argument("--stress-samples", type=int, default=1 << 17)
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
+    ap.add_argument("--no-sampler", action="store_true", help="skip the near-node sampler leg")
     ap.add_argument("--batch-problems", type=int, default=256)
     return ap.parse_args()
 
@@ -311,6 +312,9 @@ def run_ours(args, rank, world, local_rank):
     batch = None
     if not args.no_batch and world == 1:
         batch = batch_leg(args, dev, policy)
+    sampler = None
+    if not args.no_sampler and world == 1:
+        sampler = sampler_leg(args, ws, dev)
     line = {
         "metric": METRIC, "value": nominal_all / t_max, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
@@ -324,7 +328,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-        "prm": prm, "prm_stress": prm_stress, "batch": batch,
+        "prm": prm, "prm_stress": prm_stress, "batch": batch, "sampler": sampler,
     }
     return line
 
@@ -347,6 +351,44 @@ def prm_leg(args, kind, dq, n_samples, k):
     out["scene"] = {"kind": kind, "ndof": psc.ndof, "polytopes": len(psc.polys), "pairs": len(psc.pair_from)}
     out["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
                         "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
+    return out
+
+
+def sampler_leg(args, ws, dev):
+    """Near-node sampling with the reference's acceptance rule
+    (get_random_nodes, prmsolver.cpp:2585-2624): 2^18 accepted, free
+    samples near the workload's free vertices (surrnum = their kNN degree,
+    D = 0.5, power 3) in batches of 2^16 candidates, against the CPU
+    restatement (one core) on a bounded number of samples."""
+    import torch
+    from gpuprm_b200 import workloads
+    from gpuprm_b200.sampler import sample_near
+    cs = ws["space"]
+    nodes = ws["q_soa"][:, ws["codes"] == 0].contiguous()
+    i, j = workloads.knn_pairs(nodes.T.contiguous(), 10)
+    surr = torch.bincount(torch.cat([i, j]), minlength=nodes.shape[1]).to(torch.int32)
+    num = 1 << 18
+    sample_near(cs, nodes, surr, 1024, 0.5, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    q, par, used = sample_near(cs, nodes, surr, num, 0.5, seed=args.seed + 3)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    out = {"samples": num, "candidates": int(used), "seconds": dt, "samples_per_s": num / dt,
+           "accepted_free_per_candidate": num / max(1, used), "nodes": int(nodes.shape[1])}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        import sampler_oracle as SO
+        orc = O.Oracle(ws["scene"])
+        free = lambda qq: orc.check_configs(qq, O.FP32_BAND | O.DEVICE_TRIG)[0] == 0
+        nodes_np, surr_np = nodes.T.cpu().numpy(), surr.cpu().numpy()
+        m = 2048
+        t0 = time.perf_counter()
+        SO.sample_near(nodes_np, surr_np, 3, 0.5, args.seed + 3, m, free, batch=4096)
+        cdt = time.perf_counter() - t0
+        out["cpu_port"] = {"samples": m, "seconds": cdt, "samples_per_s": m / cdt, "cores": 1,
+                           "kind": "port (numpy restatement + oracle vertex check)"}
     return out
 
 

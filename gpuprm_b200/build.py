@@ -9,7 +9,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "libgprm_b200.so")
-SOURCES = ["gprm_api.cu", "gprm_batch.cu", "gprm_kernels.cu", "gprm_mlp.cu", "gprm_nbr.cu", "gprm_graph.cu"]
+SOURCES = ["gprm_api.cu", "gprm_batch.cu", "gprm_kernels.cu", "gprm_mlp.cu", "gprm_nbr.cu", "gprm_graph.cu", "gprm_sample.cu"]
 HEADERS = ["gprm_device.cuh", "gprm_host.h", "gprm_internal.h", "gprm_sincos64.h"]
 
 NVCC_FLAGS = [

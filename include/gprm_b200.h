@@ -359,6 +359,21 @@ int  gprm_graph_sssp(gprm_graph* h, int V, int E, const int* eu, const int* ev,
                      const unsigned char* mask, const float* w, int src, float* dist, int* parent,
                      int* rounds, void* stream);
 
+/* ---- sampling near roadmap nodes ----------------------------------------
+ * get_random_nodes (prmsolver.cpp:2585-2624; get_random_nodes2 :2635-2698
+ * with power 2) as a batch: candidate t (t = t0 .. t0+B-1) picks node m
+ * uniformly among n device nodes[m + stride*j], is accepted when its 31-bit
+ * random value r <= (2^31-1) / (1+surrnum[m])^power (the reference's integer
+ * test) and becomes q = (nodes[m] - D) + (2*D) * ((float)r' / 2^31) per
+ * joint.  Writes q_out[t - t0 + out_stride*j] and parent_out[t - t0] = m, or
+ * -1 when the candidate is dismissed.  Random numbers: Philox4x32-10 with key
+ * = seed and counters (t, 0..2), so (seed, t) fixes a candidate.  The caller
+ * vertex-checks the accepted candidates (gprm_indicator_batch_device).
+ * Device pointers; asynchronous on `stream`. */
+int gprm_sample_near(int ndof, const float* nodes, int n, int stride, const int* surrnum, int power,
+                     float D, unsigned long long seed, long long t0, int B, float* q_out, int out_stride,
+                     int* parent_out, void* stream);
+
 /* ---- diagnostics (no counterpart in the reference) -------------------- */
 
 /* The FP32 frames the kernels compute for one configuration q[ndof]:
