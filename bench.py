@@ -356,9 +356,9 @@ def prm_leg(args, kind, dq, n_samples, k):
 
 def sampler_leg(args, ws, dev):
     """Near-node sampling with the reference's acceptance rule
-    (get_random_nodes, prmsolver.cpp:2585-2624): 2^18 accepted, free
-    samples near the workload's free vertices (surrnum = their kNN degree,
-    D = 0.5, power 3) in batches of 2^16 candidates, against the CPU
+    (get_random_nodes2, prmsolver.cpp:2635-2698: power 2): 2^16 accepted,
+    free samples near the workload's free vertices (surrnum = their kNN
+    degree, D = 0.5) in batches of 2^20 candidates, against the CPU
     restatement (one core) on a bounded number of samples."""
     import torch
     from gpuprm_b200 import workloads
@@ -367,15 +367,17 @@ def sampler_leg(args, ws, dev):
     nodes = ws["q_soa"][:, ws["codes"] == 0].contiguous()
     i, j = workloads.knn_pairs(nodes.T.contiguous(), 10)
     surr = torch.bincount(torch.cat([i, j]), minlength=nodes.shape[1]).to(torch.int32)
-    num = 1 << 18
-    sample_near(cs, nodes, surr, 1024, 0.5, seed=1)
+    num, power, batch = 1 << 16, 2, 1 << 20
+    sample_near(cs, nodes, surr, 1024, 0.5, seed=1, power=power, batch=batch)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    q, par, used = sample_near(cs, nodes, surr, num, 0.5, seed=args.seed + 3)
+    q, par, used = sample_near(cs, nodes, surr, num, 0.5, seed=args.seed + 3, power=power, batch=batch)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    out = {"samples": num, "candidates": int(used), "seconds": dt, "samples_per_s": num / dt,
-           "accepted_free_per_candidate": num / max(1, used), "nodes": int(nodes.shape[1])}
+    got = int(q.shape[1])
+    out = {"samples": got, "requested": num, "power": power, "candidates": int(used), "seconds": dt,
+           "samples_per_s": got / dt, "candidates_per_s": used / dt,
+           "accepted_free_per_candidate": got / max(1, used), "nodes": int(nodes.shape[1])}
     if not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
@@ -383,9 +385,9 @@ def sampler_leg(args, ws, dev):
         orc = O.Oracle(ws["scene"])
         free = lambda qq: orc.check_configs(qq, O.FP32_BAND | O.DEVICE_TRIG)[0] == 0
         nodes_np, surr_np = nodes.T.cpu().numpy(), surr.cpu().numpy()
-        m = 2048
+        m = 1024
         t0 = time.perf_counter()
-        SO.sample_near(nodes_np, surr_np, 3, 0.5, args.seed + 3, m, free, batch=4096)
+        SO.sample_near(nodes_np, surr_np, power, 0.5, args.seed + 3, m, free, batch=1 << 16)
         cdt = time.perf_counter() - t0
         out["cpu_port"] = {"samples": m, "seconds": cdt, "samples_per_s": m / cdt, "cores": 1,
                            "kind": "port (numpy restatement + oracle vertex check)"}
