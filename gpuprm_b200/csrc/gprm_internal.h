@@ -70,14 +70,17 @@ cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const
                                  const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
 
 /* Per-lane shared floats of a warp's block: frames 1..ndof (12 floats
- * each), the ball centres of the slots (3 floats each), lane-interleaved,
- * then SWEEP_LANE_FLOATS per lane that together hold the warp's per-slot
+ * each), the ball centres of the slots (3 floats each), lane-interleaved;
+ * then DEFER_LANE_FLOATS per lane, together the warp's queue of deferred
+ * exact pair tests (64 items) and one batch's results (32 codes, 32
+ * margins); then SWEEP_LANE_FLOATS per lane, together the warp's per-slot
  * sweep balls (GPRM_MAX_SLOTS float4). */
 #define SWEEP_LANE_FLOATS 2
 static_assert(SWEEP_LANE_FLOATS * 32 >= GPRM_MAX_SLOTS * 4, "sweep area too small");
+#define DEFER_LANE_FLOATS 4
 __host__ __device__ __forceinline__ size_t lane_floats(const DevScene& sc)
 {
-    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 3 + SWEEP_LANE_FLOATS;
+    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 3 + DEFER_LANE_FLOATS + SWEEP_LANE_FLOATS;
 }
 
 /* Scene bytes when staged in shared memory; per-lane frame bytes of a block. */

@@ -60,6 +60,7 @@ struct SceneView {
     float* frames;   /* this lane's frames (lane-interleaved, stride 32) */
     float* cen;      /* this lane's slot ball centres */
     float4* sweep;   /* the warp's per-slot sweep balls (GPRM_MAX_SLOTS) */
+    unsigned* defer; /* the warp's deferred-test queue (64) and batch results (32 + 32) */
 };
 
 /* The warp's sweep area: the last SWEEP_LANE_FLOATS entries of its block. */
@@ -67,6 +68,14 @@ __device__ __forceinline__ float4* sweep_area(const DevScene& sc, float* lane_fr
 {
     const int lane = threadIdx.x & 31;
     return reinterpret_cast<float4*>(lane_frames - lane + (lane_floats(sc) - SWEEP_LANE_FLOATS) * 32);
+}
+
+/* The warp's deferred-test area: the DEFER_LANE_FLOATS entries before the sweep area. */
+__device__ __forceinline__ unsigned* defer_area(const DevScene& sc, float* lane_frames)
+{
+    const int lane = threadIdx.x & 31;
+    return reinterpret_cast<unsigned*>(lane_frames - lane +
+                                       (lane_floats(sc) - SWEEP_LANE_FLOATS - DEFER_LANE_FLOATS) * 32);
 }
 
 /* Copies the scene into shared memory (SMEM) and returns the pointers the
@@ -107,6 +116,7 @@ __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned ch
     s.frames = reinterpret_cast<float*>(smem + off) + (size_t)warp * lane_floats(sc) * 32 + lane;
     s.cen = s.frames + (size_t)sc.ndof * 12 * 32;
     s.sweep = sweep_area(sc, s.frames);
+    s.defer = defer_area(sc, s.frames);
     __syncthreads();
     return s;
 }
@@ -276,6 +286,118 @@ __device__ __forceinline__ void flush_counts(PairCounts pc, Control* ctl)
     }
 }
 
+/* ------------------------------------------------------------------ */
+/* deferred exact pair tests                                            */
+/* ------------------------------------------------------------------ */
+/*
+ * Within a chunk of 32 pairs, the pairs a lane must test exactly are not run
+ * where they are found (where most of the warp would idle) but queued as
+ * items (owner lane, pair - j0) in the warp's shared area; every 32 items
+ * the whole warp runs one each on its owner's frames.  Items reach the
+ * queue in pair order, so each owner applies its results in pair order:
+ * the first colliding pair decides its code (later items are ignored) and
+ * the free ones before it feed its minimum margin, exactly as the
+ * sequential loop.  first_k records the chunk index of that first
+ * collision (DEFER_NONE: none in this chunk).
+ *
+ * Vertex checks use it: their lanes hold unrelated configurations, so the
+ * pairs left to test differ from lane to lane (measured on hull6 with 2^20
+ * samples: 11.0 -> 8.6 ms).  The lanes of an edge check hold neighbouring
+ * steps of one edge, which mostly need the same pairs; there the queue
+ * costs more than it saves (357 -> 436 ms) and the sequential loop stays.
+ */
+constexpr int DEFER_NONE = 32;
+
+struct LaneState {
+    int code;
+    float mdec, mmin;
+    bool active;
+    int first_k;
+};
+
+__device__ __forceinline__ void defer_push(unsigned* q, int& n, bool want, int k)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(FULL_MASK, want);
+    if (want) q[n + __popc(m & ((1u << lane) - 1u))] = (unsigned)lane | ((unsigned)k << 5);
+    n += __popc(m);
+}
+
+/* Runs the first cnt (<= 32) queued items, one per lane, and lets every
+ * owner apply its results; the remaining items move to the front. */
+__device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S, int j0, int& n, int cnt,
+                                          LaneState& st, PairCounts& pc)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned* q = S.defer;
+    int* rcode = reinterpret_cast<int*>(q + 64);
+    float* rm = reinterpret_cast<float*>(q + 96);
+    __syncwarp();
+    int c = 0;
+    float m = 0.0f;
+    if (lane < cnt) {
+        const unsigned it = q[lane];
+        const int owner = (int)(it & 31u);
+        const int4 pr = S.pairs[j0 + (int)(it >> 5)];
+        Frame<float> tp, tq;
+        pair_frames(S.frames - lane + owner, pr, tp, tq);
+        c = pair_test<PF32>(sc, S.tab, pr, tp, tq, &m);
+        ++pc.full;
+    }
+    rcode[lane] = c;
+    rm[lane] = m;
+    __syncwarp();
+#pragma unroll 1
+    for (int t = 0; t < cnt; ++t) {
+        const unsigned it = q[t];
+        if ((int)(it & 31u) == lane && st.first_k == DEFER_NONE) {
+            const int ct = rcode[t];
+            if (ct != 0) {
+                st.code = ct;
+                st.mdec = rm[t];
+                st.first_k = (int)(it >> 5);
+                st.active = false;
+            } else {
+                st.mmin = min_nan(st.mmin, rm[t]);
+            }
+        }
+    }
+    const int rest = n - cnt;
+    __syncwarp();
+    const unsigned mv = lane < rest ? q[cnt + lane] : 0u;
+    __syncwarp();
+    if (lane < rest) q[lane] = mv;
+    n = rest;
+    __syncwarp();
+}
+
+/* One chunk's ordered pass with deferral: the direction certificate runs
+ * where a pair is found; pairs it does not settle are queued. */
+__device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView& S, int j0, unsigned need,
+                                            unsigned todo, LaneState& st, PairCounts& pc)
+{
+    int n = 0;
+    st.first_k = DEFER_NONE;
+    while (todo) {
+        const int k = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        bool full = false;
+        if (st.active && ((need >> k) & 1u)) {
+            const int j = j0 + k;
+            bool used_dir;
+            if (pair_certified(sc, S.tab, S.pairs[j], S.pairs_b[j], S.cen, S.frames, &used_dir)) {
+                if (used_dir) ++pc.dir;
+                else ++pc.far;
+            } else {
+                full = true;
+            }
+        }
+        defer_push(S.defer, n, full, k);
+        if (n >= 32) defer_run(sc, S, j0, n, 32, st, pc);
+    }
+    while (n > 0) defer_run(sc, S, j0, n, n < 32 ? n : 32, st, pc);
+}
+
 /* Appends the items of the lanes with `want` set, one atomic per warp. */
 __device__ __forceinline__ void warp_append(bool want, uint2 item, uint2* queue, unsigned qcap,
                                             Control* ctl)
@@ -322,29 +444,22 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
             if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
     }
     if (active) forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
-    float mmin = PF32::inf(), mdec = 0.0f;
+    LaneState st{code, 0.0f, PF32::inf(), active, DEFER_NONE};
     /* pairs in chunks of 32: the order-free distance scan, then the
-       remaining pairs of the chunk in the reference's order */
+       remaining pairs of the chunk in the reference's order, their exact
+       tests deferred and run by the whole warp */
 #pragma unroll 1
     for (int j0 = 0; j0 < sc.npairs; j0 += 32) {
-        if (!__any_sync(FULL_MASK, active)) break;
+        if (!__any_sync(FULL_MASK, st.active)) break;
         const int jn = min(32, sc.npairs - j0);
         unsigned need = far_scan(S, j0, jn);
-        if (!active) need = 0u;
+        if (!st.active) need = 0u;
         else pc.far += (unsigned)(jn - __popc(need));
-        unsigned todo = __reduce_or_sync(FULL_MASK, need);
-        while (todo) {
-            const int k = __ffs(todo) - 1;
-            todo &= todo - 1u;
-            if (active && ((need >> k) & 1u)) {
-                float m;
-                bool hm;
-                int r = eval_pair(sc, S, j0 + k, &m, &hm, pc);
-                if (r != 0) { code = r; mdec = m; active = false; }
-                else if (hm) mmin = min_nan(mmin, m);
-            }
-        }
+        const unsigned todo = __reduce_or_sync(FULL_MASK, need);
+        defer_chunk(sc, S, j0, need, todo, st, pc);
     }
+    code = st.code;
+    const float mmin = st.mmin, mdec = st.mdec;
     if (valid) {
         exec += (code != 1);
         res[i] = code;
@@ -775,6 +890,7 @@ __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene
     S.frames = frames;
     S.cen = frames + (size_t)wsc->ndof * 12 * 32;
     S.sweep = sweep_area(*wsc, frames);
+    S.defer = defer_area(*wsc, frames);
 }
 
 __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __restrict__ q, long long offset,
