@@ -28,6 +28,10 @@ Extra legs in the same line (not part of `value`):
              2^20 exact-checker labels by the library's BF16 kernels);
   prm_stress the same on the 7-DOF wall scene (512 obstacles, two walls with
              a 0.12 m gap, dq 0.005, k 16, 2^17 samples);
+  stress_edges  checker throughput on the 7-DOF wall scene at full size
+             (2^22 samples, k=16, dq 0.005): vertex checks/s and edge-step
+             checks/s on 2^21 of the roadmap's edges, with the reference CPU
+             checker on a bounded sample of them;
   batch      256 independent problems in one graph-captured launch per kind
              against a loop of per-problem launches.
 
@@ -78,6 +82,8 @@ def parse():
     ap.add_argument("--prm-samples", type=int, default=1 << 20)
     ap.add_argument("--no-stress", action="store_true", help="skip the 7-DOF wall planner comparison")
     ap.add_argument("--stress-samples", type=int, default=1 << 17)
+    ap.add_argument("--no-stress-edges", action="store_true", help="skip the 7-DOF wall checker throughput leg")
+    ap.add_argument("--stress-edges", type=int, default=1 << 21, help="roadmap edges the stress leg checks")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
     ap.add_argument("--no-sampler", action="store_true", help="skip the near-node sampler leg")
     ap.add_argument("--batch-problems", type=int, default=256)
@@ -138,23 +144,26 @@ class ClockSampler:
 # CPU leg (GPUPRM's own CPU checker; the oracle restatement if it is absent)
 # --------------------------------------------------------------------------
 
-def cpu_reference_rate(scene, qs_np, qe_np, dq, seconds, seed=0):
+def cpu_reference_rate(scene, qs_np, qe_np, dq, seconds, seed=0, count_ops=True):
     """Times the reference CPU checker on a bounded sample of the edges with
     all host cores.  Returns (dict for cpu_baseline, work counts): the
     reference algorithm's FP32 operations per step and per pair test,
-    counted by the oracle's instrumented restatement on 256 of the edges."""
+    counted by the oracle's instrumented restatement on 256 of the edges
+    (None without count_ops)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
     rng = np.random.default_rng(seed + 77)
     order = rng.permutation(qs_np.shape[0])
     orc = O.Oracle(scene)
-    cnt_idx = order[:256]
-    ops = orc.count_ops_edges(qs_np[cnt_idx], qe_np[cnt_idx], dq)
-    tn_cnt = orc.testnum(qs_np[cnt_idx], qe_np[cnt_idx], dq)
-    flops = ops["add"] + ops["mul"] + ops["div"] + ops["sqrt"]
-    work = {"ref_flops_per_step": flops / max(1, int(tn_cnt.sum())),
-            "flops_per_pair_test": flops / max(1.0, ops["pairs"])}
+    work = None
+    if count_ops:
+        cnt_idx = order[:256]
+        ops = orc.count_ops_edges(qs_np[cnt_idx], qe_np[cnt_idx], dq)
+        tn_cnt = orc.testnum(qs_np[cnt_idx], qe_np[cnt_idx], dq)
+        flops = ops["add"] + ops["mul"] + ops["div"] + ops["sqrt"]
+        work = {"ref_flops_per_step": flops / max(1, int(tn_cnt.sum())),
+                "flops_per_pair_test": flops / max(1.0, ops["pairs"])}
     if O.ref_available():
         ref = O.RefChecker(scene, dq=dq, nbuf=4096)
         kind = "reference"
@@ -309,6 +318,9 @@ def run_ours(args, rank, world, local_rank):
         prm = prm_leg(args, "hull6", WORKLOAD["dq"], args.prm_samples, 10)
         if not args.no_stress:
             prm_stress = prm_leg(args, "wall7", 0.005, args.stress_samples, 16)
+    stress_edges = None
+    if not args.no_stress_edges and world == 1:
+        stress_edges = stress_edges_leg(args, dev, policy)
     batch = None
     if not args.no_batch and world == 1:
         batch = batch_leg(args, dev, policy)
@@ -328,7 +340,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-        "prm": prm, "prm_stress": prm_stress, "batch": batch, "sampler": sampler,
+        "prm": prm, "prm_stress": prm_stress, "stress_edges": stress_edges, "batch": batch, "sampler": sampler,
     }
     return line
 
@@ -351,6 +363,85 @@ def prm_leg(args, kind, dq, n_samples, k):
     out["scene"] = {"kind": kind, "ndof": psc.ndof, "polytopes": len(psc.polys), "pairs": len(psc.pair_from)}
     out["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
                         "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
+    return out
+
+
+STRESS = dict(workload="wall7 edges: 7-DOF arm of 8 32-vertex hull links, 512 hull obstacles (8-64 vertices) "
+                        "in 6 Gaussian clusters forming two walls with a 0.12 m gap, 2^22 samples, kNN k=16, "
+                        "dq=0.005 rad, FP64 band 1e-5 m",
+              ndof=7, obstacles=512, samples=1 << 22, k=16, dq=0.005, band_m=1e-5)
+
+
+def stress_edges_leg(args, dev, policy):
+    """Checker throughput on the 7-DOF wall scene at full size: the vertex
+    check of 2^22 samples, the kNN roadmap of the free ones (k=16), then the
+    edge checker on a seeded uniform sample of the roadmap's edges (the whole
+    roadmap takes ~2.5e9 edge steps, about half a minute), next to the
+    reference CPU checker on a bounded sample of the same edges."""
+    import torch
+    from gpuprm_b200 import scenes, workloads
+    from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
+    from gpuprm_b200.configspace import RobotConfigspace
+    sc = scenes.make_scene("wall7", args.seed)
+    cs = RobotConfigspace(sc, dq=STRESS["dq"])
+    cs.init()
+    cs.set_mode(GPRM_MODE_FP64_BAND)
+    cs.set_edge_policy(policy)
+    n = STRESS["samples"]
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, n, args.seed + 1000).T), device=dev)
+    codes = torch.zeros(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(max(3, args.warmup)):
+        cs.check_configs_device(q[:, :1 << 16].contiguous(), codes[:1 << 16])
+    torch.cuda.synchronize()
+    e0.record(stream)
+    cs.check_configs_device(q, codes)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_v = e0.elapsed_time(e1) / 1e3
+    free = torch.nonzero(codes == 0).squeeze(1)
+    qf = q[:, free].T.contiguous()
+    t0 = time.perf_counter()
+    i, j = workloads.knn_pairs(qf, STRESS["k"])
+    torch.cuda.synchronize()
+    t_knn = time.perf_counter() - t0
+    E = int(i.numel())
+    tn_all = (torch.linalg.vector_norm(qf[i] - qf[j], dim=1) / STRESS["dq"]).floor() + 1
+    g = torch.Generator(device="cpu").manual_seed(args.seed + 17)
+    m = min(E, args.stress_edges)
+    pick = torch.randperm(E, generator=g)[:m].to(dev)
+    qs = qf[i[pick]].T.contiguous()
+    qe = qf[j[pick]].T.contiguous()
+    res = torch.empty(m, dtype=torch.int32, device=dev)
+    w = min(m, 1 << 14)
+    for _ in range(max(3, args.warmup)):
+        cs.check_edges_device(qs[:, :w].contiguous(), qe[:, :w].contiguous(), res[:w])
+    torch.cuda.synchronize()
+    s0 = cs.stats()
+    e0.record(stream)
+    cs.check_edges_device(qs, qe, res)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e = e0.elapsed_time(e1) / 1e3
+    s1 = cs.stats()
+    nominal = s1["edge_steps_nominal"] - s0["edge_steps_nominal"]
+    out = {
+        "config": dict(STRESS, free_samples=int(free.numel()), roadmap_edges=E,
+                       roadmap_edge_steps=int(tn_all.sum().item()), sampled_edges=m,
+                       policy=args.policy),
+        "vertex": {"configs_per_s": n / t_v, "ms": 1e3 * t_v, "pairs_per_config": len(sc.pair_from)},
+        "knn_seconds": t_knn,
+        "edges": {"value": nominal / t_e, "unit": UNIT, "ms": 1e3 * t_e, "edge_steps_nominal": int(nominal),
+                  "edge_steps_executed": int(s1["edge_steps_executed"] - s0["edge_steps_executed"]),
+                  "colliding_edges": int((res != 0).sum().item()),
+                  "band_rechecks": int(s1["band_rechecks"] - s0["band_rechecks"])},
+    }
+    if not args.no_cpu_baseline:
+        cpu, _ = cpu_reference_rate(sc, np.ascontiguousarray(qs.T.cpu().numpy()),
+                                    np.ascontiguousarray(qe.T.cpu().numpy()), STRESS["dq"],
+                                    args.cpu_seconds, args.seed, count_ops=False)
+        out["cpu_baseline"] = cpu
     return out
 
 
