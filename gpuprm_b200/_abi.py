@@ -16,6 +16,7 @@ GPRM_EDGES_EARLY_EXIT = 0
 GPRM_EDGES_ALL_STEPS = 1
 GPRM_MLP_INFER_TCGEN05 = 0
 GPRM_MLP_INFER_TRAINING_GEMM = 1
+GPRM_MLP_INFER_TCGEN05_LAYERS = 2
 GPRM_MAX_DOF = 7
 GPRM_MAX_VERTICES = 100
 GPRM_NOALLOC_MAX_CONFIGS = 65536

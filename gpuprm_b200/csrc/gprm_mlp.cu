@@ -489,6 +489,381 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(TC_COLS) : "memory");
 }
 
+
+/* ------------------------------------------------------------------ */
+/* the whole network in one kernel (tcgen05, warp-specialised)          */
+/* ------------------------------------------------------------------ */
+/*
+ * k_mlp_fused runs all layers of a 128-row tile on one SM; the hidden
+ * activations never leave shared memory.  One persistent CTA per SM with
+ * 14 warps in four roles:
+ *   warps 0-7   epilogue: TMEM -> + bias, GELU -> BF16 activations in
+ *               shared memory (the next layer's A operand) or, after the
+ *               last hidden layer, the output head.  Warp w reads TMEM
+ *               lanes 32*(w%4).. (its rows) and the 32-column blocks
+ *               c = w/4, w/4+2, w/4+4, w/4+6;
+ *   warp 8      loads the weights of hidden layers 2-4 in chunks of K = 32
+ *               (256 x 32 BF16 = 16 KB, pre-arranged in core-matrix order
+ *               by k_mlp_relayout) with bulk copies into a 4-stage ring;
+ *   warp 9      issues the MMAs (one thread);
+ *   warps 10-13 compute the input features of the next tile.
+ * Hidden layer l accumulates into TMEM columns 256*(l%2).. and writes its
+ * activations to buffer l%2, so the epilogue of layer l overlaps the MMAs
+ * of layer l+1: chunk c of layer l+1 (K columns 32c..32c+31) is issued as
+ * soon as the epilogue has written block c of layer l.  The MMAs of a
+ * layer run in the same K order as k_mlp_tc, so the hidden activations are
+ * the same bits; only the output head sums its columns in another order.
+ * Every wait is bounded by a clock budget: an expired wait sets *err and
+ * an abort flag that ends the other roles' waits; the CTA then waits
+ * (bounded) for its own MMAs and copies before it frees TMEM and returns.
+ */
+constexpr unsigned FULL_MASK_MLP = 0xffffffffu;
+constexpr int FU_THREADS = 448;
+constexpr int FU_NS = 4;                                   /* weight ring stages */
+constexpr int FU_CK = 32;                                  /* K columns per weight chunk */
+constexpr int FU_CHUNK_BYTES = HID * FU_CK * 2;            /* 16 KB */
+constexpr int FU_CHUNKS = HID / FU_CK;                     /* 8 chunks per hidden layer */
+constexpr long long FU_WAIT_CYCLES = 1ll << 31;            /* ~1 s at the boost clock */
+constexpr size_t FU_RELAYOUT_BYTES = (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES + (size_t)HID * IN_PAD * 2;
+
+struct FuSmem {
+    static constexpr size_t BUF = 0;                                   /* 2 x 64 KB activations */
+    static constexpr size_t RING = BUF + 2 * (size_t)TC_ROWS * HID * 2;
+    static constexpr size_t W1 = RING + (size_t)FU_NS * FU_CHUNK_BYTES;  /* 8 KB */
+    static constexpr size_t FEAT = W1 + (size_t)HID * IN_PAD * 2;        /* 4 KB */
+    static constexpr size_t BIAS = FEAT + (size_t)TC_ROWS * IN_PAD * 2;  /* 4 x 256 floats */
+    static constexpr size_t W5 = BIAS + (size_t)NLAYER * HID * 4;        /* 256 floats */
+    static constexpr size_t RED = W5 + (size_t)HID * 4;                  /* 128 floats */
+    static constexpr size_t BARS = RED + (size_t)TC_ROWS * 4;
+    static constexpr int NBARS = 25;
+    static constexpr size_t TADDR = BARS + NBARS * 8;
+    static constexpr size_t ABORT = TADDR + 4;
+    static constexpr size_t B5 = ABORT + 4;
+    static constexpr size_t BYTES = B5 + 16;
+};
+static_assert(FuSmem::BYTES <= 227 * 1024, "fused MLP shared memory");
+static_assert(FuSmem::BARS % 8 == 0, "mbarrier alignment");
+
+/* mbarrier indices */
+enum {
+    FB_WFULL = 0, FB_WEMPTY = FB_WFULL + FU_NS, FB_HREADY = FB_WEMPTY + FU_NS, FB_ACCFULL = FB_HREADY + FU_CHUNKS,
+    FB_ACCEMPTY = FB_ACCFULL + 2, FB_FEATREADY = FB_ACCEMPTY + 2, FB_FEATEMPTY, FB_HEADFULL, FB_HEADEMPTY, FB_DRAIN,
+    FB_COUNT
+};
+static_assert(FB_COUNT == FuSmem::NBARS, "barrier count");
+
+struct FuParams {
+    const float* q;
+    long long qoff;
+    int ndof, n;
+    const unsigned char* wtc;       /* k_mlp_relayout output */
+    const float* bias[NLAYER];
+    const __nv_bfloat16* w5;
+    const float* b5;
+    float* p;
+    unsigned* err;
+};
+
+__device__ __forceinline__ void fu_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool fu_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred P1;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                 : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+    return done != 0;
+}
+
+/* Waits for the phase of `parity`; false when the clock budget runs out
+ * (sets the abort flag and *err) or another role has aborted. */
+__device__ __forceinline__ bool fu_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err)
+{
+    const long long t0 = clock64();
+    while (!fu_try(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > FU_WAIT_CYCLES) {
+            *abort_flag = 1;
+            atomicOr(err, 1u);
+            return false;
+        }
+    }
+    return true;
+}
+
+/* The same wait without the abort flag: used while draining. */
+__device__ __forceinline__ void fu_wait_drain(uint32_t bar, uint32_t parity, unsigned* err)
+{
+    const long long t0 = clock64();
+    while (!fu_try(bar, parity)) {
+        if (clock64() - t0 > FU_WAIT_CYCLES) {
+            atomicOr(err, 2u);
+            return;
+        }
+    }
+}
+
+__device__ __forceinline__ void fu_mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                 :: "r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void fu_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" :: "r"(bar)
+                 : "memory");
+}
+
+/* Weights of hidden layers 2-4 in chunk order (layer, K chunk), each chunk
+ * [256 rows x 32 K] in no-swizzle K-major core-matrix order (SBO 512 B,
+ * LBO 128 B), then W1 [256 x 16] in the same order (SBO 256 B). */
+__global__ void k_mlp_relayout(const __nv_bfloat16* __restrict__ wbf, long long o0, long long o1, long long o2,
+                               long long o3, unsigned char* __restrict__ out)
+{
+    const int per_layer = HID * (HID / 8);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (NLAYER - 1) * per_layer) {
+        const int l = t / per_layer, r = t % per_layer;
+        const int nrow = r % HID, kg = r / HID;
+        const long long off = l == 0 ? o1 : (l == 1 ? o2 : o3);
+        const uint4 v = *reinterpret_cast<const uint4*>(wbf + off + (long long)nrow * HID + kg * 8);
+        unsigned char* dst = out + (size_t)(l * FU_CHUNKS + kg / 4) * FU_CHUNK_BYTES + (nrow / 8) * (FU_CK * 16) +
+                             (kg % 4) * 128 + (nrow % 8) * 16;
+        *reinterpret_cast<uint4*>(dst) = v;
+    } else if (t < (NLAYER - 1) * per_layer + HID * (IN_PAD / 8)) {
+        const int r = t - (NLAYER - 1) * per_layer;
+        const int nrow = r % HID, kg = r / HID;
+        const uint4 v = *reinterpret_cast<const uint4*>(wbf + o0 + (long long)nrow * IN_PAD + kg * 8);
+        unsigned char* dst = out + (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES + (nrow / 8) * (IN_PAD * 16) +
+                             kg * 128 + (nrow % 8) * 16;
+        *reinterpret_cast<uint4*>(dst) = v;
+    }
+}
+
+__global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    using L = FuSmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t bars = smem_u32(sm + L::BARS);
+    auto bar = [&](int i) { return bars + 8u * (uint32_t)i; };
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::ABORT);
+    uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(sm + L::TADDR);
+    float* bias_s = reinterpret_cast<float*>(sm + L::BIAS);
+    float* w5_s = reinterpret_cast<float*>(sm + L::W5);
+    float* red = reinterpret_cast<float*>(sm + L::RED);
+    const float* b5_s = reinterpret_cast<const float*>(sm + L::B5);
+
+    /* resident parameters: W1 (pre-arranged), biases, head */
+    {
+        const unsigned char* w1g = P.wtc + (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES;
+        for (int i = tid; i < HID * IN_PAD * 2 / 16; i += FU_THREADS)
+            reinterpret_cast<uint4*>(sm + L::W1)[i] = reinterpret_cast<const uint4*>(w1g)[i];
+        for (int i = tid; i < NLAYER * HID; i += FU_THREADS) bias_s[i] = P.bias[i / HID][i % HID];
+        for (int i = tid; i < HID; i += FU_THREADS) w5_s[i] = __bfloat162float(P.w5[i]);
+        if (tid == 0) {
+            *reinterpret_cast<float*>(sm + L::B5) = P.b5[0];
+            *abort_flag = 0;
+            const int counts[FB_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 4, 4, 4, 4, 4, 4, 4, 4, 1, 1, 8, 8, 128, 1, 4, 4, 1};
+            for (int i = 0; i < FB_COUNT; ++i)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(bar(i)), "r"(counts[i]) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     :: "r"(smem_u32(taddr_slot)), "r"(2 * TC_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *taddr_slot;
+    const int ntiles = (P.n + TC_ROWS - 1) / TC_ROWS;
+    const uint32_t buf0 = smem_u32(sm + L::BUF), ring0 = smem_u32(sm + L::RING);
+    constexpr uint32_t BUF_BYTES = TC_ROWS * HID * 2;
+
+    if (warp < 8) {
+        /* ---------------- epilogue ---------------- */
+        const int g = warp & 3, h = warp >> 2;
+        const int rl = 32 * g + lane;
+        uint32_t af_ph[2] = {0u, 0u}, hf_ph = 0u, he_ph = 0u;
+        bool ok = true;
+        for (int tile = blockIdx.x, it = 0; tile < ntiles && ok; tile += gridDim.x, ++it) {
+            const int row0 = tile * TC_ROWS;
+            for (int l = 0; l < NLAYER && ok; ++l) {
+                const int a = l & 1;
+                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_ACCFULL + a), af_ph[a], abort_flag, P.err));
+                if (!ok) break;
+                af_ph[a] ^= 1u;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const float* bl = bias_s + l * HID;
+                unsigned char* hb_dst = sm + L::BUF + (size_t)a * BUF_BYTES + (rl / 8) * (HID * 16) + (rl % 8) * 16;
+                float part = 0.0f;
+#pragma unroll 1
+                for (int cc = 0; cc < 4; ++cc) {
+                    const int c = h + 2 * cc, col = 32 * c;
+                    float v[32];
+                    tc_ld32(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + col), v);
+                    __align__(16) __nv_bfloat16 hb[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) hb[j] = __float2bfloat16(gelu_f(v[j] + bl[col + j]));
+                    if (l < NLAYER - 1) {
+#pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4)
+                            *reinterpret_cast<uint4*>(hb_dst + (4 * c + c4) * 128) =
+                                *reinterpret_cast<const uint4*>(hb + 8 * c4);
+                        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) fu_arrive(bar(FB_HREADY + c));
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) part += __bfloat162float(hb[j]) * w5_s[col + j];
+                    }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) fu_arrive(bar(FB_ACCEMPTY + a));
+                if (l == NLAYER - 1) {
+                    /* output head: the odd-block warps hand their partial sums over */
+                    if (h == 1) {
+                        if (it > 0) {
+                            ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADEMPTY), he_ph, abort_flag, P.err));
+                            if (!ok) break;
+                            he_ph ^= 1u;
+                        }
+                        red[rl] = part;
+                        __syncwarp();
+                        if (lane == 0) fu_arrive(bar(FB_HEADFULL));
+                    } else {
+                        ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADFULL), hf_ph, abort_flag, P.err));
+                        if (!ok) break;
+                        hf_ph ^= 1u;
+                        const float logit = part + red[rl] + b5_s[0];
+                        if (row0 + rl < P.n) P.p[row0 + rl] = 1.0f / (1.0f + expf(-logit));
+                        __syncwarp();
+                        if (lane == 0) fu_arrive(bar(FB_HEADEMPTY));
+                    }
+                }
+            }
+        }
+    } else if (warp == 8) {
+        /* ---------------- weight loads ---------------- */
+        if (lane == 0) {
+            uint32_t issued = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                for (int ch = 0; ch < (NLAYER - 1) * FU_CHUNKS; ++ch, ++issued) {
+                    const uint32_t s = issued % FU_NS, k = issued / FU_NS;
+                    if (k > 0 && !(ok = fu_wait(bar(FB_WEMPTY + s), (k - 1) & 1u, abort_flag, P.err))) break;
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                                 :: "r"(bar(FB_WFULL + s)), "r"(FU_CHUNK_BYTES) : "memory");
+                    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                                 :: "r"(ring0 + s * FU_CHUNK_BYTES), "l"(P.wtc + (size_t)ch * FU_CHUNK_BYTES),
+                                    "r"(FU_CHUNK_BYTES), "r"(bar(FB_WFULL + s))
+                                 : "memory");
+                }
+            }
+            /* the copies still in flight land before the CTA leaves */
+            for (uint32_t j = issued > FU_NS ? issued - FU_NS : 0u; j < issued; ++j)
+                fu_wait_drain(bar(FB_WFULL + j % FU_NS), (j / FU_NS) & 1u, P.err);
+        }
+    } else if (warp == 9) {
+        /* ---------------- MMA issue ---------------- */
+        if (lane == 0) {
+            uint32_t consumed = 0, fr_ph = 0, ae_ph[2] = {0u, 0u}, hr_ph = 0u;
+            int uses[2] = {0, 0};
+            bool ok = true;
+            const uint64_t w1d = tc_sdesc(smem_u32(sm + L::W1), 128u, IN_PAD * 16u);
+            const uint64_t fd = tc_sdesc(smem_u32(sm + L::FEAT), 128u, IN_PAD * 16u);
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                /* layer 1: features x W1 */
+                if (!(ok = fu_wait(bar(FB_FEATREADY), fr_ph, abort_flag, P.err))) break;
+                fr_ph ^= 1u;
+                if (uses[0]++ > 0) {
+                    if (!(ok = fu_wait(bar(FB_ACCEMPTY + 0), ae_ph[0], abort_flag, P.err))) break;
+                    ae_ph[0] ^= 1u;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                fu_mma(tmem, fd, w1d, 0u);
+                fu_commit(bar(FB_FEATEMPTY));
+                fu_commit(bar(FB_ACCFULL + 0));
+                /* hidden layers 2-4 */
+                for (int l = 1; l < NLAYER && ok; ++l) {
+                    const int a = l & 1;
+                    if (uses[a]++ > 0) {
+                        if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), ae_ph[a], abort_flag, P.err))) break;
+                        ae_ph[a] ^= 1u;
+                    }
+                    const uint32_t abase = buf0 + (uint32_t)((l - 1) & 1) * BUF_BYTES;
+                    for (int c = 0; c < FU_CHUNKS; ++c, ++consumed) {
+                        /* the hready phases advance once per hidden layer, in order */
+                        if (!(ok = fu_wait(bar(FB_HREADY + c), hr_ph, abort_flag, P.err))) break;
+                        const uint32_t s = consumed % FU_NS;
+                        if (!(ok = fu_wait(bar(FB_WFULL + s), (consumed / FU_NS) & 1u, abort_flag, P.err))) break;
+                        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+                        for (int s2 = 0; s2 < 2; ++s2) {
+                            const uint64_t ad = tc_sdesc(abase + (uint32_t)(2 * c + s2) * 256u, 128u, HID * 16u);
+                            const uint64_t bd = tc_sdesc(ring0 + s * FU_CHUNK_BYTES + (uint32_t)s2 * 256u, 128u,
+                                                         FU_CK * 16u);
+                            fu_mma(tmem + (uint32_t)(a * TC_COLS), ad, bd, (c | s2) != 0 ? 1u : 0u);
+                        }
+                        fu_commit(bar(FB_WEMPTY + s));
+                    }
+                    if (!ok) break;
+                    hr_ph ^= 1u;
+                    fu_commit(bar(FB_ACCFULL + a));
+                }
+            }
+            /* every MMA issued so far completes before TMEM is freed */
+            fu_commit(bar(FB_DRAIN));
+            fu_wait_drain(bar(FB_DRAIN), 0u, P.err);
+        }
+    } else {
+        /* ---------------- input features ---------------- */
+        const int t = tid - 10 * 32;
+        uint32_t fe_ph = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x, it = 0; tile < ntiles; tile += gridDim.x, ++it) {
+            if (it > 0) {
+                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_FEATEMPTY), fe_ph, abort_flag, P.err));
+                if (!ok) break;
+                fe_ph ^= 1u;
+            }
+            const int r = tile * TC_ROWS + t;
+            __align__(16) __nv_bfloat16 x[16];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float sv = 0.0f, cv = 0.0f;
+                if (j < P.ndof && r < P.n) sincosf(P.q[r + P.qoff * j], &sv, &cv);
+                x[2 * j] = __float2bfloat16(j < P.ndof ? sv : 0.0f);
+                x[2 * j + 1] = __float2bfloat16(j < P.ndof ? cv : 0.0f);
+            }
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                *reinterpret_cast<uint4*>(sm + L::FEAT + (t / 8) * (IN_PAD * 16) + c * 128 + (t % 8) * 16) =
+                    *reinterpret_cast<const uint4*>(x + 8 * c);
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            fu_arrive(bar(FB_FEATREADY));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    __syncwarp();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(2 * TC_COLS)
+                     : "memory");
+}
+
 }  // namespace
 
 /* ====================================================================== */
@@ -519,6 +894,7 @@ struct gprm_mlp {
     int infer_path = GPRM_MLP_INFER_TCGEN05;
     __nv_bfloat16 *Ha = nullptr, *Hb = nullptr;
     int infer_rows = 0;
+    unsigned char* wtc = nullptr;       /* weights in the fused kernel's chunk order */
     unsigned* dev_err = nullptr;
     int sms = 0;
     std::string err = "no error";
@@ -638,7 +1014,55 @@ double lcg_uniform(uint64_t& s)
 
 namespace {
 
-/* Predictions of n rows (q[i + offset*j]) through the tensor-core layers. */
+/* Error flag and SM count for the tensor-core kernels (first use). */
+int tc_setup(gprm_mlp* h)
+{
+    if (h->dev_err) return GPRM_OK;
+    MLP_TRY(h, cudaMalloc((void**)&h->dev_err, sizeof(unsigned)));
+    MLP_TRY(h, cudaMemset(h->dev_err, 0, sizeof(unsigned)));
+    int dev = 0;
+    MLP_TRY(h, cudaGetDevice(&dev));
+    MLP_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev));
+    MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<IN_PAD, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TcSmem<IN_PAD>::LAUNCH));
+    MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<HID, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TcSmem<HID>::LAUNCH));
+    MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<HID, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TcSmem<HID>::LAUNCH));
+    MLP_TRY(h, cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FuSmem::BYTES));
+    return GPRM_OK;
+}
+
+/* Predictions of n rows (q[i + offset*j]) by the fused kernel: the weights
+ * are put in chunk order, then one persistent launch runs every layer. */
+int predict_fused(gprm_mlp* h, const float* q, int n, int offset, float* p, cudaStream_t st)
+{
+    int rc = tc_setup(h);
+    if (rc) return rc;
+    if (!h->wtc) MLP_TRY(h, cudaMalloc((void**)&h->wtc, FU_RELAYOUT_BYTES));
+    const int items = (NLAYER - 1) * HID * (HID / 8) + HID * (IN_PAD / 8);
+    k_mlp_relayout<<<(items + 255) / 256, 256, 0, st>>>(h->wbf, h->offWbf[0], h->offWbf[1], h->offWbf[2],
+                                                        h->offWbf[3], h->wtc);
+    FuParams P;
+    P.q = q;
+    P.qoff = offset;
+    P.ndof = h->ndof;
+    P.n = n;
+    P.wtc = h->wtc;
+    for (int l = 0; l < NLAYER; ++l) P.bias[l] = h->w + h->offB[l];
+    P.w5 = h->wbf + h->offWbf[NLAYER];
+    P.b5 = h->w + h->offB[NLAYER];
+    P.p = p;
+    P.err = h->dev_err;
+    const int tiles = (n + TC_ROWS - 1) / TC_ROWS;
+    const int grid = tiles < h->sms ? tiles : h->sms;
+    k_mlp_fused<<<grid, FU_THREADS, FuSmem::BYTES, st>>>(P);
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+/* Predictions of n rows (q[i + offset*j]) through the tensor-core layers,
+ * one kernel per layer. */
 int predict_tc(gprm_mlp* h, const float* q, int n, int offset, float* p, cudaStream_t st)
 {
     const int chunk = 1 << 18;
@@ -652,19 +1076,8 @@ int predict_tc(gprm_mlp* h, const float* q, int n, int offset, float* p, cudaStr
         MLP_TRY(h, cudaMalloc((void**)&h->Hb, (size_t)rows * HID * sizeof(__nv_bfloat16)));
         h->infer_rows = rows;
     }
-    if (!h->dev_err) {
-        MLP_TRY(h, cudaMalloc((void**)&h->dev_err, sizeof(unsigned)));
-        MLP_TRY(h, cudaMemset(h->dev_err, 0, sizeof(unsigned)));
-        int dev = 0;
-        MLP_TRY(h, cudaGetDevice(&dev));
-        MLP_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev));
-        MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<IN_PAD, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TcSmem<IN_PAD>::LAUNCH));
-        MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<HID, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TcSmem<HID>::LAUNCH));
-        MLP_TRY(h, cudaFuncSetAttribute(k_mlp_tc<HID, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TcSmem<HID>::LAUNCH));
-    }
+    int rc = tc_setup(h);
+    if (rc) return rc;
     const __nv_bfloat16* wb = h->wbf;
     const float* w = h->w;
     for (int s = 0; s < n; s += chunk) {
@@ -754,7 +1167,7 @@ void gprm_mlp_destroy(gprm_mlp* h)
     cudaFree(h->loss); cudaFree(h->X);
     for (int l = 0; l < NLAYER; ++l) { cudaFree(h->H[l]); cudaFree(h->Z[l]); cudaFree(h->dZ[l]); }
     cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
-    cudaFree(h->Ha); cudaFree(h->Hb); cudaFree(h->dev_err);
+    cudaFree(h->Ha); cudaFree(h->Hb); cudaFree(h->dev_err); cudaFree(h->wtc);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -787,7 +1200,8 @@ int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, v
     if (!h || n < 0 || (n > 0 && (!q || !p)) || offset < n) return mfail(h, GPRM_ERR_ARG, "bad arguments");
     if (n == 0) return GPRM_OK;
     cudaStream_t st = (cudaStream_t)stream;   /* NULL: the legacy default stream */
-    if (h->infer_path == GPRM_MLP_INFER_TCGEN05) return predict_tc(h, q, n, offset, p, st);
+    if (h->infer_path == GPRM_MLP_INFER_TCGEN05) return predict_fused(h, q, n, offset, p, st);
+    if (h->infer_path == GPRM_MLP_INFER_TCGEN05_LAYERS) return predict_tc(h, q, n, offset, p, st);
     const int chunk = 1 << 16;
     int rc = alloc_batch(h, n < chunk ? n : chunk);
     if (rc) return rc;
@@ -877,7 +1291,8 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
 int gprm_mlp_set_inference(gprm_mlp* h, int path)
 {
     if (!h) return GPRM_ERR_ARG;
-    if (path != GPRM_MLP_INFER_TCGEN05 && path != GPRM_MLP_INFER_TRAINING_GEMM)
+    if (path != GPRM_MLP_INFER_TCGEN05 && path != GPRM_MLP_INFER_TRAINING_GEMM &&
+        path != GPRM_MLP_INFER_TCGEN05_LAYERS)
         return mfail(h, GPRM_ERR_ARG, "unknown inference path");
     h->infer_path = path;
     return GPRM_OK;
@@ -889,7 +1304,7 @@ int gprm_mlp_device_status(gprm_mlp* h, unsigned* flags)
     *flags = 0;
     MLP_TRY(h, cudaDeviceSynchronize());
     if (h->dev_err) MLP_TRY(h, cudaMemcpy(flags, h->dev_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    if (*flags) return mfail(h, GPRM_ERR_DEVICE, "a tensor-core layer timed out waiting for its MMAs");
+    if (*flags) return mfail(h, GPRM_ERR_DEVICE, "a tensor-core kernel timed out waiting for its MMAs or copies");
     return GPRM_OK;
 }
 

@@ -83,9 +83,11 @@ class CollisionMLP:
         return out
 
     def set_inference(self, path: str) -> None:
-        """'tcgen05' (default): tensor-core layers with TMEM accumulators;
-        'training': the training GEMMs."""
-        code = {"tcgen05": _abi.GPRM_MLP_INFER_TCGEN05, "training": _abi.GPRM_MLP_INFER_TRAINING_GEMM}[path]
+        """'tcgen05' (default): one fused tensor-core kernel for all layers
+        (TMEM accumulators, activations in shared memory); 'tcgen05_layers':
+        one tensor-core kernel per layer; 'training': the training GEMMs."""
+        code = {"tcgen05": _abi.GPRM_MLP_INFER_TCGEN05, "training": _abi.GPRM_MLP_INFER_TRAINING_GEMM,
+                "tcgen05_layers": _abi.GPRM_MLP_INFER_TCGEN05_LAYERS}[path]
         self._check(self.lib.gprm_mlp_set_inference(self.h, code))
 
     def device_status(self) -> int:

@@ -201,12 +201,16 @@ int gprm_mlp_set_params(gprm_mlp* h, const float* in);
 /* p[i] = P(collision) of device configurations q[i + offset*j], launched on
  * `stream` (NULL: the legacy default stream) */
 int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, void* stream);
-/* Inference path of gprm_mlp_predict: the tcgen05 layers (default; BF16
- * tensor-core MMAs into TMEM, one persistent CTA per SM per layer) or the
- * training GEMMs.  Both compute the same function (BF16 operands and
- * activations, FP32 accumulation) up to FP32 summation order. */
+/* Inference path of gprm_mlp_predict: the fused tcgen05 kernel (default;
+ * every layer of a 128-row tile on one SM, BF16 tensor-core MMAs into TMEM,
+ * activations kept in shared memory), the tcgen05 layers (one persistent
+ * kernel per layer, activations through device memory) or the training
+ * GEMMs.  All compute the same function (BF16 operands and activations,
+ * FP32 accumulation) up to FP32 summation order; the two tcgen05 paths
+ * produce the same hidden activations bit for bit. */
 #define GPRM_MLP_INFER_TCGEN05        0
 #define GPRM_MLP_INFER_TRAINING_GEMM  1
+#define GPRM_MLP_INFER_TCGEN05_LAYERS 2
 int gprm_mlp_set_inference(gprm_mlp* h, int path);
 /* Synchronises the device; *flags != 0 (and GPRM_ERR_DEVICE) when a
  * tensor-core layer gave up waiting for its MMAs. */

@@ -128,9 +128,10 @@ def test_training_learns_exact_checker_labels():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", ["tcgen05", "tcgen05_layers"])
 @pytest.mark.parametrize("n,ndof", [(5000, 6), (131, 7), (1, 4)])
-def test_gpu_tensor_core_inference_matches_training_path_and_oracle(n, ndof):
-    """The tcgen05 inference layers compute the training forward's function
+def test_gpu_tensor_core_inference_matches_training_path_and_oracle(n, ndof, path):
+    """The tcgen05 inference paths compute the training forward's function
     (same BF16 roundings, FP32 accumulation in another order)."""
     import torch
     from gpuprm_b200.mlp import CollisionMLP
@@ -141,7 +142,7 @@ def test_gpu_tensor_core_inference_matches_training_path_and_oracle(n, ndof):
     q_soa = torch.tensor(np.ascontiguousarray(q.T), device="cuda:0")
     mlp.set_inference("training")
     p_ref = mlp.predict(q_soa).cpu().numpy()
-    mlp.set_inference("tcgen05")
+    mlp.set_inference(path)
     p_tc = mlp.predict(q_soa).cpu().numpy()
     assert mlp.device_status() == 0
     assert np.max(np.abs(p_tc - p_ref)) <= 2e-3
@@ -152,3 +153,29 @@ def test_gpu_tensor_core_inference_matches_training_path_and_oracle(n, ndof):
     assert np.max(np.abs(p_tc - p)) <= 1e-2
     if n >= 100:
         assert np.median(np.abs(p_tc - p)) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 18944, 100003, 1 << 20])
+def test_gpu_fused_inference_equals_layered_kernels(n):
+    """The fused kernel (all layers of a tile on one SM) and the per-layer
+    tcgen05 kernels issue the same MMAs in the same K order, so the hidden
+    activations are the same bits; only the output head sums its 256
+    products in another order.  Sizes cover a partial tile, exact tiles and
+    several tiles per CTA (148 CTAs x 128 rows = 18944 rows per wave)."""
+    import torch
+    from gpuprm_b200.mlp import CollisionMLP
+    rng = np.random.default_rng(n)
+    q = rng.uniform(-np.pi, np.pi, (n, 6)).astype(np.float32)
+    mlp = CollisionMLP(6, seed=3)
+    mlp.set_params(mlp.get_params() * 2.0)
+    q_soa = torch.tensor(np.ascontiguousarray(q.T), device="cuda:0")
+    mlp.set_inference("tcgen05_layers")
+    p_l = mlp.predict(q_soa).cpu().numpy()
+    mlp.set_inference("tcgen05")
+    p_f = mlp.predict(q_soa).cpu().numpy()
+    p_f2 = mlp.predict(q_soa).cpu().numpy()
+    assert mlp.device_status() == 0
+    assert np.array_equal(p_f, p_f2)
+    assert np.all(np.isfinite(p_f))
+    assert np.max(np.abs(p_f - p_l)) <= 2e-6
