@@ -32,6 +32,8 @@ Extra legs in the same line (not part of `value`):
              (2^22 samples, k=16, dq 0.005): vertex checks/s and edge-step
              checks/s on 2^21 of the roadmap's edges, with the reference CPU
              checker on a bounded sample of them;
+  mlp        collision-predictor inference on 2^22 rows: the fused tcgen05
+             kernel against per-layer tcgen05 kernels and the training GEMMs;
   batch      256 independent problems in one graph-captured launch per kind
              against a loop of per-problem launches.
 
@@ -87,6 +89,10 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
     ap.add_argument("--no-sampler", action="store_true", help="skip the near-node sampler leg")
     ap.add_argument("--batch-problems", type=int, default=256)
+    ap.add_argument("--no-mlp", action="store_true", help="skip the predictor inference leg")
+    ap.add_argument("--mlp-rows", type=int, default=1 << 22)
+    ap.add_argument("--only-mlp", action="store_true",
+                    help="run only the predictor inference leg and print it (profiling)")
     return ap.parse_args()
 
 
@@ -327,6 +333,9 @@ def run_ours(args, rank, world, local_rank):
     sampler = None
     if not args.no_sampler and world == 1:
         sampler = sampler_leg(args, ws, dev)
+    mlp = None
+    if not args.no_mlp and world == 1:
+        mlp = mlp_leg(args, dev)
     line = {
         "metric": METRIC, "value": nominal_all / t_max, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
@@ -341,6 +350,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
         "prm": prm, "prm_stress": prm_stress, "stress_edges": stress_edges, "batch": batch, "sampler": sampler,
+        "mlp": mlp,
     }
     return line
 
@@ -443,6 +453,51 @@ def stress_edges_leg(args, dev, policy):
                                     args.cpu_seconds, args.seed, count_ops=False)
         out["cpu_baseline"] = cpu
     return out
+
+
+MLP_FLOPS_PER_ROW = 2 * (16 * 256 + 3 * 256 * 256 + 256)
+
+
+def mlp_leg(args, dev):
+    """Inference of the collision predictor (6 joints, 16 -> 256 x4 -> 1,
+    BF16 operands, FP32 accumulation) on 2^22 uniform configurations: the
+    fused tcgen05 kernel (the library default), one tcgen05 kernel per
+    layer, and the training GEMMs.  FLOPs per row = 2 (16*256 + 3*256^2 +
+    256); roofline against the measured dense BF16 peak (burst figure: one
+    kernel timed alone)."""
+    import torch
+    from gpuprm_b200.mlp import CollisionMLP
+    n = args.mlp_rows
+    rng = np.random.default_rng(args.seed + 11)
+    q = torch.tensor(rng.uniform(-np.pi, np.pi, (6, n)).astype(np.float32), device=dev)
+    mlp = CollisionMLP(6, seed=args.seed + 1)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    res = {"rows": n, "flops_per_row": MLP_FLOPS_PER_ROW}
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        peak = 1590.0
+    for path in ("tcgen05", "tcgen05_layers", "training"):
+        mlp.set_inference(path)
+        for _ in range(max(3, args.warmup)):
+            mlp.predict(q, out=out)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            mlp.predict(q, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        tf = n * MLP_FLOPS_PER_ROW / (ms * 1e-3) / 1e12
+        res[path] = {"ms": ms, "tflops": tf, "rows_per_s": n / (ms * 1e-3), "frac_of_bf16_peak": tf / peak}
+    res["device_status"] = mlp.device_status()
+    res["peak_tflops"] = peak
+    res["peak_source"] = "MEASURED_PEAKS.json bf16_tflops (burst)"
+    return res
 
 
 def sampler_leg(args, ws, dev):
@@ -630,6 +685,12 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.only_mlp:
+        import torch
+        torch.cuda.set_device(local_rank)
+        if rank == 0:
+            print(json.dumps({"mlp": mlp_leg(args, torch.device("cuda", local_rank))}), flush=True)
         return
     if world > 1:
         import datetime

@@ -3,7 +3,8 @@
  *
  * No counterpart in GPUPRM.  A multilayer perceptron
  *     x (sin/cos of the joints, padded to 16) -> 256 -> 256 -> 256 -> 256 -> 1
- * with GELU (erf form) on the hidden layers and a sigmoid output, trained
+ * with GELU (erf form, erfc by Abramowitz & Stegun 7.1.28) on the hidden
+ * layers and a sigmoid output, trained
  * with binary cross-entropy and Adam.  Weights are kept in FP32 (master)
  * and BF16 (the GEMM operands); activations are stored in BF16; every GEMM
  * accumulates in FP32 on the tensor cores (warp-level BF16 MMA, m16n8k16).
@@ -54,17 +55,63 @@ struct EpiArgs {
     int ldc;
 };
 
+/* GELU(z) = z Phi(z), Phi the standard normal CDF, Phi(z) = (1 + erf(z/sqrt2))/2.
+ * erfc by the approximation of Abramowitz & Stegun, Handbook of
+ * Mathematical Functions, eq. 7.1.28: for x >= 0,
+ *     erfc(x) = 1 - erf(x) = 1 / (1 + a1 x + a2 x^2 + ... + a6 x^6)^16,
+ * |error| <= 3e-7, far below the BF16 rounding of the activations it
+ * feeds.  With x = |z|/sqrt2 and h = erfc(x)/2, Phi(z) = 1 - h for z >= 0
+ * and h for z < 0.  One reciprocal is the only special-function
+ * instruction (the multi-function unit's throughput bounds the inference
+ * epilogue); the polynomial and the four squarings run as FMAs.  For large
+ * x the 16th power overflows to infinity and erfc to 0, its limit. */
+__device__ __forceinline__ float gelu_phi(float z)
+{
+    const float x = __fmul_rn(fabsf(z), 0.70710678118654752f);
+    float y = __fmaf_rn(0.0000430638f, x, 0.0002765672f);
+    y = __fmaf_rn(y, x, 0.0001520143f);
+    y = __fmaf_rn(y, x, 0.0092705272f);
+    y = __fmaf_rn(y, x, 0.0422820123f);
+    y = __fmaf_rn(y, x, 0.0705230784f);
+    y = __fmaf_rn(y, x, 1.0f);
+    y = __fmul_rn(y, y);
+    y = __fmul_rn(y, y);
+    y = __fmul_rn(y, y);
+    y = __fmul_rn(y, y);                                   /* P(x)^16 */
+    const float h = __fdividef(0.5f, y);                   /* erfc(x) / 2 */
+    return z >= 0.0f ? 1.0f - h : h;
+}
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float r;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ float gelu_f(float z)
 {
-    return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+    return __fmul_rn(z, gelu_phi(z));
 }
 
 __device__ __forceinline__ float gelu_grad(float z)
 {
-    const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-    return cdf + z * pdf;
+    /* Phi(z) + z pdf(z), pdf(z) = exp(-z^2/2) / sqrt(2 pi) = 2^(-z^2 log2(e) / 2) / sqrt(2 pi) */
+    const float e = ex2_approx(__fmul_rn(__fmul_rn(z, z), -0.72134752044448170f));
+    return __fmaf_rn(z, 0.39894228040143268f * e, gelu_phi(z));
 }
+
+/* two floats -> a packed BF16 pair (a in the low half), round to nearest
+ * even like __float2bfloat16; kept in registers (no local arrays) */
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    uint32_t u;
+    memcpy(&u, &h, sizeof(u));
+    return u;
+}
+__device__ __forceinline__ float bf16_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
 
 __device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b)
 {
@@ -307,6 +354,16 @@ __device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+/* shared-memory matrix descriptor: 128-byte swizzle, K-major (version 1):
+ * 8-row x 128-byte atoms (64 BF16 of K), 1024 bytes apart along M/N
+ * (SBO); the leading offset is unused for swizzled K-major operands and
+ * set to 16 bytes. */
+__device__ __forceinline__ uint64_t tc_sdesc_sw128(uint32_t addr)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
 /* instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, M=128, N=256 */
 constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_COLS >> 3) << 17) |
                               ((uint32_t)(TC_ROWS >> 4) << 24);
@@ -348,8 +405,8 @@ struct TcSmem {
     static constexpr size_t A = (size_t)TC_ROWS * K * 2;
     static constexpr size_t MBAR = W + A;
     static constexpr size_t TADDR = MBAR + 8;
-    static constexpr size_t RED = TADDR + 8;                       /* 2 x 128 floats */
-    static constexpr size_t BYTES = RED + 2 * TC_ROWS * 4;
+    static constexpr size_t RED = TADDR + 8;                       /* 4 x 128 floats */
+    static constexpr size_t BYTES = RED + 4 * TC_ROWS * 4;
     /* at least half of the SM's shared memory: one CTA per SM, so that the
        256 TMEM columns this CTA allocates are always available */
     static constexpr size_t LAUNCH = BYTES > 120 * 1024 ? BYTES : 120 * 1024;
@@ -400,18 +457,17 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
         if (FEAT) {
             if (tid < TC_ROWS) {
                 const int r = row0 + tid;
-                __align__(16) __nv_bfloat16 x[16];
+                uint32_t x[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     float sv = 0.0f, cv = 0.0f;
                     if (j < ndof && r < n) sincosf(q[r + qoff * j], &sv, &cv);
-                    x[2 * j] = __float2bfloat16(j < ndof ? sv : 0.0f);
-                    x[2 * j + 1] = __float2bfloat16(j < ndof ? cv : 0.0f);
+                    x[j] = pack_bf16(j < ndof ? sv : 0.0f, j < ndof ? cv : 0.0f);
                 }
 #pragma unroll
                 for (int c = 0; c < 2; ++c)
                     *reinterpret_cast<uint4*>(As + (tid / 8) * SBO + c * LBO + (tid % 8) * 16) =
-                        *reinterpret_cast<const uint4*>(x + 8 * c);
+                        make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
             }
         } else {
             for (int idx = tid; idx < TC_ROWS * (K / 8); idx += blockDim.x) {
@@ -451,31 +507,42 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const int rl = 32 * (warp & 3) + lane;          /* this thread's row in the tile */
         const int r = row0 + rl;
-        const int colbase = 128 * (warp >> 2);
-        float part = 0.0f;
-#pragma unroll 1
+        /* warp half h owns the 32-column blocks 2h, 2h+1, 2h+4, 2h+5; the
+           output head sums block q then block q+4 into partial q and adds
+           the partials as ((0 + 1) + (2 + 3)), the same split and order as
+           the fused kernel */
+        const int h = warp >> 2;
+        float part[2] = {0.0f, 0.0f};
+#pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
-            const int col = colbase + 32 * cc;
+            const int col = 32 * (2 * h + (cc & 1) + 4 * (cc >> 1));
             float v[32];
             tc_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col, v);
-            __align__(16) __nv_bfloat16 hb[32];
+            uint32_t hp[16];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) hb[j] = __float2bfloat16(gelu_f(v[j] + bias[col + j]));
+            for (int j = 0; j < 16; ++j)
+                hp[j] = pack_bf16(gelu_f(v[2 * j] + bias[col + 2 * j]), gelu_f(v[2 * j + 1] + bias[col + 2 * j + 1]));
             if (LAST) {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) part += __bfloat162float(hb[j]) * __bfloat162float(w5[col + j]);
+                for (int j = 0; j < 16; ++j) {
+                    part[cc & 1] = __fmaf_rn(bf16_lo(hp[j]), __bfloat162float(w5[col + 2 * j]), part[cc & 1]);
+                    part[cc & 1] = __fmaf_rn(bf16_hi(hp[j]), __bfloat162float(w5[col + 2 * j + 1]), part[cc & 1]);
+                }
             } else if (r < n) {
 #pragma unroll
                 for (int c4 = 0; c4 < 4; ++c4)
                     *reinterpret_cast<uint4*>(Hout + (size_t)r * HID + col + 8 * c4) =
-                        *reinterpret_cast<const uint4*>(hb + 8 * c4);
+                        make_uint4(hp[4 * c4], hp[4 * c4 + 1], hp[4 * c4 + 2], hp[4 * c4 + 3]);
             }
         }
-        if (LAST) red[(warp >> 2) * TC_ROWS + rl] = part;
+        if (LAST) {
+            red[(2 * h) * TC_ROWS + rl] = part[0];
+            red[(2 * h + 1) * TC_ROWS + rl] = part[1];
+        }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
         __syncthreads();
         if (LAST && tid < TC_ROWS && row0 + tid < n) {
-            const float logit = red[tid] + red[TC_ROWS + tid] + b5[0];
+            const float logit = ((red[tid] + red[TC_ROWS + tid]) + (red[2 * TC_ROWS + tid] + red[3 * TC_ROWS + tid])) + b5[0];
             p[row0 + tid] = 1.0f / (1.0f + expf(-logit));
         }
     }
@@ -496,46 +563,56 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
 /*
  * k_mlp_fused runs all layers of a 128-row tile on one SM; the hidden
  * activations never leave shared memory.  One persistent CTA per SM with
- * 14 warps in four roles:
- *   warps 0-7   epilogue: TMEM -> + bias, GELU -> BF16 activations in
- *               shared memory (the next layer's A operand) or, after the
+ * 22 warps in four roles:
+ *   warps 0-15  epilogue: TMEM -> + bias, GELU -> BF16 activations (the
+ *               next layer's A operand, written in place) or, after the
  *               last hidden layer, the output head.  Warp w reads TMEM
- *               lanes 32*(w%4).. (its rows) and the 32-column blocks
- *               c = w/4, w/4+2, w/4+4, w/4+6;
- *   warp 8      loads the weights of hidden layers 2-4 in chunks of K = 32
- *               (256 x 32 BF16 = 16 KB, pre-arranged in core-matrix order
- *               by k_mlp_relayout) with bulk copies into a 4-stage ring;
- *   warp 9      issues the MMAs (one thread);
- *   warps 10-13 compute the input features of the next tile.
- * Hidden layer l accumulates into TMEM columns 256*(l%2).. and writes its
- * activations to buffer l%2, so the epilogue of layer l overlaps the MMAs
- * of layer l+1: chunk c of layer l+1 (K columns 32c..32c+31) is issued as
- * soon as the epilogue has written block c of layer l.  The MMAs of a
- * layer run in the same K order as k_mlp_tc, so the hidden activations are
- * the same bits; only the output head sums its columns in another order.
- * Every wait is bounded by a clock budget: an expired wait sets *err and
- * an abort flag that ends the other roles' waits; the CTA then waits
- * (bounded) for its own MMAs and copies before it frees TMEM and returns.
+ *               lanes 32*(w%4).. (its rows) and the 32-column blocks q and
+ *               q+4, q = w/4;
+ *   warp 16     loads the weights of hidden layers 2-4 in chunks of K = 64
+ *               (256 x 64 BF16 = 32 KB, pre-arranged by k_mlp_relayout)
+ *               with bulk copies into a 4-stage ring: a whole layer can be
+ *               in flight, so the next layer's weights arrive while the
+ *               epilogue works;
+ *   warp 17     issues the MMAs (one thread);
+ *   warps 18-21 compute the input features of the next tile.
+ * The hidden layers' operands (activations and weight chunks) use the
+ * 128-byte-swizzled K-major layout: 8-row x 64-element atoms of 1 KB in
+ * which the 16-byte group g of row r sits at group g ^ (r % 8), so the
+ * tensor core and the epilogue's row-per-thread stores read and write
+ * shared memory without bank conflicts.  Layer l accumulates into TMEM
+ * columns 256*(l%2)..: MMA chunk c of layer l+1 (K columns 64c..64c+63)
+ * is issued as soon as the epilogue has written blocks 2c and 2c+1 of
+ * layer l, so the MMAs of a layer run under the
+ * epilogue of the previous one, and the first layer of the next tile runs
+ * under the last layer's epilogue.  The MMAs run in the same K order as
+ * k_mlp_tc and the output head uses the same split and order, so both
+ * kernels give the same bits.  Every wait is bounded by a clock budget: an
+ * expired wait sets *err and an abort flag that ends the other roles'
+ * waits; the CTA then waits (bounded) for its own MMAs and copies before
+ * it frees TMEM and returns.
  */
 constexpr unsigned FULL_MASK_MLP = 0xffffffffu;
-constexpr int FU_THREADS = 448;
+constexpr int FU_EPI_WARPS = 16;
+constexpr int FU_PRODUCER_WARP = FU_EPI_WARPS, FU_MMA_WARP = FU_EPI_WARPS + 1, FU_FEAT_WARP0 = FU_EPI_WARPS + 2;
+constexpr int FU_THREADS = (FU_EPI_WARPS + 6) * 32;        /* 704 */
 constexpr int FU_NS = 4;                                   /* weight ring stages */
-constexpr int FU_CK = 32;                                  /* K columns per weight chunk */
-constexpr int FU_CHUNK_BYTES = HID * FU_CK * 2;            /* 16 KB */
-constexpr int FU_CHUNKS = HID / FU_CK;                     /* 8 chunks per hidden layer */
+constexpr int FU_CK = 64;                                  /* K columns per weight chunk: one swizzle atom */
+constexpr int FU_CHUNK_BYTES = HID * FU_CK * 2;            /* 32 KB */
+constexpr int FU_CHUNKS = HID / FU_CK;                     /* 4 chunks per hidden layer */
 constexpr long long FU_WAIT_CYCLES = 1ll << 31;            /* ~1 s at the boost clock */
 constexpr size_t FU_RELAYOUT_BYTES = (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES + (size_t)HID * IN_PAD * 2;
 
 struct FuSmem {
-    static constexpr size_t BUF = 0;                                   /* 2 x 64 KB activations */
-    static constexpr size_t RING = BUF + 2 * (size_t)TC_ROWS * HID * 2;
+    static constexpr size_t BUF = 0;                                   /* 64 KB activations */
+    static constexpr size_t RING = BUF + (size_t)TC_ROWS * HID * 2;
     static constexpr size_t W1 = RING + (size_t)FU_NS * FU_CHUNK_BYTES;  /* 8 KB */
     static constexpr size_t FEAT = W1 + (size_t)HID * IN_PAD * 2;        /* 4 KB */
     static constexpr size_t BIAS = FEAT + (size_t)TC_ROWS * IN_PAD * 2;  /* 4 x 256 floats */
     static constexpr size_t W5 = BIAS + (size_t)NLAYER * HID * 4;        /* 256 floats */
-    static constexpr size_t RED = W5 + (size_t)HID * 4;                  /* 128 floats */
-    static constexpr size_t BARS = RED + (size_t)TC_ROWS * 4;
-    static constexpr int NBARS = 25;
+    static constexpr size_t RED = W5 + (size_t)HID * 4;                  /* 4 x 128 floats */
+    static constexpr size_t BARS = RED + 4 * (size_t)TC_ROWS * 4;
+    static constexpr int NBARS = 3 * FU_NS + 9;
     static constexpr size_t TADDR = BARS + NBARS * 8;
     static constexpr size_t ABORT = TADDR + 4;
     static constexpr size_t B5 = ABORT + 4;
@@ -543,6 +620,8 @@ struct FuSmem {
 };
 static_assert(FuSmem::BYTES <= 227 * 1024, "fused MLP shared memory");
 static_assert(FuSmem::BARS % 8 == 0, "mbarrier alignment");
+static_assert(FU_CHUNKS == FU_NS, "one hready barrier per chunk; the ring holds a layer");
+static_assert(FuSmem::BUF % 1024 == 0 && FuSmem::RING % 1024 == 0, "swizzle atoms are 1024-byte aligned");
 
 /* mbarrier indices */
 enum {
@@ -580,11 +659,15 @@ __device__ __forceinline__ bool fu_try(uint32_t bar, uint32_t parity)
 }
 
 /* Waits for the phase of `parity`; false when the clock budget runs out
- * (sets the abort flag and *err) or another role has aborted. */
-__device__ __forceinline__ bool fu_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err)
+ * (sets the abort flag and *err) or another role has aborted.  Roles off
+ * the critical path pass a sleep between polls, so that their polling does
+ * not take issue slots from the epilogue warps on the same SM sub-partition. */
+__device__ __forceinline__ bool fu_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err,
+                                        unsigned sleep_ns = 0)
 {
     const long long t0 = clock64();
     while (!fu_try(bar, parity)) {
+        if (sleep_ns) __nanosleep(sleep_ns);
         if (*abort_flag) return false;
         if (clock64() - t0 > FU_WAIT_CYCLES) {
             *abort_flag = 1;
@@ -621,8 +704,9 @@ __device__ __forceinline__ void fu_commit(uint32_t bar)
 }
 
 /* Weights of hidden layers 2-4 in chunk order (layer, K chunk), each chunk
- * [256 rows x 32 K] in no-swizzle K-major core-matrix order (SBO 512 B,
- * LBO 128 B), then W1 [256 x 16] in the same order (SBO 256 B). */
+ * [256 rows x 64 K] in the 128-byte-swizzled K-major layout (row n, k at
+ * (n/8)*1024 + (n%8)*128 + ((k/8) ^ (n%8))*16 + (k%8)*2), then W1
+ * [256 x 16] in the no-swizzle core-matrix order (SBO 256 B, LBO 128 B). */
 __global__ void k_mlp_relayout(const __nv_bfloat16* __restrict__ wbf, long long o0, long long o1, long long o2,
                                long long o3, unsigned char* __restrict__ out)
 {
@@ -630,11 +714,11 @@ __global__ void k_mlp_relayout(const __nv_bfloat16* __restrict__ wbf, long long 
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < (NLAYER - 1) * per_layer) {
         const int l = t / per_layer, r = t % per_layer;
-        const int nrow = r % HID, kg = r / HID;
+        const int nrow = r % HID, kg = r / HID;   /* kg: 8-element group of K, 0..31 */
         const long long off = l == 0 ? o1 : (l == 1 ? o2 : o3);
         const uint4 v = *reinterpret_cast<const uint4*>(wbf + off + (long long)nrow * HID + kg * 8);
-        unsigned char* dst = out + (size_t)(l * FU_CHUNKS + kg / 4) * FU_CHUNK_BYTES + (nrow / 8) * (FU_CK * 16) +
-                             (kg % 4) * 128 + (nrow % 8) * 16;
+        unsigned char* dst = out + (size_t)(l * FU_CHUNKS + kg / 8) * FU_CHUNK_BYTES + (nrow / 8) * 1024 +
+                             (nrow % 8) * 128 + (((kg % 8) ^ (nrow % 8)) * 16);
         *reinterpret_cast<uint4*>(dst) = v;
     } else if (t < (NLAYER - 1) * per_layer + HID * (IN_PAD / 8)) {
         const int r = t - (NLAYER - 1) * per_layer;
@@ -659,20 +743,32 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
     float* w5_s = reinterpret_cast<float*>(sm + L::W5);
     float* red = reinterpret_cast<float*>(sm + L::RED);
     const float* b5_s = reinterpret_cast<const float*>(sm + L::B5);
+    if (smem_u32(sm) & 1023u) {     /* the swizzle atoms need 1024-byte alignment */
+        if (tid == 0) atomicOr(P.err, 4u);
+        return;
+    }
 
     /* resident parameters: W1 (pre-arranged), biases, head */
     {
         const unsigned char* w1g = P.wtc + (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES;
         for (int i = tid; i < HID * IN_PAD * 2 / 16; i += FU_THREADS)
             reinterpret_cast<uint4*>(sm + L::W1)[i] = reinterpret_cast<const uint4*>(w1g)[i];
-        for (int i = tid; i < NLAYER * HID; i += FU_THREADS) bias_s[i] = P.bias[i / HID][i % HID];
+#pragma unroll
+        for (int l = 0; l < NLAYER; ++l)   /* constant indices keep P.bias out of local memory */
+            for (int i = tid; i < HID; i += FU_THREADS) bias_s[l * HID + i] = P.bias[l][i];
         for (int i = tid; i < HID; i += FU_THREADS) w5_s[i] = __bfloat162float(P.w5[i]);
         if (tid == 0) {
             *reinterpret_cast<float*>(sm + L::B5) = P.b5[0];
             *abort_flag = 0;
-            const int counts[FB_COUNT] = {1, 1, 1, 1, 1, 1, 1, 1, 4, 4, 4, 4, 4, 4, 4, 4, 1, 1, 8, 8, 128, 1, 4, 4, 1};
-            for (int i = 0; i < FB_COUNT; ++i)
-                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(bar(i)), "r"(counts[i]) : "memory");
+            for (int i = 0; i < FB_COUNT; ++i) {
+                int cnt = 1;                                                      /* one arrive / one commit */
+                if (i >= FB_HREADY && i < FB_HREADY + FU_CHUNKS) cnt = 8;         /* blocks 2c, 2c+1: 8 warps */
+                if (i == FB_ACCEMPTY || i == FB_ACCEMPTY + 1) cnt = FU_EPI_WARPS;
+                if (i == FB_FEATREADY) cnt = TC_ROWS;                             /* the feature threads */
+                if (i == FB_HEADFULL) cnt = FU_EPI_WARPS - 4;                     /* partials 1-3 */
+                if (i == FB_HEADEMPTY) cnt = 4;                                   /* partial 0 */
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(bar(i)), "r"(cnt) : "memory");
+            }
             asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         }
     }
@@ -688,86 +784,94 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
     const uint32_t tmem = *taddr_slot;
     const int ntiles = (P.n + TC_ROWS - 1) / TC_ROWS;
     const uint32_t buf0 = smem_u32(sm + L::BUF), ring0 = smem_u32(sm + L::RING);
-    constexpr uint32_t BUF_BYTES = TC_ROWS * HID * 2;
 
-    if (warp < 8) {
+    if (warp < FU_EPI_WARPS) {
         /* ---------------- epilogue ---------------- */
-        const int g = warp & 3, h = warp >> 2;
+        const int g = warp & 3, q = warp >> 2;
         const int rl = 32 * g + lane;
-        uint32_t af_ph[2] = {0u, 0u}, hf_ph = 0u, he_ph = 0u;
+        uint32_t af_ph = 0u, hf_ph = 0u, he_ph = 0u;   /* phase bits (af: bit a = accumulator a) */
         bool ok = true;
+        /* this thread's row in the activation buffer: atom column kc at kc * 16 KB */
+        unsigned char* hb_row = sm + L::BUF + (rl / 8) * 1024 + (rl % 8) * 128;
         for (int tile = blockIdx.x, it = 0; tile < ntiles && ok; tile += gridDim.x, ++it) {
-            const int row0 = tile * TC_ROWS;
-            for (int l = 0; l < NLAYER && ok; ++l) {
+            for (int l = 0; l < NLAYER; ++l) {
                 const int a = l & 1;
-                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_ACCFULL + a), af_ph[a], abort_flag, P.err));
+                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_ACCFULL + a), (af_ph >> a) & 1u, abort_flag, P.err));
                 if (!ok) break;
-                af_ph[a] ^= 1u;
+                af_ph ^= 1u << a;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const float* bl = bias_s + l * HID;
-                unsigned char* hb_dst = sm + L::BUF + (size_t)a * BUF_BYTES + (rl / 8) * (HID * 16) + (rl % 8) * 16;
                 float part = 0.0f;
-#pragma unroll 1
-                for (int cc = 0; cc < 4; ++cc) {
-                    const int c = h + 2 * cc, col = 32 * c;
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int c = q + 4 * cc, col = 32 * c;
                     float v[32];
                     tc_ld32(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + col), v);
-                    __align__(16) __nv_bfloat16 hb[32];
+                    uint32_t hp[16];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) hb[j] = __float2bfloat16(gelu_f(v[j] + bl[col + j]));
+                    for (int j = 0; j < 16; ++j)
+                        hp[j] = pack_bf16(gelu_f(v[2 * j] + bl[col + 2 * j]), gelu_f(v[2 * j + 1] + bl[col + 2 * j + 1]));
                     if (l < NLAYER - 1) {
+                        /* block c of this layer's activations, over the previous
+                           layer's (whose MMAs have all completed) */
 #pragma unroll
                         for (int c4 = 0; c4 < 4; ++c4)
-                            *reinterpret_cast<uint4*>(hb_dst + (4 * c + c4) * 128) =
-                                *reinterpret_cast<const uint4*>(hb + 8 * c4);
+                            *reinterpret_cast<uint4*>(hb_row + (c / 2) * (TC_ROWS * 128) +
+                                                      (((4 * (c % 2) + c4) ^ (rl % 8)) * 16)) =
+                                make_uint4(hp[4 * c4], hp[4 * c4 + 1], hp[4 * c4 + 2], hp[4 * c4 + 3]);
                         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                         __syncwarp();
-                        if (lane == 0) fu_arrive(bar(FB_HREADY + c));
+                        if (lane == 0) fu_arrive(bar(FB_HREADY + c / 2));
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) part += __bfloat162float(hb[j]) * w5_s[col + j];
+                        for (int j = 0; j < 16; ++j) {
+                            part = __fmaf_rn(bf16_lo(hp[j]), w5_s[col + 2 * j], part);
+                            part = __fmaf_rn(bf16_hi(hp[j]), w5_s[col + 2 * j + 1], part);
+                        }
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
                 if (lane == 0) fu_arrive(bar(FB_ACCEMPTY + a));
                 if (l == NLAYER - 1) {
-                    /* output head: the odd-block warps hand their partial sums over */
-                    if (h == 1) {
+                    /* output head: partials 1-3 are handed to the warps of partial 0 */
+                    if (q > 0) {
                         if (it > 0) {
                             ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADEMPTY), he_ph, abort_flag, P.err));
                             if (!ok) break;
                             he_ph ^= 1u;
                         }
-                        red[rl] = part;
+                        red[q * TC_ROWS + rl] = part;
                         __syncwarp();
                         if (lane == 0) fu_arrive(bar(FB_HEADFULL));
                     } else {
                         ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADFULL), hf_ph, abort_flag, P.err));
                         if (!ok) break;
                         hf_ph ^= 1u;
-                        const float logit = part + red[rl] + b5_s[0];
-                        if (row0 + rl < P.n) P.p[row0 + rl] = 1.0f / (1.0f + expf(-logit));
+                        const float logit = ((part + red[TC_ROWS + rl]) + (red[2 * TC_ROWS + rl] + red[3 * TC_ROWS + rl])) +
+                                            b5_s[0];
+                        const int row = tile * TC_ROWS + rl;
+                        if (row < P.n) P.p[row] = 1.0f / (1.0f + expf(-logit));
                         __syncwarp();
                         if (lane == 0) fu_arrive(bar(FB_HEADEMPTY));
                     }
                 }
             }
         }
-    } else if (warp == 8) {
+    } else if (warp == FU_PRODUCER_WARP) {
         /* ---------------- weight loads ---------------- */
         if (lane == 0) {
             uint32_t issued = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 for (int ch = 0; ch < (NLAYER - 1) * FU_CHUNKS; ++ch, ++issued) {
-                    const uint32_t s = issued % FU_NS, k = issued / FU_NS;
-                    if (k > 0 && !(ok = fu_wait(bar(FB_WEMPTY + s), (k - 1) & 1u, abort_flag, P.err))) break;
+                    const uint32_t st = issued % FU_NS, k = issued / FU_NS;
+                    if (k > 0 && !(ok = fu_wait(bar(FB_WEMPTY + st), (k - 1) & 1u, abort_flag, P.err, 32u))) break;
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
-                                 :: "r"(bar(FB_WFULL + s)), "r"(FU_CHUNK_BYTES) : "memory");
+                                 :: "r"(bar(FB_WFULL + st)), "r"(FU_CHUNK_BYTES) : "memory");
                     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                                 :: "r"(ring0 + s * FU_CHUNK_BYTES), "l"(P.wtc + (size_t)ch * FU_CHUNK_BYTES),
-                                    "r"(FU_CHUNK_BYTES), "r"(bar(FB_WFULL + s))
+                                 :: "r"(ring0 + st * FU_CHUNK_BYTES), "l"(P.wtc + (size_t)ch * FU_CHUNK_BYTES),
+                                    "r"(FU_CHUNK_BYTES), "r"(bar(FB_WFULL + st))
                                  : "memory");
                 }
             }
@@ -775,51 +879,49 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
             for (uint32_t j = issued > FU_NS ? issued - FU_NS : 0u; j < issued; ++j)
                 fu_wait_drain(bar(FB_WFULL + j % FU_NS), (j / FU_NS) & 1u, P.err);
         }
-    } else if (warp == 9) {
+    } else if (warp == FU_MMA_WARP) {
         /* ---------------- MMA issue ---------------- */
         if (lane == 0) {
-            uint32_t consumed = 0, fr_ph = 0, ae_ph[2] = {0u, 0u}, hr_ph = 0u;
-            int uses[2] = {0, 0};
+            uint32_t consumed = 0, fr_ph = 0u, ae_ph = 0u, hr_ph = 0u, used = 0u;   /* bit a: accumulator a */
             bool ok = true;
             const uint64_t w1d = tc_sdesc(smem_u32(sm + L::W1), 128u, IN_PAD * 16u);
             const uint64_t fd = tc_sdesc(smem_u32(sm + L::FEAT), 128u, IN_PAD * 16u);
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                /* layer 1: features x W1 */
-                if (!(ok = fu_wait(bar(FB_FEATREADY), fr_ph, abort_flag, P.err))) break;
-                fr_ph ^= 1u;
-                if (uses[0]++ > 0) {
-                    if (!(ok = fu_wait(bar(FB_ACCEMPTY + 0), ae_ph[0], abort_flag, P.err))) break;
-                    ae_ph[0] ^= 1u;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                fu_mma(tmem, fd, w1d, 0u);
-                fu_commit(bar(FB_FEATEMPTY));
-                fu_commit(bar(FB_ACCFULL + 0));
-                /* hidden layers 2-4 */
-                for (int l = 1; l < NLAYER && ok; ++l) {
+                for (int l = 0; l < NLAYER && ok; ++l) {
                     const int a = l & 1;
-                    if (uses[a]++ > 0) {
-                        if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), ae_ph[a], abort_flag, P.err))) break;
-                        ae_ph[a] ^= 1u;
+                    /* the accumulator's previous layer has been read out */
+                    if ((used >> a) & 1u) {
+                        if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), (ae_ph >> a) & 1u, abort_flag, P.err))) break;
+                        ae_ph ^= 1u << a;
                     }
-                    const uint32_t abase = buf0 + (uint32_t)((l - 1) & 1) * BUF_BYTES;
-                    for (int c = 0; c < FU_CHUNKS; ++c, ++consumed) {
-                        /* the hready phases advance once per hidden layer, in order */
-                        if (!(ok = fu_wait(bar(FB_HREADY + c), hr_ph, abort_flag, P.err))) break;
-                        const uint32_t s = consumed % FU_NS;
-                        if (!(ok = fu_wait(bar(FB_WFULL + s), (consumed / FU_NS) & 1u, abort_flag, P.err))) break;
+                    used |= 1u << a;
+                    const uint32_t acc = tmem + (uint32_t)(a * TC_COLS);
+                    if (l == 0) {
+                        if (!(ok = fu_wait(bar(FB_FEATREADY), fr_ph, abort_flag, P.err))) break;
+                        fr_ph ^= 1u;
                         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                        fu_mma(acc, fd, w1d, 0u);
+                        fu_commit(bar(FB_FEATEMPTY));
+                    } else {
+                        for (int c = 0; c < FU_CHUNKS; ++c, ++consumed) {
+                            /* blocks 2c, 2c+1 of the previous layer's activations (hready
+                               phases advance once per hidden layer, in order) */
+                            if (!(ok = fu_wait(bar(FB_HREADY + c), hr_ph, abort_flag, P.err))) break;
+                            const uint32_t st = consumed % FU_NS;
+                            if (!(ok = fu_wait(bar(FB_WFULL + st), (consumed / FU_NS) & 1u, abort_flag, P.err))) break;
+                            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-                        for (int s2 = 0; s2 < 2; ++s2) {
-                            const uint64_t ad = tc_sdesc(abase + (uint32_t)(2 * c + s2) * 256u, 128u, HID * 16u);
-                            const uint64_t bd = tc_sdesc(ring0 + s * FU_CHUNK_BYTES + (uint32_t)s2 * 256u, 128u,
-                                                         FU_CK * 16u);
-                            fu_mma(tmem + (uint32_t)(a * TC_COLS), ad, bd, (c | s2) != 0 ? 1u : 0u);
+                            for (int s2 = 0; s2 < FU_CK / 16; ++s2) {
+                                /* K step 4c + s2: 32 bytes into the swizzle atoms of column c */
+                                const uint64_t ad = tc_sdesc_sw128(buf0 + (uint32_t)c * (TC_ROWS * 128) + (uint32_t)s2 * 32u);
+                                const uint64_t bd = tc_sdesc_sw128(ring0 + st * FU_CHUNK_BYTES + (uint32_t)s2 * 32u);
+                                fu_mma(acc, ad, bd, (c | s2) != 0 ? 1u : 0u);
+                            }
+                            fu_commit(bar(FB_WEMPTY + st));
                         }
-                        fu_commit(bar(FB_WEMPTY + s));
+                        if (!ok) break;
+                        hr_ph ^= 1u;
                     }
-                    if (!ok) break;
-                    hr_ph ^= 1u;
                     fu_commit(bar(FB_ACCFULL + a));
                 }
             }
@@ -829,28 +931,27 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
         }
     } else {
         /* ---------------- input features ---------------- */
-        const int t = tid - 10 * 32;
-        uint32_t fe_ph = 0;
+        const int t = tid - FU_FEAT_WARP0 * 32;
+        uint32_t fe_ph = 0u;
         bool ok = true;
         for (int tile = blockIdx.x, it = 0; tile < ntiles; tile += gridDim.x, ++it) {
             if (it > 0) {
-                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_FEATEMPTY), fe_ph, abort_flag, P.err));
+                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_FEATEMPTY), fe_ph, abort_flag, P.err, 256u));
                 if (!ok) break;
                 fe_ph ^= 1u;
             }
             const int r = tile * TC_ROWS + t;
-            __align__(16) __nv_bfloat16 x[16];
+            uint32_t x[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 float sv = 0.0f, cv = 0.0f;
                 if (j < P.ndof && r < P.n) sincosf(P.q[r + P.qoff * j], &sv, &cv);
-                x[2 * j] = __float2bfloat16(j < P.ndof ? sv : 0.0f);
-                x[2 * j + 1] = __float2bfloat16(j < P.ndof ? cv : 0.0f);
+                x[j] = pack_bf16(j < P.ndof ? sv : 0.0f, j < P.ndof ? cv : 0.0f);
             }
 #pragma unroll
             for (int c = 0; c < 2; ++c)
                 *reinterpret_cast<uint4*>(sm + L::FEAT + (t / 8) * (IN_PAD * 16) + c * 128 + (t % 8) * 16) =
-                    *reinterpret_cast<const uint4*>(x + 8 * c);
+                    make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
             asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
             fu_arrive(bar(FB_FEATREADY));
         }
