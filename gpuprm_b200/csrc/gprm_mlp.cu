@@ -398,6 +398,20 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v)
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v)
+{
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                   "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
 /* shared memory of k_mlp_tc<K>: W | A | mbarrier | TMEM address | row partials */
 template <int K>
 struct TcSmem {
@@ -507,15 +521,15 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const int rl = 32 * (warp & 3) + lane;          /* this thread's row in the tile */
         const int r = row0 + rl;
-        /* warp half h owns the 32-column blocks 2h, 2h+1, 2h+4, 2h+5; the
-           output head sums block q then block q+4 into partial q and adds
-           the partials as ((0 + 1) + (2 + 3)), the same split and order as
-           the fused kernel */
+        /* warp half h owns columns 64r + 32h .. 64r + 32h + 31 (r = 0..3);
+           the output head sums columns 64r + 16q .. 64r + 16q + 15 over r
+           into partial q and adds the partials as ((0 + 1) + (2 + 3)), the
+           same split and order as the fused kernel */
         const int h = warp >> 2;
         float part[2] = {0.0f, 0.0f};
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
-            const int col = 32 * (2 * h + (cc & 1) + 4 * (cc >> 1));
+            const int col = 64 * cc + 32 * h;
             float v[32];
             tc_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col, v);
             uint32_t hp[16];
@@ -525,8 +539,8 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
             if (LAST) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    part[cc & 1] = __fmaf_rn(bf16_lo(hp[j]), __bfloat162float(w5[col + 2 * j]), part[cc & 1]);
-                    part[cc & 1] = __fmaf_rn(bf16_hi(hp[j]), __bfloat162float(w5[col + 2 * j + 1]), part[cc & 1]);
+                    part[j >> 3] = __fmaf_rn(bf16_lo(hp[j]), __bfloat162float(w5[col + 2 * j]), part[j >> 3]);
+                    part[j >> 3] = __fmaf_rn(bf16_hi(hp[j]), __bfloat162float(w5[col + 2 * j + 1]), part[j >> 3]);
                 }
             } else if (r < n) {
 #pragma unroll
@@ -567,8 +581,8 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
  *   warps 0-15  epilogue: TMEM -> + bias, GELU -> BF16 activations (the
  *               next layer's A operand, written in place) or, after the
  *               last hidden layer, the output head.  Warp w reads TMEM
- *               lanes 32*(w%4).. (its rows) and the 32-column blocks q and
- *               q+4, q = w/4;
+ *               lanes 32*(w%4).. (its rows) and, in round r = 0..3, the
+ *               columns 64r + 16q .. 64r + 16q + 15, q = w/4;
  *   warp 16     loads the weights of hidden layers 2-4 in chunks of K = 64
  *               (256 x 64 BF16 = 32 KB, pre-arranged by k_mlp_relayout)
  *               with bulk copies into a 4-stage ring: a whole layer can be
@@ -582,8 +596,7 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
  * tensor core and the epilogue's row-per-thread stores read and write
  * shared memory without bank conflicts.  Layer l accumulates into TMEM
  * columns 256*(l%2)..: MMA chunk c of layer l+1 (K columns 64c..64c+63)
- * is issued as soon as the epilogue has written blocks 2c and 2c+1 of
- * layer l, so the MMAs of a layer run under the
+ * is issued as soon as the epilogue's round c of layer l has written them, so the MMAs of a layer run under the
  * epilogue of the previous one, and the first layer of the next tile runs
  * under the last layer's epilogue.  The MMAs run in the same K order as
  * k_mlp_tc and the output head uses the same split and order, so both
@@ -743,6 +756,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
     float* w5_s = reinterpret_cast<float*>(sm + L::W5);
     float* red = reinterpret_cast<float*>(sm + L::RED);
     const float* b5_s = reinterpret_cast<const float*>(sm + L::B5);
+    const unsigned char* wtc = P.wtc;
     if (smem_u32(sm) & 1023u) {     /* the swizzle atoms need 1024-byte alignment */
         if (tid == 0) atomicOr(P.err, 4u);
         return;
@@ -750,7 +764,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
 
     /* resident parameters: W1 (pre-arranged), biases, head */
     {
-        const unsigned char* w1g = P.wtc + (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES;
+        const unsigned char* w1g = wtc + (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES;
         for (int i = tid; i < HID * IN_PAD * 2 / 16; i += FU_THREADS)
             reinterpret_cast<uint4*>(sm + L::W1)[i] = reinterpret_cast<const uint4*>(w1g)[i];
 #pragma unroll
@@ -762,7 +776,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
             *abort_flag = 0;
             for (int i = 0; i < FB_COUNT; ++i) {
                 int cnt = 1;                                                      /* one arrive / one commit */
-                if (i >= FB_HREADY && i < FB_HREADY + FU_CHUNKS) cnt = 8;         /* blocks 2c, 2c+1: 8 warps */
+                if (i >= FB_HREADY && i < FB_HREADY + FU_CHUNKS) cnt = FU_EPI_WARPS;   /* every epilogue warp */
                 if (i == FB_ACCEMPTY || i == FB_ACCEMPTY + 1) cnt = FU_EPI_WARPS;
                 if (i == FB_FEATREADY) cnt = TC_ROWS;                             /* the feature threads */
                 if (i == FB_HEADFULL) cnt = FU_EPI_WARPS - 4;                     /* partials 1-3 */
@@ -802,29 +816,30 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const float* bl = bias_s + l * HID;
                 float part = 0.0f;
+                /* round r: columns 64r + 16q .. +15, so that round r completes
+                   K chunk r of the next layer's A operand */
 #pragma unroll
-                for (int cc = 0; cc < 2; ++cc) {
-                    const int c = q + 4 * cc, col = 32 * c;
-                    float v[32];
-                    tc_ld32(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + col), v);
-                    uint32_t hp[16];
+                for (int r = 0; r < FU_CHUNKS; ++r) {
+                    const int col = 64 * r + 16 * q;
+                    float v[16];
+                    tc_ld16(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + col), v);
+                    uint32_t hp[8];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j)
+                    for (int j = 0; j < 8; ++j)
                         hp[j] = pack_bf16(gelu_f(v[2 * j] + bl[col + 2 * j]), gelu_f(v[2 * j + 1] + bl[col + 2 * j + 1]));
                     if (l < NLAYER - 1) {
-                        /* block c of this layer's activations, over the previous
-                           layer's (whose MMAs have all completed) */
+                        /* over the previous layer's activations (whose MMAs have all
+                           completed): atom column r, 16-byte groups 2q, 2q+1 */
 #pragma unroll
-                        for (int c4 = 0; c4 < 4; ++c4)
-                            *reinterpret_cast<uint4*>(hb_row + (c / 2) * (TC_ROWS * 128) +
-                                                      (((4 * (c % 2) + c4) ^ (rl % 8)) * 16)) =
+                        for (int c4 = 0; c4 < 2; ++c4)
+                            *reinterpret_cast<uint4*>(hb_row + r * (TC_ROWS * 128) + (((2 * q + c4) ^ (rl % 8)) * 16)) =
                                 make_uint4(hp[4 * c4], hp[4 * c4 + 1], hp[4 * c4 + 2], hp[4 * c4 + 3]);
                         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                         __syncwarp();
-                        if (lane == 0) fu_arrive(bar(FB_HREADY + c / 2));
+                        if (lane == 0) fu_arrive(bar(FB_HREADY + r));
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
+                        for (int j = 0; j < 8; ++j) {
                             part = __fmaf_rn(bf16_lo(hp[j]), w5_s[col + 2 * j], part);
                             part = __fmaf_rn(bf16_hi(hp[j]), w5_s[col + 2 * j + 1], part);
                         }
@@ -870,7 +885,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
                                  :: "r"(bar(FB_WFULL + st)), "r"(FU_CHUNK_BYTES) : "memory");
                     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                                 :: "r"(ring0 + st * FU_CHUNK_BYTES), "l"(P.wtc + (size_t)ch * FU_CHUNK_BYTES),
+                                 :: "r"(ring0 + st * FU_CHUNK_BYTES), "l"(wtc + (size_t)ch * FU_CHUNK_BYTES),
                                     "r"(FU_CHUNK_BYTES), "r"(bar(FB_WFULL + st))
                                  : "memory");
                 }
@@ -904,7 +919,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                         fu_commit(bar(FB_FEATEMPTY));
                     } else {
                         for (int c = 0; c < FU_CHUNKS; ++c, ++consumed) {
-                            /* blocks 2c, 2c+1 of the previous layer's activations (hready
+                            /* K columns 64c.. of the previous layer's activations (hready
                                phases advance once per hidden layer, in order) */
                             if (!(ok = fu_wait(bar(FB_HREADY + c), hr_ph, abort_flag, P.err))) break;
                             const uint32_t st = consumed % FU_NS;
