@@ -60,26 +60,35 @@ struct EpiArgs {
  * Mathematical Functions, eq. 7.1.28: for x >= 0,
  *     erfc(x) = 1 - erf(x) = 1 / (1 + a1 x + a2 x^2 + ... + a6 x^6)^16,
  * |error| <= 3e-7, far below the BF16 rounding of the activations it
- * feeds.  With x = |z|/sqrt2 and h = erfc(x)/2, Phi(z) = 1 - h for z >= 0
- * and h for z < 0.  One reciprocal is the only special-function
- * instruction (the multi-function unit's throughput bounds the inference
- * epilogue); the polynomial and the four squarings run as FMAs.  For large
- * x the 16th power overflows to infinity and erfc to 0, its limit. */
-__device__ __forceinline__ float gelu_phi(float z)
+ * feeds.  The coefficients (with the 1) are scaled by 2^(1/16), so that the
+ * reciprocal of the 16th power is h = erfc(x)/2 directly; with x = |z|/sqrt2,
+ * Phi(z) = 1 - h for z >= 0 and h for z < 0, so
+ *     GELU(z) = max(z, 0) - |z| h.
+ * One approximate reciprocal is the only special-function instruction (the
+ * multi-function unit's throughput and the issue rate bound the inference
+ * epilogue).  For large x the 16th power overflows to infinity and h to 0,
+ * its limit. */
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float gelu_h(float z)   /* erfc(|z|/sqrt2) / 2 = min(Phi(z), 1 - Phi(z)) */
 {
     const float x = __fmul_rn(fabsf(z), 0.70710678118654752f);
-    float y = __fmaf_rn(0.0000430638f, x, 0.0002765672f);
-    y = __fmaf_rn(y, x, 0.0001520143f);
-    y = __fmaf_rn(y, x, 0.0092705272f);
-    y = __fmaf_rn(y, x, 0.0422820123f);
-    y = __fmaf_rn(y, x, 0.0705230784f);
-    y = __fmaf_rn(y, x, 1.0f);
+    float y = __fmaf_rn(4.497039844864048e-05f, x, 0.0002888118615373969f);
+    y = __fmaf_rn(y, x, 0.0001587445440236479f);
+    y = __fmaf_rn(y, x, 0.009680968709290028f);
+    y = __fmaf_rn(y, x, 0.04415399581193924f);
+    y = __fmaf_rn(y, x, 0.07364540547132492f);
+    y = __fmaf_rn(y, x, 1.0442737340927124f);
     y = __fmul_rn(y, y);
     y = __fmul_rn(y, y);
     y = __fmul_rn(y, y);
-    y = __fmul_rn(y, y);                                   /* P(x)^16 */
-    const float h = __fdividef(0.5f, y);                   /* erfc(x) / 2 */
-    return z >= 0.0f ? 1.0f - h : h;
+    y = __fmul_rn(y, y);                                   /* 2 P(x)^16 */
+    return rcp_approx(y);
 }
 
 __device__ __forceinline__ float ex2_approx(float x)
@@ -91,14 +100,16 @@ __device__ __forceinline__ float ex2_approx(float x)
 
 __device__ __forceinline__ float gelu_f(float z)
 {
-    return __fmul_rn(z, gelu_phi(z));
+    return __fmaf_rn(-fabsf(z), gelu_h(z), fmaxf(z, 0.0f));
 }
 
 __device__ __forceinline__ float gelu_grad(float z)
 {
     /* Phi(z) + z pdf(z), pdf(z) = exp(-z^2/2) / sqrt(2 pi) = 2^(-z^2 log2(e) / 2) / sqrt(2 pi) */
+    const float h = gelu_h(z);
+    const float phi = z >= 0.0f ? 1.0f - h : h;
     const float e = ex2_approx(__fmul_rn(__fmul_rn(z, z), -0.72134752044448170f));
-    return __fmaf_rn(z, 0.39894228040143268f * e, gelu_phi(z));
+    return __fmaf_rn(z, 0.39894228040143268f * e, phi);
 }
 
 /* two floats -> a packed BF16 pair (a in the low half), round to nearest
@@ -823,10 +834,16 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                     const int col = 64 * r + 16 * q;
                     float v[16];
                     tc_ld16(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + col), v);
+                    float bv[16];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float4 b4 = reinterpret_cast<const float4*>(bl + col)[j];
+                        bv[4 * j] = b4.x; bv[4 * j + 1] = b4.y; bv[4 * j + 2] = b4.z; bv[4 * j + 3] = b4.w;
+                    }
                     uint32_t hp[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j)
-                        hp[j] = pack_bf16(gelu_f(v[2 * j] + bl[col + 2 * j]), gelu_f(v[2 * j + 1] + bl[col + 2 * j + 1]));
+                        hp[j] = pack_bf16(gelu_f(v[2 * j] + bv[2 * j]), gelu_f(v[2 * j + 1] + bv[2 * j + 1]));
                     if (l < NLAYER - 1) {
                         /* over the previous layer's activations (whose MMAs have all
                            completed): atom column r, 16-byte groups 2q, 2q+1 */

@@ -184,13 +184,22 @@ def test_gpu_fused_inference_equals_layered_kernels(n):
 
 def test_erf_approximation_error_bound():
     """The GELU's erfc on the device is Abramowitz & Stegun 7.1.28,
-    1 / (1 + a1 x + ... + a6 x^6)^16; in exact arithmetic its error stays
-    within the published 3e-7 (FP32 rounding of the device evaluation adds
-    a few ulp, below BF16 resolution)."""
+    1 / (1 + a1 x + ... + a6 x^6)^16 (published |error| <= 3e-7), with the
+    polynomial scaled by 2^(1/16) so that the reciprocal gives h = erfc/2.
+    With the coefficients rounded to FP32 (the 16th power amplifies their
+    rounding 16-fold) h stays within 5e-7, and GELU(z) = max(z, 0) - |z| h
+    equals z Phi(z) to 1e-5 - both far below the BF16 rounding of the
+    activations."""
     import math
     x = np.linspace(0.0, 12.0, 240001)
-    a = [0.0705230784, 0.0422820123, 0.0092705272, 0.0001520143, 0.0002765672, 0.0000430638]
-    p = 1.0 + sum(c * x ** (i + 1) for i, c in enumerate(a))
-    r = 1.0 / p ** 16
-    ref = np.vectorize(math.erfc)(x)
-    assert np.max(np.abs(r - ref)) <= 3e-7
+    c = [1.0442737340927124, 0.07364540547132492, 0.04415399581193924, 0.009680968709290028,
+         0.0001587445440236479, 0.0002888118615373969, 4.497039844864048e-05]
+    p = sum(ci * x ** i for i, ci in enumerate(c))
+    h = 1.0 / p ** 16
+    ref = np.vectorize(math.erfc)(x) / 2
+    assert np.max(np.abs(h - ref)) <= 5e-7
+    z = np.linspace(-8.0, 8.0, 4001)
+    hz = np.interp(np.abs(z) / math.sqrt(2.0), x, h)
+    gelu = np.maximum(z, 0.0) - np.abs(z) * hz
+    exact = z * 0.5 * (1.0 + np.vectorize(math.erf)(z / math.sqrt(2.0)))
+    assert np.max(np.abs(gelu - exact)) <= 1e-5
