@@ -34,6 +34,7 @@ Extra legs in the same line (not part of `value`):
              checker on a bounded sample of them;
   mlp        collision-predictor inference on 2^22 rows: the fused tcgen05
              kernel against per-layer tcgen05 kernels and the training GEMMs;
+             training throughput (batch 4096) with tcgen05 and mma.sync GEMMs;
   batch      256 independent problems in one graph-captured launch per kind
              against a loop of per-problem launches.
 
@@ -494,6 +495,25 @@ def mlp_leg(args, dev):
         ms = e0.elapsed_time(e1) / args.steps
         tf = n * MLP_FLOPS_PER_ROW / (ms * 1e-3) / 1e12
         res[path] = {"ms": ms, "tflops": tf, "rows_per_s": n / (ms * 1e-3), "frac_of_bf16_peak": tf / peak}
+    # training: 2 epochs over 2^20 labelled rows, batch 4096 (each epoch one
+    # captured CUDA graph of 256 steps: features, forward, loss, backward, Adam)
+    nt, bt, ep = 1 << 20, 4096, 2
+    qt = torch.tensor(rng.uniform(-np.pi, np.pi, (6, nt)).astype(np.float32), device=dev)
+    yt = torch.tensor((rng.random(nt) < 0.4).astype(np.float32), device=dev)
+    train = {"rows": nt, "batch": bt, "epochs": ep, "flops_per_step": 3 * bt * MLP_FLOPS_PER_ROW}
+    for path in ("tcgen05", "mma_sync"):
+        m2 = CollisionMLP(6, seed=args.seed + 2)
+        m2.set_training(path)
+        m2.train(qt[:, :bt * 8].contiguous(), yt[:bt * 8].contiguous(), epochs=1, batch=bt)   # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m2.train(qt, yt, epochs=ep, batch=bt)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        steps = ep * (nt // bt)
+        train[path] = {"seconds": dt, "ms_per_step": 1e3 * dt / steps,
+                       "tflops": steps * train["flops_per_step"] / dt / 1e12, "device_status": m2.device_status()}
+    res["training"] = train
     res["device_status"] = mlp.device_status()
     res["peak_tflops"] = peak
     res["peak_source"] = "MEASURED_PEAKS.json bf16_tflops (burst)"

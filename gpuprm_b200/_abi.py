@@ -17,6 +17,8 @@ GPRM_EDGES_ALL_STEPS = 1
 GPRM_MLP_INFER_TCGEN05 = 0
 GPRM_MLP_INFER_TRAINING_GEMM = 1
 GPRM_MLP_INFER_TCGEN05_LAYERS = 2
+GPRM_MLP_TRAIN_TCGEN05 = 0
+GPRM_MLP_TRAIN_MMA_SYNC = 1
 GPRM_MAX_DOF = 7
 GPRM_MAX_VERTICES = 100
 GPRM_NOALLOC_MAX_CONFIGS = 65536
@@ -134,6 +136,7 @@ SIGNATURES = [
     ("gprm_mlp_gradients", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, _F, _F]),
     ("gprm_mlp_adam_step", C.c_int, [_P, C.c_float]),
     ("gprm_mlp_set_inference", C.c_int, [_P, C.c_int]),
+    ("gprm_mlp_set_training", C.c_int, [_P, C.c_int]),
     ("gprm_mlp_device_status", C.c_int, [_P, C.POINTER(C.c_uint)]),
     ("gprm_mlp_train", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                  C.c_float, _F]),

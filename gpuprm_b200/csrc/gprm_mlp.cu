@@ -14,6 +14,8 @@
  * H_l = gelu(Z_l).  Backward:  dZ_l = dH_l * gelu'(Z_l),
  * dW_l = dZ_l^T H_{l-1},  db_l = colsum(dZ_l),  dH_{l-1} = dZ_l W_l.
  */
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -997,6 +999,268 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                      : "memory");
 }
 
+
+/* ------------------------------------------------------------------ */
+/* training GEMMs on the tensor cores (tcgen05, operands loaded by TMA)  */
+/* ------------------------------------------------------------------ */
+/*
+ * k_tc_gemm computes one 128 x BN tile of C = A B^T over a range of K,
+ * with A [M x K] and B [N x K] row-major BF16 in global memory, both read
+ * by 2-D TMA loads (box 64 K x rows, 128-byte swizzle, zero fill outside
+ * the tensor) into a 4-stage ring; one thread issues M=128 N=BN K=16
+ * tcgen05.mma into a BN-column TMEM accumulator; four epilogue warps read
+ * it back and apply one of:
+ *   TG_FWD    z = acc + bias[n]: Z (FP32) and H = GELU(z) (BF16), row-major;
+ *   TG_DH     dZ = acc * GELU'(Zin) (BF16), row-major (backward through a layer);
+ *   TG_WPART  the FP32 partial sum of this K split, row-major into the
+ *             split's slice of a workspace (weight gradients, reduced by
+ *             k_reduce_w in a fixed order).
+ * Warps: 0 loads, 1 issues the MMAs (and owns TMEM), 2-5 run the epilogue
+ * (warp w reads TMEM lanes 32 (w % 4) ..).  Waits are bounded like those of
+ * k_mlp_fused.
+ */
+enum { TG_FWD = 0, TG_DH = 1, TG_WPART = 2 };
+constexpr int TG_STAGES = 4;
+constexpr int TG_MAX_SPLITS = 32;
+constexpr int TG_THREADS = 192;
+
+template <int BN>
+struct TgSmem {
+    static constexpr size_t A_BYTES = (size_t)TC_ROWS * 128;       /* 128 rows x 64 BF16 */
+    static constexpr size_t B_BYTES = (size_t)BN * 128;
+    static constexpr size_t STAGE = A_BYTES + B_BYTES;
+    static constexpr size_t BARS = TG_STAGES * STAGE;
+    static constexpr size_t TADDR = BARS + (2 * TG_STAGES + 2) * 8;
+    static constexpr size_t ABORT = TADDR + 4;
+    static constexpr size_t BYTES = ABORT + 4 + 1024;               /* + alignment slack */
+};
+
+struct TgArgs {
+    int M, N, K, kps;          /* rows, columns, depth, K per split (multiple of 64) */
+    const float* bias;         /* TG_FWD */
+    float* zout;               /* TG_FWD: Z [M x ldc] */
+    __nv_bfloat16* hout;       /* TG_FWD: H, TG_DH: dZ [M x ldc] */
+    const float* zin;          /* TG_DH: Z of the layer below [M x ldc] */
+    float* ws;                 /* TG_WPART: [splits][M x ldc] */
+    int ldc;
+    unsigned* err;
+};
+
+__device__ __forceinline__ void tg_tma_load(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                 :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
+}
+
+template <int EPI, int BN>
+__global__ void __launch_bounds__(TG_THREADS, 1)
+k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TgArgs g)
+{
+    extern __shared__ __align__(1024) unsigned char sm_raw[];
+    using L = TgSmem<BN>;
+    /* the swizzle atoms need 1024-byte alignment */
+    unsigned char* sm = sm_raw + ((1024u - (smem_u32(sm_raw) & 1023u)) & 1023u);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t bars = smem_u32(sm + L::BARS);
+    auto bar = [&](int i) { return bars + 8u * (uint32_t)i; };   /* full 0..3, empty 4..7, accfull 8 */
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::ABORT);
+    uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(sm + L::TADDR);
+    const int m0 = blockIdx.y * TC_ROWS, n0 = blockIdx.x * BN;
+    const int kb = blockIdx.z * g.kps;
+    const int ke = min(g.K, kb + g.kps);
+    const int nchunks = ke > kb ? (ke - kb + 63) / 64 : 0;
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(TC_ROWS >> 4) << 24);
+    if (tid == 0) {
+        *abort_flag = 0;
+        for (int i = 0; i < 2 * TG_STAGES + 1; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(bar(i)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     :: "r"(smem_u32(taddr_slot)), "r"(BN < 32 ? 32 : BN) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *taddr_slot;
+    const uint32_t st0 = smem_u32(sm);
+
+    if (warp == 0) {
+        if (lane == 0) {
+            bool ok = true;
+            int c = 0;
+            for (; c < nchunks && ok; ++c) {
+                const int s = c % TG_STAGES, k = c / TG_STAGES;
+                if (k > 0 && !(ok = fu_wait(bar(TG_STAGES + s), (k - 1) & 1u, abort_flag, g.err))) break;
+                const uint32_t a_dst = st0 + (uint32_t)(s * L::STAGE);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                             :: "r"(bar(s)), "r"((uint32_t)L::STAGE) : "memory");
+                tg_tma_load(a_dst, &mapA, kb + 64 * c, m0, bar(s));
+                tg_tma_load(a_dst + (uint32_t)L::A_BYTES, &mapB, kb + 64 * c, n0, bar(s));
+            }
+            /* the loads still in flight land before the CTA leaves */
+            for (int j = c > TG_STAGES ? c - TG_STAGES : 0; j < c; ++j)
+                fu_wait_drain(bar(j % TG_STAGES), (j / TG_STAGES) & 1u, g.err);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            bool ok = true;
+            for (int c = 0; c < nchunks && ok; ++c) {
+                const int s = c % TG_STAGES;
+                if (!(ok = fu_wait(bar(s), (c / TG_STAGES) & 1u, abort_flag, g.err))) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t a = st0 + (uint32_t)(s * L::STAGE), b = a + (uint32_t)L::A_BYTES;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint64_t ad = tc_sdesc_sw128(a + 32u * j), bd = tc_sdesc_sw128(b + 32u * j);
+                    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                                 :: "r"(tmem), "l"(ad), "l"(bd), "r"(IDESC), "r"((c | j) != 0 ? 1u : 0u),
+                                    "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                }
+                fu_commit(bar(TG_STAGES + s));
+            }
+            /* accfull: every MMA issued has completed (also on the abort path) */
+            fu_commit(bar(2 * TG_STAGES));
+        }
+    } else {
+        const int q = warp & 3;                      /* TMEM lane quarter */
+        const int rl = 32 * q + lane, m = m0 + rl;
+        const bool ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(2 * TG_STAGES), 0u, abort_flag, g.err));
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (ok) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                float v[32];
+                __syncwarp();
+                tc_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                if (nchunks == 0) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = 0.0f;
+                }
+                const int n = n0 + c0;
+                const size_t o = (size_t)m * g.ldc + n;
+                if (m >= g.M || n >= g.N) {
+                    /* row or columns outside C: nothing to store */
+                } else if (EPI == TG_FWD) {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4) {
+                        const float4 b4 = *reinterpret_cast<const float4*>(g.bias + n + j);
+                        const float4 z4 = make_float4(v[j] + b4.x, v[j + 1] + b4.y, v[j + 2] + b4.z, v[j + 3] + b4.w);
+                        *reinterpret_cast<float4*>(g.zout + o + j) = z4;
+                        v[j] = z4.x; v[j + 1] = z4.y; v[j + 2] = z4.z; v[j + 3] = z4.w;
+                    }
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4)
+                        *reinterpret_cast<uint4*>(g.hout + o + 8 * c4) = make_uint4(
+                            pack_bf16(gelu_f(v[8 * c4]), gelu_f(v[8 * c4 + 1])),
+                            pack_bf16(gelu_f(v[8 * c4 + 2]), gelu_f(v[8 * c4 + 3])),
+                            pack_bf16(gelu_f(v[8 * c4 + 4]), gelu_f(v[8 * c4 + 5])),
+                            pack_bf16(gelu_f(v[8 * c4 + 6]), gelu_f(v[8 * c4 + 7])));
+                } else if (EPI == TG_DH) {
+                    float zz[32];
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4) {
+                        const float4 z4 = *reinterpret_cast<const float4*>(g.zin + o + j);
+                        zz[j] = z4.x; zz[j + 1] = z4.y; zz[j + 2] = z4.z; zz[j + 3] = z4.w;
+                    }
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4)
+                        *reinterpret_cast<uint4*>(g.hout + o + 8 * c4) = make_uint4(
+                            pack_bf16(v[8 * c4] * gelu_grad(zz[8 * c4]), v[8 * c4 + 1] * gelu_grad(zz[8 * c4 + 1])),
+                            pack_bf16(v[8 * c4 + 2] * gelu_grad(zz[8 * c4 + 2]), v[8 * c4 + 3] * gelu_grad(zz[8 * c4 + 3])),
+                            pack_bf16(v[8 * c4 + 4] * gelu_grad(zz[8 * c4 + 4]), v[8 * c4 + 5] * gelu_grad(zz[8 * c4 + 5])),
+                            pack_bf16(v[8 * c4 + 6] * gelu_grad(zz[8 * c4 + 6]), v[8 * c4 + 7] * gelu_grad(zz[8 * c4 + 7])));
+                } else {
+                    float* w = g.ws + (size_t)blockIdx.z * ((size_t)g.M * g.ldc) + o;
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4)
+                        *reinterpret_cast<float4*>(w + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp == 1) {
+        __syncwarp();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(BN < 32 ? 32 : BN)
+                     : "memory");
+    }
+}
+
+/* g_w[o][i] (i < kin) = sum over the splits of ws[s][o][i] (ld ldw), in split order. */
+__global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* __restrict__ ws, float* __restrict__ gw)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= rows * kin) return;
+    const int o = t / kin, i = t % kin;
+    float acc = 0.0f;
+    for (int s = 0; s < splits; ++s) acc += ws[(size_t)s * rows * ldw + (size_t)o * ldw + i];
+    gw[t] = acc;
+}
+
+/* dst[c][r] = src[r][c] for r < rows, c < cols (ld of dst = ldd); 32x32 tiles. */
+__global__ void k_transpose_bf16(int rows, int cols, const __nv_bfloat16* __restrict__ src, int lds,
+                                 __nv_bfloat16* __restrict__ dst, int ldd)
+{
+    __shared__ __nv_bfloat16 t[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        t[k][threadIdx.x] = (r < rows && c < cols) ? src[(size_t)r * lds + c] : __float2bfloat16(0.0f);
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (c < cols && r < rows) dst[(size_t)c * ldd + r] = t[threadIdx.x][k];
+    }
+}
+
+/* The tensor-core training copies of the weights: W1 padded to 64 inputs
+ * (zeros) and W_l^T for the hidden layers 2..4 (the B operand of the
+ * backward GEMMs through them). */
+__global__ void k_tc_weights(const __nv_bfloat16* __restrict__ wbf, long long o0, long long o1, long long o2,
+                             long long o3, __nv_bfloat16* __restrict__ w1p, __nv_bfloat16* __restrict__ wt)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < HID * 64) {
+        const int o = t / 64, i = t % 64;
+        w1p[t] = i < IN_PAD ? wbf[o0 + (long long)o * IN_PAD + i] : __float2bfloat16(0.0f);
+    } else if (t < HID * 64 + 3 * HID * HID) {
+        const int u = t - HID * 64, l = u / (HID * HID), r = u % (HID * HID);
+        const int i = r / HID, o = r % HID;                 /* wt_l[i][o] = W_l[o][i] */
+        const long long off = l == 0 ? o1 : (l == 1 ? o2 : o3);
+        wt[u] = wbf[off + (long long)o * HID + i];
+    }
+}
+
+/* Features padded to 64 columns (the tensor-core K step): row i of X64 =
+ * sin/cos of configuration idx[i] (or i), zeros beyond 2 ndof. */
+__global__ void k_features64(const float* __restrict__ q, long long offset, int ndof, int n,
+                             const int* __restrict__ idx, __nv_bfloat16* __restrict__ X)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const long long src = idx ? idx[i] : i;
+        uint32_t x[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) x[j] = 0u;
+#pragma unroll
+        for (int j = 0; j < IN_PAD / 2; ++j) {
+            float sv = 0.0f, cv = 0.0f;
+            if (j < ndof) sincosf(q[src + offset * j], &sv, &cv);
+            x[j] = pack_bf16(j < ndof ? sv : 0.0f, j < ndof ? cv : 0.0f);
+        }
+        uint4* row = reinterpret_cast<uint4*>(X + (size_t)i * 64);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) row[c] = make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
+    }
+}
+
 }  // namespace
 
 /* ====================================================================== */
@@ -1028,6 +1292,17 @@ struct gprm_mlp {
     __nv_bfloat16 *Ha = nullptr, *Hb = nullptr;
     int infer_rows = 0;
     unsigned char* wtc = nullptr;       /* weights in the fused kernel's chunk order */
+    /* training on the tensor cores (k_tc_gemm) */
+    int train_path = GPRM_MLP_TRAIN_TCGEN05;
+    __nv_bfloat16* X64 = nullptr;       /* features padded to 64 columns [rows x 64] */
+    __nv_bfloat16 *Ta = nullptr, *Tb = nullptr;   /* transposes [256 x ldT] */
+    int ldT = 0;
+    __nv_bfloat16* w1p = nullptr;       /* W1 padded [256 x 64] */
+    __nv_bfloat16* wt = nullptr;        /* W_l^T, layers 2..4 [3 x 256 x 256] */
+    float* ws = nullptr;                /* split-K partials [TG_MAX_SPLITS x 256 x 256] */
+    int tc_n = -1;                      /* batch the tensor maps were made for */
+    int tc_attr = 0;
+    CUtensorMap m_x64, m_h[NLAYER - 1], m_dz[NLAYER], m_w1p, m_w[NLAYER - 1], m_wt[NLAYER - 1], m_ta, m_tb256, m_tb64;
     unsigned* dev_err = nullptr;
     int sms = 0;
     std::string err = "no error";
@@ -1064,15 +1339,166 @@ int alloc_batch(gprm_mlp* h, int rows)
     MLP_TRY(h, cudaMalloc((void**)&h->dlogit, R * sizeof(float)));
     MLP_TRY(h, cudaMalloc((void**)&h->ybatch, R * sizeof(float)));
     MLP_TRY(h, cudaMalloc((void**)&h->idx, R * sizeof(int)));
+    cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb);
+    h->ldT = (rows + 63) / 64 * 64;
+    MLP_TRY(h, cudaMalloc((void**)&h->X64, R * 64 * sizeof(__nv_bfloat16)));
+    MLP_TRY(h, cudaMalloc((void**)&h->Ta, (size_t)HID * h->ldT * sizeof(__nv_bfloat16)));
+    MLP_TRY(h, cudaMalloc((void**)&h->Tb, (size_t)HID * h->ldT * sizeof(__nv_bfloat16)));
+    if (!h->w1p) {
+        MLP_TRY(h, cudaMalloc((void**)&h->w1p, (size_t)HID * 64 * sizeof(__nv_bfloat16)));
+        MLP_TRY(h, cudaMalloc((void**)&h->wt, (size_t)(NLAYER - 1) * HID * HID * sizeof(__nv_bfloat16)));
+        MLP_TRY(h, cudaMalloc((void**)&h->ws, (size_t)TG_MAX_SPLITS * HID * HID * sizeof(float)));
+    }
+    h->tc_n = -1;
     h->max_batch = rows;
     return GPRM_OK;
 }
 
 dim3 ggrid(int M, int N) { return dim3((N + BN - 1) / BN, (M + BM - 1) / BM); }
 
+
+/* ---- training on the tensor cores: tensor maps, forward, backward ---- */
+
+int tc_setup(gprm_mlp* h);
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode_tiled = nullptr;
+
+int tc_map(gprm_mlp* h, CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
+           uint32_t box_outer)
+{
+    if (!g_encode_tiled) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return mfail(h, GPRM_ERR_CUDA, "cuTensorMapEncodeTiled is not available", e);
+        g_encode_tiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[2] = {inner, outer};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {64u, box_outer};
+    const cuuint32_t es[2] = {1u, 1u};
+    const CUresult r = g_encode_tiled(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                                      box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return mfail(h, GPRM_ERR_CUDA, "encoding a tensor map");
+    return GPRM_OK;
+}
+
+/* Tensor maps of the training buffers for a batch of n rows (made again
+ * when n or the buffers change). */
+int tc_maps(gprm_mlp* h, int n)
+{
+    if (h->tc_n == n) return GPRM_OK;
+    int rc;
+    const uint64_t N = (uint64_t)n;
+    if ((rc = tc_map(h, &h->m_x64, h->X64, 64, N, 64 * 2, TC_ROWS))) return rc;
+    for (int l = 0; l < NLAYER - 1; ++l)
+        if ((rc = tc_map(h, &h->m_h[l], h->H[l], HID, N, HID * 2, TC_ROWS))) return rc;
+    for (int l = 0; l < NLAYER; ++l)
+        if ((rc = tc_map(h, &h->m_dz[l], h->dZ[l], HID, N, HID * 2, TC_ROWS))) return rc;
+    if ((rc = tc_map(h, &h->m_w1p, h->w1p, 64, HID, 64 * 2, HID))) return rc;
+    for (int l = 1; l < NLAYER; ++l) {
+        if ((rc = tc_map(h, &h->m_w[l - 1], h->wbf + h->offWbf[l], HID, HID, HID * 2, HID))) return rc;
+        if ((rc = tc_map(h, &h->m_wt[l - 1], h->wt + (size_t)(l - 1) * HID * HID, HID, HID, HID * 2, HID))) return rc;
+    }
+    if ((rc = tc_map(h, &h->m_ta, h->Ta, N, HID, (uint64_t)h->ldT * 2, TC_ROWS))) return rc;
+    if ((rc = tc_map(h, &h->m_tb256, h->Tb, N, HID, (uint64_t)h->ldT * 2, HID))) return rc;
+    if ((rc = tc_map(h, &h->m_tb64, h->Tb, N, 64, (uint64_t)h->ldT * 2, 64))) return rc;
+    if (!h->tc_attr) {
+        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_FWD, HID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TgSmem<HID>::BYTES));
+        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_DH, HID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TgSmem<HID>::BYTES));
+        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_WPART, HID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TgSmem<HID>::BYTES));
+        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_WPART, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TgSmem<64>::BYTES));
+        h->tc_attr = 1;
+    }
+    h->tc_n = n;
+    return GPRM_OK;
+}
+
+/* Forward through the tensor-core GEMMs on rows featurised in h->X64. */
+int forward_tc(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, float inv_b, cudaStream_t st)
+{
+    int rc = tc_setup(h);
+    if (rc || (rc = tc_maps(h, n))) return rc;
+    const int items = HID * 64 + (NLAYER - 1) * HID * HID;
+    k_tc_weights<<<(items + 255) / 256, 256, 0, st>>>(h->wbf, h->offWbf[0], h->offWbf[1], h->offWbf[2],
+                                                      h->offWbf[3], h->w1p, h->wt);
+    const dim3 grid(1, (n + TC_ROWS - 1) / TC_ROWS, 1);
+    for (int l = 0; l < NLAYER; ++l) {
+        TgArgs a{};
+        a.M = n; a.N = HID; a.K = l == 0 ? 64 : HID; a.kps = a.K;
+        a.bias = h->w + h->offB[l]; a.zout = h->Z[l]; a.hout = h->H[l]; a.ldc = HID; a.err = h->dev_err;
+        k_tc_gemm<TG_FWD, HID><<<grid, TG_THREADS, TgSmem<HID>::BYTES, st>>>(l == 0 ? h->m_x64 : h->m_h[l - 1],
+                                                                          l == 0 ? h->m_w1p : h->m_w[l - 1], a);
+    }
+    int blocks = (n * 32 + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    k_out<<<blocks, 256, 0, st>>>(n, h->H[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->w + h->offB[NLAYER], p, y,
+                                  yidx, h->dlogit, h->loss, inv_b);
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+/* Backward through the tensor-core GEMMs (after forward_tc on the same rows). */
+int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
+{
+    MLP_TRY(h, cudaMemsetAsync(h->g, 0, (size_t)h->nparam * sizeof(float), st));
+    int blocks = n < 1024 ? n : 1024;
+    k_out_back<<<blocks, HID, 0, st>>>(n, h->H[NLAYER - 1], h->Z[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->dlogit,
+                                       h->g + h->offW[NLAYER], h->g + h->offB[NLAYER], h->dZ[NLAYER - 1]);
+    /* weight gradients: K = n split over CTAs, partials reduced in split order */
+    int splits = (n + 127) / 128;
+    if (splits > TG_MAX_SPLITS) splits = TG_MAX_SPLITS;
+    const int kps = ((n + splits - 1) / splits + 63) / 64 * 64;
+    splits = (n + kps - 1) / kps;
+    const dim3 tgrid(HID / 32, (n + 31) / 32), tblock(32, 8);
+    for (int l = NLAYER - 1; l >= 0; --l) {
+        const int kin = l == 0 ? IN_PAD : HID, kin_p = l == 0 ? 64 : HID;
+        /* dW_l = dZ_l^T H_{l-1}: A = dZ_l^T [256 x n], B = H_{l-1}^T [kin_p x n] */
+        k_transpose_bf16<<<tgrid, tblock, 0, st>>>(n, HID, h->dZ[l], HID, h->Ta, h->ldT);
+        k_transpose_bf16<<<dim3(kin_p / 32, (n + 31) / 32), tblock, 0, st>>>(n, kin_p, l == 0 ? h->X64 : h->H[l - 1],
+                                                                             kin_p, h->Tb, h->ldT);
+        TgArgs a{};
+        a.M = HID; a.N = kin_p; a.K = n; a.kps = kps; a.ws = h->ws; a.ldc = kin_p; a.err = h->dev_err;
+        if (l == 0)
+            k_tc_gemm<TG_WPART, 64><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<64>::BYTES, st>>>(
+                h->m_ta, h->m_tb64, a);
+        else
+            k_tc_gemm<TG_WPART, HID><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<HID>::BYTES, st>>>(
+                h->m_ta, h->m_tb256, a);
+        k_reduce_w<<<(HID * kin + 255) / 256, 256, 0, st>>>(splits, HID, kin_p, kin, h->ws, h->g + h->offW[l]);
+        k_colsum<<<blocks, HID, 0, st>>>(n, HID, h->dZ[l], h->g + h->offB[l]);
+        if (l > 0) {
+            /* dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}): A = dZ_l [n x 256], B = W_l^T [256 x 256] */
+            TgArgs d{};
+            d.M = n; d.N = HID; d.K = HID; d.kps = HID; d.zin = h->Z[l - 1]; d.hout = h->dZ[l - 1]; d.ldc = HID;
+            d.err = h->dev_err;
+            k_tc_gemm<TG_DH, HID><<<dim3(1, (n + TC_ROWS - 1) / TC_ROWS, 1), TG_THREADS, TgSmem<HID>::BYTES, st>>>(
+                h->m_dz[l], h->m_wt[l - 1], d);
+        }
+    }
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
+/* Features of n rows (idx: row gather or null) for the current training path. */
+void features(gprm_mlp* h, const float* q, int offset, int n, const int* idx, cudaStream_t st)
+{
+    if (h->train_path == GPRM_MLP_TRAIN_TCGEN05)
+        k_features64<<<(n + 255) / 256, 256, 0, st>>>(q, offset, h->ndof, n, idx, h->X64);
+    else
+        k_features<<<(n + 255) / 256, 256, 0, st>>>(q, offset, h->ndof, n, idx, h->X);
+}
+
 /* Forward on rows already featurised in h->X; p written to `p`. */
 int forward(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, float inv_b, cudaStream_t st)
 {
+    if (h->train_path == GPRM_MLP_TRAIN_TCGEN05) return forward_tc(h, n, p, y, yidx, inv_b, st);
     const __nv_bfloat16* in = h->X;
     int kin = IN_PAD;
     for (int l = 0; l < NLAYER; ++l) {
@@ -1098,6 +1524,7 @@ int forward(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, float
  * accumulate into h->g (zeroed here). */
 int backward(gprm_mlp* h, int n, cudaStream_t st)
 {
+    if (h->train_path == GPRM_MLP_TRAIN_TCGEN05) return backward_tc(h, n, st);
     MLP_TRY(h, cudaMemsetAsync(h->g, 0, (size_t)h->nparam * sizeof(float), st));
     int blocks = n < 1024 ? n : 1024;
     k_out_back<<<blocks, HID, 0, st>>>(n, h->H[NLAYER - 1], h->Z[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->dlogit,
@@ -1301,6 +1728,7 @@ void gprm_mlp_destroy(gprm_mlp* h)
     for (int l = 0; l < NLAYER; ++l) { cudaFree(h->H[l]); cudaFree(h->Z[l]); cudaFree(h->dZ[l]); }
     cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
     cudaFree(h->Ha); cudaFree(h->Hb); cudaFree(h->dev_err); cudaFree(h->wtc);
+    cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb); cudaFree(h->w1p); cudaFree(h->wt); cudaFree(h->ws);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -1340,7 +1768,7 @@ int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, v
     if (rc) return rc;
     for (int s = 0; s < n; s += chunk) {
         int c = n - s < chunk ? n - s : chunk;
-        k_features<<<(c + 255) / 256, 256, 0, st>>>(q + s, offset, h->ndof, c, nullptr, h->X);
+        features(h, q + s, offset, c, nullptr, st);
         rc = forward(h, c, p + s, nullptr, nullptr, 0.0f, st);
         if (rc) return rc;
     }
@@ -1356,7 +1784,7 @@ int gprm_mlp_gradients(gprm_mlp* h, const float* q, const float* y, int n, int o
     int rc = alloc_batch(h, n);
     if (rc) return rc;
     MLP_TRY(h, cudaMemsetAsync(h->loss, 0, sizeof(float), h->st));
-    k_features<<<(n + 255) / 256, 256, 0, h->st>>>(q, offset, h->ndof, n, nullptr, h->X);
+    features(h, q, offset, n, nullptr, h->st);
     if ((rc = forward(h, n, h->p, y, nullptr, 1.0f / n, h->st))) return rc;
     if ((rc = backward(h, n, h->st))) return rc;
     MLP_TRY(h, cudaStreamSynchronize(h->st));
@@ -1388,6 +1816,8 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
         return mfail(h, GPRM_ERR_ARG, "bad arguments");
     int rc = alloc_batch(h, batch);
     if (rc) return rc;
+    /* set-up that must not run inside the stream capture below */
+    if (h->train_path == GPRM_MLP_TRAIN_TCGEN05 && ((rc = tc_setup(h)) || (rc = tc_maps(h, batch)))) return rc;
     const int steps = n / batch;
     std::vector<float> ep_loss(epochs, 0.0f);
     for (int e = 0; e < epochs; ++e) {
@@ -1399,7 +1829,7 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
         cudaMemsetAsync(h->loss, 0, sizeof(float), h->st);
         for (int s = 0; s < steps && !crc; ++s) {
             const int* idx = perm + (size_t)e * n + (size_t)s * batch;
-            k_features<<<(batch + 255) / 256, 256, 0, h->st>>>(q, offset, h->ndof, batch, idx, h->X);
+            features(h, q, offset, batch, idx, h->st);
             if (!crc) crc = forward(h, batch, h->p, y, idx, 1.0f / batch, h->st);
             if (!crc) crc = backward(h, batch, h->st);
             if (!crc) crc = adam(h, lr, h->st);
@@ -1418,6 +1848,11 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
         ep_loss[e] = l / steps;
     }
     if (losses) memcpy(losses, ep_loss.data(), epochs * sizeof(float));
+    if (h->dev_err) {
+        unsigned f = 0;
+        MLP_TRY(h, cudaMemcpy(&f, h->dev_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (f) return mfail(h, GPRM_ERR_DEVICE, "a tensor-core kernel timed out waiting for its MMAs or copies");
+    }
     return GPRM_OK;
 }
 
@@ -1428,6 +1863,15 @@ int gprm_mlp_set_inference(gprm_mlp* h, int path)
         path != GPRM_MLP_INFER_TCGEN05_LAYERS)
         return mfail(h, GPRM_ERR_ARG, "unknown inference path");
     h->infer_path = path;
+    return GPRM_OK;
+}
+
+int gprm_mlp_set_training(gprm_mlp* h, int path)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (path != GPRM_MLP_TRAIN_TCGEN05 && path != GPRM_MLP_TRAIN_MMA_SYNC)
+        return mfail(h, GPRM_ERR_ARG, "unknown training path");
+    h->train_path = path;
     return GPRM_OK;
 }
 

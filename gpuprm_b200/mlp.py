@@ -90,6 +90,12 @@ class CollisionMLP:
                 "tcgen05_layers": _abi.GPRM_MLP_INFER_TCGEN05_LAYERS}[path]
         self._check(self.lib.gprm_mlp_set_inference(self.h, code))
 
+    def set_training(self, path: str) -> None:
+        """GEMMs of training: 'tcgen05' (default; tensor-core GEMMs with
+        TMA-loaded operands) or 'mma_sync' (warp-level MMA)."""
+        code = {"tcgen05": _abi.GPRM_MLP_TRAIN_TCGEN05, "mma_sync": _abi.GPRM_MLP_TRAIN_MMA_SYNC}[path]
+        self._check(self.lib.gprm_mlp_set_training(self.h, code))
+
     def device_status(self) -> int:
         """Synchronises; 0 unless a tensor-core layer gave up waiting for its MMAs."""
         f = C.c_uint(0)

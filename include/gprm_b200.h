@@ -212,8 +212,15 @@ int gprm_mlp_predict(gprm_mlp* h, const float* q, int n, int offset, float* p, v
 #define GPRM_MLP_INFER_TRAINING_GEMM  1
 #define GPRM_MLP_INFER_TCGEN05_LAYERS 2
 int gprm_mlp_set_inference(gprm_mlp* h, int path);
+/* GEMMs of training (gprm_mlp_train, gprm_mlp_gradients, and the
+ * GPRM_MLP_INFER_TRAINING_GEMM inference path): tcgen05 tensor-core GEMMs
+ * with TMA-loaded operands (default) or warp-level mma.sync GEMMs.  Both
+ * compute the same gradients up to FP32 summation order. */
+#define GPRM_MLP_TRAIN_TCGEN05        0
+#define GPRM_MLP_TRAIN_MMA_SYNC       1
+int gprm_mlp_set_training(gprm_mlp* h, int path);
 /* Synchronises the device; *flags != 0 (and GPRM_ERR_DEVICE) when a
- * tensor-core layer gave up waiting for its MMAs. */
+ * tensor-core kernel gave up waiting for its MMAs or copies. */
 int gprm_mlp_device_status(gprm_mlp* h, unsigned* flags);
 /* one forward/backward on n device configurations with labels y (device):
  * mean BCE loss and its gradient (host arrays) */

@@ -66,8 +66,10 @@ def _gpu_setup(n=512, seed=1):
 
 
 @pytest.mark.gpu
-def test_gpu_gradients_match_oracle():
+@pytest.mark.parametrize("path", ["tcgen05", "mma_sync"])
+def test_gpu_gradients_match_oracle(path):
     mlp, q, y, q_soa, y_t = _gpu_setup()
+    mlp.set_training(path)
     params = mlp.get_params().astype(np.float64)
     g_gpu, loss_gpu = mlp.gradients(q_soa, y_t)
     loss, g, _ = MO.forward_backward(params, MO.features(q), y.astype(np.float64), emulate_bf16=True)
@@ -75,6 +77,31 @@ def test_gpu_gradients_match_oracle():
     G, Gg = MO.unpack(g), MO.unpack(g_gpu.astype(np.float64))
     for k in G:
         num = np.linalg.norm(Gg[k] - G[k])
+        den = np.linalg.norm(G[k]) + 1e-12
+        assert num / den <= 2e-2, (k, num / den)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [37, 128, 4096, 5003])
+def test_gpu_tensor_core_gradients_match_mma_sync(n):
+    """The tcgen05 training GEMMs (TMA-loaded operands, split-K weight
+    gradients reduced in a fixed order) and the mma.sync GEMMs compute the
+    same gradients up to FP32 summation order and BF16 rounding of the
+    activations; sizes cover a partial tile, one tile, the training batch
+    and a batch that is not a multiple of the K step."""
+    mlp, q, y, q_soa, y_t = _gpu_setup(n=n, seed=11)
+    mlp.set_params(mlp.get_params() * 2.0)
+    mlp.set_training("mma_sync")
+    g_ref, l_ref = mlp.gradients(q_soa, y_t)
+    mlp.set_training("tcgen05")
+    g_tc, l_tc = mlp.gradients(q_soa, y_t)
+    g_tc2, _ = mlp.gradients(q_soa, y_t)
+    assert mlp.device_status() == 0
+    assert np.array_equal(g_tc, g_tc2) or np.max(np.abs(g_tc - g_tc2)) <= 1e-6 * np.max(np.abs(g_tc))
+    assert abs(l_tc - l_ref) <= 1e-3 * abs(l_ref)
+    G, Gt = MO.unpack(g_ref.astype(np.float64)), MO.unpack(g_tc.astype(np.float64))
+    for k in G:
+        num = np.linalg.norm(Gt[k] - G[k])
         den = np.linalg.norm(G[k]) + 1e-12
         assert num / den <= 2e-2, (k, num / den)
 
@@ -99,9 +126,10 @@ def test_gpu_predict_matches_oracle():
 
 
 @pytest.mark.gpu
-def test_training_learns_exact_checker_labels():
+@pytest.mark.parametrize("path", ["tcgen05", "mma_sync"])
+def test_training_learns_exact_checker_labels(path):
     """A short training run on exact-checker labels of the hull6 scene
-    lowers the loss and beats the constant predictor."""
+    lowers the loss and beats the constant predictor (both training paths)."""
     import torch
     from gpuprm_b200 import scenes
     from gpuprm_b200.configspace import RobotConfigspace
@@ -115,6 +143,7 @@ def test_training_learns_exact_checker_labels():
     cs.check_configs_device(q, codes)
     y = (codes != 0).float()
     mlp = CollisionMLP(6, seed=4)
+    mlp.set_training(path)
     losses = mlp.train(q, y, epochs=4, batch=4096, lr=1e-3, seed=5)
     assert losses[-1] < losses[0]
     qt = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, 8192, 8).T), device="cuda:0")
