@@ -513,7 +513,7 @@ def mlp_leg(args, dev):
         steps = ep * (nt // bt)
         train[path] = {"seconds": dt, "ms_per_step": 1e3 * dt / steps,
                        "tflops": steps * train["flops_per_step"] / dt / 1e12, "device_status": m2.device_status()}
-    res["training"] = train
+    res["train"] = train
     res["device_status"] = mlp.device_status()
     res["peak_tflops"] = peak
     res["peak_source"] = "MEASURED_PEAKS.json bf16_tflops (burst)"

@@ -229,10 +229,12 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
 /* features: (sin q_j, cos q_j) for j < ndof, zero padded to IN_PAD;
  * q is SoA q[i + offset*j]; rows are optionally gathered through idx */
 __global__ void k_features(const float* __restrict__ q, long long offset, int ndof, int n,
-                           const int* __restrict__ idx, __nv_bfloat16* __restrict__ X)
+                           const int* __restrict__ idx, const long long* __restrict__ idx_off,
+                           __nv_bfloat16* __restrict__ X)
 {
+    const long long io = idx_off ? *idx_off : 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const long long src = idx ? idx[i] : i;
+        const long long src = idx ? idx[io + i] : i;
         __nv_bfloat16* row = X + (size_t)i * IN_PAD;
         for (int j = 0; j < IN_PAD / 2; ++j) {
             float s = 0.0f, c = 0.0f;
@@ -247,8 +249,10 @@ __global__ void k_features(const float* __restrict__ q, long long offset, int nd
  * p = sigmoid(H4 . w5 + b5); with labels: loss += BCE, dlogit = (p - y)/B */
 __global__ void k_out(int n, const __nv_bfloat16* __restrict__ H, const __nv_bfloat16* __restrict__ w5,
                       const float* __restrict__ b5, float* __restrict__ p, const float* __restrict__ y,
-                      const int* __restrict__ yidx, float* __restrict__ dlogit, float* __restrict__ loss, float inv_b)
+                      const int* __restrict__ yidx, const long long* __restrict__ idx_off, float* __restrict__ dlogit,
+                      float* __restrict__ loss, float inv_b)
 {
+    const long long io = idx_off ? *idx_off : 0;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int r = warp; r < n; r += nw) {
@@ -261,7 +265,7 @@ __global__ void k_out(int n, const __nv_bfloat16* __restrict__ H, const __nv_bfl
             const float pr = 1.0f / (1.0f + expf(-logit));
             if (p) p[r] = pr;
             if (y) {
-                const float yy = y[yidx ? yidx[r] : r];
+                const float yy = y[yidx ? yidx[io + r] : r];
                 /* BCE with logits, stable form */
                 const float l = fmaxf(logit, 0.0f) - logit * yy + log1pf(expf(-fabsf(logit)));
                 atomicAdd(loss, l * inv_b);
@@ -304,8 +308,12 @@ __global__ void k_colsum(int n, int cols, const __nv_bfloat16* __restrict__ dZ, 
  * bf_map[i] = index into the bf16 array or -1. */
 __global__ void k_adam(long long n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                        float* __restrict__ v, const int* __restrict__ bf_map, __nv_bfloat16* __restrict__ wbf,
-                       float lr, float b1, float b2, float eps, float c1, float c2)
+                       float lr, float b1, float b2, float eps, const long long* __restrict__ t_base, long long t_step)
 {
+    /* step t = (*t_base) + t_step: read on the device so that one captured
+       training epoch serves every epoch */
+    const double t = (double)((t_base ? *t_base : 0) + t_step);
+    const float c1 = (float)(1.0 - pow(0.9, t)), c2 = (float)(1.0 - pow(0.999, t));
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const float gi = g[i];
@@ -1242,10 +1250,12 @@ __global__ void k_tc_weights(const __nv_bfloat16* __restrict__ wbf, long long o0
 /* Features padded to 64 columns (the tensor-core K step): row i of X64 =
  * sin/cos of configuration idx[i] (or i), zeros beyond 2 ndof. */
 __global__ void k_features64(const float* __restrict__ q, long long offset, int ndof, int n,
-                             const int* __restrict__ idx, __nv_bfloat16* __restrict__ X)
+                             const int* __restrict__ idx, const long long* __restrict__ idx_off,
+                             __nv_bfloat16* __restrict__ X)
 {
+    const long long io = idx_off ? *idx_off : 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const long long src = idx ? idx[i] : i;
+        const long long src = idx ? idx[io + i] : i;
         uint32_t x[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j) x[j] = 0u;
@@ -1302,6 +1312,8 @@ struct gprm_mlp {
     float* ws = nullptr;                /* split-K partials [TG_MAX_SPLITS x 256 x 256] */
     int tc_n = -1;                      /* batch the tensor maps were made for */
     int tc_attr = 0;
+    long long* d_ctl = nullptr;         /* training epoch: [row offset into perm, Adam step before it] */
+    const long long* idx_off = nullptr; /* set while a training epoch is captured */
     CUtensorMap m_x64, m_h[NLAYER - 1], m_dz[NLAYER], m_w1p, m_w[NLAYER - 1], m_wt[NLAYER - 1], m_ta, m_tb256, m_tb64;
     unsigned* dev_err = nullptr;
     int sms = 0;
@@ -1439,7 +1451,7 @@ int forward_tc(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, fl
     int blocks = (n * 32 + 255) / 256;
     if (blocks > 4096) blocks = 4096;
     k_out<<<blocks, 256, 0, st>>>(n, h->H[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->w + h->offB[NLAYER], p, y,
-                                  yidx, h->dlogit, h->loss, inv_b);
+                                  yidx, h->idx_off, h->dlogit, h->loss, inv_b);
     MLP_TRY(h, cudaGetLastError());
     return GPRM_OK;
 }
@@ -1490,9 +1502,9 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
 void features(gprm_mlp* h, const float* q, int offset, int n, const int* idx, cudaStream_t st)
 {
     if (h->train_path == GPRM_MLP_TRAIN_TCGEN05)
-        k_features64<<<(n + 255) / 256, 256, 0, st>>>(q, offset, h->ndof, n, idx, h->X64);
+        k_features64<<<(n + 255) / 256, 256, 0, st>>>(q, offset, h->ndof, n, idx, h->idx_off, h->X64);
     else
-        k_features<<<(n + 255) / 256, 256, 0, st>>>(q, offset, h->ndof, n, idx, h->X);
+        k_features<<<(n + 255) / 256, 256, 0, st>>>(q, offset, h->ndof, n, idx, h->idx_off, h->X);
 }
 
 /* Forward on rows already featurised in h->X; p written to `p`. */
@@ -1515,7 +1527,7 @@ int forward(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, float
     int blocks = (n * 32 + 255) / 256;
     if (blocks > 4096) blocks = 4096;
     k_out<<<blocks, 256, 0, st>>>(n, h->H[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->w + h->offB[NLAYER], p, y,
-                                  yidx, h->dlogit, h->loss, inv_b);
+                                  yidx, h->idx_off, h->dlogit, h->loss, inv_b);
     MLP_TRY(h, cudaGetLastError());
     return GPRM_OK;
 }
@@ -1552,14 +1564,19 @@ int backward(gprm_mlp* h, int n, cudaStream_t st)
     return GPRM_OK;
 }
 
+/* One Adam step: step number (*t_base) + t_step (t_base null: t_step). */
+int adam_at(gprm_mlp* h, float lr, const long long* t_base, long long t_step, cudaStream_t st)
+{
+    k_adam<<<1024, 256, 0, st>>>(h->nparam, h->w, h->g, h->m, h->v, h->bf_map, h->wbf, lr, 0.9f, 0.999f, 1e-8f,
+                                 t_base, t_step);
+    MLP_TRY(h, cudaGetLastError());
+    return GPRM_OK;
+}
+
 int adam(gprm_mlp* h, float lr, cudaStream_t st)
 {
     h->adam_t += 1;
-    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    const float c1 = (float)(1.0 - pow(0.9, (double)h->adam_t)), c2 = (float)(1.0 - pow(0.999, (double)h->adam_t));
-    k_adam<<<1024, 256, 0, st>>>(h->nparam, h->w, h->g, h->m, h->v, h->bf_map, h->wbf, lr, b1, b2, eps, c1, c2);
-    MLP_TRY(h, cudaGetLastError());
-    return GPRM_OK;
+    return adam_at(h, lr, nullptr, h->adam_t, st);
 }
 
 /* deterministic uniform init in [-1/sqrt(in), 1/sqrt(in)] (Linear's default
@@ -1729,6 +1746,7 @@ void gprm_mlp_destroy(gprm_mlp* h)
     cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
     cudaFree(h->Ha); cudaFree(h->Hb); cudaFree(h->dev_err); cudaFree(h->wtc);
     cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb); cudaFree(h->w1p); cudaFree(h->wt); cudaFree(h->ws);
+    cudaFree(h->d_ctl);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -1820,33 +1838,40 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
     if (h->train_path == GPRM_MLP_TRAIN_TCGEN05 && ((rc = tc_setup(h)) || (rc = tc_maps(h, batch)))) return rc;
     const int steps = n / batch;
     std::vector<float> ep_loss(epochs, 0.0f);
-    for (int e = 0; e < epochs; ++e) {
-        /* the epoch's launches are captured into one graph and replayed */
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        MLP_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-        int crc = GPRM_OK;
-        cudaMemsetAsync(h->loss, 0, sizeof(float), h->st);
-        for (int s = 0; s < steps && !crc; ++s) {
-            const int* idx = perm + (size_t)e * n + (size_t)s * batch;
-            features(h, q, offset, batch, idx, h->st);
-            if (!crc) crc = forward(h, batch, h->p, y, idx, 1.0f / batch, h->st);
-            if (!crc) crc = backward(h, batch, h->st);
-            if (!crc) crc = adam(h, lr, h->st);
-        }
-        cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
-        if (crc) { if (graph) cudaGraphDestroy(graph); return crc; }
-        if (ce != cudaSuccess) return mfail(h, GPRM_ERR_CUDA, "capturing the training epoch", ce);
-        ce = cudaGraphInstantiate(&exec, graph, 0);
-        if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, h->st);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
-        if (exec) cudaGraphExecDestroy(exec);
-        cudaGraphDestroy(graph);
-        if (ce != cudaSuccess) return mfail(h, GPRM_ERR_CUDA, "running the training epoch", ce);
-        float l = 0;
-        MLP_TRY(h, cudaMemcpy(&l, h->loss, sizeof(float), cudaMemcpyDeviceToHost));
-        ep_loss[e] = l / steps;
+    if (!h->d_ctl) MLP_TRY(h, cudaMalloc((void**)&h->d_ctl, 2 * sizeof(long long)));
+    /* one epoch's launches are captured once into a graph; each epoch sets
+       its offset into perm and its first Adam step in device memory */
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    MLP_TRY(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int crc = GPRM_OK;
+    h->idx_off = h->d_ctl;
+    cudaMemsetAsync(h->loss, 0, sizeof(float), h->st);
+    for (int s = 0; s < steps && !crc; ++s) {
+        const int* idx = perm + (size_t)s * batch;
+        features(h, q, offset, batch, idx, h->st);
+        if (!crc) crc = forward(h, batch, h->p, y, idx, 1.0f / batch, h->st);
+        if (!crc) crc = backward(h, batch, h->st);
+        if (!crc) crc = adam_at(h, lr, h->d_ctl + 1, s + 1, h->st);
     }
+    h->idx_off = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
+    if (crc) { if (graph) cudaGraphDestroy(graph); return crc; }
+    if (ce != cudaSuccess) return mfail(h, GPRM_ERR_CUDA, "capturing the training epoch", ce);
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    for (int e = 0; e < epochs && ce == cudaSuccess; ++e) {
+        const long long ctl[2] = {(long long)e * n, h->adam_t};
+        ce = cudaMemcpyAsync(h->d_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, h->st);
+        if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, h->st);
+        float l = 0;
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(&l, h->loss, sizeof(float), cudaMemcpyDeviceToHost, h->st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+        ep_loss[e] = l / steps;
+        h->adam_t += steps;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return mfail(h, GPRM_ERR_CUDA, "running the training epochs", ce);
     if (losses) memcpy(losses, ep_loss.data(), epochs * sizeof(float));
     if (h->dev_err) {
         unsigned f = 0;
