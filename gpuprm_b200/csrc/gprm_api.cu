@@ -76,6 +76,40 @@ float float_ceil(double x)
  * radii are inflated by 2*eps_pos and by 1e-5 relative for the deviation
  * of the float rotation from orthogonality.  The slack added to the band
  * covers the rounding of the reference's dp and h (a few ulps of metres). */
+/* Eigenvectors of a symmetric 3x3 matrix A (cyclic Jacobi rotations);
+ * V's columns are the eigenvectors. */
+void jacobi3(double A[3][3], double V[3][3])
+{
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) V[i][k] = i == k ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+        if (off < 1e-300) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                if (A[p][q] == 0.0) continue;
+                const double th = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+                const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < 3; ++k) {   /* A <- A J */
+                    const double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - sn * akq;
+                    A[k][q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {   /* A <- J^T A */
+                    const double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - sn * aqk;
+                    A[q][k] = sn * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; ++k) {   /* V <- V J */
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - sn * vkq;
+                    V[k][q] = sn * vkp + c * vkq;
+                }
+            }
+    }
+}
+
 void compute_certificates(gprm_space* h, const int* from, const int* to)
 {
     const double eps_pos = 1e-6 * h->extent;
@@ -118,6 +152,17 @@ void compute_certificates(gprm_space* h, const int* from, const int* to)
     }
     h->thr_dir = (float)thr;
     h->eps_dir = (float)(7.0 * eps_pos);
+    /* box records: half extents inflated like the ball radii (the
+       reference's and this code's transform rounding, 2 eps_pos per
+       polytope) and by 2e-6 r for the FP32 axes' departure from an exact
+       orthonormal basis; rounded up */
+    h->box.resize((size_t)3 * h->npoly);
+    for (int k = 0; k < h->npoly; ++k)
+        for (int a = 0; a < 3; ++a) {
+            const double e = h->box_e[3 * k + a] * (1 + 1e-5) + 2 * eps_pos + 2e-6 * h->rad[k];
+            h->box[3 * k + a] = make_float4((float)h->box_ax[9 * k + 3 * a], (float)h->box_ax[9 * k + 3 * a + 1],
+                                            (float)h->box_ax[9 * k + 3 * a + 2], nextafterf((float)e, INFINITY));
+        }
 }
 
 int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
@@ -180,6 +225,8 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
     for (int k = 0; k < h->npoly; ++k) { boff[k] = (int)ntab; ntab += 2 + (size_t)d->poly_m[k]; }
     h->tab.resize(ntab);
     h->rad.assign(h->npoly, 0.0);
+    h->box_ax.assign((size_t)9 * h->npoly, 0.0);
+    h->box_e.assign((size_t)3 * h->npoly, 0.0);
     h->slot.assign(h->npoly, -1);
     for (int k = 0; k < h->npoly; ++k) {
         int n = d->poly_n[k], m = d->poly_m[k];
@@ -240,6 +287,34 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
         }
         h->rad[k] = sqrt(r);
         h->tab[boff[k]] = make_float4(cf[0], cf[1], cf[2], (float)h->rad[k]);
+        /* bounding box about the same centre: principal axes of the
+           vertices, rounded to FP32, half extents measured along those */
+        {
+            double mean[3] = {0, 0, 0}, C[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, V[3][3];
+            for (int i = 0; i < n; ++i)
+                for (int c = 0; c < 3; ++c) mean[c] += d->vertices[3 * (size_t)(voff[k] + i) + c] / n;
+            for (int i = 0; i < n; ++i) {
+                double v[3];
+                for (int c = 0; c < 3; ++c) v[c] = d->vertices[3 * (size_t)(voff[k] + i) + c] - mean[c];
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) C[a][b] += v[a] * v[b];
+            }
+            jacobi3(C, V);
+            for (int a = 0; a < 3; ++a) {
+                double nn = sqrt(V[0][a] * V[0][a] + V[1][a] * V[1][a] + V[2][a] * V[2][a]);
+                if (!(nn > 0)) nn = 1;
+                double ax[3];
+                for (int c = 0; c < 3; ++c) ax[c] = (double)(float)(V[c][a] / nn);
+                double e = 0;
+                for (int i = 0; i < n; ++i) {
+                    double t = 0;
+                    for (int c = 0; c < 3; ++c) t += (d->vertices[3 * (size_t)(voff[k] + i) + c] - (double)cf[c]) * ax[c];
+                    e = fabs(t) > e ? fabs(t) : e;
+                }
+                for (int c = 0; c < 3; ++c) h->box_ax[9 * k + 3 * a + c] = ax[c];
+                h->box_e[3 * k + a] = e;
+            }
+        }
     }
     /* slots: moving polytopes in frame order */
     for (int f = 1; f <= h->ndof; ++f)
@@ -555,16 +630,20 @@ int gprm_init(gprm_space* h, int rank, int size)
     CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
 
-    /* d_scene: tab | pairs | pairs_b | far | far_slot */
+    /* d_scene: tab | pairs | pairs_b | far | far_slot | ppoly | box */
     size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
     size_t fsb = (size_t)h->npairs * sizeof(int2);
-    CUDA_TRY(h, cudaMalloc(&h->d_scene, tb + 3 * pb + fsb + 64));
+    size_t bxo = tb + 3 * pb + 2 * fsb, bxb = h->box.size() * sizeof(float4);
+    bxo = (bxo + 15) & ~(size_t)15;
+    CUDA_TRY(h, cudaMalloc(&h->d_scene, bxo + bxb + 64));
     char* base = (char*)h->d_scene;
     CUDA_TRY(h, cudaMemcpy(base, h->tab.data(), tb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 2 * pb, h->far.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 3 * pb, h->far_slot.data(), fsb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 3 * pb + fsb, h->pair_poly.data(), fsb, cudaMemcpyHostToDevice));
+    if (bxb) CUDA_TRY(h, cudaMemcpy(base + bxo, h->box.data(), bxb, cudaMemcpyHostToDevice));
 
     DevScene& s = h->dsc;
     memset(&s, 0, sizeof(s));
@@ -586,6 +665,8 @@ int gprm_init(gprm_space* h, int rank, int size)
     s.pairs_b = (const float4*)(base + tb + pb);
     s.far = (const float4*)(base + tb + 2 * pb);
     s.far_slot = (const int2*)(base + tb + 3 * pb);
+    s.ppoly = (const int2*)(base + tb + 3 * pb + fsb);
+    s.box = bxb ? (const float4*)(base + bxo) : nullptr;
     s.thr_dir = h->thr_dir;
     s.eps_dir = h->eps_dir;
     s.nslots = (int)h->slot_sys.size();

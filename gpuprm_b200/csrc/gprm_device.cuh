@@ -69,6 +69,10 @@ struct DevScene {
        eps_dir bounds the direction error of the approximate first direction
        times its distance (see pair_certified) */
     float thr_dir, eps_dir;
+    /* box certificate: per polytope 3 records (unit axis in its frame, half
+       extent about the ball centre, inflated); per pair the two polytopes */
+    const float4* box;
+    const int2* ppoly;
     float dq;                            /* edge resolution (batched problems) */
     int nslots;                          /* moving polytopes with a ball slot */
     int slot_sys[GPRM_MAX_SLOTS];        /* frame of each slot */
@@ -471,9 +475,32 @@ __device__ __forceinline__ int pair_test(const DevScene& sc, const float4* __res
  *              against the reference's S0 is at most eps_dir/|s| (s the
  *              vertex-0 offset), charged against G with |D| + R.
  * NaN never passes (every test is a '>' comparison). */
+/* Support of polytope box B (3 records) along u, u in world coordinates;
+ * frame f (0: world) rotates the box: its local direction is R^T u. */
+__device__ __forceinline__ float box_support(const float4* __restrict__ B, const float* frames, int f, float ux,
+                                             float uy, float uz)
+{
+    float lx = ux, ly = uy, lz = uz;
+    if (f) {
+        const float* fr = frames + (f - 1) * 12 * 32;
+        const float m0 = fr[0], m1 = fr[32], m2 = fr[64], m3 = fr[96], m4 = fr[128], m5 = fr[160];
+        const float m6 = fr[192], m7 = fr[224], m8 = fr[256];
+        lx = __fmaf_rn(m0, ux, __fmaf_rn(m1, uy, m2 * uz));
+        ly = __fmaf_rn(m3, ux, __fmaf_rn(m4, uy, m5 * uz));
+        lz = __fmaf_rn(m6, ux, __fmaf_rn(m7, uy, m8 * uz));
+    }
+    float h = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float4 b = B[a];
+        h = __fmaf_rn(b.w, fabsf(__fmaf_rn(b.x, lx, __fmaf_rn(b.y, ly, b.z * lz))), h);
+    }
+    return h;
+}
+
 __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4* __restrict__ tab,
                                                int4 pr, float4 pb, const float* cen,
-                                               const float* frames, bool* used_dir)
+                                               const float* frames, bool* used_dir, int j)
 {
     *used_dir = false;
     const int sa = __float_as_int(pb.z), sb = __float_as_int(pb.w);
@@ -513,7 +540,18 @@ __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4*
     const float dn = sqrtf(d2);
     /* direction error <= eps_dir*inv (+ rsqrt and rounding, 1e-6) */
     const float err = (dn + pb.x) * __fmaf_rn(sc.eps_dir, inv, 1e-6f);
-    return G - err > sc.thr_dir;
+    if (G - err > sc.thr_dir) return true;
+    /* box test: the same bound with each polytope's support along S taken
+       from its bounding box instead of its ball (every vertex v of X has
+       <S, v - c_X> <= sum_a e_a |<a_a, R_X^T S>|), tighter for elongated
+       links and flat obstacles */
+    if (!sc.box || !(pb.x < PF32::inf())) return false;
+    const int2 pp = sc.ppoly[j];
+    const float ux = sx * inv, uy = sy * inv, uz = sz * inv;
+    const float hp = box_support(sc.box + 3 * pp.x, frames, pr.z, ux, uy, uz);
+    const float hq = box_support(sc.box + 3 * pp.y, frames, pr.w, ux, uy, uz);
+    const float Gb = __fmaf_rn(ux, dx, __fmaf_rn(uy, dy, uz * dz)) - (hp + hq) * (1.0f + 1e-5f);
+    return Gb - err > sc.thr_dir;
 }
 
 /* The same certificate for the FP64 recheck, in double from the FP64

@@ -57,6 +57,11 @@ struct gprm_space {
     std::vector<float4> far;       /* distance test: static ball centre, T2 */
     std::vector<int2> far_slot;    /* distance test: moving slot(s), -1 none */
     std::vector<double> rad;       /* inflated ball radius per polytope */
+    /* bounding box per polytope about its ball centre: PCA axes (FP32
+       values), half extents (exact), and the device records (axis, inflated
+       half extent) x 3 */
+    std::vector<double> box_ax, box_e;
+    std::vector<float4> box;
     std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
     std::vector<int> slot_sys, slot_block;
     std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */

@@ -259,7 +259,7 @@ __device__ __forceinline__ int eval_pair(const DevScene& sc, const SceneView& S,
     const int4 pr = S.pairs[j];
     const float4 pb = S.pairs_b[j];
     bool used_dir;
-    if (pair_certified(sc, S.tab, pr, pb, S.cen, S.frames, &used_dir)) {
+    if (pair_certified(sc, S.tab, pr, pb, S.cen, S.frames, &used_dir, j)) {
         if (used_dir) ++pc.dir;
         else ++pc.far;
         *has_margin = false;
@@ -385,7 +385,7 @@ __device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView&
         if (st.active && ((need >> k) & 1u)) {
             const int j = j0 + k;
             bool used_dir;
-            if (pair_certified(sc, S.tab, S.pairs[j], S.pairs_b[j], S.cen, S.frames, &used_dir)) {
+            if (pair_certified(sc, S.tab, S.pairs[j], S.pairs_b[j], S.cen, S.frames, &used_dir, j)) {
                 if (used_dir) ++pc.dir;
                 else ++pc.far;
             } else {
