@@ -201,6 +201,31 @@ def cpu_reference_rate(scene, qs_np, qe_np, dq, seconds, seed=0, count_ops=True)
 # our arm
 # --------------------------------------------------------------------------
 
+def replica_seed(seed: int, rank: int) -> int:
+    """Each rank checks its own replica of the workload (independent seeded
+    samples, the same scene and sizes): weak scaling, no data exchange."""
+    return seed + 7919 * rank
+
+
+def reduce_over_ranks(values_max, values_sum, device=None):
+    """(max over ranks of each of values_max, sum over ranks of each of
+    values_sum) through the default process group; the values themselves
+    for a single process.  Every rank must call it with the same lengths."""
+    import torch
+    dist = torch.distributed
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values_max], [float(v) for v in values_sum]
+    out = []
+    for vals, op in ((values_max, dist.ReduceOp.MAX), (values_sum, dist.ReduceOp.SUM)):
+        if len(vals):
+            t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+            dist.all_reduce(t, op=op)
+            out.append([float(x) for x in t.cpu().tolist()])
+        else:
+            out.append([])
+    return out[0], out[1]
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from gpuprm_b200 import workloads
@@ -209,7 +234,7 @@ def run_ours(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    ws = workloads.edge_workload("hull6", seed=args.seed + 7919 * rank, n_samples=args.samples, k=args.k,
+    ws = workloads.edge_workload("hull6", seed=replica_seed(args.seed, rank), n_samples=args.samples, k=args.k,
                                  dq=WORKLOAD["dq"], device=str(dev))
     cs = ws["space"]
     cs.set_mode(GPRM_MODE_FP64_BAND)
@@ -255,14 +280,8 @@ def run_ours(args, rank, world, local_rank):
     colliding = int((res != 0).sum().item())
 
     # max over ranks of the device time; totals over ranks
-    t_max, nominal_all, executed_all = t, nominal, executed
-    if world > 1:
-        tt = torch.tensor([t], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_max = float(tt.item())
-        nn = torch.tensor([nominal, executed], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(nn)
-        nominal_all, executed_all = int(nn[0].item()), int(nn[1].item())
+    (t_max,), (nominal_all, executed_all) = reduce_over_ranks([t], [nominal, executed], dev)
+    nominal_all, executed_all = int(nominal_all), int(executed_all)
 
     # e2e through the host-buffer C ABI (H2D + D2H inside the timed region)
     qs_np = np.ascontiguousarray(qs.cpu().numpy())
@@ -275,10 +294,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.steps):
         cs.indicator2(qs_np, qe_np, res_np, E, E)
     t_e2e = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+    (t_e2e,), _ = reduce_over_ranks([t_e2e], [], dev)
     assert np.array_equal(res_np, res.cpu().numpy()), "host and device entry points disagree"
 
     if rank != 0:
