@@ -393,8 +393,8 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
 {
     if (own_stream && !r.st) CUDA_TRY(h, cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking));
     if (!r.ctl) {
-        CUDA_TRY(h, cudaMalloc((void**)&r.ctl, sizeof(Control)));
-        CUDA_TRY(h, cudaHostAlloc((void**)&r.ctl_host, sizeof(Control), cudaHostAllocDefault));
+        CUDA_TRY(h, cudaMalloc((void**)&r.ctl, HOST_PARTS * sizeof(Control)));
+        CUDA_TRY(h, cudaHostAlloc((void**)&r.ctl_host, HOST_PARTS * sizeof(Control), cudaHostAllocDefault));
     }
     size_t need_q = (kind == 0) ? n : 4 * n + 65536;
     if (n > r.cap_items || need_q > r.cap_queue || (with_host && !r.h_res && n > 0)) {
@@ -438,11 +438,22 @@ int event_pair(gprm_space* h, std::vector<cudaEvent_t>& pool, size_t& used, cuda
 
 /* Enqueues one request on stream `st` with device inputs/outputs.
  * kind 0: q -> res.  kind 1: (qs, qe) -> res. */
+int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
+                 long long offset, cudaStream_t st, Control* ctl, unsigned* key);
+
 int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
             long long offset, cudaStream_t st)
 {
+    return enqueue_part(h, r, kind, a, b, res, n, offset, st, r.ctl, r.d_key);
+}
+
+/* One check request on stream st: items a[i + offset*j] (b: edge ends),
+ * codes to res[0..n), with the control block ctl and the edge keys key. */
+int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
+                 long long offset, cudaStream_t st, Control* ctl, unsigned* key)
+{
     const int band_on = h->mode == GPRM_MODE_FP64_BAND;
-    CUDA_TRY(h, cudaMemsetAsync(r.ctl, 0, sizeof(Control), st));
+    CUDA_TRY(h, cudaMemsetAsync(ctl, 0, sizeof(Control), st));
     int recheck_blocks = h->sms * 4;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     if (h->profiling) {
@@ -451,30 +462,30 @@ int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b,
         if (band_on && (rc = event_pair(h, h->ev64, h->ev64_used, &e2, &e3))) return rc;
     }
     if (kind == 1)
-        CUDA_TRY(h, cudaMemsetAsync(r.d_key, h->policy == GPRM_EDGES_EARLY_EXIT ? 0xff : 0x00,
+        CUDA_TRY(h, cudaMemsetAsync(key, h->policy == GPRM_EDGES_EARLY_EXIT ? 0xff : 0x00,
                                     (size_t)n * sizeof(unsigned), st));
     if (e0) CUDA_TRY(h, cudaEventRecord(e0, st));
     if (kind == 0)
         CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, a, n, offset, res, band_on, h->band, r.d_queue,
-                                         (unsigned)r.cap_queue, r.ctl, st));
+                                         (unsigned)r.cap_queue, ctl, st));
     else
-        CUDA_TRY(h, launch_check_edges(h->dsc, h->cfg_e, a, b, n, offset, h->dq, h->policy, r.d_key, band_on,
-                                       h->band, r.d_queue, (unsigned)r.cap_queue, r.ctl, st));
+        CUDA_TRY(h, launch_check_edges(h->dsc, h->cfg_e, a, b, n, offset, h->dq, h->policy, key, band_on,
+                                       h->band, r.d_queue, (unsigned)r.cap_queue, ctl, st));
     if (e1) CUDA_TRY(h, cudaEventRecord(e1, st));
     if (band_on) {
         if (e2) CUDA_TRY(h, cudaEventRecord(e2, st));
         if (kind == 0)
             CUDA_TRY(h, launch_recheck(h->dsc, recheck_blocks, 0, a, nullptr, nullptr, offset, h->dq, h->policy,
-                                       res, nullptr, r.d_queue, (unsigned)r.cap_queue, r.ctl, st));
+                                       res, nullptr, r.d_queue, (unsigned)r.cap_queue, ctl, st));
         else
             CUDA_TRY(h, launch_recheck(h->dsc, recheck_blocks, 1, nullptr, a, b, offset, h->dq, h->policy,
-                                       nullptr, r.d_key, r.d_queue, (unsigned)r.cap_queue, r.ctl, st));
+                                       nullptr, key, r.d_queue, (unsigned)r.cap_queue, ctl, st));
         if (e3) CUDA_TRY(h, cudaEventRecord(e3, st));
     }
-    if (kind == 1) CUDA_TRY(h, launch_finalize_edges(n, h->policy, r.d_key, res, st));
+    if (kind == 1) CUDA_TRY(h, launch_finalize_edges(n, h->policy, key, res, st));
     /* check + accumulate, plus recheck and finalize where they run */
     h->host_stats.launches += 2 + (band_on ? 1 : 0) + (kind == 1 ? 1 : 0);
-    CUDA_TRY(h, launch_accumulate(r.ctl, h->d_total, st));
+    CUDA_TRY(h, launch_accumulate(ctl, h->d_total, st));
     return GPRM_OK;
 }
 
@@ -500,19 +511,34 @@ int submit_host(gprm_space* h, int kind, const float* a, const float* b, int* re
     int rc = ensure_request(h, r, kind, (size_t)(n > 0 ? n : 1), true, true);
     if (rc) return rc;
     const int nd = h->ndof;
-    for (int j = 0; j < nd; ++j) {
-        memcpy(r.h_a + (size_t)j * n, a + (size_t)offset * j, (size_t)n * sizeof(float));
-        if (kind == 1) memcpy(r.h_b + (size_t)j * n, b + (size_t)offset * j, (size_t)n * sizeof(float));
-    }
-    if (n > 0) {
-        CUDA_TRY(h, cudaMemcpyAsync(r.d_a, r.h_a, (size_t)n * nd * sizeof(float), cudaMemcpyHostToDevice, r.st));
+    /* parts: the host copies part p into pinned staging while the device
+       transfers and checks part p-1 (same stream, so the parts' checks run
+       in order and share the FP64 queue) */
+    const int parts = n >= (1 << 16) ? HOST_PARTS : 1;
+    r.parts = parts;
+    /* part boundaries (in 16ths): a small first part, whose staging is the
+       only one not hidden, then three equal parts */
+    static const int edge16[HOST_PARTS + 1] = {0, 1, 6, 11, 16};
+    for (int p = 0; p < parts && n > 0; ++p) {
+        const size_t c0 = parts == 1 ? 0 : (size_t)n * edge16[p] / 16;
+        const size_t c1 = parts == 1 ? (size_t)n : (size_t)n * edge16[p + 1] / 16, m = c1 - c0;
+        for (int j = 0; j < nd; ++j) {
+            memcpy(r.h_a + (size_t)j * n + c0, a + (size_t)offset * j + c0, m * sizeof(float));
+            if (kind == 1) memcpy(r.h_b + (size_t)j * n + c0, b + (size_t)offset * j + c0, m * sizeof(float));
+        }
+        const size_t pitch = (size_t)n * sizeof(float);
+        CUDA_TRY(h, cudaMemcpy2DAsync(r.d_a + c0, pitch, r.h_a + c0, pitch, m * sizeof(float), nd,
+                                      cudaMemcpyHostToDevice, r.st));
         if (kind == 1)
-            CUDA_TRY(h, cudaMemcpyAsync(r.d_b, r.h_b, (size_t)n * nd * sizeof(float), cudaMemcpyHostToDevice, r.st));
-        rc = enqueue(h, r, kind, r.d_a, kind == 1 ? r.d_b : nullptr, r.d_res, n, n, r.st);
+            CUDA_TRY(h, cudaMemcpy2DAsync(r.d_b + c0, pitch, r.h_b + c0, pitch, m * sizeof(float), nd,
+                                          cudaMemcpyHostToDevice, r.st));
+        rc = enqueue_part(h, r, kind, r.d_a + c0, kind == 1 ? r.d_b + c0 : nullptr, r.d_res + c0, (long long)m, n,
+                          r.st, r.ctl + p, r.d_key + c0);
         if (rc) return rc;
-        CUDA_TRY(h, cudaMemcpyAsync(r.h_res, r.d_res, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, r.st));
-        CUDA_TRY(h, cudaMemcpyAsync(r.ctl_host, r.ctl, sizeof(Control), cudaMemcpyDeviceToHost, r.st));
+        CUDA_TRY(h, cudaMemcpyAsync(r.h_res + c0, r.d_res + c0, m * sizeof(int), cudaMemcpyDeviceToHost, r.st));
     }
+    if (n > 0)
+        CUDA_TRY(h, cudaMemcpyAsync(r.ctl_host, r.ctl, parts * sizeof(Control), cudaMemcpyDeviceToHost, r.st));
     r.busy = true;
     r.kind = kind;
     r.user_res = res;
@@ -530,7 +556,11 @@ int complete_host(gprm_space* h, int slot)
     r.busy = false;
     if (r.n == 0) return GPRM_OK;
     CUDA_TRY(h, cudaStreamSynchronize(r.st));
-    Control c = *r.ctl_host;
+    Control c = r.ctl_host[0];
+    for (int p = 1; p < r.parts; ++p) {
+        c.flags |= r.ctl_host[p].flags;
+        c.steps_nominal += r.ctl_host[p].steps_nominal;
+    }
     if (c.flags & GPRM_DEVFLAG_BAD_EDGE)
         return fail(h, GPRM_ERR_ARG, "an edge has a non-finite or oversized length (|qe-qs|/dq >= 1e8)");
     if (c.flags & GPRM_DEVFLAG_QUEUE_FULL) {

@@ -17,10 +17,16 @@ namespace gprm {
 
 /* One request of the pool: stream, control block, device buffers and
  * pinned staging. */
+/* host-buffer requests are split into up to this many parts, so that the
+ * staging copy and the transfer of one part overlap the checks of the
+ * previous one */
+constexpr int HOST_PARTS = 4;
+
 struct Request {
     cudaStream_t st = nullptr;
-    Control* ctl = nullptr;       /* device */
-    Control* ctl_host = nullptr;  /* pinned copy read after the request */
+    Control* ctl = nullptr;       /* device, HOST_PARTS blocks (one per part) */
+    Control* ctl_host = nullptr;  /* pinned copies read after the request */
+    int parts = 1;                /* parts of the request in flight */
     float* d_a = nullptr;         /* q or qs (contiguous SoA, offset = n) */
     float* d_b = nullptr;         /* qe */
     int* d_res = nullptr;

@@ -187,6 +187,34 @@ def test_device_pointer_api_matches_host_api():
     np.testing.assert_array_equal(codes.cpu().numpy(), host_codes)
 
 
+@pytest.mark.parametrize("policy", [GPRM_EDGES_EARLY_EXIT, GPRM_EDGES_ALL_STEPS])
+def test_host_api_in_parts_matches_device_api(policy):
+    """Host-buffer requests of 2^16 items or more run in parts (staging and
+    transfer of one part under the checks of the previous one); results equal
+    the device-pointer entry point's, for edges and configurations, with an
+    item count that does not divide evenly."""
+    import torch
+    from gpuprm_b200 import scenes
+    sc = scenes.make_hull6(5)
+    cs = space(sc, 0.01, mode=GPRM_MODE_FP64_BAND, policy=policy)
+    qs, qe = scenes.random_edges(sc, 70001, 6, 0.6)
+    q = scenes.uniform_configs(sc, 100003, 7)
+    host_e = cs.check_edges(qs, qe)
+    host_v = cs.check_configs(q)
+    dev = torch.device("cuda:0")
+    tqs = torch.tensor(np.ascontiguousarray(qs.T), device=dev)
+    tqe = torch.tensor(np.ascontiguousarray(qe.T), device=dev)
+    res = torch.zeros(len(host_e), dtype=torch.int32, device=dev)
+    cs.check_edges_device(tqs, tqe, res)
+    tq = torch.tensor(np.ascontiguousarray(q.T), device=dev)
+    codes = torch.zeros(len(host_v), dtype=torch.int32, device=dev)
+    cs.check_configs_device(tq, codes)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(res.cpu().numpy(), host_e)
+    np.testing.assert_array_equal(codes.cpu().numpy(), host_v)
+    assert (host_e != 0).any() and (host_e == 0).any()
+
+
 @pytest.mark.parametrize("band", [0.0, 1e-3, 2e-2])
 def test_band_width_changes_nothing_but_the_band(band):
     """The separation certificates depend on the band; results must equal
