@@ -20,7 +20,7 @@
  *            for outside queries); a
  *            result is accepted only when its k-th distance is below the
  *            distance to the scanned block's boundary (with slack for float
- *            rounding), otherwise the query is redone by a warp that scans
+ *            rounding), otherwise the query is redone by a block that scans
  *            every node.  The result is therefore the exact top-k.
  *
  * Distances use the reference's arithmetic: d = x_j - q_j, s = s + d*d
@@ -70,6 +70,25 @@ __device__ __forceinline__ int cell_coord(float v, float lo, float inv_cell, int
     float c = floorf((v - lo) * inv_cell);
     int ci = isfinite(c) ? (int)fminf(fmaxf(c, 0.0f), (float)(nc - 1)) : 0;
     return ci;
+}
+
+/* dist2 of four consecutive nodes p..p+3: the same arithmetic per node,
+ * the four nodes' loads issued together. */
+__device__ __forceinline__ void dist2_4(const float* __restrict__ x, long long xstride, long long p, const float* qv,
+                                        int ndof, float* s)
+{
+    s[0] = s[1] = s[2] = s[3] = 0.0f;
+    for (int j = 0; j < ndof; ++j) {
+        const float* xj = x + p + xstride * j;
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = xj[u];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float d = v[u] - qv[j];
+            s[u] = s[u] + d * d;
+        }
+    }
 }
 
 /* (s, id) lexicographic order */
@@ -185,6 +204,19 @@ __global__ void k_radius(const float* __restrict__ x, int n, long long xstride, 
 
 /* ---------------------------------------------------------------- knn */
 
+/* The list's current k-th entry, kept in registers so that most
+ * candidates are rejected by one comparison, before their index is even
+ * loaded: (INFINITY, INT_MAX) until the list is full. */
+struct TopkBound {
+    float s;
+    int i;
+};
+
+__device__ __forceinline__ void topk_bound(const float* ts, const int* ti, int len, int k, TopkBound& b)
+{
+    if (len == k) { b.s = ts[k - 1]; b.i = ti[k - 1]; }
+}
+
 /* Inserts (s, i) into the sorted top list (len entries used, capacity k). */
 __device__ __forceinline__ void topk_insert(float* ts, int* ti, int& len, int k, float s, int i)
 {
@@ -265,6 +297,7 @@ __global__ void k_knn_grid(GridView g, int m, int k, int* out_idx, float* out_di
         float ts[NBR_MAX_K];
         int ti[NBR_MAX_K];
         int len = 0;
+        TopkBound bound{INFINITY, 0x7fffffff};
         int lo[NBR_MAX_GRID], hi[NBR_MAX_GRID];
         float guard;
         const bool finite = query_block(g, qv, lo, hi, &guard);
@@ -272,12 +305,31 @@ __global__ void k_knn_grid(GridView g, int m, int k, int* out_idx, float* out_di
         for (int r = 0; r < rows; ++r) {
             int b, e;
             block_row_range(g, lo, hi, r, &b, &e);
-            for (int p = b; p < e; ++p) {
-                const int nid = g.id[p];
-                if (nid == qid) continue;
+            int p = b;
+            for (; p + 4 <= e; p += 4) {
+                float s4[4];
+                dist2_4(g.xs, g.n, p, qv, g.ndof, s4);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    float sd = s4[u];
+                    if (p + u == t) continue;      /* the query itself */
+                    if (sd != sd) sd = INFINITY;   /* NaN sorts last */
+                    if (sd > bound.s) continue;    /* cannot enter the list */
+                    const int nid = g.id[p + u];
+                    if (!less_pair(sd, nid, bound.s, bound.i)) continue;
+                    topk_insert(ts, ti, len, k, sd, nid);
+                    topk_bound(ts, ti, len, k, bound);
+                }
+            }
+            for (; p < e; ++p) {
+                if (p == t) continue;
                 float sd = dist2(g.xs, g.n, p, qv, g.ndof);
-                if (sd != sd) sd = INFINITY;   /* NaN sorts last */
+                if (sd != sd) sd = INFINITY;
+                if (sd > bound.s) continue;
+                const int nid = g.id[p];
+                if (!less_pair(sd, nid, bound.s, bound.i)) continue;
                 topk_insert(ts, ti, len, k, sd, nid);
+                topk_bound(ts, ti, len, k, bound);
             }
         }
         if (knn_exact(g, finite, len, k, len ? ts[len - 1] : INFINITY, guard)) {
@@ -330,6 +382,7 @@ __global__ void k_knn_grid_warp(GridView g, const float* __restrict__ q, int m, 
         float ts[NBR_MAX_K];
         int ti[NBR_MAX_K];
         int len = 0;
+        TopkBound bound{INFINITY, 0x7fffffff};
         int lo[NBR_MAX_GRID], hi[NBR_MAX_GRID];
         float guard;
         const bool finite = query_block(g, qv, lo, hi, &guard);
@@ -340,7 +393,11 @@ __global__ void k_knn_grid_warp(GridView g, const float* __restrict__ q, int m, 
             for (int p = b + lane; p < e; p += 32) {
                 float sd = dist2(g.xs, g.n, p, qv, g.ndof);
                 if (sd != sd) sd = INFINITY;
-                topk_insert(ts, ti, len, k, sd, g.id[p]);
+                if (sd > bound.s) continue;
+                const int nid = g.id[p];
+                if (!less_pair(sd, nid, bound.s, bound.i)) continue;
+                topk_insert(ts, ti, len, k, sd, nid);
+                topk_bound(ts, ti, len, k, bound);
             }
         }
         float my_s, kth;
@@ -357,47 +414,72 @@ __global__ void k_knn_grid_warp(GridView g, const float* __restrict__ q, int m, 
     }
 }
 
-/* Redo of the queries the grid could not settle: one warp per query scans
- * every node; each lane keeps a top-k of its stride, then k rounds of a
- * warp argmin merge them. */
-__global__ void k_knn_full(const float* __restrict__ x, int n, long long xstride, const float* __restrict__ q,
-                           long long qstride, int ndof, int k, int exclude_self, const int* __restrict__ redo,
-                           const int* __restrict__ nredo, int* out_idx, float* out_dist)
+/* Redo of the queries the grid could not settle: one block per query scans
+ * every node (each thread four consecutive nodes at a time, keeping its own
+ * top-k); each warp merges its lanes' lists by k rounds of a warp argmin,
+ * then warp 0 merges the eight warp lists the same way. */
+__global__ void __launch_bounds__(256) k_knn_full(const float* __restrict__ x, int n, long long xstride,
+                                                  const float* __restrict__ q, long long qstride, int ndof, int k,
+                                                  int exclude_self, const int* __restrict__ redo,
+                                                  const int* __restrict__ nredo, int* out_idx, float* out_dist)
 {
-    const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
+    __shared__ float ms[8 * NBR_MAX_K];
+    __shared__ int mi[8 * NBR_MAX_K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int cnt = *nredo;
-    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < cnt; w += gridDim.x * wpb) {
+    for (int w = blockIdx.x; w < cnt; w += gridDim.x) {
         const int qid = redo[w];
         float qv[GPRM_MAX_DOF];
         for (int j = 0; j < ndof; ++j) qv[j] = q[qid + qstride * j];
         float ts[NBR_MAX_K];
         int ti[NBR_MAX_K];
         int len = 0;
-        for (int i = lane; i < n; i += 32) {
-            if (exclude_self && i == qid) continue;
-            float s = dist2(x, xstride, i, qv, ndof);
-            if (s != s) s = INFINITY;   /* NaN sorts last */
-            topk_insert(ts, ti, len, k, s, i);
-        }
-        int head = 0;
-        for (int r = 0; r < k; ++r) {
-            float s = head < len ? ts[head] : INFINITY;
-            int i = head < len ? ti[head] : 0x7fffffff;
-            float bs = s;
-            int bi = i;
-            for (int o = 16; o > 0; o >>= 1) {
-                const float os = __shfl_xor_sync(0xffffffffu, bs, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (less_pair(os, oi, bs, bi)) { bs = os; bi = oi; }
+        TopkBound bound{INFINITY, 0x7fffffff};
+        /* thread t takes nodes 4t.. 4t+3, 4(t+256).. : four loads in flight */
+        for (int i0 = 4 * threadIdx.x; i0 < n; i0 += 4 * 256) {
+            float s4[4];
+            if (i0 + 4 <= n) {
+                dist2_4(x, xstride, i0, qv, ndof, s4);
+            } else {
+                for (int u = 0; u < 4; ++u) s4[u] = i0 + u < n ? dist2(x, xstride, i0 + u, qv, ndof) : INFINITY;
             }
-            if (head < len && ti[head] == bi && ts[head] == bs) ++head;
-            if (lane == 0) {
-                const bool have = bi != 0x7fffffff;
-                out_idx[(long long)qid * k + r] = have ? bi : -1;
-                out_dist[(long long)qid * k + r] = have ? sqrtf(bs) : INFINITY;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = i0 + u;
+                if (i >= n || (exclude_self && i == qid)) continue;
+                float s = s4[u];
+                if (s != s) s = INFINITY;   /* NaN sorts last */
+                if (!less_pair(s, i, bound.s, bound.i)) continue;
+                topk_insert(ts, ti, len, k, s, i);
+                topk_bound(ts, ti, len, k, bound);
             }
         }
+        /* per warp: the k smallest of its lanes; then warp 0 merges the 8 lists */
+        float my_s, kth;
+        int my_i, found;
+        warp_topk_merge(ts, ti, len, k, &my_s, &my_i, &kth, &found);
+        if (lane < k) {
+            ms[warp * k + lane] = my_s;
+            mi[warp * k + lane] = my_i < 0 ? 0x7fffffff : my_i;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            len = 0;
+            bound = TopkBound{INFINITY, 0x7fffffff};
+            for (int e = lane; e < 8 * k; e += 32) {
+                if (mi[e] == 0x7fffffff) continue;
+                if (!less_pair(ms[e], mi[e], bound.s, bound.i)) continue;
+                topk_insert(ts, ti, len, k, ms[e], mi[e]);
+                topk_bound(ts, ti, len, k, bound);
+            }
+            warp_topk_merge(ts, ti, len, k, &my_s, &my_i, &kth, &found);
+            if (lane < k) {
+                const bool have = my_i >= 0;
+                out_idx[(long long)qid * k + lane] = have ? my_i : -1;
+                out_dist[(long long)qid * k + lane] = have ? sqrtf(my_s) : INFINITY;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -627,7 +709,7 @@ int gprm_nbr_knn(gprm_nbr* h, const float* q, int m, int qstride, int k, int que
         k_knn_grid_warp<<<blocks, 32 * wpb, 0, st>>>(h->g, q, m, qstride, k, idx, dist, h->redo, h->nredo);
     }
     NBR_TRY(h, cudaGetLastError());
-    k_knn_full<<<h->sms * 4, 256, 0, st>>>(h->x, h->n, h->xstride, q, qstride, h->ndof, k, queries_are_nodes ? 1 : 0,
+    k_knn_full<<<h->sms * 8, 256, 0, st>>>(h->x, h->n, h->xstride, q, qstride, h->ndof, k, queries_are_nodes ? 1 : 0,
                                            h->redo, h->nredo, idx, dist);
     NBR_TRY(h, cudaGetLastError());
     return GPRM_OK;
