@@ -560,12 +560,18 @@ __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4*
  * direction is computed in double, so its error term only needs the
  * 1e-6 relative allowance. */
 __device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float4* __restrict__ tab, int4 pr,
-                                                 float4 pb, const Frame<double>* F)
+                                                 float4 pb, const Frame<double>* F, const double* cen)
 {
-    const float4 bp = tab[pr.x], bq = tab[pr.y];
-    double px = bp.x, py = bp.y, pz = bp.z, qx = bq.x, qy = bq.y, qz = bq.z;
-    if (pr.z) { V3<double> c = xform<double>(F[pr.z], px, py, pz); px = c.x; py = c.y; pz = c.z; }
-    if (pr.w) { V3<double> c = xform<double>(F[pr.w], qx, qy, qz); qx = c.x; qy = c.y; qz = c.z; }
+    /* ball centres: a moving polytope's from its slot (the FP64 transform of
+       its ball centre, computed once per check), a static one's from the
+       table.  A moving polytope without a slot has T2 = R = infinity, so
+       neither test can pass for its pairs whatever centre is used. */
+    const int sa = __float_as_int(pb.z), sb = __float_as_int(pb.w);
+    double px, py, pz, qx, qy, qz;
+    if (sa >= 0) { px = cen[3 * sa]; py = cen[3 * sa + 1]; pz = cen[3 * sa + 2]; }
+    else { const float4 bp = tab[pr.x]; px = bp.x; py = bp.y; pz = bp.z; }
+    if (sb >= 0) { qx = cen[3 * sb]; qy = cen[3 * sb + 1]; qz = cen[3 * sb + 2]; }
+    else { const float4 bq = tab[pr.y]; qx = bq.x; qy = bq.y; qz = bq.z; }
     const double dx = qx - px, dy = qy - py, dz = qz - pz;
     const double d2 = dx * dx + dy * dy + dz * dz;
     if (d2 > (double)pb.y) return true;

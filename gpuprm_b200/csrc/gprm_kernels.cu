@@ -662,11 +662,19 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
         edge_step_config(qs, qe, (long long)it.x, offset, sc.ndof, t, tn, qi);
     }
     forward_kinematics<PF64>(sc, qi, F);
+    /* slot ball centres in FP64, once per check (the same transform the
+       certificate would apply per pair) */
+    double cen[GPRM_MAX_SLOTS * 3];
+    for (int sl = 0; sl < sc.nslots; ++sl) {
+        const float4 b = sc.tab[sc.slot_block[sl]];
+        const V3<double> c = xform<double>(F[sc.slot_sys[sl]], (double)b.x, (double)b.y, (double)b.z);
+        cen[3 * sl] = c.x; cen[3 * sl + 1] = c.y; cen[3 * sl + 2] = c.z;
+    }
     int code = 0;
 #pragma unroll 1
     for (int j = 0; j < sc.npairs; ++j) {
         const int4 pr = sc.pairs[j];
-        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F)) continue;
+        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F, cen)) continue;
         double m;
         int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
         if (r != 0) { code = r; break; }
