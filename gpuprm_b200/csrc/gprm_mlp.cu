@@ -1030,6 +1030,10 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
 enum { TG_FWD = 0, TG_DH = 1, TG_WPART = 2 };
 constexpr int TG_STAGES = 4;
 constexpr int TG_MAX_SPLITS = 32;
+/* column tile of the layer GEMMs (forward, backward through a layer): 64
+   columns, 4 x more CTAs than one 256-column tile, so that the epilogue
+   (GELU, GELU', row stores) spreads over more SMs */
+constexpr int TG_BN_LAYER = 64;
 constexpr int TG_THREADS = 192;
 
 template <int BN>
@@ -1409,19 +1413,20 @@ int tc_maps(gprm_mlp* h, int n)
         if ((rc = tc_map(h, &h->m_h[l], h->H[l], HID, N, HID * 2, TC_ROWS))) return rc;
     for (int l = 0; l < NLAYER; ++l)
         if ((rc = tc_map(h, &h->m_dz[l], h->dZ[l], HID, N, HID * 2, TC_ROWS))) return rc;
-    if ((rc = tc_map(h, &h->m_w1p, h->w1p, 64, HID, 64 * 2, HID))) return rc;
+    if ((rc = tc_map(h, &h->m_w1p, h->w1p, 64, HID, 64 * 2, TG_BN_LAYER))) return rc;
     for (int l = 1; l < NLAYER; ++l) {
-        if ((rc = tc_map(h, &h->m_w[l - 1], h->wbf + h->offWbf[l], HID, HID, HID * 2, HID))) return rc;
-        if ((rc = tc_map(h, &h->m_wt[l - 1], h->wt + (size_t)(l - 1) * HID * HID, HID, HID, HID * 2, HID))) return rc;
+        if ((rc = tc_map(h, &h->m_w[l - 1], h->wbf + h->offWbf[l], HID, HID, HID * 2, TG_BN_LAYER))) return rc;
+        if ((rc = tc_map(h, &h->m_wt[l - 1], h->wt + (size_t)(l - 1) * HID * HID, HID, HID, HID * 2, TG_BN_LAYER)))
+            return rc;
     }
     if ((rc = tc_map(h, &h->m_ta, h->Ta, N, HID, (uint64_t)h->ldT * 2, TC_ROWS))) return rc;
     if ((rc = tc_map(h, &h->m_tb256, h->Tb, N, HID, (uint64_t)h->ldT * 2, HID))) return rc;
     if ((rc = tc_map(h, &h->m_tb64, h->Tb, N, 64, (uint64_t)h->ldT * 2, 64))) return rc;
     if (!h->tc_attr) {
-        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_FWD, HID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TgSmem<HID>::BYTES));
-        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_DH, HID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TgSmem<HID>::BYTES));
+        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_FWD, TG_BN_LAYER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TgSmem<TG_BN_LAYER>::BYTES));
+        MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_DH, TG_BN_LAYER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)TgSmem<TG_BN_LAYER>::BYTES));
         MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_WPART, HID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)TgSmem<HID>::BYTES));
         MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_WPART, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1440,12 +1445,13 @@ int forward_tc(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, fl
     const int items = HID * 64 + (NLAYER - 1) * HID * HID;
     k_tc_weights<<<(items + 255) / 256, 256, 0, st>>>(h->wbf, h->offWbf[0], h->offWbf[1], h->offWbf[2],
                                                       h->offWbf[3], h->w1p, h->wt);
-    const dim3 grid(1, (n + TC_ROWS - 1) / TC_ROWS, 1);
+    const dim3 grid(HID / TG_BN_LAYER, (n + TC_ROWS - 1) / TC_ROWS, 1);
     for (int l = 0; l < NLAYER; ++l) {
         TgArgs a{};
         a.M = n; a.N = HID; a.K = l == 0 ? 64 : HID; a.kps = a.K;
         a.bias = h->w + h->offB[l]; a.zout = h->Z[l]; a.hout = h->H[l]; a.ldc = HID; a.err = h->dev_err;
-        k_tc_gemm<TG_FWD, HID><<<grid, TG_THREADS, TgSmem<HID>::BYTES, st>>>(l == 0 ? h->m_x64 : h->m_h[l - 1],
+        k_tc_gemm<TG_FWD, TG_BN_LAYER><<<grid, TG_THREADS, TgSmem<TG_BN_LAYER>::BYTES, st>>>(
+            l == 0 ? h->m_x64 : h->m_h[l - 1],
                                                                           l == 0 ? h->m_w1p : h->m_w[l - 1], a);
     }
     int blocks = (n * 32 + 255) / 256;
@@ -1490,7 +1496,8 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
             TgArgs d{};
             d.M = n; d.N = HID; d.K = HID; d.kps = HID; d.zin = h->Z[l - 1]; d.hout = h->dZ[l - 1]; d.ldc = HID;
             d.err = h->dev_err;
-            k_tc_gemm<TG_DH, HID><<<dim3(1, (n + TC_ROWS - 1) / TC_ROWS, 1), TG_THREADS, TgSmem<HID>::BYTES, st>>>(
+            k_tc_gemm<TG_DH, TG_BN_LAYER><<<dim3(HID / TG_BN_LAYER, (n + TC_ROWS - 1) / TC_ROWS, 1), TG_THREADS,
+                                            TgSmem<TG_BN_LAYER>::BYTES, st>>>(
                 h->m_dz[l], h->m_wt[l - 1], d);
         }
     }
