@@ -105,6 +105,64 @@ __device__ __forceinline__ float gelu_f(float z)
     return __fmaf_rn(-fabsf(z), gelu_h(z), fmaxf(z, 0.0f));
 }
 
+/* Two lanes of FP32 in one 64-bit register for the packed FP32 x2
+ * instructions of sm_100 (each half rounded exactly like the scalar
+ * instruction, so results equal gelu_f's bit for bit). */
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+/* gelu_f of (z0, z1) with packed x2 arithmetic: the same operations, half
+ * the instructions for the polynomial and the squarings. */
+__device__ __forceinline__ void gelu_f2(unsigned long long z, float& g0, float& g1)
+{
+    float z0, z1;
+    f2_unpack(z, z0, z1);
+    const unsigned long long az = f2_pack(fabsf(z0), fabsf(z1));
+    const unsigned long long x = f2_mul(az, f2_pack(0.70710678118654752f, 0.70710678118654752f));
+    unsigned long long y = f2_fma(f2_pack(4.497039844864048e-05f, 4.497039844864048e-05f), x,
+                                  f2_pack(0.0002888118615373969f, 0.0002888118615373969f));
+    y = f2_fma(y, x, f2_pack(0.0001587445440236479f, 0.0001587445440236479f));
+    y = f2_fma(y, x, f2_pack(0.009680968709290028f, 0.009680968709290028f));
+    y = f2_fma(y, x, f2_pack(0.04415399581193924f, 0.04415399581193924f));
+    y = f2_fma(y, x, f2_pack(0.07364540547132492f, 0.07364540547132492f));
+    y = f2_fma(y, x, f2_pack(1.0442737340927124f, 1.0442737340927124f));
+    y = f2_mul(y, y);
+    y = f2_mul(y, y);
+    y = f2_mul(y, y);
+    y = f2_mul(y, y);                                      /* 2 P(x)^16 */
+    float y0, y1;
+    f2_unpack(y, y0, y1);
+    const unsigned long long h = f2_pack(rcp_approx(y0), rcp_approx(y1));
+    const unsigned long long r = f2_fma(f2_pack(-fabsf(z0), -fabsf(z1)), h, f2_pack(fmaxf(z0, 0.0f), fmaxf(z1, 0.0f)));
+    f2_unpack(r, g0, g1);
+}
+
 __device__ __forceinline__ float gelu_grad(float z)
 {
     /* Phi(z) + z pdf(z), pdf(z) = exp(-z^2/2) / sqrt(2 pi) = 2^(-z^2 log2(e) / 2) / sqrt(2 pi) */
@@ -852,8 +910,11 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                     }
                     uint32_t hp[8];
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        hp[j] = pack_bf16(gelu_f(v[2 * j] + bv[2 * j]), gelu_f(v[2 * j + 1] + bv[2 * j + 1]));
+                    for (int j = 0; j < 8; ++j) {
+                        float g0, g1;
+                        gelu_f2(f2_add(f2_pack(v[2 * j], v[2 * j + 1]), f2_pack(bv[2 * j], bv[2 * j + 1])), g0, g1);
+                        hp[j] = pack_bf16(g0, g1);
+                    }
                     if (l < NLAYER - 1) {
                         /* over the previous layer's activations (whose MMAs have all
                            completed): atom column r, 16-byte groups 2q, 2q+1 */
