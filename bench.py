@@ -59,8 +59,8 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes per edge of one k_check_edges launch (dram__bytes_read.sum +
 # dram__bytes_write.sum under ncu on the 65536-sample case of this workload:
-# 15.56 MB for 183774 edges).
-DRAM_BYTES_PER_EDGE = 15.56e6 / 183774
+# 14.26 MB + 1.79 MB for 183774 edges).
+DRAM_BYTES_PER_EDGE = 16.04e6 / 183774
 
 METRIC = "edge-step collision checks/s"
 UNIT = "edge-steps/s"
