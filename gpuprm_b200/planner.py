@@ -415,7 +415,7 @@ def train_predictor(cs, scene, n_labels=1 << 20, epochs=10, batch=4096, lr=1e-3,
 
 
 def predictor_errors(cs, scene, mlp, n=1 << 16, seed=0, prune=0.9):
-    """The exact checker as the judge of the predictor on held-out uniform
+    """The exact checker as the arbiter of the predictor on held-out uniform
     configurations: false-free rate (colliding, predicted p < 0.5),
     false-colliding rate (free, predicted p >= 0.5), and the share of free
     configurations the planner would prune (p > prune)."""
