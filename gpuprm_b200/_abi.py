@@ -109,6 +109,7 @@ SIGNATURES = [
     ("gprm_last_error", C.c_char_p, [_P]),
     ("gprm_set_mode", C.c_int, [_P, C.c_int]),
     ("gprm_set_edge_policy", C.c_int, [_P, C.c_int]),
+    ("gprm_set_edge_split", C.c_int, [_P, C.c_int, C.c_int]),
     ("gprm_set_band", C.c_int, [_P, C.c_float]),
     ("gprm_get_stats", C.c_int, [_P, C.POINTER(Stats)]),
     ("gprm_indicator", C.c_int, [_P, _F, _I]),

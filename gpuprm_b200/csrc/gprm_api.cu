@@ -379,6 +379,7 @@ void release_request(Request& r)
     cudaFree(r.d_b);
     cudaFree(r.d_res);
     cudaFree(r.d_key);
+    cudaFree(r.d_seg);
     cudaFree(r.d_queue);
     cudaFreeHost(r.ctl_host);
     cudaFreeHost(r.h_a);
@@ -396,6 +397,8 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
         CUDA_TRY(h, cudaMalloc((void**)&r.ctl, HOST_PARTS * sizeof(Control)));
         CUDA_TRY(h, cudaHostAlloc((void**)&r.ctl_host, HOST_PARTS * sizeof(Control), cudaHostAllocDefault));
     }
+    if (kind == 1 && !r.d_seg)
+        CUDA_TRY(h, cudaMalloc((void**)&r.d_seg, (size_t)(EDGE_SPLIT_MAX + 1) * sizeof(unsigned)));
     size_t need_q = (kind == 0) ? n : 4 * n + 65536;
     if (n > r.cap_items || need_q > r.cap_queue || (with_host && !r.h_res && n > 0)) {
         size_t cap = n > r.cap_items ? n + n / 4 + 64 : r.cap_items;
@@ -468,9 +471,14 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
     if (kind == 0)
         CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, a, n, offset, res, band_on, h->band, r.d_queue,
                                          (unsigned)r.cap_queue, ctl, st));
-    else
+    else {
+        /* small batches split their long edges over several warps */
+        const bool split = r.d_seg && h->split_rounds > 0 && n <= (long long)h->split_max;
         CUDA_TRY(h, launch_check_edges(h->dsc, h->cfg_e, a, b, n, offset, h->dq, h->policy, key, band_on,
-                                       h->band, r.d_queue, (unsigned)r.cap_queue, ctl, st));
+                                       h->band, r.d_queue, (unsigned)r.cap_queue, ctl, st,
+                                       split ? r.d_seg : nullptr, split ? h->split_rounds : 0));
+        if (split) h->host_stats.launches += 1;
+    }
     if (e1) CUDA_TRY(h, cudaEventRecord(e1, st));
     if (band_on) {
         if (e2) CUDA_TRY(h, cudaEventRecord(e2, st));
@@ -748,6 +756,17 @@ int gprm_set_edge_policy(gprm_space* h, int policy)
     if (policy != GPRM_EDGES_EARLY_EXIT && policy != GPRM_EDGES_ALL_STEPS)
         return fail(h, GPRM_ERR_ARG, "unknown edge policy %d", policy);
     h->policy = policy;
+    return GPRM_OK;
+}
+
+int gprm_set_edge_split(gprm_space* h, int max_edges, int seg_rounds)
+{
+    if (!h) return GPRM_ERR_ARG;
+    if (max_edges < 0 || max_edges > (int)EDGE_SPLIT_MAX || seg_rounds < 1)
+        return fail(h, GPRM_ERR_ARG, "edge split: max_edges must be in [0, %d] and seg_rounds >= 1",
+                    (int)EDGE_SPLIT_MAX);
+    h->split_max = max_edges;
+    h->split_rounds = seg_rounds;
     return GPRM_OK;
 }
 

@@ -31,6 +31,7 @@ struct Request {
     float* d_b = nullptr;         /* qe */
     int* d_res = nullptr;
     unsigned* d_key = nullptr;
+    unsigned* d_seg = nullptr;    /* edge segment offsets (EDGE_SPLIT_MAX + 1) */
     uint2* d_queue = nullptr;
     float* h_a = nullptr;         /* pinned staging */
     float* h_b = nullptr;
@@ -84,6 +85,8 @@ struct gprm_space {
 
     int mode = GPRM_MODE_FP64_BAND;
     int policy = GPRM_EDGES_EARLY_EXIT;
+    int split_max = 16384;        /* edge batches up to this size split long edges */
+    int split_rounds = 2;         /* rounds of 32 steps per segment */
     float band = 1e-5f;
 
     std::vector<gprm::Request> reqs;

@@ -97,11 +97,16 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
                                  long long n, long long offset, int* res, int band_on, float band,
                                  uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
 
-/* Edge checks, FP32 pass: key[e] is set per the edge policy (see kernels). */
+/* Edge checks, FP32 pass: key[e] is set per the edge policy (see kernels).
+ * seg_off (EDGE_SPLIT_MAX + 1 words of scratch) or null: with it, n <=
+ * EDGE_SPLIT_MAX and every edge longer than seg_rounds rounds of 32 steps
+ * is split into segments that different warps check (small batches of long
+ * edges, where one warp per edge would leave the GPU idle). */
+constexpr long long EDGE_SPLIT_MAX = 16384;
 cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs,
                                const float* qe, long long n, long long offset, float dq, int policy,
                                unsigned* key, int band_on, float band, uint2* queue, unsigned qcap,
-                               Control* ctl, cudaStream_t st);
+                               Control* ctl, cudaStream_t st, unsigned* seg_off = nullptr, int seg_rounds = 0);
 
 /* FP64 recheck of queued vertex (kind 0) or edge-step (kind 1) items. */
 cudaError_t launch_recheck(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,

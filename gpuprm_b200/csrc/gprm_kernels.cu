@@ -506,25 +506,55 @@ __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict
 __device__ __forceinline__ unsigned early_key(unsigned order, int code) { return (order << 4) | (unsigned)(code + 1); }
 __device__ __forceinline__ unsigned all_key(int t, int code) { return ((unsigned)(t + 1) << 4) | (unsigned)(code + 1); }
 
-/* One edge e (testnum steps, rounds of 32 steps over the lanes). */
-template <int POLICY>
+/* Segments of an edge of R rounds when a batch splits its edges into
+ * pieces of about seg_rounds rounds (at most EDGE_MAX_SEGS per edge). */
+constexpr int EDGE_MAX_SEGS = 64;
+__device__ __forceinline__ int edge_seg_count(int R, int seg_rounds)
+{
+    const int s = (R + seg_rounds - 1) / seg_rounds;
+    return s < EDGE_MAX_SEGS ? s : EDGE_MAX_SEGS;
+}
+
+/* One edge e (testnum steps, rounds of 32 steps over the lanes), or with
+ * seg_rounds > 0 its segment `seg`: a contiguous range of rounds, so that
+ * several warps share a long edge.  The rounds keep their step order, a
+ * segment's decision is merged into key[e] atomically (min for early exit,
+ * max for all steps, the same merge as the FP64 recheck) and a segment
+ * stops once key[e] holds a decision that none of its remaining rounds can
+ * improve on. */
+template <int POLICY, bool SPLIT = false>
 __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& S, const float* __restrict__ qs,
                                            const float* __restrict__ qe, long long e, long long offset, float dq,
                                            unsigned* __restrict__ key, int band_on, float band,
                                            uint2* __restrict__ queue, unsigned qcap, Control* ctl, PairCounts& pc,
-                                           unsigned long long& exec, unsigned long long& nominal)
+                                           unsigned long long& exec, unsigned long long& nominal,
+                                           int seg = 0, int seg_rounds = 0)
 {
     const int lane = threadIdx.x & 31;
     const int tn = edge_testnum(qs, qe, e, offset, sc.ndof, dq);
     if (tn < 0) {
-        if (lane == 0) atomicOr(&ctl->flags, GPRM_DEVFLAG_BAD_EDGE);
+        if (lane == 0 && seg == 0) atomicOr(&ctl->flags, GPRM_DEVFLAG_BAD_EDGE);
         return;
     }
-    if (lane == 0) nominal += tn;
+    if (lane == 0 && seg == 0) nominal += tn;
     const int R = (tn + 31) >> 5;
+    int r_begin = 0, r_end = R;
+    if constexpr (SPLIT) {
+        const int ns = edge_seg_count(R, seg_rounds);
+        const int rs = (R + ns - 1) / ns;
+        r_begin = seg * rs;
+        r_end = min(R, r_begin + rs);
+    }
     bool decided = false;
 #pragma unroll 1
-    for (int r = 0; r < R && !decided; ++r) {
+    for (int r = r_begin; r < r_end && !decided; ++r) {
+        if constexpr (SPLIT) {
+            const unsigned kv = *(volatile const unsigned*)&key[e];
+            const bool beaten = (POLICY == EDGE_EARLY_EXIT)
+                ? (kv != 0xffffffffu && (kv >> 4) < (unsigned)(r * 32))
+                : (kv != 0u && (int)(kv >> 4) - 1 > tn - 1 - r * 32);
+            if (__any_sync(FULL_MASK, beaten)) break;
+        }
         int t;
         unsigned order;
         bool valid;
@@ -597,8 +627,12 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         warp_append(want, make_uint2((unsigned)e, (unsigned)t | ((unsigned)(code + 1) << 27)),
                     queue, qcap, ctl);
         if (hits) {
-            if (lane == L)
-                key[e] = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
+            if (lane == L) {
+                const unsigned kv = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
+                if constexpr (!SPLIT) key[e] = kv;
+                else if (POLICY == EDGE_EARLY_EXIT) atomicMin(&key[e], kv);
+                else atomicMax(&key[e], kv);
+            }
             decided = true;
         }
     }
@@ -616,27 +650,104 @@ __device__ __forceinline__ void flush_edge_counts(unsigned long long exec, unsig
     flush_counts(pc, ctl);
 }
 
-template <bool SMEM, int POLICY>
+/* SPLIT: the work items are the segments of the edges, edge e owning
+ * items [seg_off[e], seg_off[e+1]) (seg_off from k_edge_segments);
+ * otherwise one item per edge and seg_off is unused. */
+template <bool SMEM, int POLICY, bool SPLIT>
 __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__ qs,
                                           const float* __restrict__ qe, long long n,
                                           long long offset, float dq, unsigned* __restrict__ key,
                                           int band_on, float band, uint2* __restrict__ queue,
-                                          unsigned qcap, Control* ctl)
+                                          unsigned qcap, Control* ctl, const unsigned* __restrict__ seg_off,
+                                          int seg_rounds)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const SceneView S = stage_scene<SMEM>(sc, smem);
     const int lane = threadIdx.x & 31;
     unsigned long long exec = 0, nominal = 0;
     PairCounts pc = {0, 0, 0};
+    if constexpr (!SPLIT) {
+        for (;;) {
+            unsigned long long eu = 0;
+            if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
+            eu = __shfl_sync(FULL_MASK, eu, 0);
+            if (eu >= (unsigned long long)n) break;
+            check_edge<POLICY>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, queue, qcap, ctl, pc,
+                               exec, nominal);
+        }
+        flush_edge_counts(exec, nominal, pc, ctl);
+        return;
+    }
+    const unsigned long long items = (unsigned long long)seg_off[n];
     for (;;) {
         unsigned long long eu = 0;
-        if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
+        long long e = 0;
+        int seg = 0;
+        if (lane == 0) {
+            eu = atomicAdd(&ctl->next, 1ull);
+            if (eu < items) {
+                long long lo = 0, hi = n;       /* seg_off[lo] <= eu < seg_off[hi] */
+                while (hi - lo > 1) {
+                    const long long mid = (lo + hi) >> 1;
+                    if ((unsigned long long)seg_off[mid] <= eu) lo = mid;
+                    else hi = mid;
+                }
+                e = lo;
+                seg = (int)(eu - seg_off[lo]);
+            }
+        }
         eu = __shfl_sync(FULL_MASK, eu, 0);
-        if (eu >= (unsigned long long)n) break;
-        check_edge<POLICY>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, queue, qcap, ctl, pc, exec,
-                           nominal);
+        if (eu >= items) break;
+        e = __shfl_sync(FULL_MASK, e, 0);
+        seg = __shfl_sync(FULL_MASK, seg, 0);
+        check_edge<POLICY, true>(sc, S, qs, qe, e, offset, dq, key, band_on, band, queue, qcap, ctl, pc, exec,
+                                 nominal, seg, seg_rounds);
     }
     flush_edge_counts(exec, nominal, pc, ctl);
+}
+
+/* Segment offsets of n edges (one block): seg_off[e] = sum over e' < e of
+ * the segment count of edge e', seg_off[n] = the total.  Edges the check
+ * rejects (non-finite or oversized) count one segment. */
+__global__ void __launch_bounds__(1024) k_edge_segments(const float* __restrict__ qs, const float* __restrict__ qe,
+                                                        long long n, long long offset, int ndof, float dq,
+                                                        int seg_rounds, unsigned* __restrict__ seg_off)
+{
+    __shared__ unsigned wsum[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long per = (n + blockDim.x - 1) / blockDim.x;
+    const long long b0 = min(n, (long long)tid * per), b1 = min(n, b0 + per);
+    auto segs = [&](long long e) -> unsigned {
+        const int tn = edge_testnum(qs, qe, e, offset, ndof, dq);
+        return tn < 0 ? 1u : (unsigned)edge_seg_count((tn + 31) >> 5, seg_rounds);
+    };
+    unsigned s = 0;
+    for (long long e = b0; e < b1; ++e) s += segs(e);
+    unsigned x = s;                                    /* inclusive scan in the warp */
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned y = __shfl_up_sync(FULL_MASK, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        unsigned w = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned y = __shfl_up_sync(FULL_MASK, w, d);
+            if (lane >= d) w += y;
+        }
+        if (lane < nw) wsum[lane] = w;                 /* inclusive warp totals */
+    }
+    __syncthreads();
+    unsigned base = x - s + (warp > 0 ? wsum[warp - 1] : 0u);
+    for (long long e = b0; e < b1; ++e) {
+        seg_off[e] = base;
+        base += segs(e);
+    }
+    if (tid == (int)blockDim.x - 1) seg_off[n] = base;
 }
 
 /* ------------------------------------------------------------------ */
@@ -759,12 +870,17 @@ static cudaError_t variant_warps(const void* fn, int threads, size_t smem, int* 
     return err;
 }
 
-static const void* kernel_fn(int vertex_kernel, bool smem, int policy)
+static const void* kernel_fn(int vertex_kernel, bool smem, int policy, bool split = false)
 {
     if (vertex_kernel) return smem ? (const void*)k_check_configs<true> : (const void*)k_check_configs<false>;
+    if (split) {
+        if (policy == EDGE_EARLY_EXIT)
+            return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT, true> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT, true>;
+        return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS, true> : (const void*)k_check_edges<false, EDGE_ALL_STEPS, true>;
+    }
     if (policy == EDGE_EARLY_EXIT)
-        return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT>;
-    return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS> : (const void*)k_check_edges<false, EDGE_ALL_STEPS>;
+        return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT, false> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT, false>;
+    return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS, false> : (const void*)k_check_edges<false, EDGE_ALL_STEPS, false>;
 }
 
 cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads, int scene_in_smem,
@@ -776,10 +892,11 @@ cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads,
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     size_t smem = frame_smem_bytes(sc, threads) + (scene_in_smem ? scene_smem_bytes(sc) : 0);
-    for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol) {
-        err = open_smem_cap(kernel_fn(vertex_kernel, scene_in_smem != 0, pol), optin, smem);
-        if (err != cudaSuccess) return err;
-    }
+    for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol)
+        for (int split = 0; split < (vertex_kernel ? 1 : 2); ++split) {
+            err = open_smem_cap(kernel_fn(vertex_kernel, scene_in_smem != 0, pol, split != 0), optin, smem);
+            if (err != cudaSuccess) return err;
+        }
     int warps = 0;
     err = variant_warps(kernel_fn(vertex_kernel, scene_in_smem != 0, 0), threads, smem, &warps);
     if (err != cudaSuccess) return err;
@@ -831,17 +948,29 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
 cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs, const float* qe,
                                long long n, long long offset, float dq, int policy, unsigned* key,
                                int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
-                               cudaStream_t st)
+                               cudaStream_t st, unsigned* seg_off, int seg_rounds)
 {
     if (n <= 0) return cudaSuccess;
-    size_t sm = cfg.smem_bytes;
-    if (policy == EDGE_EARLY_EXIT) {
-        if (cfg.scene_in_smem) k_check_edges<true, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
-        else k_check_edges<false, EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
-    } else {
-        if (cfg.scene_in_smem) k_check_edges<true, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
-        else k_check_edges<false, EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl);
+    if (seg_off && (seg_rounds < 1 || n > EDGE_SPLIT_MAX)) return cudaErrorInvalidValue;
+    if (seg_off) {
+        k_edge_segments<<<1, 1024, 0, st>>>(qs, qe, n, offset, sc.ndof, dq, seg_rounds, seg_off);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
     }
+    size_t sm = cfg.smem_bytes;
+#define GPRM_EDGE_LAUNCH(SM_, POL_, SPLIT_)                                                                   \
+    k_check_edges<SM_, POL_, SPLIT_><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, \
+                                                                          band, queue, qcap, ctl, seg_off,       \
+                                                                          seg_rounds)
+    const bool split = seg_off != nullptr;
+    if (policy == EDGE_EARLY_EXIT) {
+        if (cfg.scene_in_smem) { if (split) GPRM_EDGE_LAUNCH(true, EDGE_EARLY_EXIT, true); else GPRM_EDGE_LAUNCH(true, EDGE_EARLY_EXIT, false); }
+        else { if (split) GPRM_EDGE_LAUNCH(false, EDGE_EARLY_EXIT, true); else GPRM_EDGE_LAUNCH(false, EDGE_EARLY_EXIT, false); }
+    } else {
+        if (cfg.scene_in_smem) { if (split) GPRM_EDGE_LAUNCH(true, EDGE_ALL_STEPS, true); else GPRM_EDGE_LAUNCH(true, EDGE_ALL_STEPS, false); }
+        else { if (split) GPRM_EDGE_LAUNCH(false, EDGE_ALL_STEPS, true); else GPRM_EDGE_LAUNCH(false, EDGE_ALL_STEPS, false); }
+    }
+#undef GPRM_EDGE_LAUNCH
     return cudaGetLastError();
 }
 

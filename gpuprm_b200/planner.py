@@ -8,13 +8,13 @@ get_near_vertices, prmsolver.cpp:2533-2574) and answer a batch of
 start/goal queries; every collision verdict comes from the exact checker.
 
 * ``plain_prm``: check every candidate edge, take connected components.
-* ``lazy_prm``: batched lazy Kruskal, exact connectivity with fewer checks.
+* ``lazy_prm``: batched lazy Boruvka, exact connectivity with fewer checks.
     round 1: each vertex's ``first`` lowest-weight candidate edges are
              checked; their free edges define components.
-    round r: the unchecked edges that join two different components, in
-             weight order, are checked in one batch (the first
-             ``batch_frac`` of them, all of them in the last round); the
-             components are recomputed.
+    round r: each component's m lowest-weight unchecked edges to other
+             components are checked in one batch (m = first * growth^(r-1));
+             the last round (``max_rounds``) checks every such edge; the
+             components are recomputed after each round.
   It stops when no unchecked edge joins two components.  Every free
   candidate edge is then either checked or inside a component, so the
   components are exactly those of the fully checked graph: the same
@@ -142,12 +142,64 @@ def _components(graph, V, i, j, good):
     return graph.components(V, i, j, good)
 
 
-def _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph=None):
+def _attach_lazy(cs, ends, verts, nb, label, Q, kk, rounds=4):
+    """The attachment of `_answer_queries` with fewer checks and the same
+    answer.  Each round looks, per query, at the first (start, goal)
+    neighbour pair in nearest-first order whose vertices share a component
+    and whose two attachment edges are not known to collide, and checks the
+    unknown ones of those two edges; a query whose pair has both edges free
+    is settled (every earlier pair lacks a shared component or has a
+    colliding edge), a query without such a pair has no path.  After
+    `rounds` rounds every unknown edge of the unsettled queries is checked.
+    Returns (ok (2Q, kk) bool: edge checked and free, edges checked)."""
+    import torch
+    dev = verts.device
+    lab = label[nb.clamp_min(0)].long()
+    same = lab[:Q, :, None] == lab[Q:, None, :]                               # (Q, kk, kk)
+    status = torch.where(nb >= 0, 0, 2).to(torch.int8)                        # 0 unknown, 1 free, 2 colliding
+    rows = torch.arange(Q, device=dev)
+    nchecked = 0
+    for rnd in range(rounds + 1):
+        col = status == 2
+        cand = (same & ~col[:Q, :, None] & ~col[Q:, None, :]).reshape(Q, kk * kk)
+        has = cand.any(1)
+        first = torch.argmax(cand.to(torch.int8), dim=1)
+        a, b = first // kk, first % kk
+        ns = has & (status[rows, a] == 0)
+        ng = has & (status[Q + rows, b] == 0)
+        if rnd < rounds:
+            er = torch.cat([rows[ns], Q + rows[ng]])
+            ec = torch.cat([a[ns], b[ng]])
+        else:
+            open_ = ns | ng
+            want = torch.cat([open_, open_])[:, None] & (status == 0)
+            er, ec = torch.nonzero(want, as_tuple=True)
+        if er.numel() == 0:
+            break
+        o = _longest_first(ends[er], verts[nb[er, ec].long()])
+        er, ec = er[o], ec[o]
+        ok = _check_edges(cs, ends[er], verts[nb[er, ec].long()]) == 0
+        status[er, ec] = torch.where(ok, 1, 2).to(torch.int8)
+        nchecked += int(er.numel())
+    return status == 1, nchecked
+
+
+def _longest_first(qa, qb):
+    """Order of the edges qa[i] -> qb[i] by decreasing length: a batch whose
+    long edges start first ends with short ones, so the check kernel's
+    persistent warps finish together."""
+    import torch
+    return torch.argsort(torch.linalg.norm(qb - qa, dim=1), descending=True)
+
+
+def _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph=None, lazy=False):
     """Attaches every start and goal to its k nearest roadmap vertices by
     exactly checked edges, picks the first (start, goal) attachment pair in
     nearest-first order whose vertices share a component, and returns the
-    forest paths through the roadmap, all on the device.  Returns
-    (DevicePaths, attachment edges checked)."""
+    forest paths through the roadmap, all on the device.  With lazy, only
+    the attachment edges that decide this pair are checked
+    (`_attach_lazy`, same pairs).  Returns (DevicePaths, attachment edges
+    checked)."""
     import torch
     dev = verts.device
     Q = starts.shape[0]
@@ -162,8 +214,12 @@ def _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k
     ph = ph or _Phases(False)
     nb = index.knn(kk, q=ends.T.contiguous())[0].long()                       # (2Q, kk)
     ph.mark("attach_knn")
-    qa = ends[:, None, :].expand(-1, kk, -1).reshape(-1, ends.shape[1])
-    ok = (_check_edges(cs, qa, verts[nb.reshape(-1)]) == 0).reshape(2 * Q, kk)
+    if lazy:
+        ok, nconn = _attach_lazy(cs, ends, verts, nb, label, Q, kk)
+    else:
+        qa = ends[:, None, :].expand(-1, kk, -1).reshape(-1, ends.shape[1])
+        ok = (_check_edges(cs, qa, verts[nb.reshape(-1)]) == 0).reshape(2 * Q, kk)
+        nconn = 2 * Q * kk
     ph.mark("attach_edges")
     lab = torch.where(ok, label[nb].long(), torch.full_like(nb, -1))
     ls, lg = lab[:Q], lab[Q:]
@@ -182,7 +238,7 @@ def _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k
     ph.mark("paths")
     if ph.on:
         ph.t["forest_levels"] = levels
-    return DevicePaths(verts, length, off, flat_path, starts, goals), 2 * Q * kk
+    return DevicePaths(verts, length, off, flat_path, starts, goals), nconn
 
 
 def verify_paths(cs, dp: DevicePaths):
@@ -211,7 +267,8 @@ def verify_paths(cs, dp: DevicePaths):
     tail = verts[flat[off[found] + length[found] - 1]]
     qa = torch.cat([ra, st, tail])
     qb = torch.cat([rb, head, gl])
-    return bool((_check_edges(cs, qa, qb, GPRM_EDGES_ALL_STEPS) == 0).all().item())
+    o = _longest_first(qa, qb)
+    return bool((_check_edges(cs, qa[o], qb[o], GPRM_EDGES_ALL_STEPS) == 0).all().item())
 
 
 
@@ -258,6 +315,60 @@ def _sample(scene, n, seed):
     return lo + (hi - lo) * torch.rand((n, scene.ndof), device="cuda:0", generator=g)
 
 
+def _cheapest_per_component(rest, la, lb, m):
+    """The first m edges of `rest` (edge ids in weight order; la, lb the
+    component labels of their ends, la != lb) at each component, counting
+    both ends of every edge; each selected edge once."""
+    import torch
+    ends = torch.stack([la, lb], 1).reshape(-1)
+    eid = rest.repeat_interleave(2)
+    o = torch.argsort(ends, stable=True)                # by component, then weight
+    ev = ends[o]
+    rank = torch.arange(ev.numel(), device=ev.device) - torch.searchsorted(ev, ev)
+    return torch.unique(eid[o][rank < m])
+
+
+def _lazy_rounds(V, i64, j64, cost, check, components, max_rounds, first, growth, ph, length=None):
+    """The rounds of `lazy_prm` over the candidate edges (i64[e], j64[e]):
+    check(sel) gives the exact verdicts (True = free) of the edge ids sel,
+    components(good) the component labels of the free-edge graph.  Returns
+    (good uint8, checked bool, final labels, edges per round, free edges of
+    round 1)."""
+    import torch
+    dev = i64.device
+    E = int(i64.numel())
+    good = torch.zeros(E, dtype=torch.uint8, device=dev)
+    checked = torch.zeros(E, dtype=torch.bool, device=dev)
+    # round 1: components are single vertices, so the selection is every
+    # vertex's `first` cheapest candidate edges
+    order = torch.argsort(cost, stable=True)
+    label = torch.arange(V, dtype=torch.int32, device=dev)
+    R = max(1, int(max_rounds))
+    m, rounds, free1 = int(first), [], 0
+    for rnd in range(R):
+        rest = order[~checked[order]]
+        la, lb = label[i64[rest]], label[j64[rest]]
+        cross = la != lb
+        rest, la, lb = rest[cross], la[cross], lb[cross]
+        if rest.numel() == 0:
+            break
+        take = rest if rnd == R - 1 else _cheapest_per_component(rest, la, lb, m)
+        if length is not None:
+            take = take[torch.argsort(length[take], descending=True)]     # long edges first
+        ph.mark("round1_select" if rnd == 0 else "round_select")
+        ok = check(take)
+        checked[take] = True
+        good[take] = ok.to(torch.uint8)
+        if rnd == 0:
+            free1 = int(ok.sum().item())
+        rounds.append(int(take.numel()))
+        ph.mark("round1_edges" if rnd == 0 else "round_edges")
+        label = components(good)
+        ph.mark("components")
+        m *= int(growth)
+    return good, checked, label, rounds, free1
+
+
 def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, keep_roadmap=False) -> PlanResult:
     """Eager GPU PRM: every vertex and every candidate edge checked.  With
     keep_roadmap, info["roadmap"] = (vertices, free-edge ends i, j) as host
@@ -297,9 +408,12 @@ def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, 
 
 
 def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=0.9, beta=4.0,
-             batch_frac=1.0, min_batch=4096, max_rounds=2, first=2, profile=False) -> PlanResult:
-    """Batched lazy-Kruskal PRM (exact connectivity), optionally MLP-guided;
-    the roadmap and its bookkeeping stay on the device."""
+             max_rounds=4, first=1, growth=2, lazy_attach=True, profile=False) -> PlanResult:
+    """Batched lazy-Boruvka PRM (exact connectivity), optionally MLP-guided;
+    the roadmap and its bookkeeping stay on the device.  max_rounds >= 1
+    counts round 1 (with max_rounds = 2 the second round checks every
+    edge between components of round 1); lazy_attach: the query attachment
+    of `_attach_lazy`."""
     import torch
     s0 = cs.stats()["edge_steps_nominal"]
     graph, index = _workspace(scene.ndof)
@@ -330,46 +444,13 @@ def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=
         ph.mark("predict_edges")
     else:
         cost = length
-    good = torch.zeros(E, dtype=torch.uint8, device=dev)
-    checked = torch.zeros(E, dtype=torch.bool, device=dev)
-
-    def run(sel):
-        if sel.numel() == 0:
-            return 0
-        ok_ = _check_edges(cs, verts[i64[sel]], verts[j64[sel]]) == 0
-        checked[sel] = True
-        good[sel] = ok_.to(torch.uint8)
-        return int(ok_.sum().item())
-
-    # round 1: every vertex's `first` cheapest candidate edges
-    m = int(first)
-    ends = torch.cat([i64, j64])
-    eid = torch.arange(E, device=dev).repeat(2)
-    o = torch.argsort(cost.repeat(2), stable=True)
-    o = o[torch.argsort(ends[o], stable=True)]          # by vertex, then cost
-    ev = ends[o]
-    startpos = torch.searchsorted(ev, torch.arange(V, device=dev))
-    rank = torch.arange(2 * E, device=dev) - startpos[ev]
-    r1 = torch.unique(eid[o][rank < m])
-    ph.mark("round1_select")
-    free1 = run(r1)
-    ph.mark("round1_edges")
-    rounds = [int(r1.numel())]
-    order = torch.argsort(cost, stable=True)
-    for rnd in range(max_rounds):
-        label = _components(graph, V, i, j, good)
-        rest = order[~checked[order]]
-        cross = rest[label[i64[rest]] != label[j64[rest]]]
-        if cross.numel() == 0:
-            break
-        take = cross if rnd == max_rounds - 1 else cross[:max(min_batch, int(cross.numel() * batch_frac))]
-        ph.mark("round_select")
-        run(take)
-        rounds.append(int(take.numel()))
-        ph.mark("round_edges")
-    label = _components(graph, V, i, j, good)
-    ph.mark("components")
-    dp, nconn = _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph)
+    good, checked, label, rounds, free1 = _lazy_rounds(
+        V, i64, j64, cost,
+        lambda sel: _check_edges(cs, verts[i64[sel]], verts[j64[sel]]) == 0,
+        lambda good_: _components(graph, V, i, j, good_),
+        max_rounds, first, growth, ph, length)
+    dp, nconn = _answer_queries(cs, graph, index, verts, i, j, good, label, starts, goals, k, ph,
+                                lazy=lazy_attach)
     ph.mark("queries")
     ok = verify_paths(cs, dp)
     ph.mark("verify")
@@ -378,7 +459,7 @@ def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=
     dt = time.perf_counter() - t0
     return PlanResult(found, dp, dt, int(checked.sum().item()) + nconn,
                       int(cs.stats()["edge_steps_nominal"] - s0), vchecks,
-                      {"verified": ok, "free_vertices": V, "candidate_edges": E, "round1_edges": rounds[0],
+                      {"verified": ok, "free_vertices": V, "candidate_edges": E, "round1_edges": rounds[0] if rounds else 0,
                        "round1_free": free1, "later_edges": int(sum(rounds[1:])), "rounds": len(rounds),
                        "pruned": pruned, **({"phases_ms": ph.t} if profile else {})})
 
@@ -448,7 +529,7 @@ def _median_run(fn, repeats):
 
 
 def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0, mlp=None, repeats=3,
-                     first=2, max_rounds=2):
+                     first=1, max_rounds=4):
     """Plain (eager) PRM against the lazy PRM without guidance and the
     learned-guided lazy PRM, on the same seeded queries.  Each run is
     repeated (`repeats` timed runs after one untimed) and the median is
@@ -482,5 +563,5 @@ def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0,
         out["predictor_errors"] = predictor_errors(cs, scene, mlp, seed=seed)
     out["lazy_over_plain_time"] = out["lazy"]["time_to_path_ms"] / out["plain"]["time_to_path_ms"]
     out["config"] = {"samples": n_samples, "queries": n_queries, "k": k, "seed": seed, "dq": float(cs.deltaq()),
-                     "lazy_first": first, "lazy_rounds": max_rounds}
+                     "lazy_first": first, "lazy_rounds": max_rounds, "lazy_growth": 2, "lazy_attach": True}
     return out

@@ -115,6 +115,43 @@ def test_generated_scenes_larger_sample():
         np.testing.assert_array_equal(cs.check_edges(qs, qe) != 0, want != 0)
 
 
+@pytest.mark.parametrize("mode", [GPRM_MODE_FP32, GPRM_MODE_FP64_BAND])
+@pytest.mark.parametrize("policy", [GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT])
+def test_split_edges_match_whole_edges(policy, mode):
+    """Batches of at most 16384 edges split long edges over several warps
+    (segments of seg_rounds x 32 steps, at most 64 per edge): codes and
+    nominal step counts equal those of one warp per edge, and the all-steps
+    codes equal the oracle's."""
+    sc = scenes.make_hull6(5)
+    dq = 0.003
+    qs, qe = scenes.random_edges(sc, 300, 11, 9.0)           # up to ~3000 steps (> 64 rounds)
+    cs = space(sc, dq, mode=mode, policy=policy)
+    out = {}
+    for split in ((0, 4), (16384, 4), (16384, 2), (16384, 1)):
+        cs.set_edge_split(*split)
+        s0 = cs.stats()["edge_steps_nominal"]
+        out[split] = (cs.check_edges(qs, qe), cs.stats()["edge_steps_nominal"] - s0)
+    whole, steps = out[(0, 4)]
+    assert steps > 64 * 32 * 10
+    assert (whole != 0).any() and (whole == 0).any()
+    for split, (codes, n) in out.items():
+        np.testing.assert_array_equal(codes, whole, err_msg=str(split))
+        assert n == steps
+    if policy == GPRM_EDGES_ALL_STEPS:
+        omode = (O.FP32 if mode == GPRM_MODE_FP32 else O.FP32_BAND) | O.DEVICE_TRIG
+        want, _ = O.Oracle(sc).check_edges(qs[:48], qe[:48], dq, omode)
+        np.testing.assert_array_equal(out[(16384, 1)][0][:48], want)
+
+
+def test_edge_split_arguments():
+    sc = scenes.make_box4(1)
+    cs = space(sc, 0.02)
+    for bad in ((-1, 4), (16385, 4), (100, 0)):
+        with pytest.raises(GprmError):
+            cs.set_edge_split(*bad)
+    cs.set_edge_split(0, 4)
+
+
 def test_edge_cases():
     sc = scenes.make_box4(8)
     cs = space(sc, 0.02, mode=GPRM_MODE_FP64_BAND)

@@ -7,8 +7,10 @@ from gpuprm_b200 import planner
 
 @pytest.mark.gpu
 def test_lazy_prm_has_the_connectivity_of_the_eager_prm():
-    """Two-round lazy checking solves exactly the queries the eager PRM
-    solves on the same samples, checking fewer edges; every path verifies."""
+    """Lazy checking (Boruvka rounds, lazy query attachment) solves exactly
+    the queries the eager PRM solves on the same samples, checking fewer
+    edges; every path verifies.  So do the two-round schedule and a single
+    round that checks every candidate edge."""
     from gpuprm_b200 import scenes
     from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
     from gpuprm_b200.configspace import RobotConfigspace
@@ -23,6 +25,10 @@ def test_lazy_prm_has_the_connectivity_of_the_eager_prm():
     assert plain.info["verified"] and lazy.info["verified"]
     assert lazy.edge_checks < plain.edge_checks
     assert plain.success.mean() > 0.2
+    for kw in (dict(max_rounds=2, first=2), dict(max_rounds=1), dict(max_rounds=8, first=1, growth=1)):
+        other = planner.lazy_prm(cs, sc, starts, goals, 1 << 14, k=10, seed=4, **kw)
+        np.testing.assert_array_equal(plain.success, other.success)
+        assert other.info["verified"]
 
 
 @pytest.mark.gpu
