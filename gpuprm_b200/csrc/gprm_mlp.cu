@@ -22,6 +22,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -333,13 +334,16 @@ __global__ void k_out(int n, const __nv_bfloat16* __restrict__ H, const __nv_bfl
     }
 }
 
-/* output-layer backward: dw5 = H4^T dlogit, db5 = sum dlogit,
- * dZ4 = (dlogit w5) * gelu'(Z4) */
+/* output-layer backward: dZ4 = (dlogit w5) * gelu'(Z4), and per block the
+ * partial sums of dw5 = H4^T dlogit (part[b][0..HID)) and db5 = sum dlogit
+ * (part[b][HID]) over the rows r = b (mod gridDim.x); the partials are
+ * added in block order afterwards, so the gradients do not depend on
+ * scheduling. */
 __global__ void k_out_back(int n, const __nv_bfloat16* __restrict__ H, const float* __restrict__ Z,
                            const __nv_bfloat16* __restrict__ w5, const float* __restrict__ dlogit,
-                           float* __restrict__ dw5, float* __restrict__ db5, __nv_bfloat16* __restrict__ dZ)
+                           float* __restrict__ part, __nv_bfloat16* __restrict__ dZ)
 {
-    /* block per column chunk: column k = threadIdx.x (HID threads) */
+    /* column k = threadIdx.x (HID threads) */
     const int k = threadIdx.x;
     float acc = 0.0f, accb = 0.0f;
     for (int r = blockIdx.x; r < n; r += gridDim.x) {
@@ -348,18 +352,29 @@ __global__ void k_out_back(int n, const __nv_bfloat16* __restrict__ H, const flo
         accb += d;
         dZ[(size_t)r * HID + k] = __float2bfloat16(d * __bfloat162float(w5[k]) * gelu_grad(Z[(size_t)r * HID + k]));
     }
-    atomicAdd(&dw5[k], acc);
-    if (k == 0) atomicAdd(db5, accb);
+    part[(size_t)blockIdx.x * (HID + 1) + k] = acc;
+    if (k == 0) part[(size_t)blockIdx.x * (HID + 1) + HID] = accb;
 }
 
-/* db[c] = sum_r dZ[r][c] */
-__global__ void k_colsum(int n, int cols, const __nv_bfloat16* __restrict__ dZ, float* __restrict__ db)
+/* per-block partial column sums: part[b][c] = sum over rows r = b (mod
+ * gridDim.x) of dZ[r][c] */
+__global__ void k_colsum(int n, int cols, const __nv_bfloat16* __restrict__ dZ, float* __restrict__ part)
 {
     const int c = threadIdx.x;
     if (c >= cols) return;
     float acc = 0.0f;
     for (int r = blockIdx.x; r < n; r += gridDim.x) acc += __bfloat162float(dZ[(size_t)r * cols + c]);
-    atomicAdd(&db[c], acc);
+    part[(size_t)blockIdx.x * cols + c] = acc;
+}
+
+/* out[c] = sum over b < parts of part[b][c], in b order */
+__global__ void k_reduce_parts(int parts, int cols, const float* __restrict__ part, float* __restrict__ out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float acc = 0.0f;
+    for (int b = 0; b < parts; ++b) acc += part[(size_t)b * cols + c];
+    out[c] = acc;
 }
 
 /* Adam on the FP32 master parameters, refreshing their BF16 copies.
@@ -477,18 +492,25 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v)
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v)
+/* A 16-column TMEM load in two halves, so that a load can be in flight
+ * while the previous columns are processed: the issue, then the wait, which
+ * names the destination registers so that no use of them moves above it. */
+__device__ __forceinline__ void tc_ld16_issue(uint32_t taddr, uint32_t* r)
 {
-    uint32_t r[16];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                  "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                    "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
                    "=r"(r[14]), "=r"(r[15])
                  : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+__device__ __forceinline__ void tc_ld16_wait(uint32_t* r)
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                   "+r"(r[14]), "+r"(r[15])
+                 :: "memory");
 }
 
 /* shared memory of k_mlp_tc<K>: W | A | mbarrier | TMEM address | row partials */
@@ -896,12 +918,19 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                 const float* bl = bias_s + l * HID;
                 float part = 0.0f;
                 /* round r: columns 64r + 16q .. +15, so that round r completes
-                   K chunk r of the next layer's A operand */
+                   K chunk r of the next layer's A operand; the TMEM load of
+                   round r + 1 is in flight while round r is processed */
+                const uint32_t tbase = tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + 16 * q);
+                uint32_t acc[FU_CHUNKS][16];
+                tc_ld16_issue(tbase, acc[0]);
+                tc_ld16_wait(acc[0]);
 #pragma unroll
                 for (int r = 0; r < FU_CHUNKS; ++r) {
                     const int col = 64 * r + 16 * q;
+                    if (r + 1 < FU_CHUNKS) tc_ld16_issue(tbase + (uint32_t)(64 * (r + 1)), acc[r + 1]);
                     float v[16];
-                    tc_ld16(tmem + ((uint32_t)(32 * g) << 16) + (uint32_t)(a * TC_COLS + col), v);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(acc[r][j]);
                     float bv[16];
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
@@ -932,6 +961,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                             part = __fmaf_rn(bf16_hi(hp[j]), w5_s[col + 2 * j + 1], part);
                         }
                     }
+                    if (r + 1 < FU_CHUNKS) tc_ld16_wait(acc[r + 1]);
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
@@ -1267,19 +1297,44 @@ k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
 }
 
 /* g_w[o][i] (i < kin) = sum over the splits of ws[s][o][i] (ld ldw), in split order. */
-__global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* __restrict__ ws, float* __restrict__ gw)
+/* Threads [0, rows*kin): gw = the split partials of ws added in split
+ * order.  Then, with cpart, `rows` threads: gb[o] = sum over b < cparts of
+ * cpart[b][o]; then, with opart, HID + 1 threads: go[c] = sum over
+ * b < oparts of opart[b][c] (the output layer's k_out_back partials). */
+__global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* __restrict__ ws, float* __restrict__ gw,
+                           int cparts, const float* __restrict__ cpart, float* __restrict__ gb,
+                           int oparts, const float* __restrict__ opart, float* __restrict__ go)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= rows * kin) return;
-    const int o = t / kin, i = t % kin;
-    float acc = 0.0f;
-    for (int s = 0; s < splits; ++s) acc += ws[(size_t)s * rows * ldw + (size_t)o * ldw + i];
-    gw[t] = acc;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < rows * kin) {
+        const int o = t / kin, i = t % kin;
+        float acc = 0.0f;
+        for (int s = 0; s < splits; ++s) acc += ws[(size_t)s * rows * ldw + (size_t)o * ldw + i];
+        gw[t] = acc;
+        return;
+    }
+    t -= rows * kin;
+    if (cpart) {
+        if (t < rows) {
+            float acc = 0.0f;
+            for (int b = 0; b < cparts; ++b) acc += cpart[(size_t)b * rows + t];
+            gb[t] = acc;
+            return;
+        }
+        t -= rows;
+    }
+    if (opart && t < HID + 1) {
+        float acc = 0.0f;
+        for (int b = 0; b < oparts; ++b) acc += opart[(size_t)b * (HID + 1) + t];
+        go[t] = acc;
+    }
 }
 
-/* dst[c][r] = src[r][c] for r < rows, c < cols (ld of dst = ldd); 32x32 tiles. */
+/* dst[c][r] = src[r][c] for r < rows, c < cols (ld of dst = ldd); 32x32 tiles.
+ * With colsum: colsum[blockIdx.y][c] = the sum of the tile's 32 rows of
+ * column c (rows past the end count zero), for deterministic column sums. */
 __global__ void k_transpose_bf16(int rows, int cols, const __nv_bfloat16* __restrict__ src, int lds,
-                                 __nv_bfloat16* __restrict__ dst, int ldd)
+                                 __nv_bfloat16* __restrict__ dst, int ldd, float* __restrict__ colsum = nullptr)
 {
     __shared__ __nv_bfloat16 t[32][33];
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
@@ -1288,6 +1343,11 @@ __global__ void k_transpose_bf16(int rows, int cols, const __nv_bfloat16* __rest
         t[k][threadIdx.x] = (r < rows && c < cols) ? src[(size_t)r * lds + c] : __float2bfloat16(0.0f);
     }
     __syncthreads();
+    if (colsum && threadIdx.y == 0 && c0 + threadIdx.x < cols) {
+        float acc = 0.0f;
+        for (int k = 0; k < 32; ++k) acc += __bfloat162float(t[k][threadIdx.x]);
+        colsum[(size_t)blockIdx.y * cols + c0 + threadIdx.x] = acc;
+    }
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int c = c0 + k, r = r0 + threadIdx.x;
         if (c < cols && r < rows) dst[(size_t)c * ldd + r] = t[threadIdx.x][k];
@@ -1375,6 +1435,8 @@ struct gprm_mlp {
     __nv_bfloat16* w1p = nullptr;       /* W1 padded [256 x 64] */
     __nv_bfloat16* wt = nullptr;        /* W_l^T, layers 2..4 [3 x 256 x 256] */
     float* ws = nullptr;                /* split-K partials [TG_MAX_SPLITS x 256 x 256] */
+    float* cpart = nullptr;             /* bias-gradient partials [max(1024, rows/32) x 256] */
+    float* opart = nullptr;             /* output-layer gradient partials [1024 x 257] */
     int tc_n = -1;                      /* batch the tensor maps were made for */
     int tc_attr = 0;
     long long* d_ctl = nullptr;         /* training epoch: [row offset into perm, Adam step before it] */
@@ -1416,7 +1478,11 @@ int alloc_batch(gprm_mlp* h, int rows)
     MLP_TRY(h, cudaMalloc((void**)&h->dlogit, R * sizeof(float)));
     MLP_TRY(h, cudaMalloc((void**)&h->ybatch, R * sizeof(float)));
     MLP_TRY(h, cudaMalloc((void**)&h->idx, R * sizeof(int)));
-    cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb);
+    cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb); cudaFree(h->cpart);
+    h->cpart = nullptr;
+    const size_t cparts = std::max<size_t>(1024, (R + 31) / 32);
+    MLP_TRY(h, cudaMalloc((void**)&h->cpart, cparts * HID * sizeof(float)));
+    if (!h->opart) MLP_TRY(h, cudaMalloc((void**)&h->opart, (size_t)1024 * (HID + 1) * sizeof(float)));
     h->ldT = (rows + 63) / 64 * 64;
     MLP_TRY(h, cudaMalloc((void**)&h->X64, R * 64 * sizeof(__nv_bfloat16)));
     MLP_TRY(h, cudaMalloc((void**)&h->Ta, (size_t)HID * h->ldT * sizeof(__nv_bfloat16)));
@@ -1526,10 +1592,11 @@ int forward_tc(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, fl
 /* Backward through the tensor-core GEMMs (after forward_tc on the same rows). */
 int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
 {
-    MLP_TRY(h, cudaMemsetAsync(h->g, 0, (size_t)h->nparam * sizeof(float), st));
+    /* every gradient entry is written below (weights and biases by the
+       ordered reductions of k_reduce_w), so h->g needs no clearing */
     int blocks = n < 1024 ? n : 1024;
     k_out_back<<<blocks, HID, 0, st>>>(n, h->H[NLAYER - 1], h->Z[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->dlogit,
-                                       h->g + h->offW[NLAYER], h->g + h->offB[NLAYER], h->dZ[NLAYER - 1]);
+                                       h->opart, h->dZ[NLAYER - 1]);
     /* weight gradients: K = n split over CTAs, partials reduced in split order */
     int splits = (n + 127) / 128;
     if (splits > TG_MAX_SPLITS) splits = TG_MAX_SPLITS;
@@ -1539,7 +1606,7 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
     for (int l = NLAYER - 1; l >= 0; --l) {
         const int kin = l == 0 ? IN_PAD : HID, kin_p = l == 0 ? 64 : HID;
         /* dW_l = dZ_l^T H_{l-1}: A = dZ_l^T [256 x n], B = H_{l-1}^T [kin_p x n] */
-        k_transpose_bf16<<<tgrid, tblock, 0, st>>>(n, HID, h->dZ[l], HID, h->Ta, h->ldT);
+        k_transpose_bf16<<<tgrid, tblock, 0, st>>>(n, HID, h->dZ[l], HID, h->Ta, h->ldT, h->cpart);
         k_transpose_bf16<<<dim3(kin_p / 32, (n + 31) / 32), tblock, 0, st>>>(n, kin_p, l == 0 ? h->X64 : h->H[l - 1],
                                                                              kin_p, h->Tb, h->ldT);
         TgArgs a{};
@@ -1550,8 +1617,14 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
         else
             k_tc_gemm<TG_WPART, HID><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<HID>::BYTES, st>>>(
                 h->m_ta, h->m_tb256, a);
-        k_reduce_w<<<(HID * kin + 255) / 256, 256, 0, st>>>(splits, HID, kin_p, kin, h->ws, h->g + h->offW[l]);
-        k_colsum<<<blocks, HID, 0, st>>>(n, HID, h->dZ[l], h->g + h->offB[l]);
+        /* weights, this layer's biases (column sums of dZ_l from the transpose)
+           and, with the last layer, the output layer's partials */
+        const bool out_l = l == NLAYER - 1;
+        const int red_threads = HID * kin + HID + (out_l ? HID + 1 : 0);
+        k_reduce_w<<<(red_threads + 255) / 256, 256, 0, st>>>(splits, HID, kin_p, kin, h->ws, h->g + h->offW[l],
+                                                              (n + 31) / 32, h->cpart, h->g + h->offB[l],
+                                                              out_l ? blocks : 0, out_l ? h->opart : nullptr,
+                                                              h->g + h->offW[NLAYER]);
         if (l > 0) {
             /* dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}): A = dZ_l [n x 256], B = W_l^T [256 x 256] */
             TgArgs d{};
@@ -1608,7 +1681,8 @@ int backward(gprm_mlp* h, int n, cudaStream_t st)
     MLP_TRY(h, cudaMemsetAsync(h->g, 0, (size_t)h->nparam * sizeof(float), st));
     int blocks = n < 1024 ? n : 1024;
     k_out_back<<<blocks, HID, 0, st>>>(n, h->H[NLAYER - 1], h->Z[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->dlogit,
-                                       h->g + h->offW[NLAYER], h->g + h->offB[NLAYER], h->dZ[NLAYER - 1]);
+                                       h->opart, h->dZ[NLAYER - 1]);
+    k_reduce_parts<<<(HID + 1 + 255) / 256, 256, 0, st>>>(blocks, HID + 1, h->opart, h->g + h->offW[NLAYER]);
     for (int l = NLAYER - 1; l >= 0; --l) {
         const int kin = l == 0 ? IN_PAD : HID;
         const __nv_bfloat16* hin = l == 0 ? h->X : h->H[l - 1];
@@ -1617,7 +1691,8 @@ int backward(gprm_mlp* h, int n, cudaStream_t st)
         eg.gout = h->g + h->offW[l];
         eg.ldc = kin;
         k_gemm<true, false, EPI_GRAD_W><<<ggrid(HID, kin), 128, 0, st>>>(HID, kin, n, h->dZ[l], HID, hin, kin, eg);
-        k_colsum<<<blocks, HID, 0, st>>>(n, HID, h->dZ[l], h->g + h->offB[l]);
+        k_colsum<<<blocks, HID, 0, st>>>(n, HID, h->dZ[l], h->cpart);
+        k_reduce_parts<<<1, HID, 0, st>>>(blocks, HID, h->cpart, h->g + h->offB[l]);
         if (l > 0) {
             /* dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}): M = n, N = HID, K = HID */
             EpiArgs ed{};
@@ -1814,6 +1889,7 @@ void gprm_mlp_destroy(gprm_mlp* h)
     cudaFree(h->p); cudaFree(h->dlogit); cudaFree(h->ybatch); cudaFree(h->idx);
     cudaFree(h->Ha); cudaFree(h->Hb); cudaFree(h->dev_err); cudaFree(h->wtc);
     cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb); cudaFree(h->w1p); cudaFree(h->wt); cudaFree(h->ws);
+    cudaFree(h->cpart); cudaFree(h->opart);
     cudaFree(h->d_ctl);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
