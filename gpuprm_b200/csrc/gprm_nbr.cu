@@ -14,8 +14,8 @@
  *            (the reference's "terminate if buffer full");
  *   knn      the k nearest nodes under the same distance, ties broken by
  *            the lower index.  Nodes are bucketed into a uniform grid over
- *            the first min(4, ndof) joints (counting sort by cell); a query
- *            scans the 3^G cells around its own and keeps a sorted top-k
+ *            all joints (counting sort by cell); a query scans the
+ *            3^ndof cells around its own and keeps a sorted top-k
  *            (a thread per query for the nodes themselves, a warp per query
  *            for outside queries); a
  *            result is accepted only when its k-th distance is below the
@@ -38,7 +38,7 @@
 
 namespace {
 
-constexpr int NBR_MAX_GRID = 4;
+constexpr int NBR_MAX_GRID = GPRM_MAX_DOF;
 constexpr int NBR_MAX_K = 32;
 constexpr int NBR_MAX_CELLS = 1 << 21;
 
@@ -387,10 +387,13 @@ __global__ void k_knn_grid_warp(GridView g, const float* __restrict__ q, int m, 
         float guard;
         const bool finite = query_block(g, qv, lo, hi, &guard);
         const int rows = block_rows(g, lo, hi);
-        for (int r = 0; r < rows; ++r) {
+        /* many short rows (every joint gridded): the lanes split the rows;
+           few long rows: the lanes split each row's nodes */
+        const bool by_row = rows >= 32;
+        for (int r = by_row ? lane : 0; r < rows; r += by_row ? 32 : 1) {
             int b, e;
             block_row_range(g, lo, hi, r, &b, &e);
-            for (int p = b + lane; p < e; p += 32) {
+            for (int p = b + (by_row ? 0 : lane); p < e; p += by_row ? 1 : 32) {
                 float sd = dist2(g.xs, g.n, p, qv, g.ndof);
                 if (sd != sd) sd = INFINITY;
                 if (sd > bound.s) continue;
@@ -588,6 +591,9 @@ int gprm_nbr_build(gprm_nbr* h, const float* x, int n, int stride, float cell, v
     if (!(cell >= 0.0f) || !isfinite(cell)) return nfail(h, GPRM_ERR_ARG, "cell must be finite and >= 0");
     NBR_TRY(h, cudaSetDevice(h->device));
     cudaStream_t st = (cudaStream_t)stream;
+    /* every joint is gridded: a query's block of 3^ndof cells then holds
+       about 3^ndof x (nodes per cell) candidates, far fewer than a grid over
+       some joints whose block spans the others' whole range */
     const int nd = h->ndof, G = nd < NBR_MAX_GRID ? nd : NBR_MAX_GRID;
     h->n = n;
     h->x = x;
