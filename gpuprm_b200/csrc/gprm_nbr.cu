@@ -20,8 +20,10 @@
  *            for outside queries); a
  *            result is accepted only when its k-th distance is below the
  *            distance to the scanned block's boundary (with slack for float
- *            rounding), otherwise the query is redone by a block that scans
- *            every node.  The result is therefore the exact top-k.
+ *            rounding), otherwise the query is redone over the 5^ndof block
+ *            by a block of threads, and if that block's test fails too, by a
+ *            block that scans every node.  The result is therefore the exact
+ *            top-k.
  *
  * Distances use the reference's arithmetic: d = x_j - q_j, s = s + d*d
  * (no FMA; the library is compiled with -fmad=false), dist = sqrt(s).
@@ -232,19 +234,20 @@ __device__ __forceinline__ void topk_insert(float* ts, int* ti, int& len, int k,
     if (len < k) ++len;
 }
 
-/* The block of cells a query scans: cells c-1..c+1 in each gridded joint
- * (clipped to the grid); guard = the distance from q to the block's faces
+/* The block of cells a query scans: cells c-radius..c+radius in each
+ * gridded joint (clipped to the grid); guard = the distance from q to the block's faces
  * that have cells beyond them (infinite when none).  Returns false when a
  * gridded coordinate is not finite. */
-__device__ __forceinline__ bool query_block(const GridView& g, const float* qv, int* lo, int* hi, float* guard)
+__device__ __forceinline__ bool query_block(const GridView& g, const float* qv, int* lo, int* hi, float* guard,
+                                            int radius = 1)
 {
     bool finite = true;
     float gd = INFINITY;
     for (int d = 0; d < g.G; ++d) {
         finite &= isfinite(qv[d]);
         const int c = cell_coord(qv[d], g.lo[d], g.inv_cell, g.nc[d]);
-        lo[d] = max(c - 1, 0);
-        hi[d] = min(c + 1, g.nc[d] - 1);
+        lo[d] = max(c - radius, 0);
+        hi[d] = min(c + radius, g.nc[d] - 1);
         if (lo[d] > 0) gd = fminf(gd, qv[d] - (g.lo[d] + (float)lo[d] * g.cell));
         if (hi[d] < g.nc[d] - 1) gd = fminf(gd, (g.lo[d] + (float)(hi[d] + 1) * g.cell) - qv[d]);
     }
@@ -417,6 +420,76 @@ __global__ void k_knn_grid_warp(GridView g, const float* __restrict__ q, int m, 
     }
 }
 
+/* Second try for the queries the 3^ndof block could not settle: one block
+ * of threads per query scans the 5^ndof block around it (its rows split
+ * over the threads, each keeping its own top-k, merged as in k_knn_full)
+ * and applies the same exactness test with that block's guard; a query it
+ * cannot settle either goes to the full scan (redo2). */
+__global__ void __launch_bounds__(256) k_knn_wide(GridView g, const float* __restrict__ q, long long qstride, int k,
+                                                  int exclude_self, const int* __restrict__ redo,
+                                                  const int* __restrict__ nredo, int* redo2, int* nredo2,
+                                                  int* out_idx, float* out_dist)
+{
+    __shared__ float ms[8 * NBR_MAX_K];
+    __shared__ int mi[8 * NBR_MAX_K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cnt = *nredo;
+    for (int w = blockIdx.x; w < cnt; w += gridDim.x) {
+        const int qid = redo[w];
+        float qv[GPRM_MAX_DOF];
+        for (int j = 0; j < g.ndof; ++j) qv[j] = q[qid + qstride * j];
+        float ts[NBR_MAX_K];
+        int ti[NBR_MAX_K];
+        int len = 0;
+        TopkBound bound{INFINITY, 0x7fffffff};
+        int lo[NBR_MAX_GRID], hi[NBR_MAX_GRID];
+        float guard;
+        const bool finite = query_block(g, qv, lo, hi, &guard, 2);
+        const int rows = block_rows(g, lo, hi);
+        for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+            int b, e;
+            block_row_range(g, lo, hi, r, &b, &e);
+            for (int p = b; p < e; ++p) {
+                const int nid = g.id[p];
+                if (exclude_self && nid == qid) continue;
+                float sd = dist2(g.xs, g.n, p, qv, g.ndof);
+                if (sd != sd) sd = INFINITY;
+                if (!less_pair(sd, nid, bound.s, bound.i)) continue;
+                topk_insert(ts, ti, len, k, sd, nid);
+                topk_bound(ts, ti, len, k, bound);
+            }
+        }
+        float my_s, kth;
+        int my_i, found;
+        warp_topk_merge(ts, ti, len, k, &my_s, &my_i, &kth, &found);
+        if (lane < k) {
+            ms[warp * k + lane] = my_s;
+            mi[warp * k + lane] = my_i < 0 ? 0x7fffffff : my_i;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            len = 0;
+            bound = TopkBound{INFINITY, 0x7fffffff};
+            for (int e = lane; e < 8 * k; e += 32) {
+                if (mi[e] == 0x7fffffff) continue;
+                if (!less_pair(ms[e], mi[e], bound.s, bound.i)) continue;
+                topk_insert(ts, ti, len, k, ms[e], mi[e]);
+                topk_bound(ts, ti, len, k, bound);
+            }
+            warp_topk_merge(ts, ti, len, k, &my_s, &my_i, &kth, &found);
+            if (knn_exact(g, finite, found, k, kth, guard)) {
+                if (lane < k) {
+                    out_idx[(long long)qid * k + lane] = my_i;
+                    out_dist[(long long)qid * k + lane] = sqrtf(my_s);
+                }
+            } else if (lane == 0) {
+                redo2[atomicAdd(nredo2, 1)] = qid;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 /* Redo of the queries the grid could not settle: one block per query scans
  * every node (each thread four consecutive nodes at a time, keeping its own
  * top-k); each warp merges its lanes' lists by k rounds of a warp argmin,
@@ -504,8 +577,10 @@ struct gprm_nbr {
     int* cursor = nullptr;
     float* mm = nullptr;
     int* redo = nullptr;
-    int* nredo = nullptr;
-    size_t cap_xs = 0, cap_id = 0, cap_key = 0, cap_start = 0, cap_count = 0, cap_cursor = 0, cap_redo = 0;
+    int* nredo = nullptr;          /* [0]: queries the 3^ndof block left, [1]: the 5^ndof block */
+    int* redo2 = nullptr;
+    size_t cap_xs = 0, cap_id = 0, cap_key = 0, cap_start = 0, cap_count = 0, cap_cursor = 0, cap_redo = 0,
+           cap_redo2 = 0;
     std::string err = "no error";
 };
 
@@ -578,6 +653,7 @@ void gprm_nbr_destroy(gprm_nbr* h)
     cudaFree(h->cursor);
     cudaFree(h->mm);
     cudaFree(h->redo);
+    cudaFree(h->redo2);
     cudaFree(h->nredo);
     delete h;
 }
@@ -605,7 +681,7 @@ int gprm_nbr_build(gprm_nbr* h, const float* x, int n, int stride, float cell, v
     g.n = n;
     int rc;
     if (!h->mm) NBR_TRY(h, cudaMalloc((void**)&h->mm, 2 * GPRM_MAX_DOF * sizeof(float)));
-    if (!h->nredo) NBR_TRY(h, cudaMalloc((void**)&h->nredo, sizeof(int)));
+    if (!h->nredo) NBR_TRY(h, cudaMalloc((void**)&h->nredo, 2 * sizeof(int)));
     std::vector<float> mm(2 * nd);
     for (int j = 0; j < nd; ++j) { mm[2 * j] = INFINITY; mm[2 * j + 1] = -INFINITY; }
     NBR_TRY(h, cudaMemcpyAsync(h->mm, mm.data(), 2 * nd * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -703,7 +779,8 @@ int gprm_nbr_knn(gprm_nbr* h, const float* q, int m, int qstride, int k, int que
     cudaStream_t st = (cudaStream_t)stream;
     int rc = grow(h, &h->redo, h->cap_redo, (size_t)m);
     if (rc) return rc;
-    NBR_TRY(h, cudaMemsetAsync(h->nredo, 0, sizeof(int), st));
+    if ((rc = grow(h, &h->redo2, h->cap_redo2, (size_t)m))) return rc;
+    NBR_TRY(h, cudaMemsetAsync(h->nredo, 0, 2 * sizeof(int), st));
     if (queries_are_nodes) {
         const int threads = 128;
         const int blocks = (int)((m + threads - 1) / threads);
@@ -715,8 +792,11 @@ int gprm_nbr_knn(gprm_nbr* h, const float* q, int m, int qstride, int k, int que
         k_knn_grid_warp<<<blocks, 32 * wpb, 0, st>>>(h->g, q, m, qstride, k, idx, dist, h->redo, h->nredo);
     }
     NBR_TRY(h, cudaGetLastError());
+    k_knn_wide<<<h->sms * 8, 256, 0, st>>>(h->g, q, qstride, k, queries_are_nodes ? 1 : 0, h->redo, h->nredo,
+                                           h->redo2, h->nredo + 1, idx, dist);
+    NBR_TRY(h, cudaGetLastError());
     k_knn_full<<<h->sms * 8, 256, 0, st>>>(h->x, h->n, h->xstride, q, qstride, h->ndof, k, queries_are_nodes ? 1 : 0,
-                                           h->redo, h->nredo, idx, dist);
+                                           h->redo2, h->nredo + 1, idx, dist);
     NBR_TRY(h, cudaGetLastError());
     return GPRM_OK;
 }
