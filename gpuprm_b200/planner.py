@@ -331,9 +331,10 @@ def _cheapest_per_component(rest, la, lb, m):
 def _lazy_rounds(V, i64, j64, cost, check, components, max_rounds, first, growth, ph, length=None):
     """The rounds of `lazy_prm` over the candidate edges (i64[e], j64[e]):
     check(sel) gives the exact verdicts (True = free) of the edge ids sel,
-    components(good) the component labels of the free-edge graph.  Returns
-    (good uint8, checked bool, final labels, edges per round, free edges of
-    round 1)."""
+    components(good) the component labels of the free-edge graph; with
+    `length`, each round's batch is checked longest edge first; ph: the
+    phase timer.  Returns (good uint8, checked bool, final labels, edges per
+    round, free edges of round 1)."""
     import torch
     dev = i64.device
     E = int(i64.numel())
