@@ -112,3 +112,41 @@ def test_lazy_attachment_picks_the_pairs_of_full_checking(seed, monkeypatch):
         assert n <= 2 * Q * kk
         if rounds:
             assert n < 2 * Q * kk
+
+
+def test_lazy_rounds_without_edges():
+    i = torch.zeros(0, dtype=torch.int64)
+    good, checked, label, per_round, free1 = planner._lazy_rounds(
+        5, i, i, torch.zeros(0), lambda sel: torch.zeros(0, dtype=torch.bool),
+        lambda g: torch.arange(5, dtype=torch.int32), 4, 1, 2, planner._Phases(False))
+    assert good.numel() == 0 and checked.numel() == 0 and per_round == [] and free1 == 0
+    np.testing.assert_array_equal(label.numpy(), np.arange(5))
+
+
+def test_cheapest_per_component_takes_whole_small_groups():
+    rest = torch.tensor([7, 3, 9])
+    la = torch.tensor([0, 0, 1], dtype=torch.int32)
+    lb = torch.tensor([1, 2, 2], dtype=torch.int32)
+    assert planner._cheapest_per_component(rest, la, lb, 10).tolist() == [3, 7, 9]
+    # m = 1: component 0 -> 7, component 1 -> 7, component 2 -> 3
+    assert planner._cheapest_per_component(rest, la, lb, 1).tolist() == [3, 7]
+
+
+def test_lazy_attachment_skips_missing_neighbours(monkeypatch):
+    """Neighbour slots marked -1 (fewer nodes than k) never count as free."""
+    rng = np.random.default_rng(11)
+    d, V, Q, kk = 2, 40, 30, 5
+    verts = torch.tensor(rng.random((V, d)), dtype=torch.float32)
+    ends = torch.tensor(rng.random((2 * Q, d)), dtype=torch.float32)
+    label = torch.tensor(rng.integers(0, 3, V), dtype=torch.int32)
+    nb = torch.tensor(np.stack([rng.choice(V, kk, replace=False) for _ in range(2 * Q)]))
+    nb[:, -1] = -1
+    w = torch.tensor(rng.normal(size=(2, d)), dtype=torch.float32)
+    monkeypatch.setattr(planner, "_check_edges", _fake_checker(w))
+    qa = ends[:, None, :].expand(-1, kk, -1).reshape(-1, d)
+    ok_all = (planner._check_edges(None, qa, verts[nb.clamp_min(0).reshape(-1)]) == 0).reshape(2 * Q, kk)
+    ok_all &= nb >= 0
+    ok, n = planner._attach_lazy(None, ends, verts, nb, label, Q, kk)
+    assert not bool(ok[:, -1].any())
+    torch.testing.assert_close(_first_pairs(ok, label, nb.clamp_min(0), Q, kk),
+                               _first_pairs(ok_all, label, nb.clamp_min(0), Q, kk))
