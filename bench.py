@@ -472,16 +472,19 @@ def stress_edges_leg(args, dev, policy):
     return out
 
 
-MLP_FLOPS_PER_ROW = 2 * (16 * 256 + 3 * 256 * 256 + 256)
+# the network's own work for 6 joints: 12 inputs (sin, cos), three 256x256
+# layers and the output; the first layer's operand is padded to 16 inputs
+# for the MMA K step, and the padding is not counted
+MLP_FLOPS_PER_ROW = 2 * (12 * 256 + 3 * 256 * 256 + 256)
 
 
 def mlp_leg(args, dev):
     """Inference of the collision predictor (6 joints, 16 -> 256 x4 -> 1,
     BF16 operands, FP32 accumulation) on 2^22 uniform configurations: the
     fused tcgen05 kernel (the library default), one tcgen05 kernel per
-    layer, and the training GEMMs.  FLOPs per row = 2 (16*256 + 3*256^2 +
-    256); roofline against the measured dense BF16 peak (burst figure: one
-    kernel timed alone)."""
+    layer, and the training GEMMs.  FLOPs per row = 2 (12*256 + 3*256^2 +
+    256) (the 12 real inputs); roofline against the measured dense BF16
+    peak (burst figure: one kernel timed alone)."""
     import torch
     from gpuprm_b200.mlp import CollisionMLP
     n = args.mlp_rows
