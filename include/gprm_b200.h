@@ -251,7 +251,10 @@ int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offse
  * (about 0.5 MB, held by every GPU that loads the library until the process
  * exits).  Larger n is rejected with GPRM_ERR_ARG.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array:
+ * that first call before any stream capture.  The address is kept for the
+ * life of the process: do not use this entry point after cudaDeviceReset
+ * (or any other teardown of the device's primary context), which may move
+ * the array.  All calls share the array:
  * calls that overlap on the GPU (other streams, other handles, other host
  * threads) race and must be serialised by the caller.  q and res are
  * device pointers as in gprm_indicator_batch_device; `stream` NULL is the

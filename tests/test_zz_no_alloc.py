@@ -40,6 +40,8 @@ def test_noalloc_matches_allocating_entry_point(name):
     want = torch.zeros(n, dtype=torch.int32, device="cuda:0")
     assert lib.gprm_indicator_batch_device(h, C.c_void_p(q.data_ptr()), C.c_void_p(want.data_ptr()), n, n,
                                            C.c_void_p(stream)) == 0
+    torch.cuda.synchronize()
+    rechecks = cs.stats()["band_rechecks"]   # after the allocating call
     for _ in range(2):   # two calls in a row share the same scratch array
         got = torch.full((n,), 99, dtype=torch.int32, device="cuda:0")
         rc = lib.gprm_indicator_batch_device_noalloc(h, C.c_void_p(q.data_ptr()), C.c_void_p(got.data_ptr()),
@@ -47,7 +49,10 @@ def test_noalloc_matches_allocating_entry_point(name):
         assert rc == 0, lib.gprm_last_error(h)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(got.cpu().numpy(), want.cpu().numpy())
-    assert cs.stats()["band_rechecks"] > 0
+        # this call ran its own FP64 recheck through the queue in the shared array
+        now = cs.stats()["band_rechecks"]
+        assert now > rechecks
+        rechecks = now
 
 
 def test_noalloc_rejects_oversized_batches():
