@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--policy", default="early", choices=["early", "all"])
+    ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
+                    help="FP32 arithmetic of the checks: fast (GPRM_MODE_FAST) or the reference's exact operations")
     ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
     ap.add_argument("--prm-samples", type=int, default=1 << 20)
     ap.add_argument("--no-stress", action="store_true", help="skip the 7-DOF wall planner comparison")
@@ -153,10 +155,12 @@ class ClockSampler:
 
 def cpu_reference_rate(scene, qs_np, qe_np, dq, seconds, seed=0, count_ops=True):
     """Times the reference CPU checker on a bounded sample of the edges with
-    all host cores.  Returns (dict for cpu_baseline, work counts): the
-    reference algorithm's FP32 operations per step and per pair test,
-    counted by the oracle's instrumented restatement on 256 of the edges
-    (None without count_ops)."""
+    all host cores.  Returns (dict for cpu_baseline, work counts, sample):
+    the work counts are the reference algorithm's FP32 operations per step
+    and per pair test, counted by the oracle's instrumented restatement on
+    256 of the edges (None without count_ops); the sample holds the edge
+    indices timed and the reference's codes for them (kept for the verdict
+    parity check)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     cores = os.cpu_count() or 1
@@ -190,16 +194,41 @@ def cpu_reference_rate(scene, qs_np, qe_np, dq, seconds, seed=0, count_ops=True)
     a, b = qs_np[idx], qe_np[idx]
     steps = int(orc.testnum(a, b, dq).sum())
     t0 = time.perf_counter()
-    run(a, b)
+    ref_res = run(a, b)
     dt = time.perf_counter() - t0
     return ({"value": steps / dt, "unit": UNIT, "cores": cores, "kind": kind,
              "sample": f"{n} random edges of the workload ({steps} edge steps), indicator2 in chunks "
-                       f"of <=4096 edges per thread, {dt:.1f} s"}, work)
+                       f"of <=4096 edges per thread, {dt:.1f} s"}, work,
+            {"idx": idx, "ref_res": np.asarray(ref_res), "kind": kind, "steps": steps})
+
+
+def edge_parity(scene, qs_np, qe_np, dq, band, sample, gpu_res, what):
+    """Verdict parity of the GPU's edge results with the reference CPU
+    checker's on the timed CPU sample: the oracle classifies every sampled
+    edge as decided outside the band (free / not free) or inside it (with
+    its FP32 + FP64-band result), all host threads; see oracle/parity.py."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import parity as P
+    idx = sample["idx"]
+    t0 = time.perf_counter()
+    cls, band_res, nin = O.Oracle(scene).edge_classify(qs_np[idx], qe_np[idx], dq, O.DEVICE_TRIG, band,
+                                                       threads=os.cpu_count() or 1)
+    d = P.verdict_parity(gpu_res[idx], sample["ref_res"], cls, band_res, nin)
+    d.update({"what": what, "reference": sample["kind"], "edge_steps": int(sample["steps"]), "band_m": band,
+              "oracle_seconds": time.perf_counter() - t0, "ok": P.parity_ok(d)})
+    return d
 
 
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
+
+def check_mode(args) -> int:
+    """FP32 with the FP64 band recheck, in the requested arithmetic."""
+    from gpuprm_b200._abi import GPRM_MODE_FAST, GPRM_MODE_FP64_BAND
+    return GPRM_MODE_FP64_BAND | (GPRM_MODE_FAST if args.arith == "fast" else 0)
+
 
 def replica_seed(seed: int, rank: int) -> int:
     """Each rank checks its own replica of the workload (independent seeded
@@ -229,7 +258,7 @@ def reduce_over_ranks(values_max, values_sum, device=None):
 def run_ours(args, rank, world, local_rank):
     import torch
     from gpuprm_b200 import workloads
-    from gpuprm_b200._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT, GPRM_MODE_FP64_BAND
+    from gpuprm_b200._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT
     from gpuprm_b200.configspace import measure_fp32_peak
 
     dev = torch.device("cuda", local_rank)
@@ -237,7 +266,7 @@ def run_ours(args, rank, world, local_rank):
     ws = workloads.edge_workload("hull6", seed=replica_seed(args.seed, rank), n_samples=args.samples, k=args.k,
                                  dq=WORKLOAD["dq"], device=str(dev))
     cs = ws["space"]
-    cs.set_mode(GPRM_MODE_FP64_BAND)
+    cs.set_mode(check_mode(args))
     policy = GPRM_EDGES_EARLY_EXIT if args.policy == "early" else GPRM_EDGES_ALL_STEPS
     cs.set_edge_policy(policy)
     qs, qe = ws["qs"], ws["qe"]
@@ -302,10 +331,14 @@ def run_ours(args, rank, world, local_rank):
     peak = measure_fp32_peak()
     cpu = None
     work = None
+    parity = None
     if not args.no_cpu_baseline and world == 1:
         qs_r = np.ascontiguousarray(qs_np.T)
         qe_r = np.ascontiguousarray(qe_np.T)
-        cpu, work = cpu_reference_rate(ws["scene"], qs_r, qe_r, WORKLOAD["dq"], args.cpu_seconds, args.seed)
+        cpu, work, sample = cpu_reference_rate(ws["scene"], qs_r, qe_r, WORKLOAD["dq"], args.cpu_seconds,
+                                               args.seed)
+        parity = edge_parity(ws["scene"], qs_r, qe_r, WORKLOAD["dq"], WORKLOAD["band_m"], sample, res_np,
+                             "headline edges (FP64 band mode, early exit) vs the reference CPU checker")
     k_ms = prof["fp32_ms"] / max(1, prof["fp32_launches"])
     per = lambda key: (s1[key] - s0[key]) / max(1, args.steps)
     full_pl, cert_pl, exec_pl = per("pairs_tested"), per("pairs_certified"), executed / max(1, args.steps)
@@ -358,14 +391,14 @@ def run_ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (+f64 band)",
         "data": "synthetic (seeded)",
-        "config": dict(WORKLOAD, edges_per_gpu=E, free_samples=ws["n_free"], policy=args.policy,
+        "config": dict(WORKLOAD, edges_per_gpu=E, free_samples=ws["n_free"], policy=args.policy, arith=args.arith,
                        l2="inputs (qs,qe: %.0f MB) larger than L2" % (2 * qs.numel() * 4 / 1e6)),
         "executed_steps_per_s": executed_all / t_max,
         "nominal_steps_per_step": nominal // args.steps, "executed_steps_per_step": executed // args.steps,
         "colliding_edges": colliding, "band_rechecks_per_step": band / args.steps,
         "e2e": {"value": nominal_all / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(2 * qs.numel() * 4),
                 "d2h_bytes_per_step": int(E * 4)},
-        "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+        "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "gpu_launches": launches,
         "prm": prm, "prm_stress": prm_stress, "stress_edges": stress_edges, "batch": batch, "sampler": sampler,
         "mlp": mlp,
     }
@@ -377,12 +410,11 @@ def prm_leg(args, kind, dq, n_samples, k):
     on 2^20 exact-checker labels (10 epochs, batch 4096, lr 1e-3) by the
     library's BF16 kernels, then the planners answer 1000 seeded queries."""
     from gpuprm_b200 import planner, scenes as _sc
-    from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
     from gpuprm_b200.configspace import RobotConfigspace as _RC
     psc = _sc.make_scene(kind, args.seed)
     pcs = _RC(psc, dq=dq)
     pcs.init()
-    pcs.set_mode(GPRM_MODE_FP64_BAND)
+    pcs.set_mode(check_mode(args))
     mlp, losses, t_lab, t_train = planner.train_predictor(pcs, psc, n_labels=1 << 20, epochs=10, batch=4096,
                                                           lr=1e-3, seed=args.seed)
     out = planner.compare_planners(pcs, psc, n_samples=n_samples, n_queries=1000, k=k, seed=args.seed, mlp=mlp,
@@ -407,12 +439,11 @@ def stress_edges_leg(args, dev, policy):
     reference CPU checker on a bounded sample of the same edges."""
     import torch
     from gpuprm_b200 import scenes, workloads
-    from gpuprm_b200._abi import GPRM_MODE_FP64_BAND
     from gpuprm_b200.configspace import RobotConfigspace
     sc = scenes.make_scene("wall7", args.seed)
     cs = RobotConfigspace(sc, dq=STRESS["dq"])
     cs.init()
-    cs.set_mode(GPRM_MODE_FP64_BAND)
+    cs.set_mode(check_mode(args))
     cs.set_edge_policy(policy)
     n = STRESS["samples"]
     q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, n, args.seed + 1000).T), device=dev)
@@ -465,10 +496,13 @@ def stress_edges_leg(args, dev, policy):
                   "band_rechecks": int(s1["band_rechecks"] - s0["band_rechecks"])},
     }
     if not args.no_cpu_baseline:
-        cpu, _ = cpu_reference_rate(sc, np.ascontiguousarray(qs.T.cpu().numpy()),
-                                    np.ascontiguousarray(qe.T.cpu().numpy()), STRESS["dq"],
-                                    args.cpu_seconds, args.seed, count_ops=False)
+        qs_r = np.ascontiguousarray(qs.T.cpu().numpy())
+        qe_r = np.ascontiguousarray(qe.T.cpu().numpy())
+        cpu, _, sample = cpu_reference_rate(sc, qs_r, qe_r, STRESS["dq"], args.cpu_seconds, args.seed,
+                                            count_ops=False)
         out["cpu_baseline"] = cpu
+        out["parity"] = edge_parity(sc, qs_r, qe_r, STRESS["dq"], STRESS["band_m"], sample, res.cpu().numpy(),
+                                    "7-DOF wall edges (512 obstacles, FP64 band mode) vs the reference CPU checker")
     return out
 
 
@@ -592,6 +626,7 @@ def batch_leg(args, dev, policy):
     spaces = ws["spaces"]
     for cs in spaces:
         cs.set_edge_policy(policy)
+        cs.set_mode(check_mode(args))
     B = ProblemBatch(spaces)
     Q, A, Bq = ws["q"], ws["qs"], ws["qe"]
     nv, ne = Q.shape[1], A.shape[1]
@@ -743,6 +778,11 @@ def main():
         torch.distributed.destroy_process_group()
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
+        bad = [p["what"] for p in (line.get("parity"), (line.get("stress_edges") or {}).get("parity"))
+               if p is not None and not p["ok"]]
+        if bad:
+            sys.stderr.write("verdict parity with the reference failed: %s\n" % "; ".join(bad))
+            sys.exit(3)
 
 
 if __name__ == "__main__":

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(PKG_DIR, "libgprm_b200.so")
 GPRM_OK = 0
 GPRM_MODE_FP32 = 0
 GPRM_MODE_FP64_BAND = 1
+GPRM_MODE_FAST = 2
 GPRM_EDGES_EARLY_EXIT = 0
 GPRM_EDGES_ALL_STEPS = 1
 GPRM_MLP_INFER_TCGEN05 = 0
@@ -143,7 +144,9 @@ SIGNATURES = [
                                  C.c_float, _F]),
     ("gprm_debug_fk", C.c_int, [_P, _F, _F]),
     ("gprm_device_sm_count", C.c_int, [_P]),
+    ("gprm_debug_support_candidates", C.c_int, [_P, C.c_int, C.c_int, _I, C.c_int]),
     ("gprm_set_launch", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    ("gprm_set_launch_shape", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("gprm_get_launch", C.c_int, [_P, C.c_int, _I, _I, _I]),
     ("gprm_profile_enable", C.c_int, [_P, C.c_int]),
     ("gprm_profile_read", C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]),

@@ -40,18 +40,40 @@ def needs_build() -> bool:
 
 def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False, out: str = OUT,
           defines=()) -> str:
+    """Compiles every source to an object in parallel (one nvcc per file,
+    objects under a build folder beside `out`), then links the shared
+    library."""
     if not force and out == OUT and not needs_build():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + [f"-D{d}" for d in defines] + [
-        "-o", out] + [os.path.join(CSRC, f) for f in SOURCES]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(os.path.dirname(os.path.abspath(out)), "_build",
+                          os.path.splitext(os.path.basename(out))[0])
+    os.makedirs(objdir, exist_ok=True)
+    flags = NVCC_FLAGS[:]
+    flags.remove("-shared")
+    extra = (["-Xptxas", "-v"] if ptxas_info else []) + [f"-D{d}" for d in defines]
+
+    def compile_one(f):
+        obj = os.path.join(objdir, f.replace(".cu", ".o"))
+        cmd = [nvcc()] + flags + extra + ["-c", "-o", obj, os.path.join(CSRC, f)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for obj, r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc failed compiling " + os.path.basename(obj))
+        if verbose or ptxas_info:
+            sys.stderr.write(r.stderr)
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC", "-ccbin",
+            "/usr/bin/g++", "-o", out] + [o for o, _ in results]
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libgprm_b200.so")
-    if verbose or ptxas_info:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libgprm_b200.so")
     return out
 
 

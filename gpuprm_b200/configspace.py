@@ -182,8 +182,12 @@ class RobotConfigspace:
             self.h, C.c_void_p(qs_soa.data_ptr()), C.c_void_p(qe_soa.data_ptr()), C.c_void_p(res.data_ptr()),
             n, n, C.c_void_p(st)))
 
-    def set_launch(self, vertex_kernel: bool, threads: int, scene_in_smem: bool) -> None:
-        _check(self.lib, self.h, self.lib.gprm_set_launch(self.h, int(vertex_kernel), threads, int(scene_in_smem)))
+    def set_launch(self, vertex_kernel: bool, threads: int, scene_in_smem: bool, blocks_per_sm: int = 0) -> None:
+        """Launch shape of the FP32 kernels: threads per block, scene table in
+        shared memory or through L1, and at most blocks_per_sm resident
+        blocks per SM (0: as many as fit; fewer leave more L1)."""
+        _check(self.lib, self.h, self.lib.gprm_set_launch_shape(self.h, int(vertex_kernel), threads,
+                                                                int(scene_in_smem), int(blocks_per_sm)))
 
     def get_launch(self, vertex_kernel: bool) -> dict:
         t, s, w = C.c_int(0), C.c_int(0), C.c_int(0)

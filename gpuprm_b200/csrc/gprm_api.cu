@@ -110,6 +110,71 @@ void jacobi3(double A[3][3], double V[3][3])
     }
 }
 
+/* Clips the convex polygon `poly` (points (u, v)) by a*u + b*v + c >= 0. */
+void clip_halfplane(std::vector<double>& poly, double a, double b, double c)
+{
+    std::vector<double> out;
+    const size_t n = poly.size() / 2;
+    for (size_t i = 0; i < n; ++i) {
+        const double pu = poly[2 * i], pv = poly[2 * i + 1];
+        const double qu = poly[2 * ((i + 1) % n)], qv = poly[2 * ((i + 1) % n) + 1];
+        const double fp = a * pu + b * pv + c, fq = a * qu + b * qv + c;
+        if (fp >= 0) { out.push_back(pu); out.push_back(pv); }
+        if ((fp >= 0) != (fq >= 0)) {
+            const double t = fp / (fp - fq);
+            out.push_back(pu + t * (qu - pu));
+            out.push_back(pv + t * (qv - pv));
+        }
+    }
+    poly.swap(out);
+}
+
+/* Support candidates of every polytope for every direction bin of dir_bin:
+ * vertex i is a candidate of a bin when some direction d of the bin has
+ * <d, x_i - x_j> >= 0 for every CRS neighbour j of i (its normal cone,
+ * enlarged when the adjacency misses an edge, so the set can only grow).
+ * A bin's directions are d = s e_a + u e_b + v e_c on its cube face, with
+ * (u, v) in the bin's cell of [-1, 1]^2 widened by 1e-3 on every side to
+ * cover the float evaluation of dir_bin near cell and face borders.  Lists
+ * hold ascending vertex indices; an empty list (rounding) falls back to
+ * every vertex. */
+void compute_support_candidates(gprm_space* h, const gprm_scene_desc* d, const std::vector<int>& voff,
+                                const std::vector<int>& moff)
+{
+    h->cbin.assign((size_t)GPRM_START_BINS * h->npoly, 0u);
+    h->cidx.clear();
+    const double eps = 1e-3, lo[3] = {-1.0 - eps, -1.0 / 3.0 - eps, 1.0 / 3.0 - eps},
+                 hi[3] = {-1.0 / 3.0 + eps, 1.0 / 3.0 + eps, 1.0 + eps};
+    std::vector<double> poly;
+    std::vector<unsigned char> list;
+    for (int k = 0; k < h->npoly; ++k) {
+        const int n = d->poly_n[k];
+        for (int b = 0; b < GPRM_START_BINS; ++b) {
+            const int face = b / 9, iu = (b % 9) / 3, iv = b % 3;
+            const double s = (face & 1) ? -1.0 : 1.0;
+            const int ax = face / 2, bu = (ax + 1) % 3, bv = (ax + 2) % 3;   /* x:(y,z) y:(z,x) z:(x,y) */
+            list.clear();
+            for (int i = 0; i < n; ++i) {
+                poly = {lo[iu], lo[iv], hi[iu], lo[iv], hi[iu], hi[iv], lo[iu], hi[iv]};
+                const float* xi = d->vertices + 3 * (size_t)(voff[k] + i);
+                const int g = voff[k] + i;
+                for (int e = 0; e < d->cnt[g] && !poly.empty(); ++e) {
+                    const int j = d->dest[moff[k] + d->dsp[g] + e];
+                    const float* xj = d->vertices + 3 * (size_t)(voff[k] + j);
+                    const double D[3] = {(double)xi[0] - xj[0], (double)xi[1] - xj[1], (double)xi[2] - xj[2]};
+                    const double norm = sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
+                    clip_halfplane(poly, D[bu], D[bv], s * D[ax] + 1e-9 * norm);
+                }
+                if (poly.size() >= 2) list.push_back((unsigned char)i);
+            }
+            if (list.empty())
+                for (int i = 0; i < n; ++i) list.push_back((unsigned char)i);
+            h->cbin[(size_t)GPRM_START_BINS * k + b] = ((unsigned)h->cidx.size() << 8) | (unsigned)list.size();
+            h->cidx.insert(h->cidx.end(), list.begin(), list.end());
+        }
+    }
+}
+
 void compute_certificates(gprm_space* h, const int* from, const int* to)
 {
     const double eps_pos = 1e-6 * h->extent;
@@ -119,7 +184,8 @@ void compute_certificates(gprm_space* h, const int* from, const int* to)
     (void)to;
     h->pairs_b.resize(h->npairs);
     h->far.resize(h->npairs);
-    h->far_slot.resize(h->npairs);
+    h->scan_c.resize(h->npairs);
+    h->scan_b.resize(h->npairs);
     for (int j = 0; j < h->npairs; ++j) {
         int a = h->pair_poly[2 * j], b = h->pair_poly[2 * j + 1];
         bool ok = (h->pair_sys[2 * j] == 0 || h->slot[a] >= 0) && (h->pair_sys[2 * j + 1] == 0 || h->slot[b] >= 0);
@@ -134,21 +200,32 @@ void compute_certificates(gprm_space* h, const int* from, const int* to)
         memcpy(&fa, &sa, 4);
         memcpy(&fb, &sb, 4);
         h->pairs_b[j] = make_float4(Rf, T2, fa, fb);
-        /* distance-test record: the moving ball's slot first, the static
-         * partner's ball centre inline; no slot -> never certified here */
+        /* certificate-scan records: the static partner's ball centre and
+         * vertex 0 inline (a polytope in frame 0 is used untransformed), the
+         * slots of the moving ones, T2 and sqrt(T2) rounded up (for the
+         * sweep test), R.  A pair without a slot for each moving polytope,
+         * or with two static polytopes, is not usable by the scan (its
+         * certificates go through pair_certified). */
         float4 fr = make_float4(0.0f, 0.0f, 0.0f, INFINITY);
-        int2 fs = make_int2(-1, -1);
+        float4 sbv = make_float4(0.0f, 0.0f, 0.0f, Rf);
+        int usable = 0;
         if (T2 < INFINITY && (sa >= 0 || sb >= 0)) {
-            fs = sa >= 0 ? make_int2(sa, sb) : make_int2(sb, -1);
+            usable = 1;
             if (sa < 0 || sb < 0) {
-                const float4 c = h->tab[sa < 0 ? h->pairs[j].x : h->pairs[j].y];
+                const int blk = sa < 0 ? h->pairs[j].x : h->pairs[j].y;
+                const float4 c = h->tab[blk], v = h->tab[blk + 1];
                 fr = make_float4(c.x, c.y, c.z, T2);
+                sbv = make_float4(v.x, v.y, v.z, Rf);
             } else {
                 fr.w = T2;
             }
         }
+        float sq = nextafterf((float)sqrt((double)T2), INFINITY);
+        int sqb;
+        memcpy(&sqb, &sq, 4);
         h->far[j] = fr;
-        h->far_slot[j] = fs;
+        h->scan_c[j] = make_int4(sa, sb, sqb, usable);
+        h->scan_b[j] = sbv;
     }
     h->thr_dir = (float)thr;
     h->eps_dir = (float)(7.0 * eps_pos);
@@ -265,6 +342,8 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
             h->tab[boff[k] + 2 + j] = entry(v);
         }
         h->tab[boff[k] + 1] = entry(0);
+        h->vinfo.push_back(make_int2((int)h->vtab.size(), n));
+        for (int i = 0; i < n; ++i) h->vtab.push_back(entry(i));
         /* bounding ball: centre of the bounding box, radius to the farthest
            vertex (inflated in compute_certificates) */
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -316,6 +395,44 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
             }
         }
     }
+    /* start tables of the fast path: for the centre direction of each
+       direction bin, the support vertex (the first of the maximisers in
+       double) and a table entry that carries it (entry 1 for vertex 0, else
+       the first CRS entry naming it; entry 1 when none does or the offset
+       does not fit 16 bits).  Any entry is a correct start: the climb
+       reaches a maximiser from every vertex. */
+    h->start.assign((size_t)GPRM_START_BINS * h->npoly, 1);
+    for (int k = 0; k < h->npoly; ++k) {
+        const int n = d->poly_n[k], m = d->poly_m[k];
+        for (int b = 0; b < GPRM_START_BINS; ++b) {
+            const int face = b / 9, iu = (b % 9) / 3, iv = b % 3;
+            const double sgn = (face & 1) ? -1.0 : 1.0, u = (iu - 1) * (2.0 / 3.0), v = (iv - 1) * (2.0 / 3.0);
+            double dir[3];
+            if (face < 2) { dir[0] = sgn; dir[1] = u; dir[2] = v; }
+            else if (face < 4) { dir[1] = sgn; dir[2] = u; dir[0] = v; }
+            else { dir[2] = sgn; dir[0] = u; dir[1] = v; }
+            int best = 0;
+            double bd = -1e300;
+            for (int i = 0; i < n; ++i) {
+                const float* x = d->vertices + 3 * (size_t)(voff[k] + i);
+                const double dd = x[0] * dir[0] + x[1] * dir[1] + x[2] * dir[2];
+                if (dd > bd) { bd = dd; best = i; }
+            }
+            int off = 1;
+            if (best != 0)
+                for (int j = 0; j < m; ++j)
+                    if (d->dest[moff[k] + j] == best) {
+                        if (2 + j <= 65535) off = 2 + j;
+                        break;
+                    }
+            h->start[(size_t)GPRM_START_BINS * k + b] = (unsigned short)off;
+        }
+    }
+    if ((size_t)sn * GPRM_START_BINS >= (1u << 24)) {
+        delete h;
+        return fail(nullptr, GPRM_ERR_SCENE, "scene too large for the support candidate lists");
+    }
+    compute_support_candidates(h, d, voff, moff);
     /* slots: moving polytopes in frame order */
     for (int f = 1; f <= h->ndof; ++f)
         for (int k = 0; k < h->npoly; ++k)
@@ -455,7 +572,7 @@ int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b,
 int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
                  long long offset, cudaStream_t st, Control* ctl, unsigned* key)
 {
-    const int band_on = h->mode == GPRM_MODE_FP64_BAND;
+    const int band_on = (h->mode & GPRM_MODE_FP64_BAND) != 0;
     CUDA_TRY(h, cudaMemsetAsync(ctl, 0, sizeof(Control), st));
     int recheck_blocks = h->sms * 4;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
@@ -668,20 +785,31 @@ int gprm_init(gprm_space* h, int rank, int size)
     CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
 
-    /* d_scene: tab | pairs | pairs_b | far | far_slot | ppoly | box */
+    /* d_scene: tab | pairs | pairs_b | far | scan_c | scan_b | ppoly | box | start | vtab | vinfo | cbin | cidx */
     size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
     size_t fsb = (size_t)h->npairs * sizeof(int2);
-    size_t bxo = tb + 3 * pb + 2 * fsb, bxb = h->box.size() * sizeof(float4);
+    size_t bxo = tb + 5 * pb + fsb, bxb = h->box.size() * sizeof(float4);
     bxo = (bxo + 15) & ~(size_t)15;
-    CUDA_TRY(h, cudaMalloc(&h->d_scene, bxo + bxb + 64));
+    const size_t sto = bxo + bxb, stb = h->start.size() * sizeof(unsigned short);
+    const size_t vto = (sto + stb + 15) & ~(size_t)15, vtb = h->vtab.size() * sizeof(float4);
+    const size_t vio = vto + vtb, vib = h->vinfo.size() * sizeof(int2);
+    const size_t cbo = (vio + vib + 15) & ~(size_t)15, cbb = h->cbin.size() * sizeof(unsigned);
+    const size_t cio = cbo + cbb, cib = h->cidx.size();
+    CUDA_TRY(h, cudaMalloc(&h->d_scene, cio + cib + 64));
     char* base = (char*)h->d_scene;
     CUDA_TRY(h, cudaMemcpy(base, h->tab.data(), tb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 2 * pb, h->far.data(), pb, cudaMemcpyHostToDevice));
-    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 3 * pb, h->far_slot.data(), fsb, cudaMemcpyHostToDevice));
-    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 3 * pb + fsb, h->pair_poly.data(), fsb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 3 * pb, h->scan_c.data(), pb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 4 * pb, h->scan_b.data(), pb, cudaMemcpyHostToDevice));
+    if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 5 * pb, h->pair_poly.data(), fsb, cudaMemcpyHostToDevice));
     if (bxb) CUDA_TRY(h, cudaMemcpy(base + bxo, h->box.data(), bxb, cudaMemcpyHostToDevice));
+    if (stb) CUDA_TRY(h, cudaMemcpy(base + sto, h->start.data(), stb, cudaMemcpyHostToDevice));
+    if (vtb) CUDA_TRY(h, cudaMemcpy(base + vto, h->vtab.data(), vtb, cudaMemcpyHostToDevice));
+    if (vib) CUDA_TRY(h, cudaMemcpy(base + vio, h->vinfo.data(), vib, cudaMemcpyHostToDevice));
+    if (cbb) CUDA_TRY(h, cudaMemcpy(base + cbo, h->cbin.data(), cbb, cudaMemcpyHostToDevice));
+    if (cib) CUDA_TRY(h, cudaMemcpy(base + cio, h->cidx.data(), cib, cudaMemcpyHostToDevice));
 
     DevScene& s = h->dsc;
     memset(&s, 0, sizeof(s));
@@ -702,9 +830,16 @@ int gprm_init(gprm_space* h, int rank, int size)
     s.pairs = (const int4*)(base + tb);
     s.pairs_b = (const float4*)(base + tb + pb);
     s.far = (const float4*)(base + tb + 2 * pb);
-    s.far_slot = (const int2*)(base + tb + 3 * pb);
-    s.ppoly = (const int2*)(base + tb + 3 * pb + fsb);
+    s.scan_c = (const int4*)(base + tb + 3 * pb);
+    s.scan_b = (const float4*)(base + tb + 4 * pb);
+    s.ppoly = (const int2*)(base + tb + 5 * pb);
     s.box = bxb ? (const float4*)(base + bxo) : nullptr;
+    s.start = stb ? (const unsigned short*)(base + sto) : nullptr;
+    s.vtab = (const float4*)(base + vto);
+    s.vinfo = (const int2*)(base + vio);
+    s.cbin = cbb ? (const unsigned*)(base + cbo) : nullptr;
+    s.cidx = (const unsigned char*)(base + cio);
+    s.fast = (h->mode & GPRM_MODE_FAST) != 0;
     s.thr_dir = h->thr_dir;
     s.eps_dir = h->eps_dir;
     s.nslots = (int)h->slot_sys.size();
@@ -745,8 +880,9 @@ const char* gprm_last_error(const gprm_space* h)
 int gprm_set_mode(gprm_space* h, int mode)
 {
     if (!h) return GPRM_ERR_ARG;
-    if (mode != GPRM_MODE_FP32 && mode != GPRM_MODE_FP64_BAND) return fail(h, GPRM_ERR_ARG, "unknown mode %d", mode);
+    if (mode & ~(GPRM_MODE_FP64_BAND | GPRM_MODE_FAST)) return fail(h, GPRM_ERR_ARG, "unknown mode %d", mode);
     h->mode = mode;
+    h->dsc.fast = (mode & GPRM_MODE_FAST) != 0;
     return GPRM_OK;
 }
 
@@ -782,6 +918,8 @@ int gprm_set_band(gprm_space* h, float band_m)
         size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
         if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + pb, h->pairs_b.data(), pb, cudaMemcpyHostToDevice));
         if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + 2 * pb, h->far.data(), pb, cudaMemcpyHostToDevice));
+        if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + 3 * pb, h->scan_c.data(), pb, cudaMemcpyHostToDevice));
+        if (pb) CUDA_TRY(h, cudaMemcpy((char*)h->d_scene + tb + 4 * pb, h->scan_b.data(), pb, cudaMemcpyHostToDevice));
         h->dsc.thr_dir = h->thr_dir;
         h->dsc.eps_dir = h->eps_dir;
     }
@@ -937,18 +1075,35 @@ int gprm_debug_fk(gprm_space* h, const float* q, float* out)
 
 int gprm_device_sm_count(const gprm_space* h) { return h ? h->sms : 0; }
 
+int gprm_debug_support_candidates(const gprm_space* h, int polytope, int bin, int* idx, int cap)
+{
+    if (!h || polytope < 0 || polytope >= h->npoly || bin < 0 || bin >= GPRM_START_BINS || (cap > 0 && !idx))
+        return GPRM_ERR_ARG;
+    const unsigned hb = h->cbin[(size_t)GPRM_START_BINS * polytope + bin];
+    const int n = (int)(hb & 255u);
+    for (int i = 0; i < n && i < cap; ++i) idx[i] = h->cidx[(hb >> 8) + i];
+    return n;
+}
+
 int gprm_set_launch(gprm_space* h, int vertex_kernel, int threads, int scene_in_smem)
+{
+    return gprm_set_launch_shape(h, vertex_kernel, threads, scene_in_smem, 0);
+}
+
+int gprm_set_launch_shape(gprm_space* h, int vertex_kernel, int threads, int scene_in_smem, int blocks_per_sm)
 {
     int rc = check_ready(h);
     if (rc) return rc;
     if (threads < 32 || threads > 512 || threads % 32) return fail(h, GPRM_ERR_ARG, "threads must be 32..512, a multiple of 32");
+    if (blocks_per_sm < 0 || blocks_per_sm > 64) return fail(h, GPRM_ERR_ARG, "blocks_per_sm must be 0..64");
     LaunchCfg c{};
-    cudaError_t e = configure_launch(h->dsc, vertex_kernel ? 1 : 0, threads, scene_in_smem ? 1 : 0, &c);
+    cudaError_t e = configure_launch(h->dsc, vertex_kernel ? 1 : 0, threads, scene_in_smem ? 1 : 0, &c, blocks_per_sm);
     if (e != cudaSuccess) {
         cudaGetLastError();
         /* restore the attribute of the current shape */
         LaunchCfg& cur = vertex_kernel ? h->cfg_v : h->cfg_e;
-        configure_launch(h->dsc, vertex_kernel ? 1 : 0, cur.threads, cur.scene_in_smem, &cur);
+        configure_launch(h->dsc, vertex_kernel ? 1 : 0, cur.threads, cur.scene_in_smem, &cur,
+                         cur.carveout < 0 ? 0 : cur.blocks_per_sm);
         return fail(h, GPRM_ERR_UNSUPPORTED, "launch shape %d threads / scene_in_smem=%d does not fit: %s",
                     threads, scene_in_smem, cudaGetErrorString(e));
     }
@@ -1086,7 +1241,7 @@ extern "C" int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q
     uint2* queue = (uint2*)(base + NOALLOC_QUEUE_OFFSET);
     const unsigned qcap = (unsigned)GPRM_NOALLOC_MAX_CONFIGS;
     cudaStream_t st = (cudaStream_t)stream;
-    const int band_on = h->mode == GPRM_MODE_FP64_BAND;
+    const int band_on = (h->mode & GPRM_MODE_FP64_BAND) != 0;
     CUDA_TRY(h, cudaMemsetAsync(ctl, 0, sizeof(Control), st));
     CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, q, n, offset, res, band_on, h->band, queue, qcap, ctl, st));
     if (band_on)

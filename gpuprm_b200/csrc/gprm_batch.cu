@@ -66,7 +66,7 @@ struct gprm_batch {
     int mode = GPRM_MODE_FP64_BAND;
     int policy = GPRM_EDGES_EARLY_EXIT;
     float band = 1e-5f;
-    int lane_floats = 0;
+    int lane_floats[2] = {0, 0};    /* [0] edge kernels, [1] vertex kernels */
     DevScene* d_scenes = nullptr;
     Control* ctl = nullptr;          /* per-call control block */
     Control* d_total = nullptr;      /* counters of all calls */
@@ -112,7 +112,8 @@ BatchView view_of(const gprm_batch* b, int vertex_kernel)
     v.chunks = L.d_chunks;
     v.nwork = vertex_kernel ? L.nchunks : L.total;
     v.S = (int)b->spaces.size();
-    v.lane_floats = b->lane_floats;
+    v.lane_floats = b->lane_floats[vertex_kernel ? 1 : 0];
+    v.fast = (b->mode & GPRM_MODE_FAST) != 0;
     return v;
 }
 
@@ -123,7 +124,7 @@ int enqueue_batch(gprm_batch* b, int vertex_kernel, const float* qa, const float
 {
     Layout& L = b->lay[vertex_kernel];
     const BatchView v = view_of(b, vertex_kernel);
-    const int band_on = b->mode == GPRM_MODE_FP64_BAND;
+    const int band_on = (b->mode & GPRM_MODE_FP64_BAND) != 0;
     const int recheck_blocks = b->sms * 4;
     BATCH_TRY(b, cudaMemsetAsync(b->ctl, 0, sizeof(Control), st));
     if (vertex_kernel) {
@@ -148,7 +149,7 @@ int enqueue_batch(gprm_batch* b, int vertex_kernel, const float* qa, const float
 
 int launches_per_call(const gprm_batch* b, int vertex_kernel)
 {
-    const int band_on = b->mode == GPRM_MODE_FP64_BAND;
+    const int band_on = (b->mode & GPRM_MODE_FP64_BAND) != 0;
     return 2 + band_on + (vertex_kernel ? 0 : 1);
 }
 
@@ -191,8 +192,10 @@ int gprm_batch_create(gprm_space* const* spaces, int count, gprm_batch** out)
     std::vector<DevScene> sc(count);
     for (int i = 0; i < count; ++i) {
         sc[i] = spaces[i]->dsc;
-        int lf = (int)lane_floats(sc[i]);
-        if (lf > b->lane_floats) b->lane_floats = lf;
+        for (int k = 0; k < 2; ++k) {
+            const int lf = (int)lane_floats(sc[i], k == 1);
+            if (lf > b->lane_floats[k]) b->lane_floats[k] = lf;
+        }
     }
     auto bad = [&](int rc) {
         g_batch_create_error = b->err;

@@ -59,11 +59,13 @@ struct DevScene {
     const float4* tab;
     const int4* pairs;
     const float4* pairs_b;
-    /* distance test per pair: (static partner's ball centre, T2) and the
-       moving ball slot(s) (x: moving slot, y: second moving slot or -1;
-       x = -1: the pair is never settled by the distance test) */
+    /* certificate scan per pair: far = (static partner's ball centre, T2);
+       scan_c = (slot of P, slot of Q (-1: in frame 0), sqrt(T2) rounded up
+       (float bits), usable by the scan); scan_b = (static partner's vertex
+       0, R) */
     const float4* far;
-    const int2* far_slot;
+    const int4* scan_c;
+    const float4* scan_b;
     /* certificates: a pair whose guaranteed separation along the first
        search direction exceeds thr_dir is reported free without the test;
        eps_dir bounds the direction error of the approximate first direction
@@ -77,6 +79,20 @@ struct DevScene {
     int nslots;                          /* moving polytopes with a ball slot */
     int slot_sys[GPRM_MAX_SLOTS];        /* frame of each slot */
     int slot_block[GPRM_MAX_SLOTS];      /* its table block (entry 0 = ball) */
+    /* fast arithmetic (GPRM_MODE_FAST): the kernels run pair_test_fast */
+    int fast;
+    /* per polytope GPRM_START_BINS start entries (offsets into its table
+       block) of the first support climbs, indexed by dir_bin */
+    const unsigned short* start;
+    /* every polytope's vertices as table entries (xyz, packed w), and per
+       polytope (first entry, vertex count): the fast path's support search
+       over all vertices */
+    const float4* vtab;
+    const int2* vinfo;
+    /* per polytope and direction bin: (byte offset into cidx << 8 | count)
+       of the bin's support candidates, vertex indices in ascending order */
+    const unsigned* cbin;
+    const unsigned char* cidx;
 };
 
 /* fields of a table entry's w word */
@@ -189,8 +205,23 @@ __device__ __forceinline__ void forward_kinematics(const DevScene& sc, const flo
  * lane-interleaved shared-memory array: entry e of frame f at
  * out[((f-1)*12 + e) * 32] (out already offset by the lane).  The world
  * centre of every slot's bounding ball follows at
- * cen[(slot*3 + c) * 32] (computed with FMA: it only feeds the
- * certificates, whose slack covers its rounding). */
+ * cen[(slot*3 + c) * 32], then the world position of the slot polytope's
+ * vertex 0 at cen[((nslots + slot)*3 + c) * 32] (both with FMA: they only
+ * feed the certificates, whose slack covers their rounding). */
+__device__ __forceinline__ void slot_points(const DevScene& sc, const float4* __restrict__ tab, const Frame<float>& O,
+                                            int slot, float* cen)
+{
+    const float4 b = tab[sc.slot_block[slot]];
+    cen[(slot * 3 + 0) * 32] = __fmaf_rn(O.m[0], b.x, __fmaf_rn(O.m[3], b.y, __fmaf_rn(O.m[6], b.z, O.m[9])));
+    cen[(slot * 3 + 1) * 32] = __fmaf_rn(O.m[1], b.x, __fmaf_rn(O.m[4], b.y, __fmaf_rn(O.m[7], b.z, O.m[10])));
+    cen[(slot * 3 + 2) * 32] = __fmaf_rn(O.m[2], b.x, __fmaf_rn(O.m[5], b.y, __fmaf_rn(O.m[8], b.z, O.m[11])));
+    const float4 v = tab[sc.slot_block[slot] + 1];
+    float* w = cen + sc.nslots * 3 * 32;
+    w[(slot * 3 + 0) * 32] = __fmaf_rn(O.m[0], v.x, __fmaf_rn(O.m[3], v.y, __fmaf_rn(O.m[6], v.z, O.m[9])));
+    w[(slot * 3 + 1) * 32] = __fmaf_rn(O.m[1], v.x, __fmaf_rn(O.m[4], v.y, __fmaf_rn(O.m[7], v.z, O.m[10])));
+    w[(slot * 3 + 2) * 32] = __fmaf_rn(O.m[2], v.x, __fmaf_rn(O.m[5], v.y, __fmaf_rn(O.m[8], v.z, O.m[11])));
+}
+
 __device__ __forceinline__ void forward_kinematics_smem(const DevScene& sc, const float4* __restrict__ tab,
                                                         const float* q, float* out, float* cen)
 {
@@ -223,12 +254,7 @@ __device__ __forceinline__ void forward_kinematics_smem(const DevScene& sc, cons
         }
 #pragma unroll
         for (int e = 0; e < 12; ++e) out[(i * 12 + e) * 32] = O.m[e];
-        for (; slot < sc.nslots && sc.slot_sys[slot] == i + 1; ++slot) {
-            float4 b = tab[sc.slot_block[slot]];
-            cen[(slot * 3 + 0) * 32] = __fmaf_rn(O.m[0], b.x, __fmaf_rn(O.m[3], b.y, __fmaf_rn(O.m[6], b.z, O.m[9])));
-            cen[(slot * 3 + 1) * 32] = __fmaf_rn(O.m[1], b.x, __fmaf_rn(O.m[4], b.y, __fmaf_rn(O.m[7], b.z, O.m[10])));
-            cen[(slot * 3 + 2) * 32] = __fmaf_rn(O.m[2], b.x, __fmaf_rn(O.m[5], b.y, __fmaf_rn(O.m[8], b.z, O.m[11])));
-        }
+        for (; slot < sc.nslots && sc.slot_sys[slot] == i + 1; ++slot) slot_points(sc, tab, O, slot, cen);
         T = O;
     }
 }
@@ -498,6 +524,48 @@ __device__ __forceinline__ float box_support(const float4* __restrict__ B, const
     return h;
 }
 
+/* The direction and box tests of pair_certified, for a pair whose distance
+ * test failed: D = c_Q - c_P and d2 = |D|^2 as that test computed them.
+ * The world vertex 0 of a moving polytope comes from its slot (written by
+ * the FK pass with the FMA chain T*v0; cen points at the slot ball
+ * centres, the vertex-0 points follow them), that of a static polytope is
+ * its body-frame vertex 0.  A moving polytope without a slot has R = T2 =
+ * infinity: nothing can be certified. */
+__device__ __forceinline__ bool pair_certified_dir(const DevScene& sc, const float4* __restrict__ tab, int4 pr,
+                                                   float4 pb, const float* cen, const float* frames, int j,
+                                                   float dx, float dy, float dz, float d2, bool box_only = false)
+{
+    if (!(pb.x < PF32::inf())) return false;
+    const int sa = __float_as_int(pb.z), sb = __float_as_int(pb.w);
+    const float* v0w = cen + sc.nslots * 3 * 32;
+    float ax, ay, az, bx, by, bz;
+    if (sa >= 0) { ax = v0w[(sa * 3) * 32]; ay = v0w[(sa * 3 + 1) * 32]; az = v0w[(sa * 3 + 2) * 32]; }
+    else { const float4 v = tab[pr.x + 1]; ax = v.x; ay = v.y; az = v.z; }
+    if (sb >= 0) { bx = v0w[(sb * 3) * 32]; by = v0w[(sb * 3 + 1) * 32]; bz = v0w[(sb * 3 + 2) * 32]; }
+    else { const float4 v = tab[pr.y + 1]; bx = v.x; by = v.y; bz = v.z; }
+    const float sx = bx - ax, sy = by - ay, sz = bz - az;
+    const float n2 = __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, sz * sz));
+    if (!(n2 > 1e-6f)) return false;           /* |s| < 1e-3: leave it to the test */
+    const float inv = rsqrtf(n2);
+    const float G = __fmaf_rn(sx, dx, __fmaf_rn(sy, dy, sz * dz)) * inv - pb.x;
+    /* |D| from above (d2 * rsqrt(d2) is within 3 ulp of it) */
+    const float dn = d2 * rsqrtf(d2) * (1.0f + 2e-6f);
+    /* direction error <= eps_dir*inv (+ rsqrt and rounding, 1e-6) */
+    const float err = (dn + pb.x) * __fmaf_rn(sc.eps_dir, inv, 1e-6f);
+    if (!box_only && G - err > sc.thr_dir) return true;
+    /* box test: the same bound with each polytope's support along S taken
+       from its bounding box instead of its ball (every vertex v of X has
+       <S, v - c_X> <= sum_a e_a |<a_a, R_X^T S>|), tighter for elongated
+       links and flat obstacles */
+    if (!sc.box || !(pb.x < PF32::inf())) return false;
+    const int2 pp = sc.ppoly[j];
+    const float ux = sx * inv, uy = sy * inv, uz = sz * inv;
+    const float hp = box_support(sc.box + 3 * pp.x, frames, pr.z, ux, uy, uz);
+    const float hq = box_support(sc.box + 3 * pp.y, frames, pr.w, ux, uy, uz);
+    const float Gb = __fmaf_rn(ux, dx, __fmaf_rn(uy, dy, uz * dz)) - (hp + hq) * (1.0f + 1e-5f);
+    return Gb - err > sc.thr_dir;
+}
+
 __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4* __restrict__ tab,
                                                int4 pr, float4 pb, const float* cen,
                                                const float* frames, bool* used_dir, int j)
@@ -514,44 +582,7 @@ __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4*
     if (d2 > pb.y) return true;
     /* direction test: approximate first direction from vertex 0 of each */
     *used_dir = true;
-    float4 v0p = tab[pr.x + 1], v0q = tab[pr.y + 1];
-    float ax = v0p.x, ay = v0p.y, az = v0p.z, bx = v0q.x, by = v0q.y, bz = v0q.z;
-    if (pr.z) {
-        Frame<float> T;
-        load_frame(frames, pr.z, T);
-        float x = __fmaf_rn(T.m[0], ax, __fmaf_rn(T.m[3], ay, __fmaf_rn(T.m[6], az, T.m[9])));
-        float y = __fmaf_rn(T.m[1], ax, __fmaf_rn(T.m[4], ay, __fmaf_rn(T.m[7], az, T.m[10])));
-        float z = __fmaf_rn(T.m[2], ax, __fmaf_rn(T.m[5], ay, __fmaf_rn(T.m[8], az, T.m[11])));
-        ax = x; ay = y; az = z;
-    }
-    if (pr.w) {
-        Frame<float> T;
-        load_frame(frames, pr.w, T);
-        float x = __fmaf_rn(T.m[0], bx, __fmaf_rn(T.m[3], by, __fmaf_rn(T.m[6], bz, T.m[9])));
-        float y = __fmaf_rn(T.m[1], bx, __fmaf_rn(T.m[4], by, __fmaf_rn(T.m[7], bz, T.m[10])));
-        float z = __fmaf_rn(T.m[2], bx, __fmaf_rn(T.m[5], by, __fmaf_rn(T.m[8], bz, T.m[11])));
-        bx = x; by = y; bz = z;
-    }
-    const float sx = bx - ax, sy = by - ay, sz = bz - az;
-    const float n2 = __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, sz * sz));
-    if (!(n2 > 1e-6f)) return false;           /* |s| < 1e-3: leave it to the test */
-    const float inv = rsqrtf(n2);
-    const float G = __fmaf_rn(sx, dx, __fmaf_rn(sy, dy, sz * dz)) * inv - pb.x;
-    const float dn = sqrtf(d2);
-    /* direction error <= eps_dir*inv (+ rsqrt and rounding, 1e-6) */
-    const float err = (dn + pb.x) * __fmaf_rn(sc.eps_dir, inv, 1e-6f);
-    if (G - err > sc.thr_dir) return true;
-    /* box test: the same bound with each polytope's support along S taken
-       from its bounding box instead of its ball (every vertex v of X has
-       <S, v - c_X> <= sum_a e_a |<a_a, R_X^T S>|), tighter for elongated
-       links and flat obstacles */
-    if (!sc.box || !(pb.x < PF32::inf())) return false;
-    const int2 pp = sc.ppoly[j];
-    const float ux = sx * inv, uy = sy * inv, uz = sz * inv;
-    const float hp = box_support(sc.box + 3 * pp.x, frames, pr.z, ux, uy, uz);
-    const float hq = box_support(sc.box + 3 * pp.y, frames, pr.w, ux, uy, uz);
-    const float Gb = __fmaf_rn(ux, dx, __fmaf_rn(uy, dy, uz * dz)) - (hp + hq) * (1.0f + 1e-5f);
-    return Gb - err > sc.thr_dir;
+    return pair_certified_dir(sc, tab, pr, pb, cen, frames, j, dx, dy, dz, d2);
 }
 
 /* The same certificate for the FP64 recheck, in double from the FP64
@@ -588,6 +619,384 @@ __device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float
     const double G = (sx * dx + sy * dy + sz * dz) * inv - (double)pb.x;
     const double err = (sqrt(d2) + (double)pb.x) * 1e-6;
     return G - err > (double)sc.thr_dir;
+}
+
+/* ---------------------------------------------------------------- */
+/* fast FP32 arithmetic (GPRM_MODE_FAST)                             */
+/* ---------------------------------------------------------------- */
+/*
+ * The separating-vector algorithm of collision4.h:226-332 with the same
+ * steps, decisions and thresholds as pair_test, in contracted arithmetic:
+ *   - dot products and transforms as fused multiply-add chains;
+ *   - normalisation by the reciprocal square root of the MUFU unit
+ *     (rsqrtf, <= 2 ulp) instead of IEEE sqrt and division, and the
+ *     half-plane basis (orthtrafo23) by one reciprocal square root instead
+ *     of four divisions;
+ *   - the first iteration's two support climbs start at the support vertex
+ *     of a direction bin (dir_bin, a table per polytope) instead of vertex
+ *     0.  On a convex polytope a first-improvement climb ends at a maximiser
+ *     of the dot product from any start, so the support vertex is the same
+ *     one unless several vertices tie within rounding.
+ * Results differ from the reference's FP32 arithmetic by rounding: codes
+ * (iteration counts) may differ, free/not-free verdicts agree wherever the
+ * separation margin lies outside the FP64 band, which is what the band
+ * exists for.  The exact policy (PF32) stays the drop-in default.
+ */
+#define GPRM_START_BINS 54   /* 6 cube faces x 3 x 3 cells */
+
+/* Cube-map bin of a direction: the face of the largest |component| (with
+ * its sign), then each of the other two components against a third of it.
+ * Any input, NaN included, gives a bin in [0, GPRM_START_BINS). */
+__host__ __device__ __forceinline__ int dir_bin(float x, float y, float z)
+{
+    const float ax = fabsf(x), ay = fabsf(y), az = fabsf(z);
+    int face;
+    float m, u, v;
+    if (ax >= ay && ax >= az) { face = x < 0.0f ? 1 : 0; m = ax; u = y; v = z; }
+    else if (ay >= az) { face = y < 0.0f ? 3 : 2; m = ay; u = z; v = x; }
+    else { face = z < 0.0f ? 5 : 4; m = az; u = x; v = y; }
+    const float t = m * (1.0f / 3.0f);
+    const int iu = (u > t) - (u < -t) + 1, iv = (v > t) - (v < -t) + 1;
+    return face * 9 + iu * 3 + iv;
+}
+
+__device__ __forceinline__ float fdot3(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return __fmaf_rn(ax, bx, __fmaf_rn(ay, by, az * bz));
+}
+
+__device__ __forceinline__ V3<float> fxform(const Frame<float>& T, float x, float y, float z)
+{
+    V3<float> o;
+    o.x = __fmaf_rn(T.m[0], x, __fmaf_rn(T.m[3], y, __fmaf_rn(T.m[6], z, T.m[9])));
+    o.y = __fmaf_rn(T.m[1], x, __fmaf_rn(T.m[4], y, __fmaf_rn(T.m[7], z, T.m[10])));
+    o.z = __fmaf_rn(T.m[2], x, __fmaf_rn(T.m[5], y, __fmaf_rn(T.m[8], z, T.m[11])));
+    return o;
+}
+
+__device__ __forceinline__ V3<float> frot_t(const Frame<float>& T, float x, float y, float z)
+{
+    V3<float> o;
+    o.x = fdot3(T.m[0], T.m[1], T.m[2], x, y, z);
+    o.y = fdot3(T.m[3], T.m[4], T.m[5], x, y, z);
+    o.z = fdot3(T.m[6], T.m[7], T.m[8], x, y, z);
+    return o;
+}
+
+/* normalize (geo4.h:165-171): a zero vector stays zero; returns the norm */
+__device__ __forceinline__ float fnormalize3(V3<float>& u)
+{
+    const float n2 = fdot3(u.x, u.y, u.z, u.x, u.y, u.z);
+    const float f = n2 > 0.0f ? rsqrtf(n2) : 0.0f;
+    u.x *= f; u.y *= f; u.z *= f;
+    return n2 * f;
+}
+
+/* First-improvement climb (collision4.h:66-103) in FMA arithmetic; the
+ * neighbours of the current vertex are loaded and evaluated
+ * GPRM_FAST_CLIMB_CHUNK at a time, the move going to the first improving
+ * one in CRS order. */
+#ifndef GPRM_FAST_CLIMB_CHUNK
+#define GPRM_FAST_CLIMB_CHUNK 1
+#endif
+__device__ __forceinline__ float4 fclimb(const float4* __restrict__ B, float4 cur, float dx, float dy, float dz)
+{
+    float best = fdot3(cur.x, cur.y, cur.z, dx, dy, dz);
+#pragma unroll 1
+    for (int guard = 0; guard < 128; ++guard) {
+        const float4* e = B + 2 + ent_dsp(cur);
+        const int c = ent_cnt(cur);
+        bool moved = false;
+#if GPRM_FAST_CLIMB_CHUNK == 1
+#pragma unroll 1
+        for (int i = 0; i < c; ++i) {
+            const float4 u = e[i];
+            const float d = fdot3(u.x, u.y, u.z, dx, dy, dz);
+            if (d > best) { best = d; cur = u; moved = true; break; }
+        }
+#else
+#pragma unroll 1
+        for (int i = 0; i < c && !moved; i += GPRM_FAST_CLIMB_CHUNK) {
+            float4 u[GPRM_FAST_CLIMB_CHUNK];
+            float d[GPRM_FAST_CLIMB_CHUNK];
+#pragma unroll
+            for (int k = 0; k < GPRM_FAST_CLIMB_CHUNK; ++k) {
+                u[k] = e[i + k < c ? i + k : i];
+                d[k] = fdot3(u[k].x, u[k].y, u[k].z, dx, dy, dz);
+            }
+#pragma unroll
+            for (int k = 0; k < GPRM_FAST_CLIMB_CHUNK; ++k)
+                if (!moved && i + k < c && d[k] > best) { best = d[k]; cur = u[k]; moved = true; }
+        }
+#endif
+        if (!moved) break;
+    }
+    return cur;
+}
+
+/* The support climbs of P (along dp) and Q (along dq) side by side: each
+ * trip of the loop evaluates the next CRS neighbour of each polytope's
+ * current vertex, so that the two dependent load-and-compare chains
+ * overlap.  Each climb still moves to the first improving neighbour in CRS
+ * order and ends where fclimb ends (chunk 1).  The trip bound only guards
+ * corrupt data (a climb makes at most n-1 moves of at most 255 neighbours). */
+__device__ __forceinline__ void fclimb2(const float4* __restrict__ BP, float4& cp, float px, float py, float pz,
+                                        const float4* __restrict__ BQ, float4& cq, float qx, float qy, float qz)
+{
+    float bp = fdot3(cp.x, cp.y, cp.z, px, py, pz), bq = fdot3(cq.x, cq.y, cq.z, qx, qy, qz);
+    const float4* ep = BP + 2 + ent_dsp(cp);
+    const float4* eq = BQ + 2 + ent_dsp(cq);
+    int np = ent_cnt(cp), nq = ent_cnt(cq), ip = 0, iq = 0;
+#pragma unroll 1
+    for (int guard = 0; guard < 32768 && (ip < np || iq < nq); ++guard) {
+        if (ip < np) {
+            const float4 u = ep[ip];
+            const float d = fdot3(u.x, u.y, u.z, px, py, pz);
+            if (d > bp) { bp = d; cp = u; ep = BP + 2 + ent_dsp(u); np = ent_cnt(u); ip = 0; }
+            else ++ip;
+        }
+        if (iq < nq) {
+            const float4 u = eq[iq];
+            const float d = fdot3(u.x, u.y, u.z, qx, qy, qz);
+            if (d > bq) { bq = d; cq = u; eq = BQ + 2 + ent_dsp(u); nq = ent_cnt(u); iq = 0; }
+            else ++iq;
+        }
+    }
+}
+
+/* Support vertices of P (along dp) and Q (along dq) by a scan of all their
+ * vertices (VP[0..nP), VQ[0..nQ), table entries), side by side: a maximiser
+ * of the dot product, the first in vertex order among equal values.  The
+ * first-improvement climb also ends at a maximiser (on a convex polytope
+ * every vertex without an improving neighbour is one), so the two agree
+ * unless several vertices tie within rounding.  Every lane of a warp that
+ * tests the same pair runs the same trip count, the loads are independent,
+ * and a NaN direction keeps vertex 0. */
+#ifndef GPRM_FAST_SCAN_MAX
+#define GPRM_FAST_SCAN_MAX 32   /* polytopes with more vertices climb */
+#endif
+__device__ __forceinline__ void fsupport_scan2(const float4* __restrict__ VP, int nP, float4& cp, float px,
+                                               float py, float pz, const float4* __restrict__ VQ, int nQ,
+                                               float4& cq, float qx, float qy, float qz)
+{
+    float4 u = VP[0], v = VQ[0];
+    float bp = fdot3(u.x, u.y, u.z, px, py, pz), bq = fdot3(v.x, v.y, v.z, qx, qy, qz);
+    int ip = 0, iq = 0;
+    const int n = nP > nQ ? nP : nQ;
+    /* past its last vertex a polytope re-reads that vertex, whose dot
+       product cannot exceed the maximum again */
+#pragma unroll 4
+    for (int i = 1; i < n; ++i) {
+        u = VP[i < nP ? i : nP - 1];
+        v = VQ[i < nQ ? i : nQ - 1];
+        const float du = fdot3(u.x, u.y, u.z, px, py, pz), dv = fdot3(v.x, v.y, v.z, qx, qy, qz);
+        if (du > bp) { bp = du; ip = i; }
+        if (dv > bq) { bq = dv; iq = i; }
+    }
+    cp = VP[ip];
+    cq = VQ[iq];
+}
+
+/* Support vertices of polytopes kP (along p) and kQ (along q) from the
+ * candidate lists of the directions' bins: every vertex whose normal cone
+ * (the directions for which it is a maximiser) meets the bin, found on the
+ * host for bins slightly larger than dir_bin's, so the maximum over the
+ * list is the maximum over the whole polytope, up to ties within rounding.
+ * A few candidates instead of every vertex; P and Q side by side. */
+__device__ __forceinline__ void fsupport_cand2(const DevScene& sc, int kP, float4& cp, float px, float py, float pz,
+                                               int kQ, float4& cq, float qx, float qy, float qz)
+{
+    const int2 vP = sc.vinfo[kP], vQ = sc.vinfo[kQ];
+    const unsigned hP = sc.cbin[kP * GPRM_START_BINS + dir_bin(px, py, pz)];
+    const unsigned hQ = sc.cbin[kQ * GPRM_START_BINS + dir_bin(qx, qy, qz)];
+    const unsigned char* LP = sc.cidx + (hP >> 8);
+    const unsigned char* LQ = sc.cidx + (hQ >> 8);
+    const int nP = (int)(hP & 255u), nQ = (int)(hQ & 255u);
+    const float4* VP = sc.vtab + vP.x;
+    const float4* VQ = sc.vtab + vQ.x;
+    int ip = LP[0], iq = LQ[0];
+    float4 u = VP[ip], v = VQ[iq];
+    float bp = fdot3(u.x, u.y, u.z, px, py, pz), bq = fdot3(v.x, v.y, v.z, qx, qy, qz);
+    const int n = nP > nQ ? nP : nQ;
+    /* past its last candidate a list re-reads that candidate */
+#pragma unroll 1
+    for (int c = 1; c < n; ++c) {
+        const int a = LP[c < nP ? c : nP - 1], b = LQ[c < nQ ? c : nQ - 1];
+        u = VP[a];
+        v = VQ[b];
+        const float du = fdot3(u.x, u.y, u.z, px, py, pz), dv = fdot3(v.x, v.y, v.z, qx, qy, qz);
+        if (du > bp) { bp = du; ip = a; }
+        if (dv > bq) { bq = dv; iq = b; }
+    }
+    cp = VP[ip];
+    cq = VQ[iq];
+}
+
+/* find_half_plane with orthtrafo23 (collision4.h:111-223), contracted */
+__device__ __forceinline__ bool fhalf_plane(const V3<float>* hist, int k, V3<float>& w, const V3<float>& rk)
+{
+    if (fdot3(w.x, w.y, w.z, rk.x, rk.y, rk.z) > 0.0f) return true;
+    const float x = rk.x, y = rk.y, z = rk.z;
+    const float inv = rsqrtf(__fmaf_rn(x, x, y * y));   /* 1/d, d = |(x, y)| */
+    const float m0 = x * z * inv, m1 = y * z * inv, m2 = -__fmaf_rn(x, x, y * y) * inv;
+    const float m3 = -y * inv, m4 = x * inv;
+    V2<float> ra, rb, t;
+    ra.x = fdot3(m0, m1, m2, hist[0].x, hist[0].y, hist[0].z);
+    ra.y = __fmaf_rn(m3, hist[0].x, m4 * hist[0].y);
+    rb.x = fdot3(m0, m1, m2, hist[1].x, hist[1].y, hist[1].z);
+    rb.y = __fmaf_rn(m3, hist[1].x, m4 * hist[1].y);
+    if (__fmaf_rn(ra.x, rb.y, -ra.y * rb.x) < 0.0f) { V2<float> tmp = ra; ra = rb; rb = tmp; }
+#pragma unroll 1
+    for (int i = 2; i < k; ++i) {
+        t.x = fdot3(m0, m1, m2, hist[i].x, hist[i].y, hist[i].z);
+        t.y = __fmaf_rn(m3, hist[i].x, m4 * hist[i].y);
+        const float cb = __fmaf_rn(rb.x, t.y, -rb.y * t.x);
+        if (__fmaf_rn(ra.x, t.y, -ra.y * t.x) > 0.0f) {
+            if (cb > 0.0f) rb = t;
+        } else {
+            if (cb < 0.0f) ra = t;
+            else return false;
+        }
+    }
+    float f = rsqrtf(__fmaf_rn(ra.x, ra.x, ra.y * ra.y));
+    ra.x *= f; ra.y *= f;
+    f = rsqrtf(__fmaf_rn(rb.x, rb.x, rb.y * rb.y));
+    rb.x *= f; rb.y *= f;
+    t.x = ra.x + rb.x;
+    t.y = ra.y + rb.y;
+    f = rsqrtf(__fmaf_rn(t.x, t.x, t.y * t.y));
+    t.x *= f; t.y *= f;
+    w.x = __fmaf_rn(m0, t.x, m3 * t.y);
+    w.y = __fmaf_rn(m1, t.x, m4 * t.y);
+    w.z = m2 * t.x;
+    return true;
+}
+
+/* pair_test in fast arithmetic.  pp: the pair's two polytope indices (for
+ * the vertex lists and start tables).  Same returns and margin as
+ * pair_test, and the same first search direction (the line between the
+ * two vertices 0): the iteration cap (code -1, always inside the band)
+ * depends on the path from it, so a different start would change which
+ * checks the band recomputes. */
+__device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* __restrict__ tab, int4 pr, int2 pp,
+                                              const Frame<float>& tp, const Frame<float>& tq, float* margin)
+{
+    const float4* BP = tab + pr.x;
+    const float4* BQ = tab + pr.y;
+    const bool idP = pr.z == 0, idQ = pr.w == 0;
+    float4 ep = BP[1], eq = BQ[1];
+    V3<float> Sa, Sb;
+    if (idQ) { Sa.x = eq.x; Sa.y = eq.y; Sa.z = eq.z; }
+    else Sa = fxform(tq, eq.x, eq.y, eq.z);
+    if (idP) { Sb.x = ep.x; Sb.y = ep.y; Sb.z = ep.z; }
+    else Sb = fxform(tp, ep.x, ep.y, ep.z);
+    V3<float> S;
+    S.x = Sa.x - Sb.x; S.y = Sa.y - Sb.y; S.z = Sa.z - Sb.z;
+    const float norm = fnormalize3(S);
+    if (norm < sc.tiny_thr) S.x = 1.0f;
+    V3<float> w; w.x = w.y = w.z = 0.0f;
+    V3<float> hist[GPRM_MAX_ITERS];
+    int combs[GPRM_MAX_ITERS];
+    float best = 0.0f;
+    int k = 0, l = 0;
+    /* small polytopes: support by scanning every vertex (warp-uniform trip
+       counts); larger ones: climbs, the first from the direction tables */
+    const int2 vP = sc.vinfo[pp.x], vQ = sc.vinfo[pp.y];
+    const bool scan = vP.y <= GPRM_FAST_SCAN_MAX && vQ.y <= GPRM_FAST_SCAN_MAX;
+#pragma unroll 1
+    for (; k < GPRM_MAX_ITERS && l < GPRM_MAX_ITERS; ++l) {
+        V3<float> Sp, Sq;
+        if (idP) Sp = S;
+        else Sp = frot_t(tp, S.x, S.y, S.z);
+        if (idQ) { Sq.x = -S.x; Sq.y = -S.y; Sq.z = -S.z; }
+        else Sq = frot_t(tq, -S.x, -S.y, -S.z);
+        if (sc.cbin) {
+            fsupport_cand2(sc, pp.x, ep, Sp.x, Sp.y, Sp.z, pp.y, eq, Sq.x, Sq.y, Sq.z);
+        } else if (scan) {
+            fsupport_scan2(sc.vtab + vP.x, vP.y, ep, Sp.x, Sp.y, Sp.z, sc.vtab + vQ.x, vQ.y, eq, Sq.x, Sq.y, Sq.z);
+        } else {
+            if (l == 0 && sc.start) {
+                ep = BP[sc.start[pp.x * GPRM_START_BINS + dir_bin(Sp.x, Sp.y, Sp.z)]];
+                eq = BQ[sc.start[pp.y * GPRM_START_BINS + dir_bin(Sq.x, Sq.y, Sq.z)]];
+            }
+            fclimb2(BP, ep, Sp.x, Sp.y, Sp.z, BQ, eq, Sq.x, Sq.y, Sq.z);
+        }
+        V3<float> p0, q0;
+        if (idP) { p0.x = ep.x; p0.y = ep.y; p0.z = ep.z; }
+        else p0 = fxform(tp, ep.x, ep.y, ep.z);
+        if (idQ) { q0.x = eq.x; q0.y = eq.y; q0.z = eq.z; }
+        else q0 = fxform(tq, eq.x, eq.y, eq.z);
+        V3<float> r;
+        r.x = q0.x - p0.x; r.y = q0.y - p0.y; r.z = q0.z - p0.z;
+        const float rn = fnormalize3(r);
+        const float dp = fdot3(S.x, S.y, S.z, r.x, r.y, r.z);
+        const float h = dp * rn;
+        if (l == 0 || h > best) best = h;
+        if (dp >= sc.sep_thr) {
+            *margin = h;
+            return 0;
+        }
+        hist[k] = r;
+        const int comb = ent_idx(ep) | (ent_idx(eq) << 8);
+        combs[k] = comb;
+        bool rep = false;
+#pragma unroll 1
+        for (int j = 0; j < k; ++j)
+            if (combs[j] == comb) { rep = true; break; }
+        if (rep) {
+            S = w;
+        } else {
+            if (k == 1) {
+                w.x = hist[0].x + r.x; w.y = hist[0].y + r.y; w.z = hist[0].z + r.z;
+                fnormalize3(w);
+            }
+            if (k >= 2 && !fhalf_plane(hist, k, w, r)) {
+                *margin = best;
+                return l + 1;
+            }
+            const float b = -2.0f * dp;
+            S.x = __fmaf_rn(b, r.x, S.x); S.y = __fmaf_rn(b, r.y, S.y); S.z = __fmaf_rn(b, r.z, S.z);
+            ++k;
+        }
+    }
+    *margin = best;
+    return -1;
+}
+
+/* Forward kinematics of the fast path into the lane's shared-memory frames
+ * (same layout as forward_kinematics_smem): sincosf of the joint angles and
+ * FMA products. */
+__device__ __forceinline__ void forward_kinematics_smem_fast(const DevScene& sc, const float4* __restrict__ tab,
+                                                             const float* q, float* out, float* cen)
+{
+    Frame<float> T;
+#pragma unroll
+    for (int e = 0; e < 12; ++e) T.m[e] = 0.0f;
+    T.m[0] = T.m[4] = T.m[8] = 1.0f;
+    int slot = 0;
+#pragma unroll 1
+    for (int i = 0; i < sc.ndof; ++i) {
+        float th = sc.q0[i], d = sc.d0[i];
+        if (sc.types[i] == 0) th = q[i];
+        else d = q[i];
+        float cq, sq;
+        sincosf(th, &sq, &cq);
+        const float ca = sc.ca[i], sa = sc.sa[i];
+        Frame<float> L;
+        dh_frame<PF32>(L, cq, sq, ca, sa, sc.a[i], d);
+        Frame<float> O;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float ux = L.m[3 * c], uy = L.m[3 * c + 1], uz = L.m[3 * c + 2];
+            O.m[3 * c] = __fmaf_rn(T.m[0], ux, __fmaf_rn(T.m[3], uy, __fmaf_rn(T.m[6], uz, c == 3 ? T.m[9] : 0.0f)));
+            O.m[3 * c + 1] = __fmaf_rn(T.m[1], ux, __fmaf_rn(T.m[4], uy, __fmaf_rn(T.m[7], uz, c == 3 ? T.m[10] : 0.0f)));
+            O.m[3 * c + 2] = __fmaf_rn(T.m[2], ux, __fmaf_rn(T.m[5], uy, __fmaf_rn(T.m[8], uz, c == 3 ? T.m[11] : 0.0f)));
+        }
+#pragma unroll
+        for (int e = 0; e < 12; ++e) out[(i * 12 + e) * 32] = O.m[e];
+        for (; slot < sc.nslots && sc.slot_sys[slot] == i + 1; ++slot) slot_points(sc, tab, O, slot, cen);
+        T = O;
+    }
 }
 
 /* FP32 check band test: the check's result is decided within `band` of

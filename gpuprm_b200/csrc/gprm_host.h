@@ -62,7 +62,8 @@ struct gprm_space {
     std::vector<int4> pairs;
     std::vector<float4> pairs_b;   /* certificate data per pair */
     std::vector<float4> far;       /* distance test: static ball centre, T2 */
-    std::vector<int2> far_slot;    /* distance test: moving slot(s), -1 none */
+    std::vector<int4> scan_c;      /* certificate scan: slots of P and Q (-1 static), sqrt(T2) up, usable */
+    std::vector<float4> scan_b;    /* certificate scan: static polytope's vertex 0, R */
     std::vector<double> rad;       /* inflated ball radius per polytope */
     /* bounding box per polytope about its ball centre: PCA axes (FP32
        values), half extents (exact), and the device records (axis, inflated
@@ -72,6 +73,15 @@ struct gprm_space {
     std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
     std::vector<int> slot_sys, slot_block;
     std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */
+    /* start entries of the fast path's first support climbs: per polytope
+       GPRM_START_BINS offsets into its table block (see dir_bin) */
+    std::vector<unsigned short> start;
+    /* every polytope's vertices as table entries, and (first, count) per polytope */
+    std::vector<float4> vtab;
+    std::vector<int2> vinfo;
+    /* support candidates per polytope and direction bin (see fsupport_cand2) */
+    std::vector<unsigned> cbin;
+    std::vector<unsigned char> cidx;
     double extent = 1.0;           /* length scale of the scene (m) */
     float thr_dir = 0, eps_dir = 0;
 

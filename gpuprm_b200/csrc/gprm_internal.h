@@ -36,6 +36,8 @@ struct LaunchCfg {
     size_t smem_bytes;   /* dynamic shared memory: per-lane frames (+ scene copy) */
     int scene_in_smem;   /* the scene table is copied into shared memory */
     int warps_per_sm;    /* resident warps per SM at this configuration */
+    int blocks_per_sm;   /* resident blocks per SM of the persistent grid */
+    int carveout;        /* shared-memory carveout (percent) set before each launch; -1: default */
 };
 
 enum EdgePolicy { EDGE_EARLY_EXIT = 0, EDGE_ALL_STEPS = 1 };
@@ -55,6 +57,7 @@ struct BatchView {
     long long nwork;          /* chunks (vertex) or edges (edge) */
     int S;
     int lane_floats;          /* per-lane shared floats: max over the problems */
+    int fast;                 /* GPRM_MODE_FAST arithmetic (the problems share the mode) */
 };
 
 /* Launch shape of the batched kernels. */
@@ -70,27 +73,30 @@ cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const
                                  const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
 
 /* Per-lane shared floats of a warp's block: frames 1..ndof (12 floats
- * each), the ball centres of the slots (3 floats each), lane-interleaved;
- * then DEFER_LANE_FLOATS per lane, together the warp's queue of deferred
- * exact pair tests (64 items) and one batch's results (32 codes, 32
- * margins); then SWEEP_LANE_FLOATS per lane, together the warp's per-slot
- * sweep balls (GPRM_MAX_SLOTS float4). */
+ * each), the world ball centres of the slots (3 floats each), the world
+ * vertex 0 of the slots' polytopes (3 floats each), lane-interleaved; then,
+ * in the vertex kernels only, DEFER_LANE_FLOATS per lane, together the
+ * warp's queue of deferred exact pair tests (64 items) and one batch's
+ * results (32 codes, 32 margins); then SWEEP_LANE_FLOATS per lane,
+ * together the warp's per-slot sweep balls (GPRM_MAX_SLOTS float4). */
 #define SWEEP_LANE_FLOATS 2
 static_assert(SWEEP_LANE_FLOATS * 32 >= GPRM_MAX_SLOTS * 4, "sweep area too small");
 #define DEFER_LANE_FLOATS 4
-__host__ __device__ __forceinline__ size_t lane_floats(const DevScene& sc)
+__host__ __device__ __forceinline__ size_t lane_floats(const DevScene& sc, bool vertex_kernel)
 {
-    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 3 + DEFER_LANE_FLOATS + SWEEP_LANE_FLOATS;
+    return (size_t)sc.ndof * 12 + (size_t)sc.nslots * 6 + (vertex_kernel ? DEFER_LANE_FLOATS : 0) +
+           SWEEP_LANE_FLOATS;
 }
 
 /* Scene bytes when staged in shared memory; per-lane frame bytes of a block. */
 size_t scene_smem_bytes(const DevScene& sc);
-size_t frame_smem_bytes(const DevScene& sc, int threads);
+size_t frame_smem_bytes(const DevScene& sc, int threads, bool vertex_kernel);
 
 /* Sets up one launch variant (threads per block, scene in shared memory or
- * read through L1) and its persistent grid; fails if it does not fit. */
+ * read through L1, at most blocks_cap resident blocks per SM, 0 = as many
+ * as fit) and its persistent grid; fails if it does not fit. */
 cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads, int scene_in_smem,
-                             LaunchCfg* cfg);
+                             LaunchCfg* cfg, int blocks_cap = 0);
 
 /* Vertex checks: res[i] = code of configuration q[i + offset*j]. */
 cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q,

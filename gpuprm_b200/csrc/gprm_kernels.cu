@@ -25,6 +25,10 @@
  */
 #include "gprm_internal.h"
 
+#include <math.h>
+#include <mutex>
+#include <unordered_map>
+
 namespace gprm {
 
 #define FULL_MASK 0xffffffffu
@@ -42,13 +46,13 @@ namespace gprm {
 
 size_t scene_smem_bytes(const DevScene& sc)
 {
-    /* tab | pairs | pairs_b | far | far_slot, padded to 16 bytes */
-    return ((size_t)sc.ntab * 16 + (size_t)sc.npairs * 56 + 15) & ~(size_t)15;
+    /* tab | pairs | pairs_b | far | scan_c | scan_b, padded to 16 bytes */
+    return ((size_t)sc.ntab * 16 + (size_t)sc.npairs * 80 + 15) & ~(size_t)15;
 }
 
-size_t frame_smem_bytes(const DevScene& sc, int threads)
+size_t frame_smem_bytes(const DevScene& sc, int threads, bool vertex_kernel)
 {
-    return (size_t)(threads / 32) * lane_floats(sc) * 32 * sizeof(float);
+    return (size_t)(threads / 32) * lane_floats(sc, vertex_kernel) * 32 * sizeof(float);
 }
 
 struct SceneView {
@@ -56,31 +60,37 @@ struct SceneView {
     const int4* pairs;
     const float4* pairs_b;
     const float4* far;
-    const int2* far_slot;
+    const int4* scan_c;
+    const float4* scan_b;
     float* frames;   /* this lane's frames (lane-interleaved, stride 32) */
-    float* cen;      /* this lane's slot ball centres */
+    float* cen;      /* this lane's slot ball centres, then the slots' world vertex 0 */
     float4* sweep;   /* the warp's per-slot sweep balls (GPRM_MAX_SLOTS) */
     unsigned* defer; /* the warp's deferred-test queue (64) and batch results (32 + 32) */
 };
 
 /* The warp's sweep area: the last SWEEP_LANE_FLOATS entries of its block. */
+template <bool VERTEX>
 __device__ __forceinline__ float4* sweep_area(const DevScene& sc, float* lane_frames)
 {
     const int lane = threadIdx.x & 31;
-    return reinterpret_cast<float4*>(lane_frames - lane + (lane_floats(sc) - SWEEP_LANE_FLOATS) * 32);
+    return reinterpret_cast<float4*>(lane_frames - lane + (lane_floats(sc, VERTEX) - SWEEP_LANE_FLOATS) * 32);
 }
 
-/* The warp's deferred-test area: the DEFER_LANE_FLOATS entries before the sweep area. */
+/* The warp's deferred-test area (vertex kernels): the DEFER_LANE_FLOATS
+ * entries before the sweep area; null in the edge kernels. */
+template <bool VERTEX>
 __device__ __forceinline__ unsigned* defer_area(const DevScene& sc, float* lane_frames)
 {
+    if constexpr (!VERTEX) return nullptr;
     const int lane = threadIdx.x & 31;
     return reinterpret_cast<unsigned*>(lane_frames - lane +
-                                       (lane_floats(sc) - SWEEP_LANE_FLOATS - DEFER_LANE_FLOATS) * 32);
+                                       (lane_floats(sc, true) - SWEEP_LANE_FLOATS - DEFER_LANE_FLOATS) * 32);
 }
 
 /* Copies the scene into shared memory (SMEM) and returns the pointers the
- * warp uses, including its lane's slice of the frame array. */
-template <bool SMEM>
+ * warp uses, including its lane's slice of the frame array (laid out for
+ * the vertex or the edge kernels, VERTEX). */
+template <bool SMEM, bool VERTEX>
 __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned char* smem)
 {
     SceneView s;
@@ -91,64 +101,38 @@ __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned ch
         int4* p = reinterpret_cast<int4*>(smem + (size_t)sc.ntab * 16);
         float4* pb = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + np * 16);
         float4* fr = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + np * 32);
-        int2* fs = reinterpret_cast<int2*>(smem + (size_t)sc.ntab * 16 + np * 48);
+        int4* scc = reinterpret_cast<int4*>(smem + (size_t)sc.ntab * 16 + np * 48);
+        float4* scb = reinterpret_cast<float4*>(smem + (size_t)sc.ntab * 16 + np * 64);
         for (int i = threadIdx.x; i < sc.ntab; i += blockDim.x) t[i] = sc.tab[i];
         for (int i = threadIdx.x; i < sc.npairs; i += blockDim.x) {
             p[i] = sc.pairs[i];
             pb[i] = sc.pairs_b[i];
             fr[i] = sc.far[i];
-            fs[i] = sc.far_slot[i];
+            scc[i] = sc.scan_c[i];
+            scb[i] = sc.scan_b[i];
         }
         s.tab = t;
         s.pairs = p;
         s.pairs_b = pb;
         s.far = fr;
-        s.far_slot = fs;
-        off = ((size_t)sc.ntab * 16 + np * 56 + 15) & ~(size_t)15;   /* frames stay 16-byte aligned */
+        s.scan_c = scc;
+        s.scan_b = scb;
+        off = ((size_t)sc.ntab * 16 + np * 80 + 15) & ~(size_t)15;   /* frames stay 16-byte aligned */
     } else {
         s.tab = sc.tab;
         s.pairs = sc.pairs;
         s.pairs_b = sc.pairs_b;
         s.far = sc.far;
-        s.far_slot = sc.far_slot;
+        s.scan_c = sc.scan_c;
+        s.scan_b = sc.scan_b;
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    s.frames = reinterpret_cast<float*>(smem + off) + (size_t)warp * lane_floats(sc) * 32 + lane;
+    s.frames = reinterpret_cast<float*>(smem + off) + (size_t)warp * lane_floats(sc, VERTEX) * 32 + lane;
     s.cen = s.frames + (size_t)sc.ndof * 12 * 32;
-    s.sweep = sweep_area(sc, s.frames);
-    s.defer = defer_area(sc, s.frames);
+    s.sweep = sweep_area<VERTEX>(sc, s.frames);
+    s.defer = defer_area<VERTEX>(sc, s.frames);
     __syncthreads();
     return s;
-}
-
-/* Distance-test scan of pairs j0 .. j0+jn-1 (jn <= 32) for this lane: bit
- * k of the result is set when pair j0+k is NOT settled by the distance
- * certificate (the same test as the first half of pair_certified, on the
- * same values).  Order-free: a settled pair is free with its margin above
- * the band, so it changes neither a code nor a band decision. */
-__device__ __forceinline__ unsigned far_scan(const SceneView& S, int j0, int jn)
-{
-    unsigned need = 0;
-#pragma unroll 4
-    for (int k = 0; k < jn; ++k) {
-        const float4 f = S.far[j0 + k];
-        const int2 fs = S.far_slot[j0 + k];
-        bool cert = false;
-        if (fs.x >= 0) {
-            const float px = S.cen[(fs.x * 3) * 32], py = S.cen[(fs.x * 3 + 1) * 32], pz = S.cen[(fs.x * 3 + 2) * 32];
-            float qx = f.x, qy = f.y, qz = f.z;
-            if (fs.y >= 0) {
-                qx = S.cen[(fs.y * 3) * 32];
-                qy = S.cen[(fs.y * 3 + 1) * 32];
-                qz = S.cen[(fs.y * 3 + 2) * 32];
-            }
-            const float dx = qx - px, dy = qy - py, dz = qz - pz;
-            const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
-            cert = d2 > f.w;
-        }
-        need |= (cert ? 0u : 1u) << k;
-    }
-    return need;
 }
 
 /* Per slot, a ball holding that slot's ball centre in every lane of `mask`
@@ -187,64 +171,141 @@ __device__ __forceinline__ void sweep_bounds(const DevScene& sc, const SceneView
     __syncwarp();
 }
 
-/* far_scan for a warp whose lanes hold nearby configurations: lane k first
- * tests pair j0+k against the sweep ball of its moving slot; a pair whose
- * static partner lies farther than rho + sqrt(T2) from the sweep centre is
- * settled for every lane at once (each lane's exact distance then exceeds
- * sqrt(T2), the per-lane test's threshold).  The other pairs get the
- * per-lane test of far_scan. */
-__device__ __forceinline__ unsigned far_scan_swept(const SceneView& S, int j0, int jn)
-{
-    const int lane = threadIdx.x & 31;
-    bool maybe = false;
-    if (lane < jn) {
-        maybe = true;
-        const int2 fs = S.far_slot[j0 + lane];
-        if (fs.x >= 0 && fs.y < 0) {
-            const float4 f = S.far[j0 + lane];
-            const float4 b = S.sweep[fs.x];
-            const float dx = f.x - b.x, dy = f.y - b.y, dz = f.z - b.z;
-            const float dd2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
-            const float A = (__fsqrt_ru(f.w) + b.w) * (1.0f + 1e-6f);
-            /* |m - c|^2 >= dd2 (1 - 1e-6) > A^2 >= (rho + sqrt(T2))^2 */
-            if (dd2 * (1.0f - 1e-6f) > A * A) maybe = false;
-        }
-    }
-    unsigned cand = __ballot_sync(FULL_MASK, maybe);
-    unsigned need = 0;
-    while (cand) {
-        const int k = __ffs(cand) - 1;
-        cand &= cand - 1u;
-        const float4 f = S.far[j0 + k];
-        const int2 fs = S.far_slot[j0 + k];
-        bool cert = false;
-        if (fs.x >= 0) {
-            const float px = S.cen[(fs.x * 3) * 32], py = S.cen[(fs.x * 3 + 1) * 32], pz = S.cen[(fs.x * 3 + 2) * 32];
-            float qx = f.x, qy = f.y, qz = f.z;
-            if (fs.y >= 0) {
-                qx = S.cen[(fs.y * 3) * 32];
-                qy = S.cen[(fs.y * 3 + 1) * 32];
-                qz = S.cen[(fs.y * 3 + 2) * 32];
-            }
-            const float dx = qx - px, dy = qy - py, dz = qz - pz;
-            const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
-            cert = d2 > f.w;
-        }
-        need |= (cert ? 0u : 1u) << k;
-    }
-    return need;
-}
-
 /* Per-lane counts of how pair tests were settled. */
 struct PairCounts {
     unsigned long long far, dir, full;
 };
 
-/* One pair of the reference's pair loop for this lane: the certificate
- * first, the exact test otherwise.  Returns the pair's code; *margin is set
- * (and *has_margin true) only when the exact test ran. */
+/* The distance and direction certificates of a usable pair (scan_c.w) for
+ * this lane, branch-free so that two pairs can be evaluated side by side:
+ * the ball-distance test of pair_certified, then its direction test with
+ * the world vertex 0 of a moving polytope from its slot (the FK pass wrote
+ * it with the FMA chain T*v0) and that of a static one from scan_b.
+ * Returns 1 (distance), 2 (direction) or 0 (neither; *d2o and *Do get
+ * |D|^2 and D = c_Q - c_P for the box test). */
+__device__ __forceinline__ int cert_dist_dir(const DevScene& sc, const SceneView& S, int4 c, float4 f, float4 b,
+                                             float* d2o, float3* Do)
+{
+    const float* cen = S.cen;
+    const float* v0w = S.cen + sc.nslots * 3 * 32;
+    float px = f.x, py = f.y, pz = f.z, qx = f.x, qy = f.y, qz = f.z;
+    float ax = b.x, ay = b.y, az = b.z, bx = b.x, by = b.y, bz = b.z;
+    if (c.x >= 0) {
+        px = cen[(c.x * 3) * 32]; py = cen[(c.x * 3 + 1) * 32]; pz = cen[(c.x * 3 + 2) * 32];
+        ax = v0w[(c.x * 3) * 32]; ay = v0w[(c.x * 3 + 1) * 32]; az = v0w[(c.x * 3 + 2) * 32];
+    }
+    if (c.y >= 0) {
+        qx = cen[(c.y * 3) * 32]; qy = cen[(c.y * 3 + 1) * 32]; qz = cen[(c.y * 3 + 2) * 32];
+        bx = v0w[(c.y * 3) * 32]; by = v0w[(c.y * 3 + 1) * 32]; bz = v0w[(c.y * 3 + 2) * 32];
+    }
+    const float dx = qx - px, dy = qy - py, dz = qz - pz;
+    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+    const float sx = bx - ax, sy = by - ay, sz = bz - az;
+    const float n2 = __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, sz * sz));
+    const float inv = rsqrtf(n2);
+    const float G = __fmaf_rn(sx, dx, __fmaf_rn(sy, dy, sz * dz)) * inv - b.w;
+    /* |D| from above: d2 * rsqrt(d2) is within 3 ulp of |D| (rsqrtf <= 2
+       ulp), the factor covers it; d2 = 0 gives NaN, which fails the test */
+    const float dn = d2 * rsqrtf(d2) * (1.0f + 2e-6f);
+    /* direction error <= eps_dir*inv (+ rsqrt and rounding, 1e-6) */
+    const float err = (dn + b.w) * __fmaf_rn(sc.eps_dir, inv, 1e-6f);
+    *d2o = d2;
+    *Do = make_float3(dx, dy, dz);
+    if (d2 > f.w) return 1;
+    return (n2 > 1e-6f && G - err > sc.thr_dir) ? 2 : 0;
+}
+
+/* Certificates of pairs j0 .. j0+jn-1 (jn <= 32) for this lane, all
+ * order-free (a certified pair is free with its margin above the band, so
+ * it changes neither a code nor a band decision), in three stages:
+ *   sweep     (SWEPT, lanes holding nearby configurations) lane k tests pair
+ *             j0+k against the sweep ball of its moving slot: a pair whose
+ *             static partner lies farther than rho + sqrt(T2) from the sweep
+ *             centre is settled for every lane at once (each lane's exact
+ *             distance then exceeds sqrt(T2));
+ *   per lane  the other pairs, two at a time: the ball-distance and
+ *             direction tests (cert_dist_dir), then for the few pairs both
+ *             miss the box test of pair_certified_dir; pairs the scan cannot
+ *             use go through pair_certified.
+ * Returns the pairs that need the exact test (bit k: pair j0+k); 0 for an
+ * inactive lane.  Every lane of the warp must call it (the sweep stage
+ * votes). */
+template <bool SWEPT>
+__device__ __forceinline__ unsigned cert_scan(const DevScene& sc, const SceneView& S, int j0, int jn, bool active,
+                                              PairCounts& pc)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned all = jn >= 32 ? FULL_MASK : ((1u << jn) - 1u);
+    unsigned cand = all;
+    if constexpr (SWEPT) {
+        bool maybe = false;
+        if (lane < jn) {
+            maybe = true;
+            const int4 c = S.scan_c[j0 + lane];
+            if (c.w && ((c.x < 0) != (c.y < 0))) {
+                const float4 f = S.far[j0 + lane];
+                const float4 b = S.sweep[c.x >= 0 ? c.x : c.y];
+                const float dx = f.x - b.x, dy = f.y - b.y, dz = f.z - b.z;
+                const float dd2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+                const float A = (__int_as_float(c.z) + b.w) * (1.0f + 1e-6f);
+                /* |m - c|^2 >= dd2 (1 - 1e-6) > A^2 >= (rho + sqrt(T2))^2 */
+                if (dd2 * (1.0f - 1e-6f) > A * A) maybe = false;
+            }
+        }
+        cand = __ballot_sync(FULL_MASK, maybe);
+    }
+    if (!active) return 0u;
+    pc.far += (unsigned)__popc(all & ~cand);
+    unsigned need = 0;
+#pragma unroll 1
+    while (cand) {
+        const int k0 = __ffs(cand) - 1;
+        cand &= cand - 1u;
+        int k1 = k0;
+        const bool two = cand != 0;
+        if (two) {
+            k1 = __ffs(cand) - 1;
+            cand &= cand - 1u;
+        }
+        const int ja = j0 + k0, jb = j0 + k1;
+        const int4 ca = S.scan_c[ja], cb = S.scan_c[jb];
+        const float4 fa = S.far[ja], fb = S.far[jb];
+        const float4 ba = S.scan_b[ja], bb = S.scan_b[jb];
+        float d2a, d2b;
+        float3 Da, Db;
+        int ra = ca.w ? cert_dist_dir(sc, S, ca, fa, ba, &d2a, &Da) : -1;
+        int rb = (two && cb.w) ? cert_dist_dir(sc, S, cb, fb, bb, &d2b, &Db) : -1;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (h == 1 && !two) break;
+            const int r = h ? rb : ra;
+            const int j = h ? jb : ja;
+            const int k = h ? k1 : k0;
+            if (r == 1) { ++pc.far; continue; }
+            if (r == 2) { ++pc.dir; continue; }
+            bool ok;
+            if (r == 0) {
+                /* the box test (pair_certified_dir's last stage) */
+                const float3 D = h ? Db : Da;
+                ok = pair_certified_dir(sc, S.tab, S.pairs[j], S.pairs_b[j], S.cen, S.frames, j, D.x, D.y, D.z,
+                                        h ? d2b : d2a, true);
+                if (ok) ++pc.dir;
+            } else {
+                bool used_dir;
+                ok = pair_certified(sc, S.tab, S.pairs[j], S.pairs_b[j], S.cen, S.frames, &used_dir, j);
+                if (ok) { if (used_dir) ++pc.dir; else ++pc.far; }
+            }
+            if (!ok) need |= 1u << k;
+        }
+    }
+    return need;
+}
+
+/* The exact test of pair j for this lane (its certificates failed in
+ * cert_scan): the pair's code, and its margin in *margin. */
+template <bool FAST>
 __device__ __forceinline__ int eval_pair(const DevScene& sc, const SceneView& S, int j, float* margin,
-                                         bool* has_margin, PairCounts& pc);
+                                         PairCounts& pc);
 
 /* The frames of a pair, from the lane's frame array (frame 0 is unused). */
 __device__ __forceinline__ void pair_frames(const float* fr, int4 pr, Frame<float>& tp, Frame<float>& tq)
@@ -253,23 +314,25 @@ __device__ __forceinline__ void pair_frames(const float* fr, int4 pr, Frame<floa
     if (pr.w) load_frame(fr, pr.w, tq);
 }
 
+template <bool FAST>
 __device__ __forceinline__ int eval_pair(const DevScene& sc, const SceneView& S, int j, float* margin,
-                                         bool* has_margin, PairCounts& pc)
+                                         PairCounts& pc)
 {
     const int4 pr = S.pairs[j];
-    const float4 pb = S.pairs_b[j];
-    bool used_dir;
-    if (pair_certified(sc, S.tab, pr, pb, S.cen, S.frames, &used_dir, j)) {
-        if (used_dir) ++pc.dir;
-        else ++pc.far;
-        *has_margin = false;
-        return 0;
-    }
     ++pc.full;
     Frame<float> tp, tq;
     pair_frames(S.frames, pr, tp, tq);
-    *has_margin = true;
-    return pair_test<PF32>(sc, S.tab, pr, tp, tq, margin);
+    if constexpr (FAST) return pair_test_fast(sc, S.tab, pr, sc.ppoly[j], tp, tq, margin);
+    else return pair_test<PF32>(sc, S.tab, pr, tp, tq, margin);
+}
+
+/* Forward kinematics of a lane into its shared-memory frames, in the
+ * arithmetic of the kernel variant. */
+template <bool FAST>
+__device__ __forceinline__ void lane_fk(const DevScene& sc, const SceneView& S, const float* q)
+{
+    if constexpr (FAST) forward_kinematics_smem_fast(sc, S.tab, q, S.frames, S.cen);
+    else forward_kinematics_smem(sc, S.tab, q, S.frames, S.cen);
 }
 
 __device__ __forceinline__ void flush_counts(PairCounts pc, Control* ctl)
@@ -325,6 +388,7 @@ __device__ __forceinline__ void defer_push(unsigned* q, int& n, bool want, int k
 
 /* Runs the first cnt (<= 32) queued items, one per lane, and lets every
  * owner apply its results; the remaining items move to the front. */
+template <bool FAST>
 __device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S, int j0, int& n, int cnt,
                                           LaneState& st, PairCounts& pc)
 {
@@ -338,10 +402,12 @@ __device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S
     if (lane < cnt) {
         const unsigned it = q[lane];
         const int owner = (int)(it & 31u);
-        const int4 pr = S.pairs[j0 + (int)(it >> 5)];
+        const int jj = j0 + (int)(it >> 5);
+        const int4 pr = S.pairs[jj];
         Frame<float> tp, tq;
         pair_frames(S.frames - lane + owner, pr, tp, tq);
-        c = pair_test<PF32>(sc, S.tab, pr, tp, tq, &m);
+        if constexpr (FAST) c = pair_test_fast(sc, S.tab, pr, sc.ppoly[jj], tp, tq, &m);
+        else c = pair_test<PF32>(sc, S.tab, pr, tp, tq, &m);
         ++pc.full;
     }
     rcode[lane] = c;
@@ -371,8 +437,9 @@ __device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S
     __syncwarp();
 }
 
-/* One chunk's ordered pass with deferral: the direction certificate runs
- * where a pair is found; pairs it does not settle are queued. */
+/* One chunk's ordered pass with deferral: the pairs whose certificates
+ * failed (need, from cert_scan) are queued in pair order. */
+template <bool FAST>
 __device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView& S, int j0, unsigned need,
                                             unsigned todo, LaneState& st, PairCounts& pc)
 {
@@ -381,21 +448,11 @@ __device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView&
     while (todo) {
         const int k = __ffs(todo) - 1;
         todo &= todo - 1u;
-        bool full = false;
-        if (st.active && ((need >> k) & 1u)) {
-            const int j = j0 + k;
-            bool used_dir;
-            if (pair_certified(sc, S.tab, S.pairs[j], S.pairs_b[j], S.cen, S.frames, &used_dir, j)) {
-                if (used_dir) ++pc.dir;
-                else ++pc.far;
-            } else {
-                full = true;
-            }
-        }
+        const bool full = st.active && ((need >> k) & 1u);
         defer_push(S.defer, n, full, k);
-        if (n >= 32) defer_run(sc, S, j0, n, 32, st, pc);
+        if (n >= 32) defer_run<FAST>(sc, S, j0, n, 32, st, pc);
     }
-    while (n > 0) defer_run(sc, S, j0, n, n < 32 ? n : 32, st, pc);
+    while (n > 0) defer_run<FAST>(sc, S, j0, n, n < 32 ? n : 32, st, pc);
 }
 
 /* Appends the items of the lanes with `want` set, one atomic per warp. */
@@ -426,6 +483,7 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
 /* ------------------------------------------------------------------ */
 
 /* Configurations i0 .. i0+count-1 (count <= 32), one per lane. */
+template <bool FAST>
 __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const SceneView& S, const float* __restrict__ q,
                                                    long long offset, long long i0, int count, int* __restrict__ res,
                                                    int band_on, float band, uint2* __restrict__ queue, unsigned qcap,
@@ -443,20 +501,18 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
         for (int j = 0; j < sc.ndof; ++j)
             if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
     }
-    if (active) forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
+    if (active) lane_fk<FAST>(sc, S, qi);
     LaneState st{code, 0.0f, PF32::inf(), active, DEFER_NONE};
-    /* pairs in chunks of 32: the order-free distance scan, then the
-       remaining pairs of the chunk in the reference's order, their exact
+    /* pairs in chunks of 32: the order-free certificate scan, then the
+       pairs left for the exact test in the reference's order, their exact
        tests deferred and run by the whole warp */
 #pragma unroll 1
     for (int j0 = 0; j0 < sc.npairs; j0 += 32) {
         if (!__any_sync(FULL_MASK, st.active)) break;
         const int jn = min(32, sc.npairs - j0);
-        unsigned need = far_scan(S, j0, jn);
-        if (!st.active) need = 0u;
-        else pc.far += (unsigned)(jn - __popc(need));
+        const unsigned need = cert_scan<false>(sc, S, j0, jn, st.active, pc);
         const unsigned todo = __reduce_or_sync(FULL_MASK, need);
-        defer_chunk(sc, S, j0, need, todo, st, pc);
+        defer_chunk<FAST>(sc, S, j0, need, todo, st, pc);
     }
     code = st.code;
     const float mmin = st.mmin, mdec = st.mdec;
@@ -468,7 +524,7 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
     warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), queue, qcap, ctl);
 }
 
-template <bool SMEM>
+template <bool SMEM, bool FAST>
 __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict__ q,
                                             long long n, long long offset,
                                             int* __restrict__ res, int band_on, float band,
@@ -476,7 +532,7 @@ __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict
                                             Control* ctl)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const SceneView S = stage_scene<SMEM>(sc, smem);
+    const SceneView S = stage_scene<SMEM, true>(sc, smem);
     const int lane = threadIdx.x & 31;
     unsigned long long exec = 0;
     PairCounts pc = {0, 0, 0};
@@ -486,8 +542,8 @@ __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict
         base = __shfl_sync(FULL_MASK, base, 0);
         if (base >= (unsigned long long)n) break;
         const long long left = n - (long long)base;
-        check_config_chunk(sc, S, q, offset, (long long)base, left < 32 ? (int)left : 32, res, band_on, band,
-                           queue, qcap, ctl, pc, exec);
+        check_config_chunk<FAST>(sc, S, q, offset, (long long)base, left < 32 ? (int)left : 32, res, band_on,
+                                 band, queue, qcap, ctl, pc, exec);
     }
     exec = warp_sum(exec);
     if (lane == 0 && exec) atomicAdd(&ctl->configs_exec, exec);
@@ -522,7 +578,7 @@ __device__ __forceinline__ int edge_seg_count(int R, int seg_rounds)
  * max for all steps, the same merge as the FP64 recheck) and a segment
  * stops once key[e] holds a decision that none of its remaining rounds can
  * improve on. */
-template <int POLICY, bool SPLIT = false>
+template <int POLICY, bool SPLIT, bool FAST>
 __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& S, const float* __restrict__ qs,
                                            const float* __restrict__ qe, long long e, long long offset, float dq,
                                            unsigned* __restrict__ key, int band_on, float band,
@@ -571,7 +627,7 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         float qi[GPRM_MAX_FRAMES];
         if (valid) {
             edge_step_config(qs, qe, e, offset, sc.ndof, t, tn, qi);
-            forward_kinematics_smem(sc, S.tab, qi, S.frames, S.cen);
+            lane_fk<FAST>(sc, S, qi);
         }
         const unsigned valid_mask = __ballot_sync(FULL_MASK, valid);
         if (lane == 0) exec += __popc(valid_mask);
@@ -582,26 +638,23 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         int cut = 32;   /* lanes above the highest-priority colliding lane no longer matter */
         int jend = 0;   /* pairs processed by the warp */
         bool stop = false;
-        /* pairs in chunks of 32: the order-free distance scan, then the
-           remaining pairs of the chunk in the reference's order; a code can
-           only change at a remaining pair, so the vote runs only there */
+        /* pairs in chunks of 32: the order-free certificate scan, then the
+           pairs left for the exact test in the reference's order; a code can
+           only change at such a pair, so the vote runs only there */
 #pragma unroll 1
         for (int j0 = 0; j0 < sc.npairs && !stop; j0 += 32) {
             if (!__any_sync(FULL_MASK, active)) break;
             const int jn = min(32, sc.npairs - j0);
-            unsigned need = far_scan_swept(S, j0, jn);
-            if (!active) need = 0u;
-            else pc.far += (unsigned)(jn - __popc(need));
+            const unsigned need = cert_scan<true>(sc, S, j0, jn, active, pc);
             unsigned todo = __reduce_or_sync(FULL_MASK, need);
             while (todo) {
                 const int k = __ffs(todo) - 1;
                 todo &= todo - 1u;
                 if (active && ((need >> k) & 1u)) {
                     float m;
-                    bool hm;
-                    int rr = eval_pair(sc, S, j0 + k, &m, &hm, pc);
+                    const int rr = eval_pair<FAST>(sc, S, j0 + k, &m, pc);
                     if (rr != 0) { code = rr; mdec = m; active = false; }
-                    else if (hm) mmin = min_nan(mmin, m);
+                    else mmin = min_nan(mmin, m);
                 }
                 jend = j0 + k + 1;
                 bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
@@ -653,7 +706,7 @@ __device__ __forceinline__ void flush_edge_counts(unsigned long long exec, unsig
 /* SPLIT: the work items are the segments of the edges, edge e owning
  * items [seg_off[e], seg_off[e+1]) (seg_off from k_edge_segments);
  * otherwise one item per edge and seg_off is unused. */
-template <bool SMEM, int POLICY, bool SPLIT>
+template <bool SMEM, int POLICY, bool SPLIT, bool FAST>
 __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__ qs,
                                           const float* __restrict__ qe, long long n,
                                           long long offset, float dq, unsigned* __restrict__ key,
@@ -662,7 +715,7 @@ __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__
                                           int seg_rounds)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const SceneView S = stage_scene<SMEM>(sc, smem);
+    const SceneView S = stage_scene<SMEM, false>(sc, smem);
     const int lane = threadIdx.x & 31;
     unsigned long long exec = 0, nominal = 0;
     PairCounts pc = {0, 0, 0};
@@ -672,8 +725,8 @@ __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__
             if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
             eu = __shfl_sync(FULL_MASK, eu, 0);
             if (eu >= (unsigned long long)n) break;
-            check_edge<POLICY>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, queue, qcap, ctl, pc,
-                               exec, nominal);
+            check_edge<POLICY, false, FAST>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, queue,
+                                            qcap, ctl, pc, exec, nominal);
         }
         flush_edge_counts(exec, nominal, pc, ctl);
         return;
@@ -700,8 +753,8 @@ __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__
         if (eu >= items) break;
         e = __shfl_sync(FULL_MASK, e, 0);
         seg = __shfl_sync(FULL_MASK, seg, 0);
-        check_edge<POLICY, true>(sc, S, qs, qe, e, offset, dq, key, band_on, band, queue, qcap, ctl, pc, exec,
-                                 nominal, seg, seg_rounds);
+        check_edge<POLICY, true, FAST>(sc, S, qs, qe, e, offset, dq, key, band_on, band, queue, qcap, ctl, pc,
+                                       exec, nominal, seg, seg_rounds);
     }
     flush_edge_counts(exec, nominal, pc, ctl);
 }
@@ -870,42 +923,98 @@ static cudaError_t variant_warps(const void* fn, int threads, size_t smem, int* 
     return err;
 }
 
-static const void* kernel_fn(int vertex_kernel, bool smem, int policy, bool split = false)
+template <bool FAST>
+static const void* kernel_fn_t(int vertex_kernel, bool smem, int policy, bool split)
 {
-    if (vertex_kernel) return smem ? (const void*)k_check_configs<true> : (const void*)k_check_configs<false>;
+    if (vertex_kernel) return smem ? (const void*)k_check_configs<true, FAST> : (const void*)k_check_configs<false, FAST>;
     if (split) {
         if (policy == EDGE_EARLY_EXIT)
-            return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT, true> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT, true>;
-        return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS, true> : (const void*)k_check_edges<false, EDGE_ALL_STEPS, true>;
+            return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT, true, FAST>
+                        : (const void*)k_check_edges<false, EDGE_EARLY_EXIT, true, FAST>;
+        return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS, true, FAST>
+                    : (const void*)k_check_edges<false, EDGE_ALL_STEPS, true, FAST>;
     }
     if (policy == EDGE_EARLY_EXIT)
-        return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT, false> : (const void*)k_check_edges<false, EDGE_EARLY_EXIT, false>;
-    return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS, false> : (const void*)k_check_edges<false, EDGE_ALL_STEPS, false>;
+        return smem ? (const void*)k_check_edges<true, EDGE_EARLY_EXIT, false, FAST>
+                    : (const void*)k_check_edges<false, EDGE_EARLY_EXIT, false, FAST>;
+    return smem ? (const void*)k_check_edges<true, EDGE_ALL_STEPS, false, FAST>
+                : (const void*)k_check_edges<false, EDGE_ALL_STEPS, false, FAST>;
+}
+
+static const void* kernel_fn(int vertex_kernel, bool smem, int policy, bool split = false, bool fast = false)
+{
+    return fast ? kernel_fn_t<true>(vertex_kernel, smem, policy, split)
+                : kernel_fn_t<false>(vertex_kernel, smem, policy, split);
+}
+
+/* Sets a kernel's preferred shared-memory carveout (percent of the SM's
+ * maximum; -1 restores the default) when it differs from the value last
+ * set for it, so that every launch runs with its own handle's split of the
+ * SM's L1 and shared memory. */
+static cudaError_t apply_carveout(const void* fn, int pct)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> last;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = last.find(fn);
+    const int cur = it == last.end() ? -1 : it->second;
+    if (cur == pct) return cudaSuccess;
+    cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    if (err == cudaSuccess) last[fn] = pct;
+    return err;
 }
 
 cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads, int scene_in_smem,
-                             LaunchCfg* cfg)
+                             LaunchCfg* cfg, int blocks_cap)
 {
     int dev = 0, sms = 0, optin = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    size_t smem = frame_smem_bytes(sc, threads) + (scene_in_smem ? scene_smem_bytes(sc) : 0);
+    size_t smem = frame_smem_bytes(sc, threads, vertex_kernel != 0) + (scene_in_smem ? scene_smem_bytes(sc) : 0);
     for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol)
-        for (int split = 0; split < (vertex_kernel ? 1 : 2); ++split) {
-            err = open_smem_cap(kernel_fn(vertex_kernel, scene_in_smem != 0, pol, split != 0), optin, smem);
-            if (err != cudaSuccess) return err;
-        }
-    int warps = 0;
+        for (int split = 0; split < (vertex_kernel ? 1 : 2); ++split)
+            for (int fast = 0; fast < 2; ++fast) {
+                err = open_smem_cap(kernel_fn(vertex_kernel, scene_in_smem != 0, pol, split != 0, fast != 0), optin,
+                                    smem);
+                if (err != cudaSuccess) return err;
+            }
+    /* occupancy of the slower-to-fit of the two arithmetic variants, with
+       the default carveout */
+    for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol)
+        for (int split = 0; split < (vertex_kernel ? 1 : 2); ++split)
+            for (int fast = 0; fast < 2; ++fast) {
+                err = apply_carveout(kernel_fn(vertex_kernel, scene_in_smem != 0, pol, split != 0, fast != 0), -1);
+                if (err != cudaSuccess) return err;
+            }
+    int warps = 0, warps_fast = 0;
     err = variant_warps(kernel_fn(vertex_kernel, scene_in_smem != 0, 0), threads, smem, &warps);
     if (err != cudaSuccess) return err;
+    err = variant_warps(kernel_fn(vertex_kernel, scene_in_smem != 0, 0, false, true), threads, smem, &warps_fast);
+    if (err != cudaSuccess) return err;
+    if (warps_fast < warps) warps = warps_fast;
     if (warps < 1) return cudaErrorInvalidConfiguration;
+    int per_sm = warps / (threads / 32);
+    int carveout = -1;
+    if (blocks_cap > 0 && blocks_cap < per_sm) {
+        /* fewer resident blocks: a carveout just large enough for them (each
+           block also reserves 1 KB), the rest of the SM's combined L1 and
+           shared memory left to L1 */
+        int smem_sm = 0;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        per_sm = blocks_cap;
+        const double need = (double)per_sm * (double)(smem + 1024);
+        carveout = smem_sm > 0 ? (int)ceil(100.0 * need / smem_sm) : -1;
+        if (carveout > 100) carveout = 100;
+    }
     cfg->threads = threads;
     cfg->smem_bytes = smem;
     cfg->scene_in_smem = scene_in_smem;
-    cfg->blocks = sms * (warps / (threads / 32));
-    cfg->warps_per_sm = warps;
+    cfg->blocks = sms * per_sm;
+    cfg->blocks_per_sm = per_sm;
+    cfg->warps_per_sm = per_sm * (threads / 32);
+    cfg->carveout = carveout;
     return cudaSuccess;
 }
 
@@ -936,12 +1045,16 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
                                  unsigned qcap, Control* ctl, cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
-    if (cfg.scene_in_smem)
-        k_check_configs<true><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on,
-                                                                              band, queue, qcap, ctl);
-    else
-        k_check_configs<false><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on,
-                                                                               band, queue, qcap, ctl);
+    {
+        cudaError_t err = apply_carveout(kernel_fn(1, cfg.scene_in_smem != 0, 0, false, sc.fast != 0), cfg.carveout);
+        if (err != cudaSuccess) return err;
+    }
+#define GPRM_CFG_LAUNCH(SM_, FAST_)                                                                            \
+    k_check_configs<SM_, FAST_><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on, \
+                                                                                band, queue, qcap, ctl)
+    if (cfg.scene_in_smem) { if (sc.fast) GPRM_CFG_LAUNCH(true, true); else GPRM_CFG_LAUNCH(true, false); }
+    else { if (sc.fast) GPRM_CFG_LAUNCH(false, true); else GPRM_CFG_LAUNCH(false, false); }
+#undef GPRM_CFG_LAUNCH
     return cudaGetLastError();
 }
 
@@ -958,10 +1071,17 @@ cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const f
         if (err != cudaSuccess) return err;
     }
     size_t sm = cfg.smem_bytes;
+    {
+        cudaError_t err = apply_carveout(kernel_fn(0, cfg.scene_in_smem != 0, policy, seg_off != nullptr, sc.fast != 0),
+                                         cfg.carveout);
+        if (err != cudaSuccess) return err;
+    }
+#define GPRM_EDGE_LAUNCH2(SM_, POL_, SPLIT_, FAST_)                                                           \
+    k_check_edges<SM_, POL_, SPLIT_, FAST_><<<cfg.blocks, cfg.threads, sm, st>>>(                                 \
+        sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl, seg_off, seg_rounds)
 #define GPRM_EDGE_LAUNCH(SM_, POL_, SPLIT_)                                                                   \
-    k_check_edges<SM_, POL_, SPLIT_><<<cfg.blocks, cfg.threads, sm, st>>>(sc, qs, qe, n, offset, dq, key, band_on, \
-                                                                          band, queue, qcap, ctl, seg_off,       \
-                                                                          seg_rounds)
+    do { if (sc.fast) GPRM_EDGE_LAUNCH2(SM_, POL_, SPLIT_, true); else GPRM_EDGE_LAUNCH2(SM_, POL_, SPLIT_, false); } \
+    while (0)
     const bool split = seg_off != nullptr;
     if (policy == EDGE_EARLY_EXIT) {
         if (cfg.scene_in_smem) { if (split) GPRM_EDGE_LAUNCH(true, EDGE_EARLY_EXIT, true); else GPRM_EDGE_LAUNCH(true, EDGE_EARLY_EXIT, false); }
@@ -971,6 +1091,7 @@ cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const f
         else { if (split) GPRM_EDGE_LAUNCH(false, EDGE_ALL_STEPS, true); else GPRM_EDGE_LAUNCH(false, EDGE_ALL_STEPS, false); }
     }
 #undef GPRM_EDGE_LAUNCH
+#undef GPRM_EDGE_LAUNCH2
     return cudaGetLastError();
 }
 
@@ -1012,6 +1133,7 @@ __device__ __forceinline__ int problem_of(const BatchView& B, long long it)
 }
 
 /* Makes problem p's descriptor the warp's current scene (warp-uniform p). */
+template <bool VERTEX>
 __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene* wsc, float* frames, SceneView& S)
 {
     __syncwarp();
@@ -1023,13 +1145,15 @@ __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene
     S.pairs = wsc->pairs;
     S.pairs_b = wsc->pairs_b;
     S.far = wsc->far;
-    S.far_slot = wsc->far_slot;
+    S.scan_c = wsc->scan_c;
+    S.scan_b = wsc->scan_b;
     S.frames = frames;
     S.cen = frames + (size_t)wsc->ndof * 12 * 32;
-    S.sweep = sweep_area(*wsc, frames);
-    S.defer = defer_area(*wsc, frames);
+    S.sweep = sweep_area<VERTEX>(*wsc, frames);
+    S.defer = defer_area<VERTEX>(*wsc, frames);
 }
 
+template <bool FAST>
 __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __restrict__ q, long long offset,
                                                   int* __restrict__ res, int band_on, float band,
                                                   uint2* __restrict__ queue, unsigned qcap, Control* ctl)
@@ -1048,15 +1172,16 @@ __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __re
         c = __shfl_sync(FULL_MASK, c, 0);
         if (c >= (unsigned long long)B.nwork) break;
         const int4 ch = B.chunks[c];
-        if (ch.x != cur) { switch_scene(B, ch.x, wsc, frames, S); cur = ch.x; }
-        check_config_chunk(*wsc, S, q, offset, (long long)ch.y, ch.z, res, band_on, band, queue, qcap, ctl, pc, exec);
+        if (ch.x != cur) { switch_scene<true>(B, ch.x, wsc, frames, S); cur = ch.x; }
+        check_config_chunk<FAST>(*wsc, S, q, offset, (long long)ch.y, ch.z, res, band_on, band, queue, qcap, ctl, pc,
+                                 exec);
     }
     exec = warp_sum(exec);
     if (lane == 0 && exec) atomicAdd(&ctl->configs_exec, exec);
     flush_counts(pc, ctl);
 }
 
-template <int POLICY>
+template <int POLICY, bool FAST>
 __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __restrict__ qs, const float* __restrict__ qe,
                                                 long long offset, unsigned* __restrict__ key, int band_on, float band,
                                                 uint2* __restrict__ queue, unsigned qcap, Control* ctl)
@@ -1075,9 +1200,9 @@ __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __rest
         eu = __shfl_sync(FULL_MASK, eu, 0);
         if (eu >= (unsigned long long)B.nwork) break;
         const int p = problem_of(B, (long long)eu);
-        if (p != cur) { switch_scene(B, p, wsc, frames, S); cur = p; }
-        check_edge<POLICY>(*wsc, S, qs, qe, (long long)eu, offset, wsc->dq, key, band_on, band, queue, qcap, ctl,
-                           pc, exec, nominal);
+        if (p != cur) { switch_scene<false>(B, p, wsc, frames, S); cur = p; }
+        check_edge<POLICY, false, FAST>(*wsc, S, qs, qe, (long long)eu, offset, wsc->dq, key, band_on, band, queue,
+                                        qcap, ctl, pc, exec, nominal);
     }
     flush_edge_counts(exec, nominal, pc, ctl);
 }
@@ -1100,11 +1225,14 @@ __global__ void __launch_bounds__(128) k_recheck_multi(BatchView B, int kind, co
     if (flips) atomicAdd(&ctl->band_flips, flips);
 }
 
-static const void* batch_kernel_fn(int vertex_kernel, int policy)
+static const void* batch_kernel_fn(int vertex_kernel, int policy, bool fast)
 {
-    if (vertex_kernel) return (const void*)k_check_configs_multi;
-    return policy == EDGE_EARLY_EXIT ? (const void*)k_check_edges_multi<EDGE_EARLY_EXIT>
-                                     : (const void*)k_check_edges_multi<EDGE_ALL_STEPS>;
+    if (vertex_kernel) return fast ? (const void*)k_check_configs_multi<true> : (const void*)k_check_configs_multi<false>;
+    if (fast)
+        return policy == EDGE_EARLY_EXIT ? (const void*)k_check_edges_multi<EDGE_EARLY_EXIT, true>
+                                         : (const void*)k_check_edges_multi<EDGE_ALL_STEPS, true>;
+    return policy == EDGE_EARLY_EXIT ? (const void*)k_check_edges_multi<EDGE_EARLY_EXIT, false>
+                                     : (const void*)k_check_edges_multi<EDGE_ALL_STEPS, false>;
 }
 
 cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg)
@@ -1117,11 +1245,11 @@ cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int th
     const int nw = threads / 32;
     size_t smem = (size_t)nw * SCENE_CACHE_BYTES + (size_t)nw * B.lane_floats * 32 * sizeof(float);
     for (int pol = 0; pol < (vertex_kernel ? 1 : 2); ++pol) {
-        err = open_smem_cap(batch_kernel_fn(vertex_kernel, pol), optin, smem);
+        err = open_smem_cap(batch_kernel_fn(vertex_kernel, pol, B.fast != 0), optin, smem);
         if (err != cudaSuccess) return err;
     }
     int warps = 0;
-    err = variant_warps(batch_kernel_fn(vertex_kernel, 0), threads, smem, &warps);
+    err = variant_warps(batch_kernel_fn(vertex_kernel, 0, B.fast != 0), threads, smem, &warps);
     if (err != cudaSuccess) return err;
     if (warps < 1) return cudaErrorInvalidConfiguration;
     cfg->threads = threads;
@@ -1129,6 +1257,8 @@ cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int th
     cfg->scene_in_smem = 0;
     cfg->blocks = sms * (warps / nw);
     cfg->warps_per_sm = warps;
+    cfg->blocks_per_sm = warps / nw;
+    cfg->carveout = -1;
     return cudaSuccess;
 }
 
@@ -1137,8 +1267,12 @@ cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg,
                                        cudaStream_t st)
 {
     if (B.nwork <= 0) return cudaSuccess;
-    k_check_configs_multi<<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on, band, queue,
-                                                                          qcap, ctl);
+    if (B.fast)
+        k_check_configs_multi<true><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on, band,
+                                                                                    queue, qcap, ctl);
+    else
+        k_check_configs_multi<false><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on,
+                                                                                     band, queue, qcap, ctl);
     return cudaGetLastError();
 }
 
@@ -1147,12 +1281,13 @@ cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, c
                                      uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
 {
     if (B.nwork <= 0) return cudaSuccess;
-    if (policy == EDGE_EARLY_EXIT)
-        k_check_edges_multi<EDGE_EARLY_EXIT><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(
-            B, qs, qe, offset, key, band_on, band, queue, qcap, ctl);
-    else
-        k_check_edges_multi<EDGE_ALL_STEPS><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(
-            B, qs, qe, offset, key, band_on, band, queue, qcap, ctl);
+#define GPRM_MULTI_LAUNCH(POL_, FAST_)                                                                       \
+    k_check_edges_multi<POL_, FAST_><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, qs, qe, offset, key,    \
+                                                                                     band_on, band, queue, qcap, \
+                                                                                     ctl)
+    if (policy == EDGE_EARLY_EXIT) { if (B.fast) GPRM_MULTI_LAUNCH(EDGE_EARLY_EXIT, true); else GPRM_MULTI_LAUNCH(EDGE_EARLY_EXIT, false); }
+    else { if (B.fast) GPRM_MULTI_LAUNCH(EDGE_ALL_STEPS, true); else GPRM_MULTI_LAUNCH(EDGE_ALL_STEPS, false); }
+#undef GPRM_MULTI_LAUNCH
     return cudaGetLastError();
 }
 

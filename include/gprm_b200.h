@@ -55,6 +55,17 @@ extern "C" {
 /* FP32, then every check whose separation margin is inside the band is
  * recomputed in FP64 and the FP64 verdict is returned for it. */
 #define GPRM_MODE_FP64_BAND   1
+/* Flag, or-ed with either mode: the FP32 pass runs the same algorithm in
+ * contracted arithmetic (fused multiply-add, hardware reciprocal square
+ * roots, sincosf) and starts the first support climbs from per-polytope
+ * direction tables.  Codes may differ from the reference's by rounding
+ * (iteration counts, and verdicts of checks within rounding of contact);
+ * with GPRM_MODE_FP64_BAND the free/not-free verdicts equal the
+ * reference's for every check whose margin lies outside the band, and the
+ * checks inside it get their FP64 verdict.  No counterpart in the
+ * reference (its kernels and CPU path share the FP32 arithmetic of
+ * collision4.h:226-332). */
+#define GPRM_MODE_FAST        2
 
 /* Edge evaluation (gprm_set_edge_policy). */
 /* Stop an edge at its first colliding step; res[e] is that step's code. */
@@ -403,6 +414,14 @@ int gprm_sample_near(int ndof, const float* nodes, int n, int stride, const int*
  * column layout of trafo4 (geo4.h:24). */
 int gprm_debug_fk(gprm_space* h, const float* q, float* out);
 
+/* Support candidates of the fast path (GPRM_MODE_FAST) for polytope
+ * `polytope` and direction bin `bin` (0..53: cube face 0..5 = +x,-x,+y,-y,
+ * +z,-z, then the 3 x 3 cell of the other two components, each compared
+ * with a third of the face component): writes up to cap vertex indices
+ * (ascending) and returns their count, or a negative status.  Host data,
+ * available after gprm_create; no counterpart in the reference. */
+int gprm_debug_support_candidates(const gprm_space* h, int polytope, int bin, int* idx, int cap);
+
 /* Streaming multiprocessors of the handle's device (0 before init). */
 int gprm_device_sm_count(const gprm_space* h);
 
@@ -412,6 +431,13 @@ int gprm_device_sm_count(const gprm_space* h);
  * L1 (0).  Fails without changing anything if the shape does not fit.
  * gprm_init picks the shape with the most resident warps. */
 int gprm_set_launch(gprm_space* h, int vertex_kernel, int threads, int scene_in_smem);
+/* The same with at most blocks_per_sm resident blocks per SM (0 = as many
+ * as fit): the kernel's shared-memory carveout is then set, before each
+ * launch with this shape, to what those blocks need, and the rest of the
+ * SM's combined L1/shared memory caches the scene table and the pair
+ * records.  Fewer resident warps, more L1.  No counterpart in the
+ * reference (one CUDA thread per edge step, robotconfigspace.cpp:676-693). */
+int gprm_set_launch_shape(gprm_space* h, int vertex_kernel, int threads, int scene_in_smem, int blocks_per_sm);
 int gprm_get_launch(const gprm_space* h, int vertex_kernel, int* threads, int* scene_in_smem,
                     int* warps_per_sm);
 

@@ -612,6 +612,67 @@ int orc_edge_steps(void* h, const float* qs, const float* qe, int n, int offset,
     return 0;
 }
 
+/* Verdict classes of edges, for comparing any FP32 checker's free/not-free
+ * verdicts with the reference's at scale.  From the FP32 results of every
+ * step (mode & 4: F32D trigonometry, else libm's):
+ *   cls[l] = 1  a step collides outside the band (code > 0 with margin
+ *               <= -band): the edge is "not free" whatever the rounding
+ *            0  every step is free outside the band (margin >= band): "free"
+ *            2  neither: the verdict is decided inside the band
+ *   band_res[l]     the FP32 + FP64-band result (code of the last colliding
+ *                   step, in-band steps recomputed in FP64), the value the
+ *                   GPU's band mode must reproduce
+ *   inband_steps[l] the number of in-band steps
+ * (band_res and inband_steps may be NULL.)  Edge semantics as in
+ * orc_check_edges (robotconfigspace.cpp:378-465, 694-705). */
+int orc_edge_classify(void* h, const float* qs, const float* qe, int n, int offset, float dq, int mode,
+                      float band, unsigned char* cls, int* band_res, int* inband_steps)
+{
+    const Scene& s = *(const Scene*)h;
+    std::vector<int> tn(n > 0 ? n : 1);
+    orc_edge_testnum(qs, qe, n, offset, s.ndof, dq, tn.data());
+    float q[GPRM_MAX_DOF];
+    for (int l = 0; l < n; ++l) {
+        bool coll_out = false, any_in = false;
+        int last = 0, nin = 0;
+        for (int t = 0; t < tn[l]; ++t) {
+            edge_step_config(qs, qe, l, offset, s.ndof, t, tn[l], q);
+            float m = 0.0f;
+            int c = check32(s, q, &m, mode & 4);
+            const bool ib = in_band(c, m, band);
+            if (ib) {
+                any_in = true;
+                ++nin;
+                c = check_config<F64>(s, q, NULL);
+            } else if (c != 0) {
+                coll_out = true;
+            }
+            if (c != 0) last = c;
+        }
+        cls[l] = coll_out ? 1 : (any_in ? 2 : 0);
+        if (band_res) band_res[l] = last;
+        if (inband_steps) inband_steps[l] = nin;
+    }
+    return 0;
+}
+
+/* The same classes for vertex checks (indicator(q) semantics: out of
+ * bounds is code 1, decided outside the band); band_code gets the FP32 +
+ * FP64-band code. */
+int orc_config_classify(void* h, const float* q, int n, int offset, int mode, float band, unsigned char* cls,
+                        int* band_code)
+{
+    std::vector<int> code(n > 0 ? n : 1);
+    std::vector<float> margin(n > 0 ? n : 1);
+    std::vector<unsigned char> ib(n > 0 ? n : 1);
+    orc_check_configs(h, q, n, offset, 2 | (mode & 4), band, code.data(), margin.data(), ib.data());
+    for (int i = 0; i < n; ++i) {
+        cls[i] = ib[i] ? 2 : (code[i] != 0 ? 1 : 0);
+        if (band_code) band_code[i] = code[i];
+    }
+    return 0;
+}
+
 /* Counted FP32 work of vertex checks (no bounds short cut is taken for
  * in-bounds configurations; out-of-bounds ones count nothing).
  * out[0..9] = adds, muls, divs, sqrts, trig, compares, pairs, iterations,

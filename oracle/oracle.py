@@ -56,6 +56,9 @@ def _load_oracle():
     lib.orc_count_ops_edges.argtypes = [C.c_void_p, _F, _F, C.c_int, C.c_int, C.c_float, _D]
     lib.orc_forward_kinematics.argtypes = [C.c_void_p, _F, C.c_int, _F]
     lib.orc_sincos64.argtypes = [_D, C.c_int, _D, _D]
+    lib.orc_edge_classify.argtypes = [C.c_void_p, _F, _F, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float,
+                                      _U8, _I, _I]
+    lib.orc_config_classify.argtypes = [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_float, _U8, _I]
     return lib
 
 
@@ -104,6 +107,50 @@ class Oracle:
                                  C.byref(steps))
         return res, int(steps.value)
 
+    def edge_classify(self, qs: np.ndarray, qe: np.ndarray, dq: float, mode: int = DEVICE_TRIG,
+                      band: float = 1e-5, threads: int = 1):
+        """Verdict classes of edges (orc_edge_classify): returns (cls uint8:
+        0 free outside the band, 1 colliding outside the band, 2 decided in
+        the band; band_res int32, the FP32 + FP64-band result; inband_steps
+        int32).  threads > 1 splits the edges over host threads (the scene
+        is read-only and ctypes releases the GIL during the call)."""
+        n = qs.shape[0]
+        cls = np.zeros(n, np.uint8)
+        res = np.zeros(n, np.int32)
+        nin = np.zeros(n, np.int32)
+
+        def run(lo, hi):
+            m = hi - lo
+            if m <= 0:
+                return
+            bs, be = soa(qs[lo:hi]), soa(qe[lo:hi])
+            c, r, k = np.zeros(m, np.uint8), np.zeros(m, np.int32), np.zeros(m, np.int32)
+            self.lib.orc_edge_classify(self.h, _f(bs), _f(be), m, m, dq, mode, band, c.ctypes.data_as(_U8),
+                                       _i(r), _i(k))
+            cls[lo:hi], res[lo:hi], nin[lo:hi] = c, r, k
+
+        _split(run, n, threads)
+        return cls, res, nin
+
+    def config_classify(self, q: np.ndarray, mode: int = DEVICE_TRIG, band: float = 1e-5, threads: int = 1):
+        """Verdict classes of vertex checks (orc_config_classify): returns
+        (cls uint8 as in edge_classify, band_code int32)."""
+        n = q.shape[0]
+        cls = np.zeros(n, np.uint8)
+        code = np.zeros(n, np.int32)
+
+        def run(lo, hi):
+            m = hi - lo
+            if m <= 0:
+                return
+            buf = soa(q[lo:hi])
+            c, k = np.zeros(m, np.uint8), np.zeros(m, np.int32)
+            self.lib.orc_config_classify(self.h, _f(buf), m, m, mode, band, c.ctypes.data_as(_U8), _i(k))
+            cls[lo:hi], code[lo:hi] = c, k
+
+        _split(run, n, threads)
+        return cls, code
+
     def edge_steps(self, qs, qe, dq, mode: int = 0):
         n = qs.shape[0]
         tn = self.testnum(qs, qe, dq)
@@ -140,6 +187,40 @@ class Oracle:
         qq = np.ascontiguousarray(np.asarray(q, np.float32))
         self.lib.orc_forward_kinematics(self.h, _f(qq), mode, _f(out))
         return out.reshape(self.scene.ndof + 1, 4, 3)
+
+
+def _split(fn, n: int, threads: int, chunk: int = 64):
+    """Runs fn(lo, hi) over [0, n) in pieces of `chunk` items on `threads`
+    host threads (work-stealing order; each piece is independent)."""
+    threads = max(1, int(threads))
+    if threads == 1 or n <= chunk:
+        fn(0, n)
+        return
+    import threading
+    lock = threading.Lock()
+    nxt = [0]
+    err = []
+
+    def worker():
+        while True:
+            with lock:
+                lo = nxt[0]
+                nxt[0] += chunk
+            if lo >= n or err:
+                return
+            try:
+                fn(lo, min(n, lo + chunk))
+            except Exception as e:   # surfaced after join
+                err.append(e)
+                return
+
+    ts = [threading.Thread(target=worker) for _ in range(threads)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if err:
+        raise err[0]
 
 
 def sincos64(x: np.ndarray):

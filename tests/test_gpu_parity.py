@@ -281,7 +281,7 @@ def test_handles_keep_their_launch_shapes():
     sc, z = load_golden("hull6")
     a = space(sc, float(z["dq"]), mode=GPRM_MODE_FP64_BAND)
     want = a.check_configs(z["q"])
-    a.set_launch(True, 256, True)
+    a.set_launch(True, 128, True)
     assert a.get_launch(True)["scene_in_smem"]
     b = space(scenes.make_box4(3), 0.02, mode=GPRM_MODE_FP64_BAND)
     b.check_configs(scenes.uniform_configs(scenes.make_box4(3), 100, 1))

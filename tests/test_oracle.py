@@ -167,3 +167,28 @@ def test_op_counter_consistency():
     # counting does not change results
     codes, _, _ = orc.check_configs(q, O.FP32)
     assert codes.shape == (200,)
+
+
+@pytest.mark.parametrize("name", GOLDEN_NAMES)
+def test_band_classes_agree_with_reference(name):
+    """The oracle's verdict classes (orc_config_classify, orc_edge_classify)
+    against the reference's golden codes: every configuration or edge the
+    oracle decides outside the band has the reference's verdict, and the
+    FP32 + FP64-band results equal the existing band-mode oracle path."""
+    import parity as P
+    sc, z = load_golden(name)
+    dq = float(z["dq"])
+    orc = O.Oracle(sc)
+    cls, band = orc.config_classify(z["q"], threads=4)
+    d = P.verdict_parity(band, z["codes"], cls, band)
+    assert d["reference_vs_class_outside_band"] == 0 and d["mismatches_outside_band"] == 0, d
+    np.testing.assert_array_equal(band, orc.check_configs(z["q"], O.FP32_BAND | O.DEVICE_TRIG)[0])
+    ecls, eband, nin = orc.edge_classify(z["qs"], z["qe"], dq, threads=4)
+    d = P.verdict_parity(eband, z["edge_res"], ecls, eband, nin)
+    assert d["reference_vs_class_outside_band"] == 0 and d["mismatches_outside_band"] == 0, d
+    np.testing.assert_array_equal(eband, orc.check_edges(z["qs"], z["qe"], dq, O.FP32_BAND | O.DEVICE_TRIG)[0])
+    # single-threaded and multi-threaded classification agree
+    c1, b1, n1 = orc.edge_classify(z["qs"], z["qe"], dq, threads=1)
+    np.testing.assert_array_equal(c1, ecls)
+    np.testing.assert_array_equal(b1, eband)
+    np.testing.assert_array_equal(n1, nin)
