@@ -395,39 +395,6 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
             }
         }
     }
-    /* start tables of the fast path: for the centre direction of each
-       direction bin, the support vertex (the first of the maximisers in
-       double) and a table entry that carries it (entry 1 for vertex 0, else
-       the first CRS entry naming it; entry 1 when none does or the offset
-       does not fit 16 bits).  Any entry is a correct start: the climb
-       reaches a maximiser from every vertex. */
-    h->start.assign((size_t)GPRM_START_BINS * h->npoly, 1);
-    for (int k = 0; k < h->npoly; ++k) {
-        const int n = d->poly_n[k], m = d->poly_m[k];
-        for (int b = 0; b < GPRM_START_BINS; ++b) {
-            const int face = b / 9, iu = (b % 9) / 3, iv = b % 3;
-            const double sgn = (face & 1) ? -1.0 : 1.0, u = (iu - 1) * (2.0 / 3.0), v = (iv - 1) * (2.0 / 3.0);
-            double dir[3];
-            if (face < 2) { dir[0] = sgn; dir[1] = u; dir[2] = v; }
-            else if (face < 4) { dir[1] = sgn; dir[2] = u; dir[0] = v; }
-            else { dir[2] = sgn; dir[0] = u; dir[1] = v; }
-            int best = 0;
-            double bd = -1e300;
-            for (int i = 0; i < n; ++i) {
-                const float* x = d->vertices + 3 * (size_t)(voff[k] + i);
-                const double dd = x[0] * dir[0] + x[1] * dir[1] + x[2] * dir[2];
-                if (dd > bd) { bd = dd; best = i; }
-            }
-            int off = 1;
-            if (best != 0)
-                for (int j = 0; j < m; ++j)
-                    if (d->dest[moff[k] + j] == best) {
-                        if (2 + j <= 65535) off = 2 + j;
-                        break;
-                    }
-            h->start[(size_t)GPRM_START_BINS * k + b] = (unsigned short)off;
-        }
-    }
     if ((size_t)sn * GPRM_START_BINS >= (1u << 24)) {
         delete h;
         return fail(nullptr, GPRM_ERR_SCENE, "scene too large for the support candidate lists");
@@ -785,13 +752,12 @@ int gprm_init(gprm_space* h, int rank, int size)
     CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
 
-    /* d_scene: tab | pairs | pairs_b | far | scan_c | scan_b | ppoly | box | start | vtab | vinfo | cbin | cidx */
+    /* d_scene: tab | pairs | pairs_b | far | scan_c | scan_b | ppoly | box | vtab | vinfo | cbin | cidx */
     size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
     size_t fsb = (size_t)h->npairs * sizeof(int2);
     size_t bxo = tb + 5 * pb + fsb, bxb = h->box.size() * sizeof(float4);
     bxo = (bxo + 15) & ~(size_t)15;
-    const size_t sto = bxo + bxb, stb = h->start.size() * sizeof(unsigned short);
-    const size_t vto = (sto + stb + 15) & ~(size_t)15, vtb = h->vtab.size() * sizeof(float4);
+    const size_t vto = (bxo + bxb + 15) & ~(size_t)15, vtb = h->vtab.size() * sizeof(float4);
     const size_t vio = vto + vtb, vib = h->vinfo.size() * sizeof(int2);
     const size_t cbo = (vio + vib + 15) & ~(size_t)15, cbb = h->cbin.size() * sizeof(unsigned);
     const size_t cio = cbo + cbb, cib = h->cidx.size();
@@ -805,7 +771,6 @@ int gprm_init(gprm_space* h, int rank, int size)
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 4 * pb, h->scan_b.data(), pb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb + 5 * pb, h->pair_poly.data(), fsb, cudaMemcpyHostToDevice));
     if (bxb) CUDA_TRY(h, cudaMemcpy(base + bxo, h->box.data(), bxb, cudaMemcpyHostToDevice));
-    if (stb) CUDA_TRY(h, cudaMemcpy(base + sto, h->start.data(), stb, cudaMemcpyHostToDevice));
     if (vtb) CUDA_TRY(h, cudaMemcpy(base + vto, h->vtab.data(), vtb, cudaMemcpyHostToDevice));
     if (vib) CUDA_TRY(h, cudaMemcpy(base + vio, h->vinfo.data(), vib, cudaMemcpyHostToDevice));
     if (cbb) CUDA_TRY(h, cudaMemcpy(base + cbo, h->cbin.data(), cbb, cudaMemcpyHostToDevice));
@@ -834,7 +799,6 @@ int gprm_init(gprm_space* h, int rank, int size)
     s.scan_b = (const float4*)(base + tb + 4 * pb);
     s.ppoly = (const int2*)(base + tb + 5 * pb);
     s.box = bxb ? (const float4*)(base + bxo) : nullptr;
-    s.start = stb ? (const unsigned short*)(base + sto) : nullptr;
     s.vtab = (const float4*)(base + vto);
     s.vinfo = (const int2*)(base + vio);
     s.cbin = cbb ? (const unsigned*)(base + cbo) : nullptr;

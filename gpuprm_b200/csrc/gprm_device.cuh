@@ -81,12 +81,8 @@ struct DevScene {
     int slot_block[GPRM_MAX_SLOTS];      /* its table block (entry 0 = ball) */
     /* fast arithmetic (GPRM_MODE_FAST): the kernels run pair_test_fast */
     int fast;
-    /* per polytope GPRM_START_BINS start entries (offsets into its table
-       block) of the first support climbs, indexed by dir_bin */
-    const unsigned short* start;
     /* every polytope's vertices as table entries (xyz, packed w), and per
-       polytope (first entry, vertex count): the fast path's support search
-       over all vertices */
+       polytope (first entry, vertex count): the fast path's support search */
     const float4* vtab;
     const int2* vinfo;
     /* per polytope and direction bin: (byte offset into cidx << 8 | count)
@@ -632,17 +628,18 @@ __device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float
  *     (rsqrtf, <= 2 ulp) instead of IEEE sqrt and division, and the
  *     half-plane basis (orthtrafo23) by one reciprocal square root instead
  *     of four divisions;
- *   - the first iteration's two support climbs start at the support vertex
- *     of a direction bin (dir_bin, a table per polytope) instead of vertex
- *     0.  On a convex polytope a first-improvement climb ends at a maximiser
- *     of the dot product from any start, so the support vertex is the same
- *     one unless several vertices tie within rounding.
+ *   - support vertices by a maximum over the few candidates of the
+ *     direction's bin (fsupport_cand2) instead of the first-improvement
+ *     climb from the previous support; the climb ends at a maximiser of the
+ *     dot product too (on a convex polytope every vertex without an
+ *     improving neighbour is one), so the two agree unless several vertices
+ *     tie within rounding.
  * Results differ from the reference's FP32 arithmetic by rounding: codes
  * (iteration counts) may differ, free/not-free verdicts agree wherever the
  * separation margin lies outside the FP64 band, which is what the band
  * exists for.  The exact policy (PF32) stays the drop-in default.
  */
-#define GPRM_START_BINS 54   /* 6 cube faces x 3 x 3 cells */
+#define GPRM_START_BINS 54   /* direction bins: 6 cube faces x 3 x 3 cells */
 
 /* Cube-map bin of a direction: the face of the largest |component| (with
  * its sign), then each of the other two components against a third of it.
@@ -690,111 +687,6 @@ __device__ __forceinline__ float fnormalize3(V3<float>& u)
     const float f = n2 > 0.0f ? rsqrtf(n2) : 0.0f;
     u.x *= f; u.y *= f; u.z *= f;
     return n2 * f;
-}
-
-/* First-improvement climb (collision4.h:66-103) in FMA arithmetic; the
- * neighbours of the current vertex are loaded and evaluated
- * GPRM_FAST_CLIMB_CHUNK at a time, the move going to the first improving
- * one in CRS order. */
-#ifndef GPRM_FAST_CLIMB_CHUNK
-#define GPRM_FAST_CLIMB_CHUNK 1
-#endif
-__device__ __forceinline__ float4 fclimb(const float4* __restrict__ B, float4 cur, float dx, float dy, float dz)
-{
-    float best = fdot3(cur.x, cur.y, cur.z, dx, dy, dz);
-#pragma unroll 1
-    for (int guard = 0; guard < 128; ++guard) {
-        const float4* e = B + 2 + ent_dsp(cur);
-        const int c = ent_cnt(cur);
-        bool moved = false;
-#if GPRM_FAST_CLIMB_CHUNK == 1
-#pragma unroll 1
-        for (int i = 0; i < c; ++i) {
-            const float4 u = e[i];
-            const float d = fdot3(u.x, u.y, u.z, dx, dy, dz);
-            if (d > best) { best = d; cur = u; moved = true; break; }
-        }
-#else
-#pragma unroll 1
-        for (int i = 0; i < c && !moved; i += GPRM_FAST_CLIMB_CHUNK) {
-            float4 u[GPRM_FAST_CLIMB_CHUNK];
-            float d[GPRM_FAST_CLIMB_CHUNK];
-#pragma unroll
-            for (int k = 0; k < GPRM_FAST_CLIMB_CHUNK; ++k) {
-                u[k] = e[i + k < c ? i + k : i];
-                d[k] = fdot3(u[k].x, u[k].y, u[k].z, dx, dy, dz);
-            }
-#pragma unroll
-            for (int k = 0; k < GPRM_FAST_CLIMB_CHUNK; ++k)
-                if (!moved && i + k < c && d[k] > best) { best = d[k]; cur = u[k]; moved = true; }
-        }
-#endif
-        if (!moved) break;
-    }
-    return cur;
-}
-
-/* The support climbs of P (along dp) and Q (along dq) side by side: each
- * trip of the loop evaluates the next CRS neighbour of each polytope's
- * current vertex, so that the two dependent load-and-compare chains
- * overlap.  Each climb still moves to the first improving neighbour in CRS
- * order and ends where fclimb ends (chunk 1).  The trip bound only guards
- * corrupt data (a climb makes at most n-1 moves of at most 255 neighbours). */
-__device__ __forceinline__ void fclimb2(const float4* __restrict__ BP, float4& cp, float px, float py, float pz,
-                                        const float4* __restrict__ BQ, float4& cq, float qx, float qy, float qz)
-{
-    float bp = fdot3(cp.x, cp.y, cp.z, px, py, pz), bq = fdot3(cq.x, cq.y, cq.z, qx, qy, qz);
-    const float4* ep = BP + 2 + ent_dsp(cp);
-    const float4* eq = BQ + 2 + ent_dsp(cq);
-    int np = ent_cnt(cp), nq = ent_cnt(cq), ip = 0, iq = 0;
-#pragma unroll 1
-    for (int guard = 0; guard < 32768 && (ip < np || iq < nq); ++guard) {
-        if (ip < np) {
-            const float4 u = ep[ip];
-            const float d = fdot3(u.x, u.y, u.z, px, py, pz);
-            if (d > bp) { bp = d; cp = u; ep = BP + 2 + ent_dsp(u); np = ent_cnt(u); ip = 0; }
-            else ++ip;
-        }
-        if (iq < nq) {
-            const float4 u = eq[iq];
-            const float d = fdot3(u.x, u.y, u.z, qx, qy, qz);
-            if (d > bq) { bq = d; cq = u; eq = BQ + 2 + ent_dsp(u); nq = ent_cnt(u); iq = 0; }
-            else ++iq;
-        }
-    }
-}
-
-/* Support vertices of P (along dp) and Q (along dq) by a scan of all their
- * vertices (VP[0..nP), VQ[0..nQ), table entries), side by side: a maximiser
- * of the dot product, the first in vertex order among equal values.  The
- * first-improvement climb also ends at a maximiser (on a convex polytope
- * every vertex without an improving neighbour is one), so the two agree
- * unless several vertices tie within rounding.  Every lane of a warp that
- * tests the same pair runs the same trip count, the loads are independent,
- * and a NaN direction keeps vertex 0. */
-#ifndef GPRM_FAST_SCAN_MAX
-#define GPRM_FAST_SCAN_MAX 32   /* polytopes with more vertices climb */
-#endif
-__device__ __forceinline__ void fsupport_scan2(const float4* __restrict__ VP, int nP, float4& cp, float px,
-                                               float py, float pz, const float4* __restrict__ VQ, int nQ,
-                                               float4& cq, float qx, float qy, float qz)
-{
-    float4 u = VP[0], v = VQ[0];
-    float bp = fdot3(u.x, u.y, u.z, px, py, pz), bq = fdot3(v.x, v.y, v.z, qx, qy, qz);
-    int ip = 0, iq = 0;
-    const int n = nP > nQ ? nP : nQ;
-    /* past its last vertex a polytope re-reads that vertex, whose dot
-       product cannot exceed the maximum again */
-#pragma unroll 4
-    for (int i = 1; i < n; ++i) {
-        u = VP[i < nP ? i : nP - 1];
-        v = VQ[i < nQ ? i : nQ - 1];
-        const float du = fdot3(u.x, u.y, u.z, px, py, pz), dv = fdot3(v.x, v.y, v.z, qx, qy, qz);
-        if (du > bp) { bp = du; ip = i; }
-        if (dv > bq) { bq = dv; iq = i; }
-    }
-    cp = VP[ip];
-    cq = VQ[iq];
 }
 
 /* Support vertices of polytopes kP (along p) and kQ (along q) from the
@@ -899,10 +791,6 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
     int combs[GPRM_MAX_ITERS];
     float best = 0.0f;
     int k = 0, l = 0;
-    /* small polytopes: support by scanning every vertex (warp-uniform trip
-       counts); larger ones: climbs, the first from the direction tables */
-    const int2 vP = sc.vinfo[pp.x], vQ = sc.vinfo[pp.y];
-    const bool scan = vP.y <= GPRM_FAST_SCAN_MAX && vQ.y <= GPRM_FAST_SCAN_MAX;
 #pragma unroll 1
     for (; k < GPRM_MAX_ITERS && l < GPRM_MAX_ITERS; ++l) {
         V3<float> Sp, Sq;
@@ -910,17 +798,7 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
         else Sp = frot_t(tp, S.x, S.y, S.z);
         if (idQ) { Sq.x = -S.x; Sq.y = -S.y; Sq.z = -S.z; }
         else Sq = frot_t(tq, -S.x, -S.y, -S.z);
-        if (sc.cbin) {
-            fsupport_cand2(sc, pp.x, ep, Sp.x, Sp.y, Sp.z, pp.y, eq, Sq.x, Sq.y, Sq.z);
-        } else if (scan) {
-            fsupport_scan2(sc.vtab + vP.x, vP.y, ep, Sp.x, Sp.y, Sp.z, sc.vtab + vQ.x, vQ.y, eq, Sq.x, Sq.y, Sq.z);
-        } else {
-            if (l == 0 && sc.start) {
-                ep = BP[sc.start[pp.x * GPRM_START_BINS + dir_bin(Sp.x, Sp.y, Sp.z)]];
-                eq = BQ[sc.start[pp.y * GPRM_START_BINS + dir_bin(Sq.x, Sq.y, Sq.z)]];
-            }
-            fclimb2(BP, ep, Sp.x, Sp.y, Sp.z, BQ, eq, Sq.x, Sq.y, Sq.z);
-        }
+        fsupport_cand2(sc, pp.x, ep, Sp.x, Sp.y, Sp.z, pp.y, eq, Sq.x, Sq.y, Sq.z);
         V3<float> p0, q0;
         if (idP) { p0.x = ep.x; p0.y = ep.y; p0.z = ep.z; }
         else p0 = fxform(tp, ep.x, ep.y, ep.z);

@@ -73,9 +73,6 @@ struct gprm_space {
     std::vector<int> slot;         /* ball-centre slot of moving polytopes, -1 otherwise */
     std::vector<int> slot_sys, slot_block;
     std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */
-    /* start entries of the fast path's first support climbs: per polytope
-       GPRM_START_BINS offsets into its table block (see dir_bin) */
-    std::vector<unsigned short> start;
     /* every polytope's vertices as table entries, and (first, count) per polytope */
     std::vector<float4> vtab;
     std::vector<int2> vinfo;

@@ -57,8 +57,8 @@ extern "C" {
 #define GPRM_MODE_FP64_BAND   1
 /* Flag, or-ed with either mode: the FP32 pass runs the same algorithm in
  * contracted arithmetic (fused multiply-add, hardware reciprocal square
- * roots, sincosf) and starts the first support climbs from per-polytope
- * direction tables.  Codes may differ from the reference's by rounding
+ * roots, sincosf) and finds support vertices among per-direction-bin
+ * candidate lists instead of by hill climbing.  Codes may differ from the reference's by rounding
  * (iteration counts, and verdicts of checks within rounding of contact);
  * with GPRM_MODE_FP64_BAND the free/not-free verdicts equal the
  * reference's for every check whose margin lies outside the band, and the
