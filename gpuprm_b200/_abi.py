@@ -59,6 +59,7 @@ class Stats(C.Structure):
         ("launches", C.c_int64),
         ("pairs_certified", C.c_int64),
         ("pairs_tested", C.c_int64),
+        ("band_overflow_items", C.c_int64),
     ]
 
 
@@ -140,11 +141,14 @@ SIGNATURES = [
     ("gprm_mlp_set_inference", C.c_int, [_P, C.c_int]),
     ("gprm_mlp_set_training", C.c_int, [_P, C.c_int]),
     ("gprm_mlp_device_status", C.c_int, [_P, C.POINTER(C.c_uint)]),
+    ("gprm_mlp_set_wait_budget", C.c_int, [_P, C.c_longlong]),
     ("gprm_mlp_train", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                  C.c_float, _F]),
     ("gprm_debug_fk", C.c_int, [_P, _F, _F]),
     ("gprm_device_sm_count", C.c_int, [_P]),
     ("gprm_debug_support_candidates", C.c_int, [_P, C.c_int, C.c_int, _I, C.c_int]),
+    ("gprm_debug_set_queue_capacity", C.c_int, [_P, C.c_uint]),
+    ("gprm_debug_fail_device_alloc", None, [C.c_longlong]),
     ("gprm_set_launch", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
     ("gprm_set_launch_shape", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("gprm_get_launch", C.c_int, [_P, C.c_int, _I, _I, _I]),

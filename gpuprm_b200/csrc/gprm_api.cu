@@ -27,6 +27,8 @@
 #include <string>
 #include <vector>
 
+#include <atomic>
+
 #include "../../include/gprm_b200.h"
 #include "gprm_host.h"
 #include "gprm_internal.h"
@@ -37,7 +39,30 @@ namespace {
 
 thread_local std::string g_create_error = "no error";
 
+/* allocation-failure test hook: the n-th device allocation from the time
+   it is set fails (0 = none) */
+std::atomic<long long> g_fail_alloc{0};
+
 }  // namespace
+
+namespace gprm {
+
+cudaError_t dev_malloc(void** p, size_t bytes)
+{
+    long long k = g_fail_alloc.load();
+    while (k > 0) {
+        if (g_fail_alloc.compare_exchange_weak(k, k - 1)) {
+            if (k == 1) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
+}  // namespace gprm
 
 namespace {
 
@@ -465,6 +490,7 @@ void release_request(Request& r)
     cudaFree(r.d_key);
     cudaFree(r.d_seg);
     cudaFree(r.d_queue);
+    cudaFree(r.d_ovf);
     cudaFreeHost(r.ctl_host);
     cudaFreeHost(r.h_a);
     cudaFreeHost(r.h_b);
@@ -478,25 +504,30 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
 {
     if (own_stream && !r.st) CUDA_TRY(h, cudaStreamCreateWithFlags(&r.st, cudaStreamNonBlocking));
     if (!r.ctl) {
-        CUDA_TRY(h, cudaMalloc((void**)&r.ctl, HOST_PARTS * sizeof(Control)));
+        CUDA_TRY(h, dev_malloc((void**)&r.ctl, HOST_PARTS * sizeof(Control)));
         CUDA_TRY(h, cudaHostAlloc((void**)&r.ctl_host, HOST_PARTS * sizeof(Control), cudaHostAllocDefault));
     }
     if (kind == 1 && !r.d_seg)
-        CUDA_TRY(h, cudaMalloc((void**)&r.d_seg, (size_t)(EDGE_SPLIT_MAX + 1) * sizeof(unsigned)));
+        CUDA_TRY(h, dev_malloc((void**)&r.d_seg, (size_t)(EDGE_SPLIT_MAX + 1) * sizeof(unsigned)));
     size_t need_q = (kind == 0) ? n : 4 * n + 65536;
     if (n > r.cap_items || need_q > r.cap_queue || (with_host && !r.h_res && n > 0)) {
         size_t cap = n > r.cap_items ? n + n / 4 + 64 : r.cap_items;
         size_t qcap = (need_q > r.cap_queue) ? need_q + need_q / 4 : r.cap_queue;
         if (qcap < cap * 4 + 65536) qcap = cap * 4 + 65536;
         cudaFree(r.d_a); cudaFree(r.d_b); cudaFree(r.d_res); cudaFree(r.d_key); cudaFree(r.d_queue);
-        r.d_a = r.d_b = nullptr; r.d_res = nullptr; r.d_key = nullptr; r.d_queue = nullptr;
+        cudaFree(r.d_ovf);
+        r.d_a = r.d_b = nullptr; r.d_res = nullptr; r.d_key = nullptr; r.d_queue = nullptr; r.d_ovf = nullptr;
+        /* the capacities describe the buffers only once every one exists */
+        r.cap_items = 0;
+        r.cap_queue = 0;
         size_t nd = (size_t)h->ndof;
-        CUDA_TRY(h, cudaMalloc((void**)&r.d_res, cap * sizeof(int)));
-        CUDA_TRY(h, cudaMalloc((void**)&r.d_key, cap * sizeof(unsigned)));
-        CUDA_TRY(h, cudaMalloc((void**)&r.d_queue, qcap * sizeof(uint2)));
+        CUDA_TRY(h, dev_malloc((void**)&r.d_res, cap * sizeof(int)));
+        CUDA_TRY(h, dev_malloc((void**)&r.d_key, cap * sizeof(unsigned)));
+        CUDA_TRY(h, dev_malloc((void**)&r.d_queue, qcap * sizeof(uint2)));
+        CUDA_TRY(h, dev_malloc((void**)&r.d_ovf, (2 * cap + 2 * HOST_PARTS + 64) * sizeof(unsigned)));
         if (with_host) {
-            CUDA_TRY(h, cudaMalloc((void**)&r.d_a, cap * nd * sizeof(float)));
-            CUDA_TRY(h, cudaMalloc((void**)&r.d_b, cap * nd * sizeof(float)));
+            CUDA_TRY(h, dev_malloc((void**)&r.d_a, cap * nd * sizeof(float)));
+            CUDA_TRY(h, dev_malloc((void**)&r.d_b, cap * nd * sizeof(float)));
             cudaFreeHost(r.h_a); cudaFreeHost(r.h_b); cudaFreeHost(r.h_res);
             r.h_a = r.h_b = nullptr; r.h_res = nullptr;
             CUDA_TRY(h, cudaHostAlloc((void**)&r.h_a, cap * nd * sizeof(float), cudaHostAllocDefault));
@@ -542,6 +573,19 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
     const int band_on = (h->mode & GPRM_MODE_FP64_BAND) != 0;
     CUDA_TRY(h, cudaMemsetAsync(ctl, 0, sizeof(Control), st));
     int recheck_blocks = h->sms * 4;
+    /* the FP64 queue and, after the items' own region of the request
+       (2 words per item from the part's first item), its overflow record */
+    BandQueue bq;
+    bq.items = r.d_queue;
+    bq.cap = (unsigned)(r.cap_queue < 0xffffffffull ? r.cap_queue : 0xffffffffull);
+    if (h->debug_qcap && h->debug_qcap < bq.cap) bq.cap = h->debug_qcap;
+    bq.n = n;
+    bq.ovf = nullptr;
+    if (band_on && r.d_ovf) {
+        /* every part's keys start at its first item (key = d_key + c0) */
+        bq.ovf = r.d_ovf + 2 * (size_t)(key - r.d_key);
+        CUDA_TRY(h, cudaMemsetAsync(bq.ovf + n, 0, (size_t)((n + 31) / 32) * sizeof(unsigned), st));
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
     if (h->profiling) {
         int rc = event_pair(h, h->ev32, h->ev32_used, &e0, &e1);
@@ -553,14 +597,12 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
                                     (size_t)n * sizeof(unsigned), st));
     if (e0) CUDA_TRY(h, cudaEventRecord(e0, st));
     if (kind == 0)
-        CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, a, n, offset, res, band_on, h->band, r.d_queue,
-                                         (unsigned)r.cap_queue, ctl, st));
+        CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, a, n, offset, res, band_on, h->band, bq, ctl, st));
     else {
         /* small batches split their long edges over several warps */
         const bool split = r.d_seg && h->split_rounds > 0 && n <= (long long)h->split_max;
         CUDA_TRY(h, launch_check_edges(h->dsc, h->cfg_e, a, b, n, offset, h->dq, h->policy, key, band_on,
-                                       h->band, r.d_queue, (unsigned)r.cap_queue, ctl, st,
-                                       split ? r.d_seg : nullptr, split ? h->split_rounds : 0));
+                                       h->band, bq, ctl, st, split ? r.d_seg : nullptr, split ? h->split_rounds : 0));
         if (split) h->host_stats.launches += 1;
     }
     if (e1) CUDA_TRY(h, cudaEventRecord(e1, st));
@@ -568,15 +610,18 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
         if (e2) CUDA_TRY(h, cudaEventRecord(e2, st));
         if (kind == 0)
             CUDA_TRY(h, launch_recheck(h->dsc, recheck_blocks, 0, a, nullptr, nullptr, offset, h->dq, h->policy,
-                                       res, nullptr, r.d_queue, (unsigned)r.cap_queue, ctl, st));
+                                       res, nullptr, bq, ctl, st));
         else
             CUDA_TRY(h, launch_recheck(h->dsc, recheck_blocks, 1, nullptr, a, b, offset, h->dq, h->policy,
-                                       nullptr, key, r.d_queue, (unsigned)r.cap_queue, ctl, st));
+                                       nullptr, key, bq, ctl, st));
+        /* items the queue could not hold, recomputed in full */
+        CUDA_TRY(h, launch_overflow(h->dsc, recheck_blocks, kind, kind == 0 ? a : nullptr, kind == 1 ? a : nullptr,
+                                    b, offset, h->dq, h->policy, h->band, res, key, bq, ctl, st));
         if (e3) CUDA_TRY(h, cudaEventRecord(e3, st));
     }
     if (kind == 1) CUDA_TRY(h, launch_finalize_edges(n, h->policy, key, res, st));
-    /* check + accumulate, plus recheck and finalize where they run */
-    h->host_stats.launches += 2 + (band_on ? 1 : 0) + (kind == 1 ? 1 : 0);
+    /* check + accumulate, plus recheck, overflow pass and finalize where they run */
+    h->host_stats.launches += 2 + (band_on ? 2 : 0) + (kind == 1 ? 1 : 0);
     CUDA_TRY(h, launch_accumulate(ctl, h->d_total, st));
     return GPRM_OK;
 }
@@ -655,21 +700,7 @@ int complete_host(gprm_space* h, int slot)
     }
     if (c.flags & GPRM_DEVFLAG_BAD_EDGE)
         return fail(h, GPRM_ERR_ARG, "an edge has a non-finite or oversized length (|qe-qs|/dq >= 1e8)");
-    if (c.flags & GPRM_DEVFLAG_QUEUE_FULL) {
-        /* rerun with a queue that holds every check of the request */
-        size_t need = (r.kind == 0) ? (size_t)r.n : (size_t)c.steps_nominal + 1;
-        cudaFree(r.d_queue);
-        r.d_queue = nullptr;
-        CUDA_TRY(h, cudaMalloc((void**)&r.d_queue, need * sizeof(uint2)));
-        r.cap_queue = need;
-        int rc = enqueue(h, r, r.kind, r.d_a, r.kind == 1 ? r.d_b : nullptr, r.d_res, r.n, r.n, r.st);
-        if (rc) return rc;
-        CUDA_TRY(h, cudaMemcpyAsync(r.h_res, r.d_res, (size_t)r.n * sizeof(int), cudaMemcpyDeviceToHost, r.st));
-        CUDA_TRY(h, cudaMemcpyAsync(r.ctl_host, r.ctl, sizeof(Control), cudaMemcpyDeviceToHost, r.st));
-        CUDA_TRY(h, cudaStreamSynchronize(r.st));
-        c = *r.ctl_host;
-        if (c.flags) return fail(h, GPRM_ERR_DEVICE, "device flags 0x%x after rerun", c.flags);
-    }
+    /* GPRM_DEVFLAG_QUEUE_FULL: the overflow pass has completed the results */
     memcpy(r.user_res, r.h_res, (size_t)r.n * sizeof(int));
     /* edge-step and band counters accumulate on the device (d_total) */
     if (r.kind == 0) h->host_stats.vertex_checks += r.n;
@@ -761,7 +792,7 @@ int gprm_init(gprm_space* h, int rank, int size)
     const size_t vio = vto + vtb, vib = h->vinfo.size() * sizeof(int2);
     const size_t cbo = (vio + vib + 15) & ~(size_t)15, cbb = h->cbin.size() * sizeof(unsigned);
     const size_t cio = cbo + cbb, cib = h->cidx.size();
-    CUDA_TRY(h, cudaMalloc(&h->d_scene, cio + cib + 64));
+    CUDA_TRY(h, dev_malloc((void**)&h->d_scene, cio + cib + 64));
     char* base = (char*)h->d_scene;
     CUDA_TRY(h, cudaMemcpy(base, h->tab.data(), tb, cudaMemcpyHostToDevice));
     if (pb) CUDA_TRY(h, cudaMemcpy(base + tb, h->pairs.data(), pb, cudaMemcpyHostToDevice));
@@ -811,7 +842,7 @@ int gprm_init(gprm_space* h, int rank, int size)
 
     CUDA_TRY(h, plan_launch(s, 1, 128, &h->cfg_v));
     CUDA_TRY(h, plan_launch(s, 0, 128, &h->cfg_e));
-    CUDA_TRY(h, cudaMalloc((void**)&h->d_total, sizeof(Control)));
+    CUDA_TRY(h, dev_malloc((void**)&h->d_total, sizeof(Control)));
     CUDA_TRY(h, cudaMemset(h->d_total, 0, sizeof(Control)));
     memset(&h->host_stats, 0, sizeof(h->host_stats));
     h->inited = true;
@@ -908,8 +939,7 @@ int gprm_get_stats(const gprm_space* hc, gprm_stats* out)
     out->band_flips = (int64_t)tot.band_flips;
     out->pairs_certified = (int64_t)(tot.cert_far + tot.cert_dir);
     out->pairs_tested = (int64_t)tot.full_tests;
-    if (tot.flags & GPRM_DEVFLAG_QUEUE_FULL)
-        return fail(h, GPRM_ERR_DEVICE, "a device-pointer request overflowed the FP64 queue; its band results are incomplete");
+    out->band_overflow_items = (int64_t)tot.ovf_count;
     if (tot.flags & GPRM_DEVFLAG_BAD_EDGE)
         return fail(h, GPRM_ERR_DEVICE, "a device-pointer request held a non-finite or oversized edge");
     return GPRM_OK;
@@ -1027,7 +1057,7 @@ int gprm_debug_fk(gprm_space* h, const float* q, float* out)
     if (!q || !out) return fail(h, GPRM_ERR_ARG, "null argument");
     float* d = nullptr;
     size_t nf = (size_t)(h->ndof + 1) * 12;
-    CUDA_TRY(h, cudaMalloc((void**)&d, (nf + 8) * sizeof(float)));
+    CUDA_TRY(h, dev_malloc((void**)&d, (nf + 8) * sizeof(float)));
     cudaMemcpy(d + nf, q, h->ndof * sizeof(float), cudaMemcpyHostToDevice);
     cudaError_t e = launch_fk_probe(h->dsc, d + nf, d, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -1038,6 +1068,18 @@ int gprm_debug_fk(gprm_space* h, const float* q, float* out)
 }
 
 int gprm_device_sm_count(const gprm_space* h) { return h ? h->sms : 0; }
+
+void gprm_debug_fail_device_alloc(long long nth)
+{
+    g_fail_alloc.store(nth > 0 ? nth : 0);
+}
+
+int gprm_debug_set_queue_capacity(gprm_space* h, unsigned capacity)
+{
+    if (!h) return GPRM_ERR_ARG;
+    h->debug_qcap = capacity;
+    return GPRM_OK;
+}
 
 int gprm_debug_support_candidates(const gprm_space* h, int polytope, int bin, int* idx, int cap)
 {
@@ -1126,7 +1168,7 @@ int gprm_measure_fp32_peak(double* tflops)
     if (cudaGetDevice(&dev) != cudaSuccess) return GPRM_ERR_CUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     float* out = nullptr;
-    if (cudaMalloc((void**)&out, sizeof(float) * 1024 * 1024) != cudaSuccess) return GPRM_ERR_NOMEM;
+    if (dev_malloc((void**)&out, sizeof(float) * 1024 * 1024) != cudaSuccess) return GPRM_ERR_NOMEM;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -1202,15 +1244,19 @@ extern "C" int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q
     rc = noalloc_scratch(h, h->device, &base);
     if (rc) return rc;
     Control* ctl = (Control*)base;
-    uint2* queue = (uint2*)(base + NOALLOC_QUEUE_OFFSET);
-    const unsigned qcap = (unsigned)GPRM_NOALLOC_MAX_CONFIGS;
+    /* one queue entry per configuration: the queue cannot overflow */
+    BandQueue bq;
+    bq.items = (uint2*)(base + NOALLOC_QUEUE_OFFSET);
+    bq.cap = (unsigned)GPRM_NOALLOC_MAX_CONFIGS;
+    bq.ovf = nullptr;
+    bq.n = n;
     cudaStream_t st = (cudaStream_t)stream;
     const int band_on = (h->mode & GPRM_MODE_FP64_BAND) != 0;
     CUDA_TRY(h, cudaMemsetAsync(ctl, 0, sizeof(Control), st));
-    CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, q, n, offset, res, band_on, h->band, queue, qcap, ctl, st));
+    CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, q, n, offset, res, band_on, h->band, bq, ctl, st));
     if (band_on)
         CUDA_TRY(h, launch_recheck(h->dsc, h->sms * 4, 0, q, nullptr, nullptr, offset, h->dq, h->policy, res,
-                                   nullptr, queue, qcap, ctl, st));
+                                   nullptr, bq, ctl, st));
     CUDA_TRY(h, launch_accumulate(ctl, h->d_total, st));
     h->host_stats.vertex_checks += n;
     h->host_stats.launches += 2 + (band_on ? 1 : 0);

@@ -44,6 +44,7 @@ struct Layout {
     unsigned* d_key = nullptr;       /* edges: per-edge decision key */
     uint2* d_queue = nullptr;
     size_t qcap = 0;
+    unsigned* d_ovf = nullptr;       /* overflow record of the queue (BandQueue), 2 words per item */
     cudaGraphExec_t graph = nullptr; /* captured call sequence */
 };
 
@@ -53,6 +54,7 @@ void free_layout(Layout& L)
     cudaFree(L.d_chunks);
     cudaFree(L.d_key);
     cudaFree(L.d_queue);
+    cudaFree(L.d_ovf);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     L = Layout();
 }
@@ -126,21 +128,33 @@ int enqueue_batch(gprm_batch* b, int vertex_kernel, const float* qa, const float
     const BatchView v = view_of(b, vertex_kernel);
     const int band_on = (b->mode & GPRM_MODE_FP64_BAND) != 0;
     const int recheck_blocks = b->sms * 4;
+    BandQueue bq;
+    bq.items = L.d_queue;
+    bq.cap = (unsigned)L.qcap;
+    bq.ovf = band_on ? L.d_ovf : nullptr;
+    bq.n = L.total;
     BATCH_TRY(b, cudaMemsetAsync(b->ctl, 0, sizeof(Control), st));
+    if (bq.ovf)
+        BATCH_TRY(b, cudaMemsetAsync(bq.ovf + L.total, 0, (size_t)((L.total + 31) / 32) * sizeof(unsigned), st));
     if (vertex_kernel) {
-        BATCH_TRY(b, launch_check_configs_multi(v, cfg, qa, stride, res, band_on, b->band, L.d_queue,
-                                                (unsigned)L.qcap, b->ctl, st));
-        if (band_on)
+        BATCH_TRY(b, launch_check_configs_multi(v, cfg, qa, stride, res, band_on, b->band, bq, b->ctl, st));
+        if (band_on) {
             BATCH_TRY(b, launch_recheck_multi(v, recheck_blocks, 0, qa, nullptr, nullptr, stride, b->policy, res,
-                                              nullptr, L.d_queue, (unsigned)L.qcap, b->ctl, st));
+                                              nullptr, bq, b->ctl, st));
+            BATCH_TRY(b, launch_overflow_multi(v, recheck_blocks, 0, qa, nullptr, nullptr, stride, b->policy, b->band,
+                                               res, nullptr, bq, b->ctl, st));
+        }
     } else {
         BATCH_TRY(b, cudaMemsetAsync(L.d_key, b->policy == GPRM_EDGES_EARLY_EXIT ? 0xff : 0x00,
                                      (size_t)L.total * sizeof(unsigned), st));
         BATCH_TRY(b, launch_check_edges_multi(v, cfg, qa, qb, stride, b->policy, L.d_key, band_on, b->band,
-                                              L.d_queue, (unsigned)L.qcap, b->ctl, st));
-        if (band_on)
+                                              bq, b->ctl, st));
+        if (band_on) {
             BATCH_TRY(b, launch_recheck_multi(v, recheck_blocks, 1, nullptr, qa, qb, stride, b->policy, nullptr,
-                                              L.d_key, L.d_queue, (unsigned)L.qcap, b->ctl, st));
+                                              L.d_key, bq, b->ctl, st));
+            BATCH_TRY(b, launch_overflow_multi(v, recheck_blocks, 1, nullptr, qa, qb, stride, b->policy, b->band,
+                                               nullptr, L.d_key, bq, b->ctl, st));
+        }
         BATCH_TRY(b, launch_finalize_edges(L.total, b->policy, L.d_key, res, st));
     }
     BATCH_TRY(b, launch_accumulate(b->ctl, total, st));
@@ -150,7 +164,7 @@ int enqueue_batch(gprm_batch* b, int vertex_kernel, const float* qa, const float
 int launches_per_call(const gprm_batch* b, int vertex_kernel)
 {
     const int band_on = (b->mode & GPRM_MODE_FP64_BAND) != 0;
-    return 2 + band_on + (vertex_kernel ? 0 : 1);
+    return 2 + 2 * band_on + (vertex_kernel ? 0 : 1);
 }
 
 int check_call(gprm_batch* b, int vertex_kernel, const float* qa, const float* qb, const int* res, long long stride)
@@ -206,11 +220,11 @@ int gprm_batch_create(gprm_space* const* spaces, int count, gprm_batch** out)
     if ((rc = [&]() -> int {
             BATCH_TRY(b, cudaSetDevice(b->device));
             BATCH_TRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-            BATCH_TRY(b, cudaMalloc((void**)&b->d_scenes, sizeof(DevScene) * count));
+            BATCH_TRY(b, dev_malloc((void**)&b->d_scenes, sizeof(DevScene) * count));
             BATCH_TRY(b, cudaMemcpy(b->d_scenes, sc.data(), sizeof(DevScene) * count, cudaMemcpyHostToDevice));
-            BATCH_TRY(b, cudaMalloc((void**)&b->ctl, sizeof(Control)));
-            BATCH_TRY(b, cudaMalloc((void**)&b->d_total, sizeof(Control)));
-            BATCH_TRY(b, cudaMalloc((void**)&b->d_scratch_total, sizeof(Control)));
+            BATCH_TRY(b, dev_malloc((void**)&b->ctl, sizeof(Control)));
+            BATCH_TRY(b, dev_malloc((void**)&b->d_total, sizeof(Control)));
+            BATCH_TRY(b, dev_malloc((void**)&b->d_scratch_total, sizeof(Control)));
             BATCH_TRY(b, cudaMemset(b->d_total, 0, sizeof(Control)));
             BatchView v = view_of(b, 1);
             BATCH_TRY(b, configure_batch_launch(v, 1, 128, &b->cfg[1]));
@@ -264,9 +278,10 @@ int gprm_batch_set_layout(gprm_batch* b, int vertex_kernel, const long long* off
     if (queue_capacity > 0) L.qcap = (size_t)queue_capacity;
     else L.qcap = vertex_kernel ? (size_t)total : (size_t)total * 4 + 65536;   /* one entry per configuration */
     if (L.qcap < 1) L.qcap = 1;
-    BATCH_TRY(b, cudaMalloc((void**)&L.d_offs, sizeof(long long) * (S + 1)));
+    BATCH_TRY(b, dev_malloc((void**)&L.d_offs, sizeof(long long) * (S + 1)));
     BATCH_TRY(b, cudaMemcpy(L.d_offs, offsets, sizeof(long long) * (S + 1), cudaMemcpyHostToDevice));
-    BATCH_TRY(b, cudaMalloc((void**)&L.d_queue, sizeof(uint2) * L.qcap));
+    BATCH_TRY(b, dev_malloc((void**)&L.d_queue, sizeof(uint2) * L.qcap));
+    BATCH_TRY(b, dev_malloc((void**)&L.d_ovf, sizeof(unsigned) * (2 * (size_t)total + 64)));
     if (vertex_kernel) {
         /* chunks of at most 32 configurations of one problem, problems in order */
         std::vector<int4> ch;
@@ -278,11 +293,11 @@ int gprm_batch_set_layout(gprm_batch* b, int vertex_kernel, const long long* off
             }
         L.nchunks = (long long)ch.size();
         if (!ch.empty()) {
-            BATCH_TRY(b, cudaMalloc((void**)&L.d_chunks, sizeof(int4) * ch.size()));
+            BATCH_TRY(b, dev_malloc((void**)&L.d_chunks, sizeof(int4) * ch.size()));
             BATCH_TRY(b, cudaMemcpy(L.d_chunks, ch.data(), sizeof(int4) * ch.size(), cudaMemcpyHostToDevice));
         }
     } else if (total > 0) {
-        BATCH_TRY(b, cudaMalloc((void**)&L.d_key, sizeof(unsigned) * total));
+        BATCH_TRY(b, dev_malloc((void**)&L.d_key, sizeof(unsigned) * total));
     }
     L.set = true;
     return GPRM_OK;
@@ -456,9 +471,7 @@ int gprm_batch_get_stats(const gprm_batch* bc, gprm_stats* out)
     out->band_flips = (int64_t)tot.band_flips;
     out->pairs_certified = (int64_t)(tot.cert_far + tot.cert_dir);
     out->pairs_tested = (int64_t)tot.full_tests;
-    if (tot.flags & GPRM_DEVFLAG_QUEUE_FULL)
-        return bfail(b, GPRM_ERR_DEVICE, "a call overflowed the FP64 queue; its band results are incomplete "
-                                         "(raise the layout's queue capacity)");
+    out->band_overflow_items = (int64_t)tot.ovf_count;
     if (tot.flags & GPRM_DEVFLAG_BAD_EDGE)
         return bfail(b, GPRM_ERR_DEVICE, "a call held a non-finite or oversized edge");
     return GPRM_OK;

@@ -841,35 +841,56 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
     return -1;
 }
 
+/* Frame i+1 of the fast path from frame i (T): sincosf of the joint angle
+ * and FMA products.  Shared by the shared-memory and register versions so
+ * that both give the same bits. */
+__device__ __forceinline__ Frame<float> fast_link(const DevScene& sc, const Frame<float>& T, const float* q, int i)
+{
+    float th = sc.q0[i], d = sc.d0[i];
+    if (sc.types[i] == 0) th = q[i];
+    else d = q[i];
+    float cq, sq;
+    sincosf(th, &sq, &cq);
+    const float ca = sc.ca[i], sa = sc.sa[i];
+    Frame<float> L;
+    dh_frame<PF32>(L, cq, sq, ca, sa, sc.a[i], d);
+    Frame<float> O;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float ux = L.m[3 * c], uy = L.m[3 * c + 1], uz = L.m[3 * c + 2];
+        O.m[3 * c] = __fmaf_rn(T.m[0], ux, __fmaf_rn(T.m[3], uy, __fmaf_rn(T.m[6], uz, c == 3 ? T.m[9] : 0.0f)));
+        O.m[3 * c + 1] = __fmaf_rn(T.m[1], ux, __fmaf_rn(T.m[4], uy, __fmaf_rn(T.m[7], uz, c == 3 ? T.m[10] : 0.0f)));
+        O.m[3 * c + 2] = __fmaf_rn(T.m[2], ux, __fmaf_rn(T.m[5], uy, __fmaf_rn(T.m[8], uz, c == 3 ? T.m[11] : 0.0f)));
+    }
+    return O;
+}
+
+__device__ __forceinline__ void identity_frame(Frame<float>& T)
+{
+#pragma unroll
+    for (int e = 0; e < 12; ++e) T.m[e] = 0.0f;
+    T.m[0] = T.m[4] = T.m[8] = 1.0f;
+}
+
+/* The fast path's frames 0..ndof in registers (the overflow pass). */
+__device__ __forceinline__ void forward_kinematics_fast(const DevScene& sc, const float* q, Frame<float>* F)
+{
+    identity_frame(F[0]);
+#pragma unroll 1
+    for (int i = 0; i < sc.ndof; ++i) F[i + 1] = fast_link(sc, F[i], q, i);
+}
+
 /* Forward kinematics of the fast path into the lane's shared-memory frames
- * (same layout as forward_kinematics_smem): sincosf of the joint angles and
- * FMA products. */
+ * (same layout as forward_kinematics_smem). */
 __device__ __forceinline__ void forward_kinematics_smem_fast(const DevScene& sc, const float4* __restrict__ tab,
                                                              const float* q, float* out, float* cen)
 {
     Frame<float> T;
-#pragma unroll
-    for (int e = 0; e < 12; ++e) T.m[e] = 0.0f;
-    T.m[0] = T.m[4] = T.m[8] = 1.0f;
+    identity_frame(T);
     int slot = 0;
 #pragma unroll 1
     for (int i = 0; i < sc.ndof; ++i) {
-        float th = sc.q0[i], d = sc.d0[i];
-        if (sc.types[i] == 0) th = q[i];
-        else d = q[i];
-        float cq, sq;
-        sincosf(th, &sq, &cq);
-        const float ca = sc.ca[i], sa = sc.sa[i];
-        Frame<float> L;
-        dh_frame<PF32>(L, cq, sq, ca, sa, sc.a[i], d);
-        Frame<float> O;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const float ux = L.m[3 * c], uy = L.m[3 * c + 1], uz = L.m[3 * c + 2];
-            O.m[3 * c] = __fmaf_rn(T.m[0], ux, __fmaf_rn(T.m[3], uy, __fmaf_rn(T.m[6], uz, c == 3 ? T.m[9] : 0.0f)));
-            O.m[3 * c + 1] = __fmaf_rn(T.m[1], ux, __fmaf_rn(T.m[4], uy, __fmaf_rn(T.m[7], uz, c == 3 ? T.m[10] : 0.0f)));
-            O.m[3 * c + 2] = __fmaf_rn(T.m[2], ux, __fmaf_rn(T.m[5], uy, __fmaf_rn(T.m[8], uz, c == 3 ? T.m[11] : 0.0f)));
-        }
+        const Frame<float> O = fast_link(sc, T, q, i);
 #pragma unroll
         for (int e = 0; e < 12; ++e) out[(i * 12 + e) * 32] = O.m[e];
         for (; slot < sc.nslots && sc.slot_sys[slot] == i + 1; ++slot) slot_points(sc, tab, O, slot, cen);

@@ -15,6 +15,11 @@
 
 namespace gprm {
 
+/* cudaMalloc through the library's allocation-failure test hook
+ * (gprm_debug_fail_device_alloc): every device allocation of the checker
+ * and the batches goes through it. */
+cudaError_t dev_malloc(void** p, size_t bytes);
+
 /* One request of the pool: stream, control block, device buffers and
  * pinned staging. */
 /* host-buffer requests are split into up to this many parts, so that the
@@ -33,6 +38,7 @@ struct Request {
     unsigned* d_key = nullptr;
     unsigned* d_seg = nullptr;    /* edge segment offsets (EDGE_SPLIT_MAX + 1) */
     uint2* d_queue = nullptr;
+    unsigned* d_ovf = nullptr;    /* overflow record of the FP64 queue: 2 words per item (BandQueue) */
     float* h_a = nullptr;         /* pinned staging */
     float* h_b = nullptr;
     int* h_res = nullptr;
@@ -95,6 +101,7 @@ struct gprm_space {
     int split_max = 16384;        /* edge batches up to this size split long edges */
     int split_rounds = 2;         /* rounds of 32 steps per segment */
     float band = 1e-5f;
+    unsigned debug_qcap = 0;      /* test hook: FP64 queue capacity cap (0 = none) */
 
     std::vector<gprm::Request> reqs;
     std::map<int, int> live;       /* request id -> slot */

@@ -24,10 +24,25 @@ struct Control {
     unsigned long long cert_far;      /* pair tests settled by the distance certificate */
     unsigned long long cert_dir;      /* ... by the first-direction certificate */
     unsigned long long full_tests;    /* pair tests that ran the Chung-Wang iteration */
+    unsigned long long ovf_count;     /* items recorded in the overflow list (BandQueue) */
 };
 
 #define GPRM_DEVFLAG_BAD_EDGE    1u   /* non-finite or oversized edge length */
-#define GPRM_DEVFLAG_QUEUE_FULL  2u   /* FP64 queue overflowed; rerun needed */
+#define GPRM_DEVFLAG_QUEUE_FULL  2u   /* FP64 queue overflowed (the overflow pass completed the results) */
+
+/* The FP64 recheck queue of one request.  A check that does not fit
+ * records its item (configuration or edge) in the overflow list instead,
+ * once per item (bitmap), and the overflow pass recomputes every listed
+ * item in full, so a request's results are complete whatever the
+ * capacity.  ovf: n list words, then (n + 31) / 32 bitmap words, which the
+ * request zeroes; null where the capacity covers every check (one entry
+ * per configuration). */
+struct BandQueue {
+    uint2* items;
+    unsigned cap;
+    unsigned* ovf;
+    long long n;
+};
 
 /* How a launch reads its scene. */
 struct LaunchCfg {
@@ -63,14 +78,14 @@ struct BatchView {
 /* Launch shape of the batched kernels. */
 cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg);
 cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg, const float* q, long long offset,
-                                       int* res, int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
+                                       int* res, int band_on, float band, BandQueue bq, Control* ctl,
                                        cudaStream_t st);
 cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, const float* qs, const float* qe,
                                      long long offset, int policy, unsigned* key, int band_on, float band,
-                                     uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
+                                     BandQueue bq, Control* ctl, cudaStream_t st);
 cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,
                                  const float* qe, long long offset, int policy, int* res, unsigned* key,
-                                 const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
+                                 BandQueue bq, Control* ctl, cudaStream_t st);
 
 /* Per-lane shared floats of a warp's block: frames 1..ndof (12 floats
  * each), the world ball centres of the slots (3 floats each), the world
@@ -101,7 +116,7 @@ cudaError_t configure_launch(const DevScene& sc, int vertex_kernel, int threads,
 /* Vertex checks: res[i] = code of configuration q[i + offset*j]. */
 cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q,
                                  long long n, long long offset, int* res, int band_on, float band,
-                                 uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st);
+                                 BandQueue bq, Control* ctl, cudaStream_t st);
 
 /* Edge checks, FP32 pass: key[e] is set per the edge policy (see kernels).
  * seg_off (EDGE_SPLIT_MAX + 1 words of scratch) or null: with it, n <=
@@ -111,14 +126,24 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
 constexpr long long EDGE_SPLIT_MAX = 16384;
 cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs,
                                const float* qe, long long n, long long offset, float dq, int policy,
-                               unsigned* key, int band_on, float band, uint2* queue, unsigned qcap,
+                               unsigned* key, int band_on, float band, BandQueue bq,
                                Control* ctl, cudaStream_t st, unsigned* seg_off = nullptr, int seg_rounds = 0);
 
 /* FP64 recheck of queued vertex (kind 0) or edge-step (kind 1) items. */
 cudaError_t launch_recheck(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,
                            const float* qe, long long offset, float dq, int policy, int* res,
-                           unsigned* key, const uint2* queue, unsigned qcap, Control* ctl,
+                           unsigned* key, BandQueue bq, Control* ctl,
                            cudaStream_t st);
+
+/* The overflow pass after the recheck (band mode): recomputes every item
+ * the queue could not hold (kind 0 configurations -> res, kind 1 edges ->
+ * key).  Nothing to do when bq.ovf is null. */
+cudaError_t launch_overflow(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,
+                            const float* qe, long long offset, float dq, int policy, float band, int* res,
+                            unsigned* key, BandQueue bq, Control* ctl, cudaStream_t st);
+cudaError_t launch_overflow_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,
+                                  const float* qe, long long offset, int policy, float band, int* res, unsigned* key,
+                                  BandQueue bq, Control* ctl, cudaStream_t st);
 
 /* res[e] = code decoded from key[e] */
 cudaError_t launch_finalize_edges(long long n, int policy, const unsigned* key, int* res,

@@ -456,7 +456,7 @@ __device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView&
 }
 
 /* Appends the items of the lanes with `want` set, one atomic per warp. */
-__device__ __forceinline__ void warp_append(bool want, uint2 item, uint2* queue, unsigned qcap,
+__device__ __forceinline__ void warp_append(bool want, uint2 item, BandQueue bq,
                                             Control* ctl)
 {
     unsigned m = __ballot_sync(FULL_MASK, want);
@@ -467,8 +467,17 @@ __device__ __forceinline__ void warp_append(bool want, uint2 item, uint2* queue,
     base = __shfl_sync(FULL_MASK, base, __ffs(m) - 1);
     if (want) {
         unsigned slot = base + __popc(m & ((1u << lane) - 1));
-        if (slot < qcap) queue[slot] = item;
-        else atomicOr(&ctl->flags, GPRM_DEVFLAG_QUEUE_FULL);
+        if (slot < bq.cap) {
+            bq.items[slot] = item;
+        } else {
+            atomicOr(&ctl->flags, GPRM_DEVFLAG_QUEUE_FULL);
+            const unsigned x = item.x;
+            if (bq.ovf && (long long)x < bq.n) {
+                const unsigned bit = 1u << (x & 31u);
+                if (!(atomicOr(&bq.ovf[bq.n + (x >> 5)], bit) & bit))
+                    bq.ovf[atomicAdd(&ctl->ovf_count, 1ull)] = x;
+            }
+        }
     }
 }
 
@@ -486,7 +495,7 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
 template <bool FAST>
 __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const SceneView& S, const float* __restrict__ q,
                                                    long long offset, long long i0, int count, int* __restrict__ res,
-                                                   int band_on, float band, uint2* __restrict__ queue, unsigned qcap,
+                                                   int band_on, float band, BandQueue bq,
                                                    Control* ctl, PairCounts& pc, unsigned long long& exec)
 {
     const int lane = threadIdx.x & 31;
@@ -521,14 +530,14 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
         res[i] = code;
     }
     bool want = valid && band_on && code != 1 && in_band(code, code == 0 ? mmin : mdec, band);
-    warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), queue, qcap, ctl);
+    warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), bq, ctl);
 }
 
 template <bool SMEM, bool FAST>
 __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict__ q,
                                             long long n, long long offset,
                                             int* __restrict__ res, int band_on, float band,
-                                            uint2* __restrict__ queue, unsigned qcap,
+                                            BandQueue bq,
                                             Control* ctl)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -543,7 +552,7 @@ __global__ void GPRM_BOUNDS k_check_configs(DevScene sc, const float* __restrict
         if (base >= (unsigned long long)n) break;
         const long long left = n - (long long)base;
         check_config_chunk<FAST>(sc, S, q, offset, (long long)base, left < 32 ? (int)left : 32, res, band_on,
-                                 band, queue, qcap, ctl, pc, exec);
+                                 band, bq, ctl, pc, exec);
     }
     exec = warp_sum(exec);
     if (lane == 0 && exec) atomicAdd(&ctl->configs_exec, exec);
@@ -582,7 +591,7 @@ template <int POLICY, bool SPLIT, bool FAST>
 __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& S, const float* __restrict__ qs,
                                            const float* __restrict__ qe, long long e, long long offset, float dq,
                                            unsigned* __restrict__ key, int band_on, float band,
-                                           uint2* __restrict__ queue, unsigned qcap, Control* ctl, PairCounts& pc,
+                                           BandQueue bq, Control* ctl, PairCounts& pc,
                                            unsigned long long& exec, unsigned long long& nominal,
                                            int seg = 0, int seg_rounds = 0)
 {
@@ -678,7 +687,7 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
            than the deciding step go to the FP64 queue */
         const bool want = inb && lane < L;
         warp_append(want, make_uint2((unsigned)e, (unsigned)t | ((unsigned)(code + 1) << 27)),
-                    queue, qcap, ctl);
+                    bq, ctl);
         if (hits) {
             if (lane == L) {
                 const unsigned kv = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
@@ -710,8 +719,8 @@ template <bool SMEM, int POLICY, bool SPLIT, bool FAST>
 __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__ qs,
                                           const float* __restrict__ qe, long long n,
                                           long long offset, float dq, unsigned* __restrict__ key,
-                                          int band_on, float band, uint2* __restrict__ queue,
-                                          unsigned qcap, Control* ctl, const unsigned* __restrict__ seg_off,
+                                          int band_on, float band, BandQueue bq, Control* ctl,
+                                          const unsigned* __restrict__ seg_off,
                                           int seg_rounds)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -725,8 +734,8 @@ __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__
             if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
             eu = __shfl_sync(FULL_MASK, eu, 0);
             if (eu >= (unsigned long long)n) break;
-            check_edge<POLICY, false, FAST>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, queue,
-                                            qcap, ctl, pc, exec, nominal);
+            check_edge<POLICY, false, FAST>(sc, S, qs, qe, (long long)eu, offset, dq, key, band_on, band, bq, ctl,
+                                            pc, exec, nominal);
         }
         flush_edge_counts(exec, nominal, pc, ctl);
         return;
@@ -753,7 +762,7 @@ __global__ void GPRM_BOUNDS k_check_edges(DevScene sc, const float* __restrict__
         if (eu >= items) break;
         e = __shfl_sync(FULL_MASK, e, 0);
         seg = __shfl_sync(FULL_MASK, seg, 0);
-        check_edge<POLICY, true, FAST>(sc, S, qs, qe, e, offset, dq, key, band_on, band, queue, qcap, ctl, pc,
+        check_edge<POLICY, true, FAST>(sc, S, qs, qe, e, offset, dq, key, band_on, band, bq, ctl, pc,
                                        exec, nominal, seg, seg_rounds);
     }
     flush_edge_counts(exec, nominal, pc, ctl);
@@ -807,6 +816,31 @@ __global__ void __launch_bounds__(1024) k_edge_segments(const float* __restrict_
 /* FP64 recheck and finalisation                                        */
 /* ------------------------------------------------------------------ */
 
+/* The FP64 check of one configuration (in bounds): the reference's pair
+ * loop in double with the FP64 certificates. */
+__device__ __forceinline__ int check_config64(const DevScene& sc, const float* qi)
+{
+    Frame<double> F[GPRM_MAX_FRAMES];
+    forward_kinematics<PF64>(sc, qi, F);
+    /* slot ball centres in FP64, once per check (the same transform the
+       certificate would apply per pair) */
+    double cen[GPRM_MAX_SLOTS * 3];
+    for (int sl = 0; sl < sc.nslots; ++sl) {
+        const float4 b = sc.tab[sc.slot_block[sl]];
+        const V3<double> c = xform<double>(F[sc.slot_sys[sl]], (double)b.x, (double)b.y, (double)b.z);
+        cen[3 * sl] = c.x; cen[3 * sl + 1] = c.y; cen[3 * sl + 2] = c.z;
+    }
+#pragma unroll 1
+    for (int j = 0; j < sc.npairs; ++j) {
+        const int4 pr = sc.pairs[j];
+        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F, cen)) continue;
+        double m;
+        const int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
+        if (r != 0) return r;
+    }
+    return 0;
+}
+
 /* FP64 recheck of one queued item (vertex kind 0, edge step kind 1). */
 __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2 it, const float* __restrict__ q,
                                              const float* __restrict__ qs, const float* __restrict__ qe,
@@ -814,7 +848,6 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
                                              unsigned* __restrict__ key, unsigned long long& checks,
                                              unsigned long long& flips)
 {
-    Frame<double> F[GPRM_MAX_FRAMES];
     const int code32 = (int)(it.y >> 27) - 1;
     float qi[GPRM_MAX_FRAMES];
     int t = 0, tn = 0;
@@ -825,24 +858,7 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
         tn = edge_testnum(qs, qe, (long long)it.x, offset, sc.ndof, dq);
         edge_step_config(qs, qe, (long long)it.x, offset, sc.ndof, t, tn, qi);
     }
-    forward_kinematics<PF64>(sc, qi, F);
-    /* slot ball centres in FP64, once per check (the same transform the
-       certificate would apply per pair) */
-    double cen[GPRM_MAX_SLOTS * 3];
-    for (int sl = 0; sl < sc.nslots; ++sl) {
-        const float4 b = sc.tab[sc.slot_block[sl]];
-        const V3<double> c = xform<double>(F[sc.slot_sys[sl]], (double)b.x, (double)b.y, (double)b.z);
-        cen[3 * sl] = c.x; cen[3 * sl + 1] = c.y; cen[3 * sl + 2] = c.z;
-    }
-    int code = 0;
-#pragma unroll 1
-    for (int j = 0; j < sc.npairs; ++j) {
-        const int4 pr = sc.pairs[j];
-        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F, cen)) continue;
-        double m;
-        int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
-        if (r != 0) { code = r; break; }
-    }
+    const int code = check_config64(sc, qi);
     ++checks;
     flips += ((code != 0) != (code32 != 0));
     if (kind == 0) {
@@ -858,18 +874,124 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
     }
 }
 
+/* The FP32 check of one configuration (in bounds) in one thread, in the
+ * arithmetic of the kernel variant (FAST), frames in registers: every
+ * pair's exact test in the reference's order (the certificates only ever
+ * skip pairs whose test gives 0 with a margin above the band, so the code
+ * and the band decision are those of the warp kernels).  *margin: the
+ * deciding pair's margin, or the minimum over the pairs of a free check. */
+template <bool FAST>
+__device__ __forceinline__ int check_config32(const DevScene& sc, const float* qi, float* margin)
+{
+    Frame<float> F[GPRM_MAX_FRAMES];
+    if constexpr (FAST) forward_kinematics_fast(sc, qi, F);
+    else forward_kinematics<PF32>(sc, qi, F);
+    float mmin = PF32::inf();
+#pragma unroll 1
+    for (int j = 0; j < sc.npairs; ++j) {
+        const int4 pr = sc.pairs[j];
+        float m;
+        int r;
+        if constexpr (FAST) r = pair_test_fast(sc, sc.tab, pr, sc.ppoly[j], F[pr.z], F[pr.w], &m);
+        else r = pair_test<PF32>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
+        if (r != 0) { *margin = m; return r; }
+        mmin = min_nan(mmin, m);
+    }
+    *margin = mmin;
+    return 0;
+}
+
+/* One item of the overflow list, recomputed in full by one thread: a
+ * configuration (kind 0: bounds, FP32, FP64 inside the band -> res), or an
+ * edge (kind 1: every step so; the key is rebuilt from scratch with the
+ * merge of the check and recheck kernels - all steps: the same key;
+ * early exit: the first colliding step in step order, whose verdict is the
+ * edge's). */
+template <bool FAST>
+__device__ __forceinline__ void overflow_item(const DevScene& sc, int kind, unsigned x, const float* __restrict__ q,
+                                              const float* __restrict__ qs, const float* __restrict__ qe,
+                                              long long offset, float dq, int policy, float band,
+                                              int* __restrict__ res, unsigned* __restrict__ key,
+                                              unsigned long long& checks, unsigned long long& flips)
+{
+    float qi[GPRM_MAX_FRAMES];
+    if (kind == 0) {
+        for (int j = 0; j < sc.ndof; ++j) qi[j] = q[(long long)x + offset * j];
+        int code = 0;
+        for (int j = 0; j < sc.ndof; ++j)
+            if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; break; }
+        if (code == 0) {
+            float m;
+            code = check_config32<FAST>(sc, qi, &m);
+            if (in_band(code, m, band)) {
+                const int c64 = check_config64(sc, qi);
+                ++checks;
+                flips += ((c64 != 0) != (code != 0));
+                code = c64;
+            }
+        }
+        res[x] = code;
+        return;
+    }
+    const int tn = edge_testnum(qs, qe, (long long)x, offset, sc.ndof, dq);
+    if (tn < 0) return;   /* flagged by the check kernel */
+    const int R = (tn + 31) >> 5;
+    unsigned k = policy == EDGE_EARLY_EXIT ? 0xffffffffu : 0u;
+#pragma unroll 1
+    for (int t = 0; t < tn; ++t) {
+        edge_step_config(qs, qe, (long long)x, offset, sc.ndof, t, tn, qi);
+        float m;
+        int code = check_config32<FAST>(sc, qi, &m);
+        if (in_band(code, m, band)) {
+            const int c64 = check_config64(sc, qi);
+            ++checks;
+            flips += ((c64 != 0) != (code != 0));
+            code = c64;
+        }
+        if (code == 0) continue;
+        if (policy == EDGE_EARLY_EXIT) {
+            const unsigned kv = early_key((unsigned)((t % R) * 32 + t / R), code);
+            if (kv < k) k = kv;
+            break;
+        }
+        const unsigned kv = all_key(t, code);
+        if (kv > k) k = kv;
+    }
+    key[x] = k;
+}
+
 __global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const float* __restrict__ q,
                                                  const float* __restrict__ qs, const float* __restrict__ qe,
                                                  long long offset, float dq, int policy,
                                                  int* __restrict__ res, unsigned* __restrict__ key,
-                                                 const uint2* __restrict__ queue, unsigned qcap,
+                                                 const BandQueue bq,
                                                  Control* ctl)
 {
     unsigned cnt = ctl->qcount;
-    if (cnt > qcap) cnt = qcap;
+    if (cnt > bq.cap) cnt = bq.cap;
     unsigned long long checks = 0, flips = 0;
     for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x)
-        recheck_item(sc, kind, queue[idx], q, qs, qe, offset, dq, policy, res, key, checks, flips);
+        recheck_item(sc, kind, bq.items[idx], q, qs, qe, offset, dq, policy, res, key, checks, flips);
+    if (checks) atomicAdd(&ctl->band_checks, checks);
+    if (flips) atomicAdd(&ctl->band_flips, flips);
+}
+
+/* The overflow pass of a request: every item in the overflow list,
+ * recomputed by one thread (overflow_item).  Exits at once when nothing
+ * overflowed. */
+template <bool FAST>
+__global__ void __launch_bounds__(128) k_overflow(DevScene sc, int kind, const float* __restrict__ q,
+                                                  const float* __restrict__ qs, const float* __restrict__ qe,
+                                                  long long offset, float dq, int policy, float band,
+                                                  int* __restrict__ res, unsigned* __restrict__ key, BandQueue bq,
+                                                  Control* ctl)
+{
+    const unsigned long long cnt = ctl->ovf_count;
+    if (cnt == 0 || !bq.ovf) return;
+    unsigned long long checks = 0, flips = 0;
+    for (unsigned long long idx = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; idx < cnt;
+         idx += (unsigned long long)gridDim.x * blockDim.x)
+        overflow_item<FAST>(sc, kind, bq.ovf[idx], q, qs, qe, offset, dq, policy, band, res, key, checks, flips);
     if (checks) atomicAdd(&ctl->band_checks, checks);
     if (flips) atomicAdd(&ctl->band_flips, flips);
 }
@@ -1041,8 +1163,8 @@ cudaError_t plan_launch(const DevScene& sc, int vertex_kernel, int threads, Laun
 }
 
 cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const float* q, long long n,
-                                 long long offset, int* res, int band_on, float band, uint2* queue,
-                                 unsigned qcap, Control* ctl, cudaStream_t st)
+                                 long long offset, int* res, int band_on, float band, BandQueue bq, Control* ctl,
+                                 cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
     {
@@ -1051,7 +1173,7 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
     }
 #define GPRM_CFG_LAUNCH(SM_, FAST_)                                                                            \
     k_check_configs<SM_, FAST_><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(sc, q, n, offset, res, band_on, \
-                                                                                band, queue, qcap, ctl)
+                                                                                band, bq, ctl)
     if (cfg.scene_in_smem) { if (sc.fast) GPRM_CFG_LAUNCH(true, true); else GPRM_CFG_LAUNCH(true, false); }
     else { if (sc.fast) GPRM_CFG_LAUNCH(false, true); else GPRM_CFG_LAUNCH(false, false); }
 #undef GPRM_CFG_LAUNCH
@@ -1060,7 +1182,7 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
 
 cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs, const float* qe,
                                long long n, long long offset, float dq, int policy, unsigned* key,
-                               int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
+                               int band_on, float band, BandQueue bq, Control* ctl,
                                cudaStream_t st, unsigned* seg_off, int seg_rounds)
 {
     if (n <= 0) return cudaSuccess;
@@ -1078,7 +1200,7 @@ cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const f
     }
 #define GPRM_EDGE_LAUNCH2(SM_, POL_, SPLIT_, FAST_)                                                           \
     k_check_edges<SM_, POL_, SPLIT_, FAST_><<<cfg.blocks, cfg.threads, sm, st>>>(                                 \
-        sc, qs, qe, n, offset, dq, key, band_on, band, queue, qcap, ctl, seg_off, seg_rounds)
+        sc, qs, qe, n, offset, dq, key, band_on, band, bq, ctl, seg_off, seg_rounds)
 #define GPRM_EDGE_LAUNCH(SM_, POL_, SPLIT_)                                                                   \
     do { if (sc.fast) GPRM_EDGE_LAUNCH2(SM_, POL_, SPLIT_, true); else GPRM_EDGE_LAUNCH2(SM_, POL_, SPLIT_, false); } \
     while (0)
@@ -1097,9 +1219,21 @@ cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const f
 
 cudaError_t launch_recheck(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,
                            const float* qe, long long offset, float dq, int policy, int* res, unsigned* key,
-                           const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
+                           BandQueue bq, Control* ctl, cudaStream_t st)
 {
-    k_recheck<<<blocks, 128, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, res, key, queue, qcap, ctl);
+    k_recheck<<<blocks, 128, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, res, key, bq, ctl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_overflow(const DevScene& sc, int blocks, int kind, const float* q, const float* qs,
+                            const float* qe, long long offset, float dq, int policy, float band, int* res,
+                            unsigned* key, BandQueue bq, Control* ctl, cudaStream_t st)
+{
+    if (!bq.ovf) return cudaSuccess;
+    if (sc.fast)
+        k_overflow<true><<<blocks, 128, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, band, res, key, bq, ctl);
+    else
+        k_overflow<false><<<blocks, 128, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, band, res, key, bq, ctl);
     return cudaGetLastError();
 }
 
@@ -1156,7 +1290,7 @@ __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene
 template <bool FAST>
 __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __restrict__ q, long long offset,
                                                   int* __restrict__ res, int band_on, float band,
-                                                  uint2* __restrict__ queue, unsigned qcap, Control* ctl)
+                                                  BandQueue bq, Control* ctl)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1173,7 +1307,7 @@ __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __re
         if (c >= (unsigned long long)B.nwork) break;
         const int4 ch = B.chunks[c];
         if (ch.x != cur) { switch_scene<true>(B, ch.x, wsc, frames, S); cur = ch.x; }
-        check_config_chunk<FAST>(*wsc, S, q, offset, (long long)ch.y, ch.z, res, band_on, band, queue, qcap, ctl, pc,
+        check_config_chunk<FAST>(*wsc, S, q, offset, (long long)ch.y, ch.z, res, band_on, band, bq, ctl, pc,
                                  exec);
     }
     exec = warp_sum(exec);
@@ -1184,7 +1318,7 @@ __global__ void GPRM_BOUNDS k_check_configs_multi(BatchView B, const float* __re
 template <int POLICY, bool FAST>
 __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __restrict__ qs, const float* __restrict__ qe,
                                                 long long offset, unsigned* __restrict__ key, int band_on, float band,
-                                                uint2* __restrict__ queue, unsigned qcap, Control* ctl)
+                                                BandQueue bq, Control* ctl)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1201,8 +1335,8 @@ __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __rest
         if (eu >= (unsigned long long)B.nwork) break;
         const int p = problem_of(B, (long long)eu);
         if (p != cur) { switch_scene<false>(B, p, wsc, frames, S); cur = p; }
-        check_edge<POLICY, false, FAST>(*wsc, S, qs, qe, (long long)eu, offset, wsc->dq, key, band_on, band, queue,
-                                        qcap, ctl, pc, exec, nominal);
+        check_edge<POLICY, false, FAST>(*wsc, S, qs, qe, (long long)eu, offset, wsc->dq, key, band_on, band, bq, ctl,
+                                        pc, exec, nominal);
     }
     flush_edge_counts(exec, nominal, pc, ctl);
 }
@@ -1210,19 +1344,52 @@ __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __rest
 __global__ void __launch_bounds__(128) k_recheck_multi(BatchView B, int kind, const float* __restrict__ q,
                                                        const float* __restrict__ qs, const float* __restrict__ qe,
                                                        long long offset, int policy, int* __restrict__ res,
-                                                       unsigned* __restrict__ key, const uint2* __restrict__ queue,
-                                                       unsigned qcap, Control* ctl)
+                                                       unsigned* __restrict__ key, BandQueue bq, Control* ctl)
 {
     unsigned cnt = ctl->qcount;
-    if (cnt > qcap) cnt = qcap;
+    if (cnt > bq.cap) cnt = bq.cap;
     unsigned long long checks = 0, flips = 0;
     for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
-        const uint2 it = queue[idx];
+        const uint2 it = bq.items[idx];
         const DevScene& sc = B.scenes[problem_of(B, (long long)it.x)];
         recheck_item(sc, kind, it, q, qs, qe, offset, sc.dq, policy, res, key, checks, flips);
     }
     if (checks) atomicAdd(&ctl->band_checks, checks);
     if (flips) atomicAdd(&ctl->band_flips, flips);
+}
+
+/* The overflow pass over many problems: each item's problem by binary
+ * search over the layout's offsets. */
+template <bool FAST>
+__global__ void __launch_bounds__(128) k_overflow_multi(BatchView B, int kind, const float* __restrict__ q,
+                                                        const float* __restrict__ qs, const float* __restrict__ qe,
+                                                        long long offset, int policy, float band,
+                                                        int* __restrict__ res, unsigned* __restrict__ key,
+                                                        BandQueue bq, Control* ctl)
+{
+    const unsigned long long cnt = ctl->ovf_count;
+    if (cnt == 0 || !bq.ovf) return;
+    unsigned long long checks = 0, flips = 0;
+    for (unsigned long long idx = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; idx < cnt;
+         idx += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned x = bq.ovf[idx];
+        const DevScene& sc = B.scenes[problem_of(B, (long long)x)];
+        overflow_item<FAST>(sc, kind, x, q, qs, qe, offset, sc.dq, policy, band, res, key, checks, flips);
+    }
+    if (checks) atomicAdd(&ctl->band_checks, checks);
+    if (flips) atomicAdd(&ctl->band_flips, flips);
+}
+
+cudaError_t launch_overflow_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,
+                                  const float* qe, long long offset, int policy, float band, int* res, unsigned* key,
+                                  BandQueue bq, Control* ctl, cudaStream_t st)
+{
+    if (!bq.ovf) return cudaSuccess;
+    if (B.fast)
+        k_overflow_multi<true><<<blocks, 128, 0, st>>>(B, kind, q, qs, qe, offset, policy, band, res, key, bq, ctl);
+    else
+        k_overflow_multi<false><<<blocks, 128, 0, st>>>(B, kind, q, qs, qe, offset, policy, band, res, key, bq, ctl);
+    return cudaGetLastError();
 }
 
 static const void* batch_kernel_fn(int vertex_kernel, int policy, bool fast)
@@ -1263,27 +1430,27 @@ cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int th
 }
 
 cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg, const float* q, long long offset,
-                                       int* res, int band_on, float band, uint2* queue, unsigned qcap, Control* ctl,
+                                       int* res, int band_on, float band, BandQueue bq, Control* ctl,
                                        cudaStream_t st)
 {
     if (B.nwork <= 0) return cudaSuccess;
     if (B.fast)
         k_check_configs_multi<true><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on, band,
-                                                                                    queue, qcap, ctl);
+                                                                                    bq, ctl);
     else
         k_check_configs_multi<false><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on,
-                                                                                     band, queue, qcap, ctl);
+                                                                                     band, bq, ctl);
     return cudaGetLastError();
 }
 
 cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, const float* qs, const float* qe,
                                      long long offset, int policy, unsigned* key, int band_on, float band,
-                                     uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
+                                     BandQueue bq, Control* ctl, cudaStream_t st)
 {
     if (B.nwork <= 0) return cudaSuccess;
 #define GPRM_MULTI_LAUNCH(POL_, FAST_)                                                                       \
     k_check_edges_multi<POL_, FAST_><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, qs, qe, offset, key,    \
-                                                                                     band_on, band, queue, qcap, \
+                                                                                     band_on, band, bq, \
                                                                                      ctl)
     if (policy == EDGE_EARLY_EXIT) { if (B.fast) GPRM_MULTI_LAUNCH(EDGE_EARLY_EXIT, true); else GPRM_MULTI_LAUNCH(EDGE_EARLY_EXIT, false); }
     else { if (B.fast) GPRM_MULTI_LAUNCH(EDGE_ALL_STEPS, true); else GPRM_MULTI_LAUNCH(EDGE_ALL_STEPS, false); }
@@ -1293,9 +1460,9 @@ cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, c
 
 cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,
                                  const float* qe, long long offset, int policy, int* res, unsigned* key,
-                                 const uint2* queue, unsigned qcap, Control* ctl, cudaStream_t st)
+                                 BandQueue bq, Control* ctl, cudaStream_t st)
 {
-    k_recheck_multi<<<blocks, 128, 0, st>>>(B, kind, q, qs, qe, offset, policy, res, key, queue, qcap, ctl);
+    k_recheck_multi<<<blocks, 128, 0, st>>>(B, kind, q, qs, qe, offset, policy, res, key, bq, ctl);
     return cudaGetLastError();
 }
 
@@ -1311,6 +1478,7 @@ __global__ void k_accumulate(const Control* c, Control* total)
     atomicAdd(&total->cert_far, c->cert_far);
     atomicAdd(&total->cert_dir, c->cert_dir);
     atomicAdd(&total->full_tests, c->full_tests);
+    atomicAdd(&total->ovf_count, c->ovf_count);
     atomicOr(&total->flags, c->flags);
     atomicAdd(&total->next, 1ull);  /* requests completed */
 }

@@ -755,6 +755,7 @@ struct FuParams {
     const float* b5;
     float* p;
     unsigned* err;
+    long long wait_cycles;          /* budget of each pipeline wait (the drains keep FU_WAIT_CYCLES) */
 };
 
 __device__ __forceinline__ void fu_arrive(uint32_t bar)
@@ -772,18 +773,19 @@ __device__ __forceinline__ bool fu_try(uint32_t bar, uint32_t parity)
     return done != 0;
 }
 
-/* Waits for the phase of `parity`; false when the clock budget runs out
- * (sets the abort flag and *err) or another role has aborted.  Roles off
+/* Waits for the phase of `parity`; false when the clock budget (cycles)
+ * runs out (sets the abort flag and *err) or another role has aborted.  Roles off
  * the critical path pass a sleep between polls, so that their polling does
  * not take issue slots from the epilogue warps on the same SM sub-partition. */
 __device__ __forceinline__ bool fu_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, unsigned* err,
-                                        unsigned sleep_ns = 0)
+                                        long long budget, unsigned sleep_ns = 0)
 {
     const long long t0 = clock64();
+    if (budget <= 0) budget = FU_WAIT_CYCLES;
     while (!fu_try(bar, parity)) {
         if (sleep_ns) __nanosleep(sleep_ns);
         if (*abort_flag) return false;
-        if (clock64() - t0 > FU_WAIT_CYCLES) {
+        if (clock64() - t0 > budget) {
             *abort_flag = 1;
             atomicOr(err, 1u);
             return false;
@@ -911,7 +913,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
         for (int tile = blockIdx.x, it = 0; tile < ntiles && ok; tile += gridDim.x, ++it) {
             for (int l = 0; l < NLAYER; ++l) {
                 const int a = l & 1;
-                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_ACCFULL + a), (af_ph >> a) & 1u, abort_flag, P.err));
+                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_ACCFULL + a), (af_ph >> a) & 1u, abort_flag, P.err, P.wait_cycles));
                 if (!ok) break;
                 af_ph ^= 1u << a;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -970,7 +972,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                     /* output head: partials 1-3 are handed to the warps of partial 0 */
                     if (q > 0) {
                         if (it > 0) {
-                            ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADEMPTY), he_ph, abort_flag, P.err));
+                            ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADEMPTY), he_ph, abort_flag, P.err, P.wait_cycles));
                             if (!ok) break;
                             he_ph ^= 1u;
                         }
@@ -978,7 +980,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                         __syncwarp();
                         if (lane == 0) fu_arrive(bar(FB_HEADFULL));
                     } else {
-                        ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADFULL), hf_ph, abort_flag, P.err));
+                        ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_HEADFULL), hf_ph, abort_flag, P.err, P.wait_cycles));
                         if (!ok) break;
                         hf_ph ^= 1u;
                         const float logit = ((part + red[TC_ROWS + rl]) + (red[2 * TC_ROWS + rl] + red[3 * TC_ROWS + rl])) +
@@ -999,7 +1001,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 for (int ch = 0; ch < (NLAYER - 1) * FU_CHUNKS; ++ch, ++issued) {
                     const uint32_t st = issued % FU_NS, k = issued / FU_NS;
-                    if (k > 0 && !(ok = fu_wait(bar(FB_WEMPTY + st), (k - 1) & 1u, abort_flag, P.err, 32u))) break;
+                    if (k > 0 && !(ok = fu_wait(bar(FB_WEMPTY + st), (k - 1) & 1u, abort_flag, P.err, P.wait_cycles, 32u))) break;
                     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
                                  :: "r"(bar(FB_WFULL + st)), "r"(FU_CHUNK_BYTES) : "memory");
                     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
@@ -1024,13 +1026,13 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                     const int a = l & 1;
                     /* the accumulator's previous layer has been read out */
                     if ((used >> a) & 1u) {
-                        if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), (ae_ph >> a) & 1u, abort_flag, P.err))) break;
+                        if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), (ae_ph >> a) & 1u, abort_flag, P.err, P.wait_cycles))) break;
                         ae_ph ^= 1u << a;
                     }
                     used |= 1u << a;
                     const uint32_t acc = tmem + (uint32_t)(a * TC_COLS);
                     if (l == 0) {
-                        if (!(ok = fu_wait(bar(FB_FEATREADY), fr_ph, abort_flag, P.err))) break;
+                        if (!(ok = fu_wait(bar(FB_FEATREADY), fr_ph, abort_flag, P.err, P.wait_cycles))) break;
                         fr_ph ^= 1u;
                         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                         fu_mma(acc, fd, w1d, 0u);
@@ -1039,9 +1041,9 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                         for (int c = 0; c < FU_CHUNKS; ++c, ++consumed) {
                             /* K columns 64c.. of the previous layer's activations (hready
                                phases advance once per hidden layer, in order) */
-                            if (!(ok = fu_wait(bar(FB_HREADY + c), hr_ph, abort_flag, P.err))) break;
+                            if (!(ok = fu_wait(bar(FB_HREADY + c), hr_ph, abort_flag, P.err, P.wait_cycles))) break;
                             const uint32_t st = consumed % FU_NS;
-                            if (!(ok = fu_wait(bar(FB_WFULL + st), (consumed / FU_NS) & 1u, abort_flag, P.err))) break;
+                            if (!(ok = fu_wait(bar(FB_WFULL + st), (consumed / FU_NS) & 1u, abort_flag, P.err, P.wait_cycles))) break;
                             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
                             for (int s2 = 0; s2 < FU_CK / 16; ++s2) {
@@ -1069,7 +1071,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
         bool ok = true;
         for (int tile = blockIdx.x, it = 0; tile < ntiles; tile += gridDim.x, ++it) {
             if (it > 0) {
-                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_FEATEMPTY), fe_ph, abort_flag, P.err, 256u));
+                ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(FB_FEATEMPTY), fe_ph, abort_flag, P.err, P.wait_cycles, 256u));
                 if (!ok) break;
                 fe_ph ^= 1u;
             }
@@ -1147,6 +1149,7 @@ struct TgArgs {
     float* ws;                 /* TG_WPART: [splits][M x ldc] */
     int ldc;
     unsigned* err;
+    long long wait_cycles;     /* budget of each pipeline wait (the drains keep FU_WAIT_CYCLES) */
 };
 
 __device__ __forceinline__ void tg_tma_load(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
@@ -1197,7 +1200,7 @@ k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
             int c = 0;
             for (; c < nchunks && ok; ++c) {
                 const int s = c % TG_STAGES, k = c / TG_STAGES;
-                if (k > 0 && !(ok = fu_wait(bar(TG_STAGES + s), (k - 1) & 1u, abort_flag, g.err))) break;
+                if (k > 0 && !(ok = fu_wait(bar(TG_STAGES + s), (k - 1) & 1u, abort_flag, g.err, g.wait_cycles))) break;
                 const uint32_t a_dst = st0 + (uint32_t)(s * L::STAGE);
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
                              :: "r"(bar(s)), "r"((uint32_t)L::STAGE) : "memory");
@@ -1213,7 +1216,7 @@ k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
             bool ok = true;
             for (int c = 0; c < nchunks && ok; ++c) {
                 const int s = c % TG_STAGES;
-                if (!(ok = fu_wait(bar(s), (c / TG_STAGES) & 1u, abort_flag, g.err))) break;
+                if (!(ok = fu_wait(bar(s), (c / TG_STAGES) & 1u, abort_flag, g.err, g.wait_cycles))) break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t a = st0 + (uint32_t)(s * L::STAGE), b = a + (uint32_t)L::A_BYTES;
 #pragma unroll
@@ -1226,13 +1229,16 @@ k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
                 }
                 fu_commit(bar(TG_STAGES + s));
             }
-            /* accfull: every MMA issued has completed (also on the abort path) */
+            /* accfull: every MMA issued has completed; on the abort path the
+               epilogue stops waiting for it, so this thread waits (under the
+               drain budget) before the CTA frees its tensor memory */
             fu_commit(bar(2 * TG_STAGES));
+            fu_wait_drain(bar(2 * TG_STAGES), 0u, g.err);
         }
     } else {
         const int q = warp & 3;                      /* TMEM lane quarter */
         const int rl = 32 * q + lane, m = m0 + rl;
-        const bool ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(2 * TG_STAGES), 0u, abort_flag, g.err));
+        const bool ok = __all_sync(FULL_MASK_MLP, fu_wait(bar(2 * TG_STAGES), 0u, abort_flag, g.err, g.wait_cycles));
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         if (ok) {
 #pragma unroll 1
@@ -1443,11 +1449,15 @@ struct gprm_mlp {
     const long long* idx_off = nullptr; /* set while a training epoch is captured */
     CUtensorMap m_x64, m_h[NLAYER - 1], m_dz[NLAYER], m_w1p, m_w[NLAYER - 1], m_wt[NLAYER - 1], m_ta, m_tb256, m_tb64;
     unsigned* dev_err = nullptr;
+    long long wait_cycles = 0;          /* pipeline wait budget of the tensor-core kernels, 0 = default */
     int sms = 0;
     std::string err = "no error";
 };
 
 namespace {
+
+/* The pipeline wait budget the tensor-core kernels get (0: their default). */
+long long wait_budget(const gprm_mlp* h) { return h->wait_cycles; }
 
 int mfail(gprm_mlp* h, int code, const char* msg, cudaError_t e = cudaSuccess)
 {
@@ -1576,7 +1586,7 @@ int forward_tc(gprm_mlp* h, int n, float* p, const float* y, const int* yidx, fl
     for (int l = 0; l < NLAYER; ++l) {
         TgArgs a{};
         a.M = n; a.N = HID; a.K = l == 0 ? 64 : HID; a.kps = a.K;
-        a.bias = h->w + h->offB[l]; a.zout = h->Z[l]; a.hout = h->H[l]; a.ldc = HID; a.err = h->dev_err;
+        a.bias = h->w + h->offB[l]; a.zout = h->Z[l]; a.hout = h->H[l]; a.ldc = HID; a.err = h->dev_err; a.wait_cycles = wait_budget(h);
         k_tc_gemm<TG_FWD, TG_BN_LAYER><<<grid, TG_THREADS, TgSmem<TG_BN_LAYER>::BYTES, st>>>(
             l == 0 ? h->m_x64 : h->m_h[l - 1],
                                                                           l == 0 ? h->m_w1p : h->m_w[l - 1], a);
@@ -1610,7 +1620,7 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
         k_transpose_bf16<<<dim3(kin_p / 32, (n + 31) / 32), tblock, 0, st>>>(n, kin_p, l == 0 ? h->X64 : h->H[l - 1],
                                                                              kin_p, h->Tb, h->ldT);
         TgArgs a{};
-        a.M = HID; a.N = kin_p; a.K = n; a.kps = kps; a.ws = h->ws; a.ldc = kin_p; a.err = h->dev_err;
+        a.M = HID; a.N = kin_p; a.K = n; a.kps = kps; a.ws = h->ws; a.ldc = kin_p; a.err = h->dev_err; a.wait_cycles = wait_budget(h);
         if (l == 0)
             k_tc_gemm<TG_WPART, 64><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<64>::BYTES, st>>>(
                 h->m_ta, h->m_tb64, a);
@@ -1630,6 +1640,7 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
             TgArgs d{};
             d.M = n; d.N = HID; d.K = HID; d.kps = HID; d.zin = h->Z[l - 1]; d.hout = h->dZ[l - 1]; d.ldc = HID;
             d.err = h->dev_err;
+            d.wait_cycles = wait_budget(h);
             k_tc_gemm<TG_DH, TG_BN_LAYER><<<dim3(HID / TG_BN_LAYER, (n + TC_ROWS - 1) / TC_ROWS, 1), TG_THREADS,
                                             TgSmem<TG_BN_LAYER>::BYTES, st>>>(
                 h->m_dz[l], h->m_wt[l - 1], d);
@@ -1774,6 +1785,7 @@ int predict_fused(gprm_mlp* h, const float* q, int n, int offset, float* p, cuda
     P.b5 = h->w + h->offB[NLAYER];
     P.p = p;
     P.err = h->dev_err;
+    P.wait_cycles = wait_budget(h);
     const int tiles = (n + TC_ROWS - 1) / TC_ROWS;
     const int grid = tiles < h->sms ? tiles : h->sms;
     k_mlp_fused<<<grid, FU_THREADS, FuSmem::BYTES, st>>>(P);
@@ -2041,6 +2053,15 @@ int gprm_mlp_set_training(gprm_mlp* h, int path)
     if (path != GPRM_MLP_TRAIN_TCGEN05 && path != GPRM_MLP_TRAIN_MMA_SYNC)
         return mfail(h, GPRM_ERR_ARG, "unknown training path");
     h->train_path = path;
+    return GPRM_OK;
+}
+
+int gprm_mlp_set_wait_budget(gprm_mlp* h, long long cycles)
+{
+    if (!h || cycles < 0) return GPRM_ERR_ARG;
+    MLP_TRY(h, cudaDeviceSynchronize());
+    h->wait_cycles = cycles;
+    if (h->dev_err) MLP_TRY(h, cudaMemset(h->dev_err, 0, sizeof(unsigned)));
     return GPRM_OK;
 }
 

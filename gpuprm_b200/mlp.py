@@ -96,6 +96,13 @@ class CollisionMLP:
         code = {"tcgen05": _abi.GPRM_MLP_TRAIN_TCGEN05, "mma_sync": _abi.GPRM_MLP_TRAIN_MMA_SYNC}[path]
         self._check(self.lib.gprm_mlp_set_training(self.h, code))
 
+    def set_wait_budget(self, cycles: int = 0) -> None:
+        """Test hook: clock budget of the tensor-core kernels' pipeline waits
+        (0 = default, about a second); also clears the device status."""
+        st = self.lib.gprm_mlp_set_wait_budget(self.h, int(cycles))
+        if st != 0:
+            raise RuntimeError(self.lib.gprm_mlp_last_error(self.h).decode())
+
     def device_status(self) -> int:
         """Synchronises; 0 unless a tensor-core layer gave up waiting for its MMAs."""
         f = C.c_uint(0)

@@ -115,6 +115,8 @@ typedef struct gprm_stats {
     int64_t launches;             /* kernels launched */
     int64_t pairs_certified;      /* FP32 pair tests settled by a separation certificate */
     int64_t pairs_tested;         /* FP32 pair tests that ran the full iteration */
+    int64_t band_overflow_items;  /* configurations or edges the FP64 queue could not hold,
+                                     recomputed in full by the overflow pass */
 } gprm_stats;
 
 /* ---- lifetime --------------------------------------------------------- */
@@ -250,6 +252,14 @@ int gprm_mlp_adam_step(gprm_mlp* h, float lr);
 /* training: perm (device) holds `epochs` permutations of 0..n-1 */
 int gprm_mlp_train(gprm_mlp* h, const float* q, const float* y, int n, int offset, const int* perm,
                    int epochs, int batch, float lr, float* losses);
+/* Test hook: the clock budget (SM cycles) of every pipeline wait of the
+ * tensor-core kernels (fused inference, training GEMMs); 0 restores the
+ * default (about one second).  A budget too small for the copies and MMAs
+ * makes the waits expire: the kernel stops, drains its own copies and MMAs
+ * under the default budget, frees its tensor memory and returns, and
+ * gprm_mlp_device_status reports it.  Setting the budget also clears that
+ * status.  No counterpart in the reference. */
+int gprm_mlp_set_wait_budget(gprm_mlp* h, long long cycles);
 
 /* ---- vertex checks without allocation (no counterpart in the reference) --
  * For callers that must not allocate device memory while they run: a
@@ -292,8 +302,10 @@ int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q, int* res,
  * gprm_indicator2 would give item i on its own handle.  set_layout
  * allocates (and synchronises); the check calls allocate nothing and never
  * synchronise.  queue_capacity: FP64 recheck queue entries, 0 = total for
- * configurations (cannot overflow), 4*total + 65536 for edges; an
- * overflow is reported by gprm_batch_get_stats.  Calls on one batch share
+ * configurations, 4*total + 65536 for edges; any capacity gives complete
+ * results (the checks it cannot hold are recomputed by the overflow pass
+ * on the stream, counted in gprm_batch_get_stats' band_overflow_items).
+ * Calls on one batch share
  * its control block: do not overlap them on different streams. */
 typedef struct gprm_batch gprm_batch;
 int  gprm_batch_create(gprm_space* const* spaces, int count, gprm_batch** out);
@@ -413,6 +425,22 @@ int gprm_sample_near(int ndof, const float* nodes, int n, int stride, const int*
  * out[(ndof+1)*12], frame f column c row r at out[f*12 + c*3 + r], in the
  * column layout of trafo4 (geo4.h:24). */
 int gprm_debug_fk(gprm_space* h, const float* q, float* out);
+
+/* Test hook, process-wide: the nth device allocation of the library from
+ * now on (checker handles and batches) fails as if the device were out of
+ * memory (0 = none).  The call that makes it returns GPRM_ERR_NOMEM and
+ * leaves its handle usable: a later call allocates again.  No counterpart
+ * in the reference (it aborts on any CUDA error, util.hpp:45). */
+void gprm_debug_fail_device_alloc(long long nth);
+
+/* Test hook: caps the FP64 recheck queue of every later request at
+ * `capacity` entries (0 = no cap), so that tests can make it overflow.
+ * Results do not depend on it: checks the queue cannot hold are recorded
+ * per configuration or edge and recomputed in full on the stream after the
+ * recheck (counted in gprm_stats.band_overflow_items); only the code of an
+ * early-exit edge may change, to that of its first colliding step in step
+ * order.  No counterpart in the reference. */
+int gprm_debug_set_queue_capacity(gprm_space* h, unsigned capacity);
 
 /* Support candidates of the fast path (GPRM_MODE_FAST) for polytope
  * `polytope` and direction bin `bin` (0..53: cube face 0..5 = +x,-x,+y,-y,
