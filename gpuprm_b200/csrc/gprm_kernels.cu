@@ -139,20 +139,27 @@ __device__ __forceinline__ SceneView stage_scene(const DevScene& sc, unsigned ch
  * (lanes whose frames are current): centre m = the midpoint of the lanes'
  * bounding box, radius rho >= max |c_lane - m| (the box half-diagonal from
  * m, rounded up).  Lanes with a non-finite centre make rho infinite, which
- * disables the sweep test for the slot.  One lane per slot. */
+ * disables the sweep tests for the slot.  Lanes 0.. nslots-1 bound the
+ * slots' ball centres (sweep[slot]); with at most SWEEP_V0_SLOTS slots,
+ * lanes 16.. bound the slots' vertex 0 the same way (sweep[SWEEP_V0_SLOTS
+ * + slot]), for the swept direction test of cert_scan. */
+constexpr int SWEEP_V0_SLOTS = GPRM_MAX_SLOTS / 2;
 __device__ __forceinline__ void sweep_bounds(const DevScene& sc, const SceneView& S, unsigned mask)
 {
     const int lane = threadIdx.x & 31;
     __syncwarp();   /* the lanes' centres are written */
-    if (lane < sc.nslots) {
-        const float* c0 = S.cen - lane;   /* lane 0's centres; lane i at +i */
+    const bool v0 = lane >= 16 && lane - 16 < sc.nslots && sc.nslots <= SWEEP_V0_SLOTS;
+    if (lane < sc.nslots || v0) {
+        const int sl = v0 ? lane - 16 : lane;
+        /* lane 0's points of slot sl; lane i at +i */
+        const float* c0 = S.cen - lane + (v0 ? sc.nslots * 3 * 32 : 0) + sl * 3 * 32;
         float lo[3], hi[3];
         bool bad = false;
         for (int c = 0; c < 3; ++c) { lo[c] = PF32::inf(); hi[c] = -PF32::inf(); }
         for (unsigned m = mask; m; m &= m - 1u) {
             const int i = __ffs(m) - 1;
             for (int c = 0; c < 3; ++c) {
-                const float v = c0[(lane * 3 + c) * 32 + i];
+                const float v = c0[c * 32 + i];
                 bad |= !isfinite(v);
                 lo[c] = fminf(lo[c], v);
                 hi[c] = fmaxf(hi[c], v);
@@ -166,7 +173,7 @@ __device__ __forceinline__ void sweep_bounds(const DevScene& sc, const SceneView
         }
         float rho = __fsqrt_ru(e2) * (1.0f + 4e-6f) + 1e-30f;
         if (bad || !mask || !isfinite(rho)) rho = PF32::inf();
-        S.sweep[lane] = make_float4(mc[0], mc[1], mc[2], rho);
+        S.sweep[v0 ? SWEEP_V0_SLOTS + sl : sl] = make_float4(mc[0], mc[1], mc[2], rho);
     }
     __syncwarp();
 }
@@ -215,6 +222,40 @@ __device__ __forceinline__ int cert_dist_dir(const DevScene& sc, const SceneView
     return (n2 > 1e-6f && G - err > sc.thr_dir) ? 2 : 0;
 }
 
+/* The direction test of pair_certified_dir for every lane of the warp at
+ * once, for a pair with one moving polytope (slot balls bc: its ball
+ * centre, bv: its vertex 0, over the lanes; f: the static partner's ball
+ * centre; b: its vertex 0 and R).  With s = b_Q - a_P (vertex 0 of Q minus
+ * that of P) = sbar - alpha, |alpha| <= rho_v, and D = c_Q - c_P = Dbar -
+ * gamma, |gamma| <= rho_c, every lane has
+ *     <s, D> >= <sbar, Dbar> - |sbar| rho_c - rho_v |Dbar| - rho_v rho_c = N
+ *     |s| in [|sbar| - rho_v, |sbar| + rho_v],  |D| <= |Dbar| + rho_c,
+ * so when N > 0, its G - err of the per-lane test is at least
+ *     N / (|sbar| + rho_v) - R - (|Dbar| + rho_c + R)(eps_dir / (|sbar| - rho_v) + 1e-6),
+ * which must exceed thr_dir (with 1e-5 relative allowances for the
+ * rounding of this bound).  True when every lane's test would certify. */
+__device__ __forceinline__ bool swept_direction(const DevScene& sc, bool moving_p, float4 bc, float4 bv, float4 f,
+                                                float4 b)
+{
+    float sx, sy, sz, dx, dy, dz;
+    if (moving_p) {
+        sx = b.x - bv.x; sy = b.y - bv.y; sz = b.z - bv.z;
+        dx = f.x - bc.x; dy = f.y - bc.y; dz = f.z - bc.z;
+    } else {
+        sx = bv.x - b.x; sy = bv.y - b.y; sz = bv.z - b.z;
+        dx = bc.x - f.x; dy = bc.y - f.y; dz = bc.z - f.z;
+    }
+    const float sn = sqrtf(__fmaf_rn(sx, sx, __fmaf_rn(sy, sy, sz * sz)));
+    const float dn = sqrtf(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz)));
+    const float rv = bv.w, rc = bc.w;
+    const float N = __fmaf_rn(sx, dx, __fmaf_rn(sy, dy, sz * dz)) * (1.0f - 1e-5f) -
+                    (sn * rc + rv * dn + rv * rc) * (1.0f + 1e-5f);
+    const float slo = (sn - rv) * (1.0f - 1e-5f), sup = (sn + rv) * (1.0f + 1e-5f);
+    if (!(N > 0.0f) || !(slo > 1e-3f)) return false;
+    const float err = (dn + rc + b.w) * (sc.eps_dir / slo + 1e-6f) * (1.0f + 1e-5f);
+    return (N / sup) * (1.0f - 1e-5f) - b.w * (1.0f + 1e-5f) - err > sc.thr_dir;
+}
+
 /* Certificates of pairs j0 .. j0+jn-1 (jn <= 32) for this lane, all
  * order-free (a certified pair is free with its margin above the band, so
  * it changes neither a code nor a band decision), in three stages:
@@ -222,7 +263,9 @@ __device__ __forceinline__ int cert_dist_dir(const DevScene& sc, const SceneView
  *             j0+k against the sweep ball of its moving slot: a pair whose
  *             static partner lies farther than rho + sqrt(T2) from the sweep
  *             centre is settled for every lane at once (each lane's exact
- *             distance then exceeds sqrt(T2));
+ *             distance then exceeds sqrt(T2)); else the direction test is
+ *             bounded over every lane at once (swept_direction) from the
+ *             balls of the slot's centre and vertex 0;
  *   per lane  the other pairs, two at a time: the ball-distance and
  *             direction tests (cert_dist_dir), then for the few pairs both
  *             miss the box test of pair_certified_dir; pairs the scan cannot
@@ -236,26 +279,32 @@ __device__ __forceinline__ unsigned cert_scan(const DevScene& sc, const SceneVie
 {
     const int lane = threadIdx.x & 31;
     const unsigned all = jn >= 32 ? FULL_MASK : ((1u << jn) - 1u);
-    unsigned cand = all;
+    unsigned cand = all, swept_dir = 0u;
     if constexpr (SWEPT) {
-        bool maybe = false;
+        bool maybe = false, by_dir = false;
         if (lane < jn) {
             maybe = true;
             const int4 c = S.scan_c[j0 + lane];
             if (c.w && ((c.x < 0) != (c.y < 0))) {
+                const int ms = c.x >= 0 ? c.x : c.y;
                 const float4 f = S.far[j0 + lane];
-                const float4 b = S.sweep[c.x >= 0 ? c.x : c.y];
+                const float4 b = S.sweep[ms];
                 const float dx = f.x - b.x, dy = f.y - b.y, dz = f.z - b.z;
                 const float dd2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
                 const float A = (__int_as_float(c.z) + b.w) * (1.0f + 1e-6f);
                 /* |m - c|^2 >= dd2 (1 - 1e-6) > A^2 >= (rho + sqrt(T2))^2 */
                 if (dd2 * (1.0f - 1e-6f) > A * A) maybe = false;
+                else if (sc.nslots <= SWEEP_V0_SLOTS &&
+                         swept_direction(sc, c.x >= 0, b, S.sweep[SWEEP_V0_SLOTS + ms], f, S.scan_b[j0 + lane]))
+                    maybe = false, by_dir = true;
             }
         }
         cand = __ballot_sync(FULL_MASK, maybe);
+        swept_dir = __ballot_sync(FULL_MASK, by_dir);
     }
     if (!active) return 0u;
-    pc.far += (unsigned)__popc(all & ~cand);
+    pc.far += (unsigned)__popc(all & ~cand & ~swept_dir);
+    pc.dir += (unsigned)__popc(swept_dir);
     unsigned need = 0;
 #pragma unroll 1
     while (cand) {
