@@ -159,7 +159,7 @@ void clip_halfplane(std::vector<double>& poly, double a, double b, double c)
  * <d, x_i - x_j> >= 0 for every CRS neighbour j of i (its normal cone,
  * enlarged when the adjacency misses an edge, so the set can only grow).
  * A bin's directions are d = s e_a + u e_b + v e_c on its cube face, with
- * (u, v) in the bin's cell of [-1, 1]^2 widened by 1e-3 on every side to
+ * (u, v) in the bin's cell of [-1, 1]^2 widened by 1e-2 on every side to
  * cover the float evaluation of dir_bin near cell and face borders.  Lists
  * hold ascending vertex indices; an empty list (rounding) falls back to
  * every vertex. */
@@ -168,7 +168,7 @@ void compute_support_candidates(gprm_space* h, const gprm_scene_desc* d, const s
 {
     h->cbin.assign((size_t)GPRM_START_BINS * h->npoly, 0u);
     h->cidx.clear();
-    const double eps = 1e-3, lo[3] = {-1.0 - eps, -1.0 / 3.0 - eps, 1.0 / 3.0 - eps},
+    const double eps = 1e-2, lo[3] = {-1.0 - eps, -1.0 / 3.0 - eps, 1.0 / 3.0 - eps},
                  hi[3] = {-1.0 / 3.0 + eps, 1.0 / 3.0 + eps, 1.0 + eps};
     std::vector<double> poly;
     std::vector<unsigned char> list;
@@ -367,7 +367,22 @@ int build_space(const gprm_scene_desc* d, float dq, int nbuf, gprm_space** out)
             h->tab[boff[k] + 2 + j] = entry(v);
         }
         h->tab[boff[k] + 1] = entry(0);
-        h->vinfo.push_back(make_int2((int)h->vtab.size(), n));
+        {
+            /* near-tie tolerance of the fast path's support values: 1e-5 of
+               the largest vertex norm (body frame), about three times the
+               largest difference between its dot products and the
+               reference's (their rounding, the frames' and the search
+               directions' accumulated rounding) */
+            double vmax = 0;
+            for (int i = 0; i < n; ++i) {
+                const float* x = d->vertices + 3 * (size_t)(voff[k] + i);
+                vmax = fmax(vmax, sqrt((double)x[0] * x[0] + (double)x[1] * x[1] + (double)x[2] * x[2]));
+            }
+            const float tie = (float)(1e-5 * vmax);
+            int tb;
+            memcpy(&tb, &tie, 4);
+            h->vinfo.push_back(make_int4((int)h->vtab.size(), n, tb, 0));
+        }
         for (int i = 0; i < n; ++i) h->vtab.push_back(entry(i));
         /* bounding ball: centre of the bounding box, radius to the farthest
            vertex (inflated in compute_certificates) */
@@ -789,7 +804,7 @@ int gprm_init(gprm_space* h, int rank, int size)
     size_t bxo = tb + 5 * pb + fsb, bxb = h->box.size() * sizeof(float4);
     bxo = (bxo + 15) & ~(size_t)15;
     const size_t vto = (bxo + bxb + 15) & ~(size_t)15, vtb = h->vtab.size() * sizeof(float4);
-    const size_t vio = vto + vtb, vib = h->vinfo.size() * sizeof(int2);
+    const size_t vio = vto + vtb, vib = h->vinfo.size() * sizeof(int4);
     const size_t cbo = (vio + vib + 15) & ~(size_t)15, cbb = h->cbin.size() * sizeof(unsigned);
     const size_t cio = cbo + cbb, cib = h->cidx.size();
     CUDA_TRY(h, dev_malloc((void**)&h->d_scene, cio + cib + 64));
@@ -831,7 +846,7 @@ int gprm_init(gprm_space* h, int rank, int size)
     s.ppoly = (const int2*)(base + tb + 5 * pb);
     s.box = bxb ? (const float4*)(base + bxo) : nullptr;
     s.vtab = (const float4*)(base + vto);
-    s.vinfo = (const int2*)(base + vio);
+    s.vinfo = (const int4*)(base + vio);
     s.cbin = cbb ? (const unsigned*)(base + cbo) : nullptr;
     s.cidx = (const unsigned char*)(base + cio);
     s.fast = (h->mode & GPRM_MODE_FAST) != 0;

@@ -82,9 +82,10 @@ struct DevScene {
     /* fast arithmetic (GPRM_MODE_FAST): the kernels run pair_test_fast */
     int fast;
     /* every polytope's vertices as table entries (xyz, packed w), and per
-       polytope (first entry, vertex count): the fast path's support search */
+       polytope (first entry, vertex count, near-tie tolerance of its support
+       values (float bits), 0): the fast path's support search */
     const float4* vtab;
-    const int2* vinfo;
+    const int4* vinfo;
     /* per polytope and direction bin: (byte offset into cidx << 8 | count)
        of the bin's support candidates, vertex indices in ascending order */
     const unsigned* cbin;
@@ -694,11 +695,14 @@ __device__ __forceinline__ float fnormalize3(V3<float>& u)
  * (the directions for which it is a maximiser) meets the bin, found on the
  * host for bins slightly larger than dir_bin's, so the maximum over the
  * list is the maximum over the whole polytope, up to ties within rounding.
- * A few candidates instead of every vertex; P and Q side by side. */
-__device__ __forceinline__ void fsupport_cand2(const DevScene& sc, int kP, float4& cp, float px, float py, float pz,
-                                               int kQ, float4& cq, float qx, float qy, float qz)
+ * A few candidates instead of every vertex; P and Q side by side.
+ * Returns true when the runner-up of either list comes within tieP / tieQ
+ * of its maximum: the reference's climb, in its own rounding, may then end
+ * at a different vertex. */
+__device__ __forceinline__ bool fsupport_cand2(const DevScene& sc, int kP, int4 vP, float4& cp, float px, float py,
+                                               float pz, int kQ, int4 vQ, float4& cq, float qx, float qy, float qz)
 {
-    const int2 vP = sc.vinfo[kP], vQ = sc.vinfo[kQ];
+    const float tieP = __int_as_float(vP.z), tieQ = __int_as_float(vQ.z);
     const unsigned hP = sc.cbin[kP * GPRM_START_BINS + dir_bin(px, py, pz)];
     const unsigned hQ = sc.cbin[kQ * GPRM_START_BINS + dir_bin(qx, qy, qz)];
     const unsigned char* LP = sc.cidx + (hP >> 8);
@@ -709,19 +713,29 @@ __device__ __forceinline__ void fsupport_cand2(const DevScene& sc, int kP, float
     int ip = LP[0], iq = LQ[0];
     float4 u = VP[ip], v = VQ[iq];
     float bp = fdot3(u.x, u.y, u.z, px, py, pz), bq = fdot3(v.x, v.y, v.z, qx, qy, qz);
+    const float ninf = __int_as_float(0xff800000);
+    float sp = ninf, sq = ninf;   /* runners-up */
     const int n = nP > nQ ? nP : nQ;
-    /* past its last candidate a list re-reads that candidate */
+    /* branch-free top two; past its last candidate a list re-reads that
+       candidate and counts it as -infinity */
 #pragma unroll 1
     for (int c = 1; c < n; ++c) {
         const int a = LP[c < nP ? c : nP - 1], b = LQ[c < nQ ? c : nQ - 1];
         u = VP[a];
         v = VQ[b];
-        const float du = fdot3(u.x, u.y, u.z, px, py, pz), dv = fdot3(v.x, v.y, v.z, qx, qy, qz);
-        if (du > bp) { bp = du; ip = a; }
-        if (dv > bq) { bq = dv; iq = b; }
+        float du = fdot3(u.x, u.y, u.z, px, py, pz), dv = fdot3(v.x, v.y, v.z, qx, qy, qz);
+        du = c < nP ? du : ninf;
+        dv = c < nQ ? dv : ninf;
+        ip = du > bp ? a : ip;
+        iq = dv > bq ? b : iq;
+        sp = fmaxf(sp, fminf(bp, du));
+        sq = fmaxf(sq, fminf(bq, dv));
+        bp = fmaxf(bp, du);
+        bq = fmaxf(bq, dv);
     }
     cp = VP[ip];
     cq = VQ[iq];
+    return !(bp - sp > tieP) || !(bq - sq > tieQ);
 }
 
 /* find_half_plane with orthtrafo23 (collision4.h:111-223), contracted */
@@ -791,6 +805,9 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
     int combs[GPRM_MAX_ITERS];
     float best = 0.0f;
     int k = 0, l = 0;
+    /* vertex lists, candidate lists and near-tie tolerances of the two */
+    const int4 vP = sc.vinfo[pp.x], vQ = sc.vinfo[pp.y];
+    bool tie = false;
 #pragma unroll 1
     for (; k < GPRM_MAX_ITERS && l < GPRM_MAX_ITERS; ++l) {
         V3<float> Sp, Sq;
@@ -798,7 +815,7 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
         else Sp = frot_t(tp, S.x, S.y, S.z);
         if (idQ) { Sq.x = -S.x; Sq.y = -S.y; Sq.z = -S.z; }
         else Sq = frot_t(tq, -S.x, -S.y, -S.z);
-        fsupport_cand2(sc, pp.x, ep, Sp.x, Sp.y, Sp.z, pp.y, eq, Sq.x, Sq.y, Sq.z);
+        tie |= fsupport_cand2(sc, pp.x, vP, ep, Sp.x, Sp.y, Sp.z, pp.y, vQ, eq, Sq.x, Sq.y, Sq.z);
         V3<float> p0, q0;
         if (idP) { p0.x = ep.x; p0.y = ep.y; p0.z = ep.z; }
         else p0 = fxform(tp, ep.x, ep.y, ep.z);
@@ -811,7 +828,7 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
         const float h = dp * rn;
         if (l == 0 || h > best) best = h;
         if (dp >= sc.sep_thr) {
-            *margin = h;
+            *margin = tie ? 0.0f : h;
             return 0;
         }
         hist[k] = r;
@@ -829,7 +846,7 @@ __device__ __forceinline__ int pair_test_fast(const DevScene& sc, const float4* 
                 fnormalize3(w);
             }
             if (k >= 2 && !fhalf_plane(hist, k, w, r)) {
-                *margin = best;
+                *margin = tie ? 0.0f : best;
                 return l + 1;
             }
             const float b = -2.0f * dp;

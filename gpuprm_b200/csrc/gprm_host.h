@@ -81,7 +81,7 @@ struct gprm_space {
     std::vector<int> pair_poly, pair_sys;  /* polytopes and frames of each pair */
     /* every polytope's vertices as table entries, and (first, count) per polytope */
     std::vector<float4> vtab;
-    std::vector<int2> vinfo;
+    std::vector<int4> vinfo;
     /* support candidates per polytope and direction bin (see fsupport_cand2) */
     std::vector<unsigned> cbin;
     std::vector<unsigned char> cidx;

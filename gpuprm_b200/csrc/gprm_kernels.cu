@@ -183,30 +183,36 @@ struct PairCounts {
     unsigned long long far, dir, full;
 };
 
-/* The distance and direction certificates of a usable pair (scan_c.w) for
- * this lane, branch-free so that two pairs can be evaluated side by side:
- * the ball-distance test of pair_certified, then its direction test with
- * the world vertex 0 of a moving polytope from its slot (the FK pass wrote
- * it with the FMA chain T*v0) and that of a static one from scan_b.
- * Returns 1 (distance), 2 (direction) or 0 (neither; *d2o and *Do get
- * |D|^2 and D = c_Q - c_P for the box test). */
-__device__ __forceinline__ int cert_dist_dir(const DevScene& sc, const SceneView& S, int4 c, float4 f, float4 b,
-                                             float* d2o, float3* Do)
+/* The ball-distance test of pair_certified for a usable pair (scan_c.w)
+ * and this lane: true when it certifies; *d2o and *Do get |D|^2 and D =
+ * c_Q - c_P (the moving ball centres from the slots, a static one from
+ * far). */
+__device__ __forceinline__ bool cert_dist(const SceneView& S, int4 c, float4 f, float* d2o, float3* Do)
 {
     const float* cen = S.cen;
-    const float* v0w = S.cen + sc.nslots * 3 * 32;
     float px = f.x, py = f.y, pz = f.z, qx = f.x, qy = f.y, qz = f.z;
-    float ax = b.x, ay = b.y, az = b.z, bx = b.x, by = b.y, bz = b.z;
-    if (c.x >= 0) {
-        px = cen[(c.x * 3) * 32]; py = cen[(c.x * 3 + 1) * 32]; pz = cen[(c.x * 3 + 2) * 32];
-        ax = v0w[(c.x * 3) * 32]; ay = v0w[(c.x * 3 + 1) * 32]; az = v0w[(c.x * 3 + 2) * 32];
-    }
-    if (c.y >= 0) {
-        qx = cen[(c.y * 3) * 32]; qy = cen[(c.y * 3 + 1) * 32]; qz = cen[(c.y * 3 + 2) * 32];
-        bx = v0w[(c.y * 3) * 32]; by = v0w[(c.y * 3 + 1) * 32]; bz = v0w[(c.y * 3 + 2) * 32];
-    }
+    if (c.x >= 0) { px = cen[(c.x * 3) * 32]; py = cen[(c.x * 3 + 1) * 32]; pz = cen[(c.x * 3 + 2) * 32]; }
+    if (c.y >= 0) { qx = cen[(c.y * 3) * 32]; qy = cen[(c.y * 3 + 1) * 32]; qz = cen[(c.y * 3 + 2) * 32]; }
     const float dx = qx - px, dy = qy - py, dz = qz - pz;
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, dz * dz));
+    *d2o = d2;
+    *Do = make_float3(dx, dy, dz);
+    return d2 > f.w;
+}
+
+/* The direction test of pair_certified for a usable pair whose distance
+ * test failed (D, d2 from cert_dist), the world vertex 0 of a moving
+ * polytope from its slot (the FK pass wrote it with the FMA chain T*v0)
+ * and that of a static one from scan_b; branch-free, so that two pairs can
+ * be evaluated side by side. */
+__device__ __forceinline__ bool cert_dir(const DevScene& sc, const SceneView& S, int4 c, float4 b, float d2,
+                                         float3 D)
+{
+    const float* v0w = S.cen + sc.nslots * 3 * 32;
+    float ax = b.x, ay = b.y, az = b.z, bx = b.x, by = b.y, bz = b.z;
+    if (c.x >= 0) { ax = v0w[(c.x * 3) * 32]; ay = v0w[(c.x * 3 + 1) * 32]; az = v0w[(c.x * 3 + 2) * 32]; }
+    if (c.y >= 0) { bx = v0w[(c.y * 3) * 32]; by = v0w[(c.y * 3 + 1) * 32]; bz = v0w[(c.y * 3 + 2) * 32]; }
+    const float dx = D.x, dy = D.y, dz = D.z;
     const float sx = bx - ax, sy = by - ay, sz = bz - az;
     const float n2 = __fmaf_rn(sx, sx, __fmaf_rn(sy, sy, sz * sz));
     const float inv = rsqrtf(n2);
@@ -216,10 +222,7 @@ __device__ __forceinline__ int cert_dist_dir(const DevScene& sc, const SceneView
     const float dn = d2 * rsqrtf(d2) * (1.0f + 2e-6f);
     /* direction error <= eps_dir*inv (+ rsqrt and rounding, 1e-6) */
     const float err = (dn + b.w) * __fmaf_rn(sc.eps_dir, inv, 1e-6f);
-    *d2o = d2;
-    *Do = make_float3(dx, dy, dz);
-    if (d2 > f.w) return 1;
-    return (n2 > 1e-6f && G - err > sc.thr_dir) ? 2 : 0;
+    return n2 > 1e-6f && G - err > sc.thr_dir;
 }
 
 /* The direction test of pair_certified_dir for every lane of the warp at
@@ -320,10 +323,20 @@ __device__ __forceinline__ unsigned cert_scan(const DevScene& sc, const SceneVie
         const int4 ca = S.scan_c[ja], cb = S.scan_c[jb];
         const float4 fa = S.far[ja], fb = S.far[jb];
         const float4 ba = S.scan_b[ja], bb = S.scan_b[jb];
-        float d2a, d2b;
-        float3 Da, Db;
-        int ra = ca.w ? cert_dist_dir(sc, S, ca, fa, ba, &d2a, &Da) : -1;
-        int rb = (two && cb.w) ? cert_dist_dir(sc, S, cb, fb, bb, &d2b, &Db) : -1;
+        float d2a = 0.0f, d2b = 0.0f;
+        float3 Da = make_float3(0.0f, 0.0f, 0.0f), Db = Da;
+        /* 1: distance, 2: direction, 0: neither, -1: not usable by the scan */
+        int ra = ca.w ? (cert_dist(S, ca, fa, &d2a, &Da) ? 1 : 0) : -1;
+        int rb = (two && cb.w) ? (cert_dist(S, cb, fb, &d2b, &Db) ? 1 : 0) : -1;
+        if (ra == 0 && rb == 0) {
+            /* both need the direction test: side by side */
+            const bool oa = cert_dir(sc, S, ca, ba, d2a, Da), ob = cert_dir(sc, S, cb, bb, d2b, Db);
+            ra = oa ? 2 : 0;
+            rb = ob ? 2 : 0;
+        } else {
+            if (ra == 0 && cert_dir(sc, S, ca, ba, d2a, Da)) ra = 2;
+            if (rb == 0 && cert_dir(sc, S, cb, bb, d2b, Db)) rb = 2;
+        }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             if (h == 1 && !two) break;
