@@ -36,7 +36,13 @@ Extra legs in the same line (not part of `value`):
              kernel against per-layer tcgen05 kernels and the training GEMMs;
              training throughput (batch 4096) with tcgen05 and mma.sync GEMMs;
   batch      256 independent problems in one graph-captured launch per kind
-             against a loop of per-problem launches.
+             against a loop of per-problem launches;
+  box4_prm   the reference's own CPU planning case: 4-DOF box arm, 16 box
+             obstacles, C-space radius 0.5 rad, dq 0.02 rad; GPUPRM's
+             planner (oracle/_ref/prm_dropin: process_mpi5 on its CPU
+             checker, and on this library's checker behind the same
+             interface) against the GPU eager and lazy PRMs, 8192 samples
+             upwards, on the same seeded free start/goal pairs.
 
 --impl reference times only that CPU checker (same metric/config).
 """
@@ -92,6 +98,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
     ap.add_argument("--no-sampler", action="store_true", help="skip the near-node sampler leg")
     ap.add_argument("--batch-problems", type=int, default=256)
+    ap.add_argument("--no-box4", action="store_true", help="skip the 4-DOF reference planner comparison")
+    ap.add_argument("--box4-queries", type=int, default=6)
     ap.add_argument("--no-mlp", action="store_true", help="skip the predictor inference leg")
     ap.add_argument("--mlp-rows", type=int, default=1 << 22)
     ap.add_argument("--only-mlp", action="store_true",
@@ -386,6 +394,9 @@ def run_ours(args, rank, world, local_rank):
     mlp = None
     if not args.no_mlp and world == 1:
         mlp = mlp_leg(args, dev)
+    box4 = None
+    if not args.no_box4 and world == 1:
+        box4 = box4_leg(args)
     line = {
         "metric": METRIC, "value": nominal_all / t_max, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
@@ -400,7 +411,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(E * 4)},
         "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clocks, "gpu_launches": launches,
         "prm": prm, "prm_stress": prm_stress, "stress_edges": stress_edges, "batch": batch, "sampler": sampler,
-        "mlp": mlp,
+        "mlp": mlp, "box4_prm": box4,
     }
     return line
 
@@ -422,6 +433,106 @@ def prm_leg(args, kind, dq, n_samples, k):
     out["scene"] = {"kind": kind, "ndof": psc.ndof, "polytopes": len(psc.polys), "pairs": len(psc.pair_from)}
     out["predictor"] = {"labels": 1 << 20, "epochs": 10, "batch": 4096, "lr": 1e-3,
                         "label_seconds": t_lab, "train_seconds": t_train, "final_loss": float(losses[-1])}
+    # what the network itself gains: the learned planner against the same
+    # lazy planner without it, with and without the cost of its labels and
+    # training spread over the query batch (the planners' times are whole
+    # batches of 1000 queries); the lazy scheduling's own gain over the
+    # eager planner is lazy_over_plain_time
+    lz, ln = out["lazy"]["batch_seconds"], out["learned"]["batch_seconds"]
+    out["network_gain"] = {
+        "learned_over_lazy_time": ln / lz,
+        "learned_with_training_over_lazy_time": (ln + t_lab + t_train) / lz,
+        "false_free_rate": out["predictor_errors"]["false_free_rate"],
+        "lazy_over_plain_time": out["lazy_over_plain_time"],
+        "note": "the <= 0.5x time-to-path of the learned planner against the eager one comes from the lazy "
+                "scheduling (lazy_over_plain_time); the network's own gain is learned_over_lazy_time",
+    }
+    return out
+
+
+BOX4 = dict(workload="box4 PRM: 4-DOF revolute arm of 0.3 x 0.05 x 0.05 m box links, 16 box obstacles, "
+                     "8192 uniform samples, C-space L2 radius 0.5 rad, dq=0.02 rad, start and goal free samples",
+            ndof=4, obstacles=16, samples=8192, radius=0.5, dq=0.02)
+
+
+def _dropin_plan(exe, checker, cfg_dir, s, g, seed):
+    """One run of GPUPRM's planner (process_mpi5, 32 new nodes per step,
+    nbuf 2048, distD = distH = radius, at most 5000 steps) between s and g."""
+    out = tempfile.mkdtemp(prefix="box4_out_")
+    cmd = [exe, "--checker", checker, "--config", cfg_dir, "--out", out, "--num", "32", "--nbuf", "2048",
+           "--dq", str(BOX4["dq"]), "--distD", str(BOX4["radius"]), "--distH", str(BOX4["radius"]),
+           "--maxsteps", "5000", "--seed", str(seed),
+           "--start", ",".join("%.9g" % x for x in s), "--goal", ",".join("%.9g" % x for x in g)]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    if p.returncode != 0:
+        return {"error": "exit %d: %s" % (p.returncode, p.stderr.strip()[-200:])}
+    return json.loads(p.stdout.strip().splitlines()[-1])
+
+
+def box4_leg(args):
+    """The reference's CPU planning case.  GPUPRM's planner grows two trees
+    from the start and the goal until they meet; its time per query is
+    timed per start/goal pair (one core), with its own CPU checker and with
+    this library's checker behind the same Configspace<4> interface.  The
+    GPU PRMs build a radius-0.5 roadmap of n uniform samples and answer the
+    same pairs: n starts at 8192 and doubles until every pair is answered
+    (8192 samples at this radius leave the free space in thousands of
+    components).  Each GPU run is timed alone for the whole batch of pairs
+    and for one pair."""
+    from gpuprm_b200 import planner, scenes
+    from gpuprm_b200.configspace import RobotConfigspace
+    sc = scenes.make_box4(args.seed)
+    cs = RobotConfigspace(sc, dq=BOX4["dq"])
+    cs.init()
+    cs.set_mode(check_mode(args))
+    Q = max(1, args.box4_queries)
+    starts, goals = planner.make_queries(cs, sc, Q, args.seed + 31)
+    out = {"config": dict(BOX4, queries=Q)}
+    gpu, n = [], BOX4["samples"]
+    while True:
+        row = {"samples": n}
+        for name, fn in (("plain", planner.plain_prm), ("lazy", planner.lazy_prm)):
+            fn(cs, sc, starts, goals, n, seed=args.seed, radius=BOX4["radius"])
+            runs = sorted((fn(cs, sc, starts, goals, n, seed=args.seed, radius=BOX4["radius"]) for _ in range(3)),
+                          key=lambda r: r.seconds)
+            r = runs[1]
+            one = sorted(fn(cs, sc, starts[:1], goals[:1], n, seed=args.seed, radius=BOX4["radius"]).seconds
+                         for _ in range(3))[1]
+            row[name] = {"success_rate": float(r.success.mean()), "batch_seconds": r.seconds,
+                         "seconds_one_pair": one, "paths_verified": bool(r.info["verified"]),
+                         "free_vertices": r.info["free_vertices"], "candidate_edges": r.info["candidate_edges"],
+                         "edge_checks": r.edge_checks, "edge_steps": r.edge_steps}
+        gpu.append(row)
+        if row["plain"]["success_rate"] >= 1.0 or n >= (1 << 18):
+            break
+        n *= 2
+    out["gpu"] = gpu
+    exe = os.path.join(ROOT, "oracle", "_ref", "prm_dropin")
+    if args.no_cpu_baseline or not os.path.exists(exe):
+        out["cpu_baseline"] = None if args.no_cpu_baseline else {"unavailable": "oracle/_ref/prm_dropin not built"}
+        return out
+    cfg = tempfile.mkdtemp(prefix="box4_cfg_")
+    scenes.write_config_dir(sc, cfg)
+    ref = {}
+    for checker in ("ref", "b200"):
+        runs = [_dropin_plan(exe, checker, cfg, starts[t], goals[t], args.seed + t) for t in range(Q)]
+        ok = [r for r in runs if "error" not in r]
+        secs = [r["plan_seconds"] for r in ok]
+        ref[checker] = {"runs": len(runs), "errors": [r["error"] for r in runs if "error" in r],
+                        "success_rate": sum(r["connection_found"] for r in ok) / len(runs),
+                        "median_seconds": statistics.median(secs) if secs else None,
+                        "mean_seconds": sum(secs) / len(secs) if secs else None,
+                        "median_nodes": statistics.median(r["num_nodes"] for r in ok) if ok else None,
+                        "median_edge_steps": statistics.median(r["edge_step_checks"] for r in ok) if ok else None}
+    out["cpu_baseline"] = {"kind": "reference", "cores": 1, "planner": "PRMSolver<4>::process_mpi5",
+                           "sample": "%d seeded free start/goal pairs, one planner run each" % Q,
+                           "reference_checker": ref["ref"], "library_checker_dropin": ref["b200"]}
+    best = gpu[-1]
+    if ref["ref"]["median_seconds"]:
+        out["gpu_over_reference_time"] = {
+            k: best[k]["batch_seconds"] / Q / ref["ref"]["median_seconds"] for k in ("plain", "lazy")}
+        out["gpu_one_pair_over_reference_time"] = {
+            k: best[k]["seconds_one_pair"] / ref["ref"]["median_seconds"] for k in ("plain", "lazy")}
     return out
 
 

@@ -285,10 +285,12 @@ def _workspace(ndof: int):
     return ws
 
 
-def _index_and_pairs(index, verts, k):
+def _index_and_pairs(index, verts, k, radius=None, cap=64):
     """Indexes the roadmap vertices (the index is reused for the queries)
-    and returns the undirected k-nearest-neighbour candidate edges (i < j,
-    int64)."""
+    and returns the undirected candidate edges (i < j, int64): the k
+    nearest neighbours of every vertex, or with `radius` every pair closer
+    than it (at most `cap` per vertex, in vertex order, like the
+    reference's radius query get_near_vertices, prmsolver.cpp:2533-2574)."""
     import torch
     V = verts.shape[0]
     if V < 2:
@@ -297,9 +299,12 @@ def _index_and_pairs(index, verts, k):
             index.build(verts.T.contiguous())
         return e, e
     index.build(verts.T.contiguous())
-    idx, _ = index.knn(min(k, V - 1))
+    if radius is not None:
+        _, idx, _ = index.radius(verts.T.contiguous(), float(radius), int(cap))
+    else:
+        idx, _ = index.knn(min(k, V - 1))
     rows = torch.arange(V, device=verts.device)[:, None].expand_as(idx)
-    valid = idx >= 0
+    valid = (idx >= 0) & (idx != rows)
     a, b = rows[valid].long(), idx[valid].long()
     key = torch.unique(torch.minimum(a, b) * V + torch.maximum(a, b))
     return key // V, key % V
@@ -370,8 +375,10 @@ def _lazy_rounds(V, i64, j64, cost, check, components, max_rounds, first, growth
     return good, checked, label, rounds, free1
 
 
-def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, keep_roadmap=False) -> PlanResult:
-    """Eager GPU PRM: every vertex and every candidate edge checked.  With
+def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, keep_roadmap=False,
+              radius=None) -> PlanResult:
+    """Eager GPU PRM: every vertex and every candidate edge checked (the k
+    nearest neighbours, or with `radius` every pair within it).  With
     keep_roadmap, info["roadmap"] = (vertices, free-edge ends i, j) as host
     arrays (copied after the timed region), e.g. for results.store_plan."""
     import torch
@@ -384,7 +391,7 @@ def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, 
     q = _sample(scene, n_samples, seed)
     verts = q[_check_vertices(cs, q) == 0]
     ph.mark("vertices")
-    i, j = _index_and_pairs(index, verts, k)
+    i, j = _index_and_pairs(index, verts, k, radius)
     i, j = i.to(torch.int32), j.to(torch.int32)
     ph.mark("knn")
     good = (_check_edges(cs, verts[i.long()], verts[j.long()]) == 0).to(torch.uint8)
@@ -409,7 +416,7 @@ def plain_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, profile=False, 
 
 
 def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=0.9, beta=4.0,
-             max_rounds=4, first=1, growth=2, lazy_attach=True, profile=False) -> PlanResult:
+             max_rounds=4, first=1, growth=2, lazy_attach=True, profile=False, radius=None) -> PlanResult:
     """Batched lazy-Boruvka PRM (exact connectivity), optionally MLP-guided;
     the roadmap and its bookkeeping stay on the device.  max_rounds >= 1
     counts round 1 (with max_rounds = 2 the second round checks every
@@ -432,7 +439,7 @@ def lazy_prm(cs, scene, starts, goals, n_samples, k=10, seed=0, mlp=None, prune=
     verts = q[_check_vertices(cs, q) == 0]
     vchecks = int(q.shape[0])
     ph.mark("vertices")
-    i64, j64 = _index_and_pairs(index, verts, k)
+    i64, j64 = _index_and_pairs(index, verts, k, radius)
     ph.mark("knn")
     i, j = i64.to(torch.int32), j64.to(torch.int32)
     V, E = verts.shape[0], int(i.numel())

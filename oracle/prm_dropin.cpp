@@ -28,6 +28,9 @@
  * Dijkstra path) so that a test can feed them to another store_results
  * writer and compare its files with the planner's own.
  *
+ * --start / --goal a,b,c,d replace main.cpp's start (0,0,0,0) and goal
+ * (3,3,3,3) (for scenes where those are not free).
+ *
  * --mode fp32 (default) runs the B200 checker in FP32 mode, whose verdicts
  * equal the reference's, so both runs draw the same random numbers and
  * build the same roadmap; --mode band enables the FP64 near-contact recheck.
@@ -184,6 +187,10 @@ int main(int argc, char** argv)
     int num = 32, nbuf = 2048, seed = 0, blocksize = 256, workerversion = 1, maxsteps = 10000;
     int maxstorage = 1024 * 1024;
     float dq = 0.01f, distD = 1.0f, distH = 1.0f;
+    float qstart[4] = {0, 0, 0, 0}, qend[4] = {3, 3, 3, 3};
+    auto parse4 = [](const std::string& v, float* q) {
+        return sscanf(v.c_str(), "%f,%f,%f,%f", &q[0], &q[1], &q[2], &q[3]) == 4;
+    };
     for (int i = 1; i + 1 < argc; i += 2) {
         std::string k = argv[i], v = argv[i + 1];
         if (k == "--checker") checker = v;
@@ -201,6 +208,8 @@ int main(int argc, char** argv)
         else if (k == "--mode") mode = v;
         else if (k == "--trace") trace = v;
         else if (k == "--dump") dump = v;
+        else if (k == "--start") { if (!parse4(v, qstart)) { fprintf(stderr, "bad --start\n"); return 2; } }
+        else if (k == "--goal") { if (!parse4(v, qend)) { fprintf(stderr, "bad --goal\n"); return 2; } }
         else { fprintf(stderr, "unknown argument %s\n", k.c_str()); return 2; }
     }
     if (config.empty() || out.empty() || (checker != "ref" && checker != "b200")) {
@@ -247,7 +256,6 @@ int main(int argc, char** argv)
     TracingSpace traced(space, tf);
     space = &traced;
     PRMSolver<4> prm(space, distH, distD, maxstorage, blocksize);
-    float qstart[4] = {0, 0, 0, 0}, qend[4] = {3, 3, 3, 3};
     const int start_free = space->indicator(qstart) == 0, end_free = space->indicator(qend) == 0;
     prm.init(qstart, qend);
     auto t2 = std::chrono::steady_clock::now();
@@ -282,9 +290,11 @@ int main(int argc, char** argv)
         if (gprm_get_stats(b200->handle(), &st) == GPRM_OK) steps = (long long)st.edge_steps_nominal;
     }
     printf("{\"checker\": \"%s\", \"init_seconds\": %.6f, \"plan_seconds\": %.6f, \"process_result\": %d, "
+           "\"connection_found\": %d, "
            "\"start_free\": %d, \"end_free\": %d, \"num_nodes\": %d, \"rand_nodes_all\": %d, "
            "\"rand_nodes_accepted\": %d, \"edge_step_checks\": %lld}\n",
-           checker.c_str(), init_s, plan_s, found, start_free, end_free, PRMSolver<4>::num_nodes,
+           checker.c_str(), init_s, plan_s, found, prm.connection_found ? 1 : 0, start_free, end_free,
+           PRMSolver<4>::num_nodes,
            PRMSolver<4>::rand_nodes_all, PRMSolver<4>::rand_nodes_accepted, steps);
     delete ref;
     delete b200;
