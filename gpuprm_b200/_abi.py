@@ -181,6 +181,9 @@ SIGNATURES = [
     ("gprm_sample_near", C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_float,
                                    C.c_ulonglong, C.c_longlong, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                    C.c_void_p]),
+    ("gprm_sample_near_blocks", C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                          C.c_void_p, C.c_int, C.c_float, C.c_ulonglong, C.c_longlong, C.c_int,
+                                          C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("gprm_graph_create", C.c_int, [C.POINTER(_P)]),
     ("gprm_graph_destroy", None, [_P]),
     ("gprm_graph_last_error", C.c_char_p, [_P]),

@@ -17,6 +17,17 @@
  * CPU restatement reproduces every candidate, and the "first num accepted
  * and free candidates in t order" is the same set whatever the batch size.
  * A 31-bit value r = x >> 1 stands in for rand() (RAND_MAX = 2^31 - 1).
+ *
+ * The reference picks the node in two draws over its block storage
+ * (prmsolver.cpp:2589-2597): a block uniformly among the used ones, again
+ * while it is empty, then a node uniformly among the block's num nodes, so
+ * a node's weight is 1 / (non-empty blocks * its block's num).
+ * gprm_sample_near_blocks takes that storage (block pos/num arrays over the
+ * node slots) and draws the same way: block b = r0 % nblocks among the
+ * blocks passed (the caller passes the non-empty ones; a block with num <= 0
+ * dismisses its candidates), node pos[b] + r9 % num[b].  gprm_sample_near
+ * draws the node uniformly (r0 % n), the same distribution when every node
+ * is its own block.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -42,6 +53,7 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 }
 
 __global__ void k_sample_near(int ndof, const float* __restrict__ nodes, int n, long long stride,
+                              const int* __restrict__ block_pos, const int* __restrict__ block_num, int nblocks,
                               const int* __restrict__ surrnum, int power, float D, uint2 key, long long t0, int B,
                               float* __restrict__ q_out, long long out_stride, int* __restrict__ parent_out)
 {
@@ -51,9 +63,26 @@ __global__ void k_sample_near(int ndof, const float* __restrict__ nodes, int n, 
         const uint4 a = philox4x32_10(make_uint4(tl, th, 0u, 0u), key);
         const uint4 b = philox4x32_10(make_uint4(tl, th, 1u, 0u), key);
         const uint4 c = philox4x32_10(make_uint4(tl, th, 2u, 0u), key);
-        const uint32_t r[9] = {a.x >> 1, a.y >> 1, a.z >> 1, a.w >> 1, b.x >> 1, b.y >> 1,
-                               b.z >> 1, b.w >> 1, c.x >> 1};
-        const int m = (int)(r[0] % (uint32_t)n);
+        const uint32_t r[10] = {a.x >> 1, a.y >> 1, a.z >> 1, a.w >> 1, b.x >> 1, b.y >> 1,
+                                b.z >> 1, b.w >> 1, c.x >> 1, c.y >> 1};
+        int m;
+        if (block_pos) {
+            const int blk = (int)(r[0] % (uint32_t)nblocks);
+            const int cnt = block_num[blk];
+            if (cnt <= 0) {                                  /* an empty block: dismissed */
+                for (int j = 0; j < ndof; ++j) q_out[i + out_stride * j] = 0.0f;
+                parent_out[i] = -1;
+                continue;
+            }
+            m = block_pos[blk] + (int)(r[9] % (uint32_t)cnt);
+            if (m < 0 || m >= n) {                           /* a block outside the node slots */
+                for (int j = 0; j < ndof; ++j) q_out[i + out_stride * j] = 0.0f;
+                parent_out[i] = -1;
+                continue;
+            }
+        } else {
+            m = (int)(r[0] % (uint32_t)n);
+        }
         /* prob = RAND_MAX / x^p in integers; rand() > prob dismisses */
         const long long x = 1 + (long long)max(surrnum[m], 0);
         long long xp = 1;
@@ -71,9 +100,10 @@ __global__ void k_sample_near(int ndof, const float* __restrict__ nodes, int n, 
 
 }  // namespace
 
-extern "C" int gprm_sample_near(int ndof, const float* nodes, int n, int stride, const int* surrnum, int power,
-                                float D, unsigned long long seed, long long t0, int B, float* q_out, int out_stride,
-                                int* parent_out, void* stream)
+static int launch_sample(int ndof, const float* nodes, int n, int stride, const int* block_pos,
+                         const int* block_num, int nblocks, const int* surrnum, int power, float D,
+                         unsigned long long seed, long long t0, int B, float* q_out, int out_stride, int* parent_out,
+                         void* stream)
 {
     if (ndof < 1 || ndof > GPRM_MAX_DOF || n < 1 || stride < n || !nodes || !surrnum || power < 0 || power > 8 ||
         B < 0 || (B > 0 && (!q_out || !parent_out)) || out_stride < B || t0 < 0 || !(D >= 0.0f))
@@ -86,7 +116,26 @@ extern "C" int gprm_sample_near(int ndof, const float* nodes, int n, int stride,
     long long blocks = ((long long)B + threads - 1) / threads;
     if (blocks > (long long)sms * 16) blocks = (long long)sms * 16;
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
-    k_sample_near<<<(int)blocks, threads, 0, (cudaStream_t)stream>>>(ndof, nodes, n, stride, surrnum, power, D, key, t0,
-                                                                     B, q_out, out_stride, parent_out);
+    k_sample_near<<<(int)blocks, threads, 0, (cudaStream_t)stream>>>(ndof, nodes, n, stride, block_pos, block_num,
+                                                                     nblocks, surrnum, power, D, key, t0, B, q_out,
+                                                                     out_stride, parent_out);
     return cudaGetLastError() == cudaSuccess ? GPRM_OK : GPRM_ERR_CUDA;
+}
+
+extern "C" int gprm_sample_near(int ndof, const float* nodes, int n, int stride, const int* surrnum, int power,
+                                float D, unsigned long long seed, long long t0, int B, float* q_out, int out_stride,
+                                int* parent_out, void* stream)
+{
+    return launch_sample(ndof, nodes, n, stride, nullptr, nullptr, 0, surrnum, power, D, seed, t0, B, q_out,
+                         out_stride, parent_out, stream);
+}
+
+extern "C" int gprm_sample_near_blocks(int ndof, const float* nodes, int n, int stride, const int* block_pos,
+                                       const int* block_num, int nblocks, const int* surrnum, int power, float D,
+                                       unsigned long long seed, long long t0, int B, float* q_out, int out_stride,
+                                       int* parent_out, void* stream)
+{
+    if (!block_pos || !block_num || nblocks < 1) return GPRM_ERR_ARG;
+    return launch_sample(ndof, nodes, n, stride, block_pos, block_num, nblocks, surrnum, power, D, seed, t0, B, q_out,
+                         out_stride, parent_out, stream);
 }

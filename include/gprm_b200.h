@@ -419,6 +419,20 @@ int gprm_sample_near(int ndof, const float* nodes, int n, int stride, const int*
                      float D, unsigned long long seed, long long t0, int B, float* q_out, int out_stride,
                      int* parent_out, void* stream);
 
+/* The same over the reference's block storage of a roadmap (graph::blocks,
+ * prmsolver.h:29-59; the node choice of prmsolver.cpp:2589-2597): nodes
+ * are the n storage slots, block b holds slots block_pos[b] ..
+ * block_pos[b] + block_num[b] - 1.  Candidate t picks block
+ * r0 % nblocks, then slot block_pos[b] + r9 % block_num[b] (r9 from the
+ * counter-2 block's second word), so every node weighs
+ * 1 / (nblocks * block_num[its block]) as in the reference when the blocks
+ * passed are its non-empty ones; a block with block_num <= 0, or a slot
+ * outside 0..n-1, dismisses the candidate.  Device pointers; asynchronous. */
+int gprm_sample_near_blocks(int ndof, const float* nodes, int n, int stride, const int* block_pos,
+                            const int* block_num, int nblocks, const int* surrnum, int power, float D,
+                            unsigned long long seed, long long t0, int B, float* q_out, int out_stride,
+                            int* parent_out, void* stream);
+
 /* ---- diagnostics (no counterpart in the reference) -------------------- */
 
 /* The FP32 frames the kernels compute for one configuration q[ndof]:

@@ -9,6 +9,10 @@
  * returns the neighbours within D in the solver's block order, mapped back
  * to the caller's node indices.  The members are private in the reference
  * header, so this translation unit opens them.
+ *
+ * ref_random_nodes runs the planner's node sampler get_random_nodes
+ * (prmsolver.cpp:2585-2624) on such a graph (pins oracle/sampler_oracle.py
+ * and the batched sampler distributionally).
  */
 #include <mpi.h>
 
@@ -123,5 +127,92 @@ extern "C" int ref_dijkstra(int ndof, const float* x, int n, const int* eu, cons
 {
     if (ndof == 4) return dijkstra_impl<4>(x, n, eu, ev, w, m, from, to, path, path_cap, dist_to);
     if (ndof == 6) return dijkstra_impl<6>(x, n, eu, ev, w, m, from, to, path, path_cap, dist_to);
+    return -3;
+}
+
+/* A Configspace<ndof> whose indicator(q) reports a collision exactly when
+ * q[0] > wall: the sampler's only call into the space. */
+template <int ndof>
+class WallSpace : public Configspace<ndof>
+{
+public:
+    explicit WallSpace(float wall) : wall_(wall) {}
+    int init(const int, const int) override { return 0; }
+    int indicator(const float* q, int* res, const int N, const int offset) override
+    {
+        for (int i = 0; i < N; ++i) res[i] = q[i] > wall_ ? 1 : 0;
+        (void)offset;
+        return 0;
+    }
+    int indicator(const float* q) override { return q[0] > wall_ ? 1 : 0; }
+    int indicator2(const float*, const float*, int*, const int, const int) override { return -1; }
+    int indicator2_async(const float*, const float*, int*, const int, const int, int&) override { return -1; }
+    int indicator2_async_wait(int) override { return -1; }
+    int indicator2(const float*, const int, const float*, int*, const int*, const int*, const int) override
+    {
+        return -1;
+    }
+    int check_boundaries(const float*, int*, const int, const int) override { return -1; }
+    int check_boundaries(const float*) override { return -1; }
+    float min(int) override { return -1e30f; }
+    float max(int) override { return 1e30f; }
+    float deltaq() override { return 0.01f; }
+    int dim() override { return ndof; }
+
+private:
+    float wall_;
+};
+
+template <int ndof>
+static int random_impl(const float* x, int n, const int* surrnum, float H, float D, float wall, int seed, int num,
+                       float* q_out, int* slot_of, int* block_pos, int* block_num, int* nblocks,
+                       long long* counters)
+{
+    PRMSolver<ndof>* s = new PRMSolver<ndof>(nullptr, H, D, n + 256 * 64, 256);
+    auto& g = s->graphl;
+    for (int i = 0; i < n; ++i) {
+        float v[ndof];
+        for (int j = 0; j < ndof; ++j) v[j] = x[(size_t)i * ndof + j];
+        int p = s->insert(v, 1, g);
+        if (p < 0) { delete s; return -1; }
+        slot_of[i] = p;
+        g.surrnum[p] = surrnum[i];
+    }
+    *nblocks = g.blocknum;
+    for (int b = 0; b < g.blocknum; ++b) {
+        block_pos[b] = g.blocks[b].pos;
+        block_num[b] = g.blocks[b].num;
+    }
+    WallSpace<ndof> space(wall);
+    PRMSolver<ndof>::rand_nodes_all = 0;
+    PRMSolver<ndof>::rand_nodes_dismissed_prob = 0;
+    PRMSolver<ndof>::rand_nodes_accepted = 0;
+    PRMSolver<ndof>::rand_block_numbers = 0;
+    srand(seed);
+    s->get_random_nodes(g, 0, num, q_out, D, &space);
+    counters[0] = PRMSolver<ndof>::rand_nodes_all;
+    counters[1] = PRMSolver<ndof>::rand_nodes_dismissed_prob;
+    counters[2] = PRMSolver<ndof>::rand_nodes_accepted;
+    counters[3] = PRMSolver<ndof>::rand_block_numbers;
+    delete s;
+    return 0;
+}
+
+/* x: (n, ndof) nodes inserted in order (keys of width H over joint 0) with
+ * surrnum[i]; draws num free nodes (free: q[0] <= wall) into q_out (num,
+ * ndof) after srand(seed).  slot_of[i]: node i's storage slot; the graph's
+ * blocks (pos, num) go to block_pos/block_num (capacity n + 64), their count
+ * to *nblocks; counters: rand_nodes_all, rand_nodes_dismissed_prob,
+ * rand_nodes_accepted, rand_block_numbers. */
+extern "C" int ref_random_nodes(int ndof, const float* x, int n, const int* surrnum, float H, float D, float wall,
+                                int seed, int num, float* q_out, int* slot_of, int* block_pos, int* block_num,
+                                int* nblocks, long long* counters)
+{
+    if (ndof == 4)
+        return random_impl<4>(x, n, surrnum, H, D, wall, seed, num, q_out, slot_of, block_pos, block_num, nblocks,
+                              counters);
+    if (ndof == 6)
+        return random_impl<6>(x, n, surrnum, H, D, wall, seed, num, q_out, slot_of, block_pos, block_num, nblocks,
+                              counters);
     return -3;
 }

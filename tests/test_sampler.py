@@ -67,3 +67,27 @@ def test_gpu_sample_near_matches_sequential_restatement():
     assert used == wused
     np.testing.assert_array_equal(par.cpu().numpy(), wp)
     np.testing.assert_array_equal(q.cpu().numpy().T, wq)
+
+
+@pytest.mark.gpu
+def test_gpu_block_candidates_match_oracle():
+    """The block-storage draw (gprm_sample_near_blocks) equals the
+    restatement bit for bit, with an empty block and a block reaching past
+    the node slots among the blocks passed (both dismiss)."""
+    import torch
+    from gpuprm_b200.sampler import candidates
+    rng = np.random.default_rng(4)
+    n = 3000
+    nodes = rng.uniform(-3, 3, (n, 6)).astype(np.float32)
+    surr = rng.integers(0, 5, n).astype(np.int32)
+    pos = np.array([0, 256, 512, 900, 1300, 2000, 2990, 2995], np.int32)
+    num = np.array([256, 3, 100, 0, 256, 1, 5, 40], np.int32)     # the last runs past n
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.tensor(a, device=dev)
+    q, par = candidates(T(np.ascontiguousarray(nodes.T)), T(surr), 0.4, seed=99, t0=5, B=50000, power=3,
+                        blocks=(T(pos), T(num)))
+    wq, wp = SO.candidates(nodes, surr, 3, 0.4, 99, 5, 50000, pos, num)
+    np.testing.assert_array_equal(par.cpu().numpy(), wp)
+    np.testing.assert_array_equal(q.cpu().numpy().T, wq)
+    p = par.cpu().numpy()
+    assert (p >= 0).any() and not np.isin(p, np.arange(900, 1300)).any()
