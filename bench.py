@@ -727,7 +727,11 @@ def sampler_leg(args, ws, dev):
 def batch_leg(args, dev, policy):
     """Many independent problems: one graph-captured batched launch per kind
     against a loop of per-problem launches (same stream, same inputs);
-    results must agree bit for bit."""
+    results must agree bit for bit.  The launch shape (threads per block x
+    resident blocks per SM) is autotuned on every 8th problem (the same mix
+    of DOF and scene sizes at 1/8 of the work) and applied to the whole
+    batch.  One untimed and two timed passes per arm (a full edge pass is
+    several seconds of work)."""
     import torch
     from gpuprm_b200 import workloads
     from gpuprm_b200.batch import CONFIGS, EDGES, ProblemBatch
@@ -745,14 +749,30 @@ def batch_leg(args, dev, policy):
     re = torch.zeros(ne, dtype=torch.int32, device=dev)
     B.set_layout(CONFIGS, ws["offs_v"])
     B.set_layout(EDGES, ws["offs_e"])
-    tune_v = B.autotune(CONFIGS, Q, None, rv, reps=2)
-    tune_e = B.autotune(EDGES, A, Bq, re, reps=2)
+    ov, oe = ws["offs_v"], ws["offs_e"]
+    # the tuning sub-batch: every 8th problem, packed contiguously
+    sub = list(range(0, len(spaces), 8))
+    T = ProblemBatch([spaces[p] for p in sub])
+    tq = torch.cat([Q[:, ov[p]:ov[p + 1]] for p in sub], 1).contiguous()
+    ta = torch.cat([A[:, oe[p]:oe[p + 1]] for p in sub], 1).contiguous()
+    tb = torch.cat([Bq[:, oe[p]:oe[p + 1]] for p in sub], 1).contiguous()
+    T.set_layout(CONFIGS, np.concatenate([[0], np.cumsum([ov[p + 1] - ov[p] for p in sub])]))
+    T.set_layout(EDGES, np.concatenate([[0], np.cumsum([oe[p + 1] - oe[p] for p in sub])]))
+    t_tune = time.perf_counter()
+    tune_v = T.autotune(CONFIGS, tq, None, torch.zeros(tq.shape[1], dtype=torch.int32, device=dev), reps=2)
+    tune_e = T.autotune(EDGES, ta, tb, torch.zeros(ta.shape[1], dtype=torch.int32, device=dev), reps=2)
+    t_tune = time.perf_counter() - t_tune
+    del T, tq, ta, tb
+    B.set_launch(CONFIGS, tune_v["threads"], tune_v["blocks_per_sm"])
+    B.set_launch(EDGES, tune_e["threads"], tune_e["blocks_per_sm"])
     B.capture(CONFIGS, Q, None, rv)
     B.capture(EDGES, A, Bq, re)
-    # per-problem inputs for the launch loop
-    pv = [torch.tensor(np.ascontiguousarray(q.T), device=dev) for q in ws["q_host"]]
-    pa = [torch.tensor(np.ascontiguousarray(a.T), device=dev) for a in ws["qs_host"]]
-    pb = [torch.tensor(np.ascontiguousarray(b.T), device=dev) for b in ws["qe_host"]]
+    # per-problem views of the same inputs for the launch loop
+    ov, oe = ws["offs_v"], ws["offs_e"]
+    dofs = [sc.ndof for sc in ws["scenes"]]
+    pv = [Q[:d, ov[p]:ov[p + 1]] for p, d in enumerate(dofs)]
+    pa = [A[:d, oe[p]:oe[p + 1]] for p, d in enumerate(dofs)]
+    pb = [Bq[:d, oe[p]:oe[p + 1]] for p, d in enumerate(dofs)]
     lv = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pv]
     le = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pa]
     stream = torch.cuda.current_stream()
@@ -765,8 +785,7 @@ def batch_leg(args, dev, policy):
                 cs.check_edges_device(pa[p], pb[p], le[p])
 
     def timed(fn, steps):
-        for _ in range(max(3, args.warmup)):
-            fn()
+        fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -776,29 +795,31 @@ def batch_leg(args, dev, policy):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / steps
 
+    steps = 2
     s0 = B.stats()
-    t_bv = timed(lambda: B.replay(CONFIGS), args.steps)
+    t_bv = timed(lambda: B.replay(CONFIGS), steps)
     s1 = B.stats()
-    t_be = timed(lambda: B.replay(EDGES), args.steps)
+    t_be = timed(lambda: B.replay(EDGES), steps)
     s2 = B.stats()
-    t_lv = timed(lambda: loop(CONFIGS), args.steps)
-    t_le = timed(lambda: loop(EDGES), args.steps)
-    reps = max(3, args.warmup) + args.steps
+    t_lv = timed(lambda: loop(CONFIGS), steps)
+    t_le = timed(lambda: loop(EDGES), steps)
+    reps = 1 + steps
     nominal = (s2["edge_steps_nominal"] - s1["edge_steps_nominal"]) // reps
     got_v, got_e = rv.cpu().numpy(), re.cpu().numpy()
-    ov, oe = ws["offs_v"], ws["offs_e"]
     same_v = all(np.array_equal(got_v[ov[p]:ov[p + 1]], lv[p].cpu().numpy()) for p in range(len(spaces)))
     same_e = all(np.array_equal(got_e[oe[p]:oe[p + 1]], le[p].cpu().numpy()) for p in range(len(spaces)))
-    dofs = [sc.ndof for sc in ws["scenes"]]
     return {
         "workload": "many problems: %d mixed scenes (DOF 4-7, 8-128 hull obstacles), 2^14-2^18 samples each, "
-                    "kNN k=%d of the first %d free samples, edges cut to a radius U[0.4,0.8], dq=%g"
-                    % (len(spaces), workloads.MANY["k"], workloads.MANY["edge_sources"], workloads.MANY["dq"]),
+                    "kNN k=%d of every free sample, edges cut to a radius U[0.4,0.8], dq=%g"
+                    % (len(spaces), workloads.MANY["k"], workloads.MANY["dq"]),
         "problems": len(spaces), "dof_counts": {str(d): dofs.count(d) for d in sorted(set(dofs))},
         "configs": int(nv), "edges": int(ne), "edge_steps_nominal": int(nominal),
         "batched": {"configs_per_s": nv / t_bv, "edge_steps_per_s": nominal / t_be,
                     "configs_ms": 1e3 * t_bv, "edges_ms": 1e3 * t_be, "graph_launches_per_step": 2,
-                    "threads": {"configs": tune_v["threads"], "edges": tune_e["threads"]}},
+                    "launch_shape": {"configs": B.get_launch(CONFIGS), "edges": B.get_launch(EDGES)},
+                    "autotune": {"sub_batch": "every 8th problem (%d)" % len(sub), "seconds": t_tune,
+                                 "candidates": "threads 64/128/256/512 x resident blocks per SM all/3/4/half"},
+                    "timed_passes": steps},
         "per_problem_loop": {"configs_per_s": nv / t_lv, "edge_steps_per_s": nominal / t_le,
                              "configs_ms": 1e3 * t_lv, "edges_ms": 1e3 * t_le},
         "speedup": {"configs": t_lv / t_bv, "edges": t_le / t_be},

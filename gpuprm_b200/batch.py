@@ -93,21 +93,25 @@ class ProblemBatch:
         st = stream if stream is not None else _current_stream()
         self._check(self.lib.gprm_batch_replay(self.h, int(kind), C.c_void_p(st)))
 
-    def set_launch(self, kind: int, threads: int) -> None:
-        self._check(self.lib.gprm_batch_set_launch(self.h, int(kind), int(threads)))
+    def set_launch(self, kind: int, threads: int, blocks_per_sm: int = 0) -> None:
+        """Threads per block and at most blocks_per_sm resident blocks per
+        SM (0: as many as fit)."""
+        self._check(self.lib.gprm_batch_set_launch_shape(self.h, int(kind), int(threads), int(blocks_per_sm)))
 
     def get_launch(self, kind: int) -> dict:
-        t, w = C.c_int(0), C.c_int(0)
-        self._check(self.lib.gprm_batch_get_launch(self.h, int(kind), C.byref(t), C.byref(w)))
-        return {"threads": t.value, "warps_per_sm": w.value}
+        t, b, w = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._check(self.lib.gprm_batch_get_launch_shape(self.h, int(kind), C.byref(t), C.byref(b), C.byref(w)))
+        return {"threads": t.value, "blocks_per_sm": b.value, "warps_per_sm": w.value}
 
     def autotune(self, kind: int, qa, qb, res, reps: int = 3) -> dict:
+        """Times the launch shapes on this input and keeps the fastest;
+        returns its shape and time per run (ms)."""
         t, ms = C.c_int(0), C.c_float(0)
         self._check(self.lib.gprm_batch_autotune(self.h, int(kind), C.c_void_p(qa.data_ptr()),
                                                  C.c_void_p(qb.data_ptr() if qb is not None else 0),
                                                  C.c_void_p(res.data_ptr()), int(qa.shape[1]), int(reps),
                                                  C.byref(t), C.byref(ms)))
-        return {"threads": t.value, "ms": ms.value}
+        return dict(self.get_launch(kind), ms=ms.value)
 
     def stats(self) -> dict:
         s = Stats()

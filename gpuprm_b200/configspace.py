@@ -35,6 +35,14 @@ def _f32(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, np.float32))
 
 
+def _soa_offset(t) -> int:
+    """Row stride (the C ABI's offset) of an (ndof, n) SoA tensor whose
+    columns are contiguous."""
+    if t.dim() != 2 or (t.shape[1] > 1 and t.stride(1) != 1):
+        raise ValueError("expected an (ndof, n) tensor with unit column stride")
+    return int(t.stride(0)) if t.shape[0] > 1 else int(t.shape[1])
+
+
 class RobotConfigspace:
     """One scene on one GPU.
 
@@ -169,18 +177,26 @@ class RobotConfigspace:
 
     # -- device buffers (torch tensors, SoA (ndof, n) float32 on the GPU) --------
     def check_configs_device(self, q_soa, res, stream=None) -> None:
-        """q_soa: (ndof, n) contiguous float32 CUDA tensor; res: (n,) int32."""
+        """q_soa: (ndof, n) float32 CUDA tensor with unit column stride
+        (a column slice of a wider SoA array works: its row stride is the
+        offset); res: (n,) int32."""
         n = int(q_soa.shape[1])
+        off = _soa_offset(q_soa)
         st = stream if stream is not None else _current_stream()
         _check(self.lib, self.h, self.lib.gprm_indicator_batch_device(
-            self.h, C.c_void_p(q_soa.data_ptr()), C.c_void_p(res.data_ptr()), n, n, C.c_void_p(st)))
+            self.h, C.c_void_p(q_soa.data_ptr()), C.c_void_p(res.data_ptr()), n, off, C.c_void_p(st)))
 
     def check_edges_device(self, qs_soa, qe_soa, res, stream=None) -> None:
+        """qs_soa, qe_soa: (ndof, n) float32 CUDA tensors of one row stride
+        (as check_configs_device); res: (n,) int32."""
         n = int(qs_soa.shape[1])
+        off = _soa_offset(qs_soa)
+        if _soa_offset(qe_soa) != off:
+            raise ValueError("qs and qe must have the same row stride")
         st = stream if stream is not None else _current_stream()
         _check(self.lib, self.h, self.lib.gprm_indicator2_device(
             self.h, C.c_void_p(qs_soa.data_ptr()), C.c_void_p(qe_soa.data_ptr()), C.c_void_p(res.data_ptr()),
-            n, n, C.c_void_p(st)))
+            n, off, C.c_void_p(st)))
 
     def set_launch(self, vertex_kernel: bool, threads: int, scene_in_smem: bool, blocks_per_sm: int = 0) -> None:
         """Launch shape of the FP32 kernels: threads per block, scene table in

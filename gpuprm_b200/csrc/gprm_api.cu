@@ -507,10 +507,20 @@ void release_request(Request& r)
     cudaFree(r.d_queue);
     cudaFree(r.d_ovf);
     cudaFreeHost(r.ctl_host);
+    cudaFreeHost(r.h_qwant);
+    if (r.ev_q) cudaEventDestroy(r.ev_q);
     cudaFreeHost(r.h_a);
     cudaFreeHost(r.h_b);
     cudaFreeHost(r.h_res);
     r = Request();
+}
+
+/* Records the FP64 queue demand of one edge call (or part of one): `items`
+ * queued (or wanted past the queue's end) for m edges. */
+void note_queue_demand(gprm_space* h, unsigned items, long long m)
+{
+    const double d = (double)items / (double)m;
+    if (d > h->qdens_edges) h->qdens_edges = d;
 }
 
 /* Grows the buffers of `r` to hold `n` items of `kind`; the stream and
@@ -524,7 +534,21 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
     }
     if (kind == 1 && !r.d_seg)
         CUDA_TRY(h, dev_malloc((void**)&r.d_seg, (size_t)(EDGE_SPLIT_MAX + 1) * sizeof(unsigned)));
+    /* the demand of the last device-pointer edge call, once it has finished */
+    if (r.q_pending) {
+        const cudaError_t e = cudaEventQuery(r.ev_q);
+        if (e != cudaErrorNotReady) r.q_pending = false;
+        if (e == cudaSuccess && r.q_n > 0) note_queue_demand(h, *r.h_qwant, r.q_n);
+        cudaGetLastError();   /* a query that is not ready is no error of this call */
+    }
+    /* a configuration queues at most one item; an edge as many as the
+       busiest scene so far needed per edge (the overflow pass completes any
+       call whose queue still runs over) */
     size_t need_q = (kind == 0) ? n : 4 * n + 65536;
+    if (kind == 1 && h->qdens_edges > 0.0) {
+        const double want = h->qdens_edges * (double)n * 1.25 + 65536.0;
+        if (want > (double)need_q) need_q = want < 4e9 ? (size_t)want : (size_t)4e9;
+    }
     if (n > r.cap_items || need_q > r.cap_queue || (with_host && !r.h_res && n > 0)) {
         size_t cap = n > r.cap_items ? n + n / 4 + 64 : r.cap_items;
         size_t qcap = (need_q > r.cap_queue) ? need_q + need_q / 4 : r.cap_queue;
@@ -577,7 +601,20 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
 int enqueue(gprm_space* h, Request& r, int kind, const float* a, const float* b, int* res, long long n,
             long long offset, cudaStream_t st)
 {
-    return enqueue_part(h, r, kind, a, b, res, n, offset, st, r.ctl, r.d_key);
+    int rc = enqueue_part(h, r, kind, a, b, res, n, offset, st, r.ctl, r.d_key);
+    if (rc || kind != 1 || !(h->mode & GPRM_MODE_FP64_BAND) || r.q_pending) return rc;
+    /* read the queue demand back for the next call's sizing, unless the
+       stream is being captured (a graph replays without this host) */
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(h, cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return GPRM_OK;
+    if (!r.h_qwant) CUDA_TRY(h, cudaHostAlloc((void**)&r.h_qwant, sizeof(unsigned), cudaHostAllocDefault));
+    if (!r.ev_q) CUDA_TRY(h, cudaEventCreateWithFlags(&r.ev_q, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaMemcpyAsync(r.h_qwant, &r.ctl->qcount, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(h, cudaEventRecord(r.ev_q, st));
+    r.q_pending = true;
+    r.q_n = n;
+    return GPRM_OK;
 }
 
 /* One check request on stream st: items a[i + offset*j] (b: edge ends),
@@ -715,6 +752,14 @@ int complete_host(gprm_space* h, int slot)
     }
     if (c.flags & GPRM_DEVFLAG_BAD_EDGE)
         return fail(h, GPRM_ERR_ARG, "an edge has a non-finite or oversized length (|qe-qs|/dq >= 1e8)");
+    if (r.kind == 1) {
+        static const int edge16[HOST_PARTS + 1] = {0, 1, 6, 11, 16};
+        for (int p = 0; p < r.parts; ++p) {
+            const long long m = r.parts == 1 ? r.n
+                                              : (long long)r.n * edge16[p + 1] / 16 - (long long)r.n * edge16[p] / 16;
+            if (m > 0) note_queue_demand(h, r.ctl_host[p].qcount, m);
+        }
+    }
     /* GPRM_DEVFLAG_QUEUE_FULL: the overflow pass has completed the results */
     memcpy(r.user_res, r.h_res, (size_t)r.n * sizeof(int));
     /* edge-step and band counters accumulate on the device (d_total) */

@@ -370,19 +370,21 @@ int gprm_batch_replay(gprm_batch* b, int vertex_kernel, void* stream)
     return GPRM_OK;
 }
 
-int gprm_batch_set_launch(gprm_batch* b, int vertex_kernel, int threads)
+int gprm_batch_set_launch_shape(gprm_batch* b, int vertex_kernel, int threads, int blocks_per_sm)
 {
     if (!b) return GPRM_ERR_ARG;
     vertex_kernel = vertex_kernel ? 1 : 0;
     if (threads < 32 || threads > 512 || threads % 32)
         return bfail(b, GPRM_ERR_ARG, "threads must be 32..512, a multiple of 32");
+    if (blocks_per_sm < 0 || blocks_per_sm > 64) return bfail(b, GPRM_ERR_ARG, "blocks_per_sm must be 0..64");
     BATCH_TRY(b, cudaSetDevice(b->device));
     LaunchCfg c{};
-    cudaError_t e = configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, threads, &c);
+    cudaError_t e = configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, threads, &c, blocks_per_sm);
     if (e != cudaSuccess) {
         cudaGetLastError();
         LaunchCfg& cur = b->cfg[vertex_kernel];
-        configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, cur.threads, &cur);
+        configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, cur.threads, &cur,
+                               cur.carveout >= 0 ? cur.blocks_per_sm : 0);
         return bfail(b, GPRM_ERR_UNSUPPORTED, "launch shape of %d threads does not fit: %s", threads,
                      cudaGetErrorString(e));
     }
@@ -391,11 +393,27 @@ int gprm_batch_set_launch(gprm_batch* b, int vertex_kernel, int threads)
     return GPRM_OK;
 }
 
+int gprm_batch_set_launch(gprm_batch* b, int vertex_kernel, int threads)
+{
+    return gprm_batch_set_launch_shape(b, vertex_kernel, threads, 0);
+}
+
 int gprm_batch_get_launch(const gprm_batch* b, int vertex_kernel, int* threads, int* warps_per_sm)
 {
     if (!b || !threads || !warps_per_sm) return GPRM_ERR_ARG;
     const LaunchCfg& c = b->cfg[vertex_kernel ? 1 : 0];
     *threads = c.threads;
+    *warps_per_sm = c.warps_per_sm;
+    return GPRM_OK;
+}
+
+int gprm_batch_get_launch_shape(const gprm_batch* b, int vertex_kernel, int* threads, int* blocks_per_sm,
+                                int* warps_per_sm)
+{
+    if (!b || !threads || !blocks_per_sm || !warps_per_sm) return GPRM_ERR_ARG;
+    const LaunchCfg& c = b->cfg[vertex_kernel ? 1 : 0];
+    *threads = c.threads;
+    *blocks_per_sm = c.blocks_per_sm;
     *warps_per_sm = c.warps_per_sm;
     return GPRM_OK;
 }
@@ -409,15 +427,32 @@ int gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, const
     if (reps < 1 || reps > 1000) return bfail(b, GPRM_ERR_ARG, "reps must be 1..1000");
     /* the runs use the batch's buffers on its own stream: let earlier calls finish */
     BATCH_TRY(b, cudaDeviceSynchronize());
-    static const int cand[] = {64, 128, 256, 512};
+    /* threads per block x resident blocks per SM: every block size with as
+       many blocks as fit, and with 3/4 and 1/2 of them (the L1 that the
+       smaller carveout leaves caches more of the scenes' tables) */
+    std::vector<std::pair<int, int>> cand;
+    for (int threads : {64, 128, 256, 512}) {
+        LaunchCfg full{};
+        if (configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, threads, &full) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        cand.push_back({threads, 0});
+        const int per_sm = full.blocks_per_sm;
+        const int caps[2] = {(3 * per_sm) / 4, per_sm / 2};
+        for (int k = 0; k < 2; ++k)
+            if (caps[k] >= 1 && caps[k] < per_sm && (k == 0 || caps[1] != caps[0])) cand.push_back({threads, caps[k]});
+    }
     cudaEvent_t e0, e1;
     BATCH_TRY(b, cudaEventCreate(&e0));
     BATCH_TRY(b, cudaEventCreate(&e1));
     float best = -1.0f;
     LaunchCfg best_cfg = b->cfg[vertex_kernel];
-    for (int threads : cand) {
+    int best_cap = 0;
+    for (const auto& tc : cand) {
         LaunchCfg c{};
-        if (configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, threads, &c) != cudaSuccess) {
+        if (configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, tc.first, &c, tc.second) !=
+            cudaSuccess) {
             cudaGetLastError();
             continue;
         }
@@ -440,6 +475,7 @@ int gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, const
         if (best < 0 || ms < best) {
             best = ms;
             best_cfg = c;
+            best_cap = tc.second;
         }
     }
     cudaEventDestroy(e0);
@@ -448,7 +484,7 @@ int gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, const
     if (best < 0) return bfail(b, GPRM_ERR_UNSUPPORTED, "no launch shape fits");
     /* re-apply the winner (each candidate set the kernel's shared-memory attribute) */
     BATCH_TRY(b, configure_batch_launch(view_of(b, vertex_kernel), vertex_kernel, best_cfg.threads,
-                                        &b->cfg[vertex_kernel]));
+                                        &b->cfg[vertex_kernel], best_cap));
     if (best_threads) *best_threads = best_cfg.threads;
     if (best_ms) *best_ms = best;
     return GPRM_OK;

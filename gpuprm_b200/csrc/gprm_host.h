@@ -44,6 +44,13 @@ struct Request {
     int* h_res = nullptr;
     size_t cap_items = 0;         /* edges or configurations */
     size_t cap_queue = 0;
+    /* FP64 queue demand of the last device-pointer edge call, read back
+       without a synchronisation: the items it wanted (h_qwant, pinned),
+       ready once ev_q has completed, for q_n edges */
+    unsigned* h_qwant = nullptr;
+    cudaEvent_t ev_q = nullptr;
+    bool q_pending = false;
+    long long q_n = 0;
     bool busy = false;
     /* the request in flight */
     int kind = 0;                 /* 0 vertices, 1 edges */
@@ -102,6 +109,7 @@ struct gprm_space {
     int split_rounds = 2;         /* rounds of 32 steps per segment */
     float band = 1e-5f;
     unsigned debug_qcap = 0;      /* test hook: FP64 queue capacity cap (0 = none) */
+    double qdens_edges = 0.0;     /* most FP64 queue items per edge seen in a call (sizes later queues) */
 
     std::vector<gprm::Request> reqs;
     std::map<int, int> live;       /* request id -> slot */

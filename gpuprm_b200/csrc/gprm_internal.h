@@ -76,7 +76,11 @@ struct BatchView {
 };
 
 /* Launch shape of the batched kernels. */
-cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg);
+/* blocks_cap > 0: at most that many resident blocks per SM, with a
+ * shared-memory carveout just large enough for them (the rest of the SM's
+ * L1/shared storage left to L1), applied as a launch attribute. */
+cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg,
+                                   int blocks_cap = 0);
 cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg, const float* q, long long offset,
                                        int* res, int band_on, float band, BandQueue bq, Control* ctl,
                                        cudaStream_t st);

@@ -941,9 +941,11 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
  * pair's exact test in the reference's order (the certificates only ever
  * skip pairs whose test gives 0 with a margin above the band, so the code
  * and the band decision are those of the warp kernels).  *margin: the
- * deciding pair's margin, or the minimum over the pairs of a free check. */
+ * deciding pair's margin, or the minimum over the pairs of a free check;
+ * *jdec (when given): the deciding pair's index, npairs for a free check. */
 template <bool FAST>
-__device__ __forceinline__ int check_config32(const DevScene& sc, const float* qi, float* margin)
+__device__ __forceinline__ int check_config32(const DevScene& sc, const float* qi, float* margin,
+                                              int* jdec = nullptr)
 {
     Frame<float> F[GPRM_MAX_FRAMES];
     if constexpr (FAST) forward_kinematics_fast(sc, qi, F);
@@ -956,19 +958,32 @@ __device__ __forceinline__ int check_config32(const DevScene& sc, const float* q
         int r;
         if constexpr (FAST) r = pair_test_fast(sc, sc.tab, pr, sc.ppoly[j], F[pr.z], F[pr.w], &m);
         else r = pair_test<PF32>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
-        if (r != 0) { *margin = m; return r; }
+        if (r != 0) {
+            *margin = m;
+            if (jdec) *jdec = j;
+            return r;
+        }
         mmin = min_nan(mmin, m);
     }
     *margin = mmin;
+    if (jdec) *jdec = sc.npairs;
     return 0;
 }
 
 /* One item of the overflow list, recomputed in full by one thread: a
  * configuration (kind 0: bounds, FP32, FP64 inside the band -> res), or an
- * edge (kind 1: every step so; the key is rebuilt from scratch with the
- * merge of the check and recheck kernels - all steps: the same key;
- * early exit: the first colliding step in step order, whose verdict is the
- * edge's). */
+ * edge (kind 1), whose key is rebuilt from scratch as the check and recheck
+ * kernels build it when nothing overflows:
+ *   all steps   the max over every step (FP32, FP64 inside the band);
+ *   early exit  the check kernel's rounds (round r: steps t = lane*R + r,
+ *               order r*32 + lane) until the first round with a collision
+ *               outside the band.  The kernel runs a round pair by pair in
+ *               the reference's pair order and stops at the first pair
+ *               index j* at which some step collides outside the band; its
+ *               lowest such lane L decides.  Steps of lower lanes whose
+ *               loop had ended by then in the band (a collision at a pair
+ *               <= j*, or a free check when nothing decided) go to the FP64
+ *               check, and a collision there takes the lower order. */
 template <bool FAST>
 __device__ __forceinline__ void overflow_item(const DevScene& sc, int kind, unsigned x, const float* __restrict__ q,
                                               const float* __restrict__ qs, const float* __restrict__ qe,
@@ -998,26 +1013,67 @@ __device__ __forceinline__ void overflow_item(const DevScene& sc, int kind, unsi
     const int tn = edge_testnum(qs, qe, (long long)x, offset, sc.ndof, dq);
     if (tn < 0) return;   /* flagged by the check kernel */
     const int R = (tn + 31) >> 5;
-    unsigned k = policy == EDGE_EARLY_EXIT ? 0xffffffffu : 0u;
+    if (policy != EDGE_EARLY_EXIT) {
+        unsigned k = 0u;
 #pragma unroll 1
-    for (int t = 0; t < tn; ++t) {
-        edge_step_config(qs, qe, (long long)x, offset, sc.ndof, t, tn, qi);
-        float m;
-        int code = check_config32<FAST>(sc, qi, &m);
-        if (in_band(code, m, band)) {
+        for (int t = 0; t < tn; ++t) {
+            edge_step_config(qs, qe, (long long)x, offset, sc.ndof, t, tn, qi);
+            float m;
+            int code = check_config32<FAST>(sc, qi, &m);
+            if (in_band(code, m, band)) {
+                const int c64 = check_config64(sc, qi);
+                ++checks;
+                flips += ((c64 != 0) != (code != 0));
+                code = c64;
+            }
+            if (code != 0) {
+                const unsigned kv = all_key(t, code);
+                if (kv > k) k = kv;
+            }
+        }
+        key[x] = k;
+        return;
+    }
+    unsigned k = 0xffffffffu;
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+        /* the round's deciding pair index j* and lane L */
+        int jstar = 0x7fffffff, L = 32, codeL = 0;
+#pragma unroll 1
+        for (int lane = 0; lane < 32; ++lane) {
+            const int t = lane * R + r;
+            if (t >= tn) break;
+            edge_step_config(qs, qe, (long long)x, offset, sc.ndof, t, tn, qi);
+            float m;
+            int j;
+            const int code = check_config32<FAST>(sc, qi, &m, &j);
+            if (code != 0 && !in_band(code, m, band) && j < jstar) { jstar = j; L = lane; codeL = code; }
+        }
+        /* the in-band steps below L that the kernel queues */
+#pragma unroll 1
+        for (int lane = 0; lane < L; ++lane) {
+            const int t = lane * R + r;
+            if (t >= tn) break;
+            edge_step_config(qs, qe, (long long)x, offset, sc.ndof, t, tn, qi);
+            float m;
+            int j;
+            const int code = check_config32<FAST>(sc, qi, &m, &j);
+            const bool queued = code != 0 ? (in_band(code, m, band) && j <= jstar)
+                                          : (L == 32 && in_band(0, m, band));
+            if (!queued) continue;
             const int c64 = check_config64(sc, qi);
             ++checks;
             flips += ((c64 != 0) != (code != 0));
-            code = c64;
+            if (c64 != 0) {
+                const unsigned kv = early_key((unsigned)(r * 32 + lane), c64);
+                if (kv < k) k = kv;
+            }
         }
-        if (code == 0) continue;
-        if (policy == EDGE_EARLY_EXIT) {
-            const unsigned kv = early_key((unsigned)((t % R) * 32 + t / R), code);
+        if (L < 32) {
+            const unsigned kv = early_key((unsigned)(r * 32 + L), codeL);
             if (kv < k) k = kv;
             break;
         }
-        const unsigned kv = all_key(t, code);
-        if (kv > k) k = kv;
     }
     key[x] = k;
 }
@@ -1464,7 +1520,8 @@ static const void* batch_kernel_fn(int vertex_kernel, int policy, bool fast)
                                      : (const void*)k_check_edges_multi<EDGE_ALL_STEPS, false>;
 }
 
-cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg)
+cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int threads, LaunchCfg* cfg,
+                                   int blocks_cap)
 {
     int dev = 0, sms = 0, optin = 0;
     cudaError_t err = cudaGetDevice(&dev);
@@ -1481,14 +1538,45 @@ cudaError_t configure_batch_launch(const BatchView& B, int vertex_kernel, int th
     err = variant_warps(batch_kernel_fn(vertex_kernel, 0, B.fast != 0), threads, smem, &warps);
     if (err != cudaSuccess) return err;
     if (warps < 1) return cudaErrorInvalidConfiguration;
+    int per_sm = warps / nw;
+    int carveout = -1;
+    if (blocks_cap > 0 && blocks_cap < per_sm) {
+        int smem_sm = 0;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        per_sm = blocks_cap;
+        const double need = (double)per_sm * (double)(smem + 1024);
+        carveout = smem_sm > 0 ? (int)ceil(100.0 * need / smem_sm) : -1;
+        if (carveout > 100) carveout = 100;
+    }
     cfg->threads = threads;
     cfg->smem_bytes = smem;
     cfg->scene_in_smem = 0;
-    cfg->blocks = sms * (warps / nw);
-    cfg->warps_per_sm = warps;
-    cfg->blocks_per_sm = warps / nw;
-    cfg->carveout = -1;
+    cfg->blocks = sms * per_sm;
+    cfg->warps_per_sm = per_sm * nw;
+    cfg->blocks_per_sm = per_sm;
+    cfg->carveout = carveout;
     return cudaSuccess;
+}
+
+/* Launches a persistent batch kernel with the configuration's grid and,
+ * when it caps the resident blocks, its carveout as a launch attribute
+ * (kept by a captured graph's kernel node). */
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_multi(void (*kernel)(KArgs...), const LaunchCfg& cfg, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)cfg.blocks);
+    lc.blockDim = dim3((unsigned)cfg.threads);
+    lc.dynamicSmemBytes = cfg.smem_bytes;
+    lc.stream = st;
+    cudaLaunchAttribute at[1];
+    if (cfg.carveout >= 0) {
+        at[0].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+        at[0].val.sharedMemCarveout = (unsigned)cfg.carveout;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+    }
+    return cudaLaunchKernelEx(&lc, kernel, args...);
 }
 
 cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg, const float* q, long long offset,
@@ -1496,13 +1584,8 @@ cudaError_t launch_check_configs_multi(const BatchView& B, const LaunchCfg& cfg,
                                        cudaStream_t st)
 {
     if (B.nwork <= 0) return cudaSuccess;
-    if (B.fast)
-        k_check_configs_multi<true><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on, band,
-                                                                                    bq, ctl);
-    else
-        k_check_configs_multi<false><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, q, offset, res, band_on,
-                                                                                     band, bq, ctl);
-    return cudaGetLastError();
+    if (B.fast) return launch_multi(k_check_configs_multi<true>, cfg, st, B, q, offset, res, band_on, band, bq, ctl);
+    return launch_multi(k_check_configs_multi<false>, cfg, st, B, q, offset, res, band_on, band, bq, ctl);
 }
 
 cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, const float* qs, const float* qe,
@@ -1510,14 +1593,15 @@ cudaError_t launch_check_edges_multi(const BatchView& B, const LaunchCfg& cfg, c
                                      BandQueue bq, Control* ctl, cudaStream_t st)
 {
     if (B.nwork <= 0) return cudaSuccess;
-#define GPRM_MULTI_LAUNCH(POL_, FAST_)                                                                       \
-    k_check_edges_multi<POL_, FAST_><<<cfg.blocks, cfg.threads, cfg.smem_bytes, st>>>(B, qs, qe, offset, key,    \
-                                                                                     band_on, band, bq, \
-                                                                                     ctl)
-    if (policy == EDGE_EARLY_EXIT) { if (B.fast) GPRM_MULTI_LAUNCH(EDGE_EARLY_EXIT, true); else GPRM_MULTI_LAUNCH(EDGE_EARLY_EXIT, false); }
-    else { if (B.fast) GPRM_MULTI_LAUNCH(EDGE_ALL_STEPS, true); else GPRM_MULTI_LAUNCH(EDGE_ALL_STEPS, false); }
-#undef GPRM_MULTI_LAUNCH
-    return cudaGetLastError();
+    if (policy == EDGE_EARLY_EXIT)
+        return B.fast ? launch_multi(k_check_edges_multi<EDGE_EARLY_EXIT, true>, cfg, st, B, qs, qe, offset, key,
+                                     band_on, band, bq, ctl)
+                      : launch_multi(k_check_edges_multi<EDGE_EARLY_EXIT, false>, cfg, st, B, qs, qe, offset, key,
+                                     band_on, band, bq, ctl);
+    return B.fast ? launch_multi(k_check_edges_multi<EDGE_ALL_STEPS, true>, cfg, st, B, qs, qe, offset, key, band_on,
+                                 band, bq, ctl)
+                  : launch_multi(k_check_edges_multi<EDGE_ALL_STEPS, false>, cfg, st, B, qs, qe, offset, key, band_on,
+                                 band, bq, ctl);
 }
 
 cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const float* q, const float* qs,

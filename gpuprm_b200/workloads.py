@@ -48,20 +48,23 @@ def edge_workload(kind: str = "hull6", seed: int = 0, n_samples: int = 1 << 20, 
 
 
 MANY = dict(problems=256, dof=(4, 7), obstacles=(8, 128), samples_log2=(14, 18), radius=(0.4, 0.8),
-            edge_sources=1024, k=10, dq=0.01)
+            edge_sources=None, k=10, dq=0.01)
 
 
 def batch_workload(seed: int = 0, problems: int = MANY["problems"], samples_log2=MANY["samples_log2"],
-                   radius=MANY["radius"], edge_sources: int = MANY["edge_sources"], k: int = MANY["k"],
+                   radius=MANY["radius"], edge_sources=MANY["edge_sources"], k: int = MANY["k"],
                    dq: float = MANY["dq"], device: str = "cuda:0"):
     """Many independent problems (``scenes.make_mixed``: DOF 4-7, 8-128
     obstacles), each with 2^U[lo,hi] uniform samples and a connection
-    radius U[0.4, 0.8].  Edges: the k nearest free neighbours of the first
-    ``edge_sources`` free samples of each problem, every edge longer than
-    the radius cut back to the radius along its direction (the planner
-    connects within the radius).  Returns dict(spaces, scenes, q, qs, qe
-    (7, total) float32 CUDA SoA, offs_v, offs_e (numpy), n_free)."""
+    radius U[0.4, 0.8].  Edges: the k nearest free neighbours of every free
+    sample of each problem (of its first ``edge_sources`` free samples when
+    given), each undirected edge once, every edge longer than the radius
+    cut back to the radius along its direction (the planner connects within
+    the radius).  Everything is built and packed on the device.  Returns
+    dict(spaces, scenes, q, qs, qe (7, total) float32 CUDA SoA with rows
+    ndof..6 zero, offs_v, offs_e (numpy), n_free)."""
     import torch
+    from .batch import MAX_DOF, offsets_of
     rng = np.random.default_rng(seed)
     spaces, scs, qv, qa, qb, n_free = [], [], [], [], [], []
     for p in range(problems):
@@ -74,7 +77,9 @@ def batch_workload(seed: int = 0, problems: int = MANY["problems"], samples_log2
         qd = torch.tensor(np.ascontiguousarray(q.T), device=device)
         codes = torch.zeros(n, dtype=torch.int32, device=device)
         cs.check_configs_device(qd, codes)
-        free = torch.nonzero(codes == 0).squeeze(1)[:edge_sources]
+        free = torch.nonzero(codes == 0).squeeze(1)
+        if edge_sources is not None:
+            free = free[:edge_sources]
         qf = qd[:, free].T.contiguous()
         if qf.shape[0] >= 2:
             i, j = knn_pairs(qf, k)
@@ -87,14 +92,17 @@ def batch_workload(seed: int = 0, problems: int = MANY["problems"], samples_log2
             a = b = qf[:0]
         spaces.append(cs)
         scs.append(sc)
-        qv.append(q)
-        qa.append(a.cpu().numpy())
-        qb.append(b.cpu().numpy())
+        qv.append(qd)
+        qa.append(a.T)
+        qb.append(b.T)
         n_free.append(int((codes == 0).sum().item()))
-    from .batch import pack_items
-    Q, offs_v = pack_items(qv)
-    A, offs_e = pack_items(qa)
-    B, _ = pack_items(qb)
-    return dict(spaces=spaces, scenes=scs, q=torch.tensor(Q, device=device), qs=torch.tensor(A, device=device),
-                qe=torch.tensor(B, device=device), offs_v=offs_v, offs_e=offs_e, n_free=n_free,
-                q_host=qv, qs_host=qa, qe_host=qb)
+    offs_v = offsets_of([x.shape[1] for x in qv])
+    offs_e = offsets_of([x.shape[1] for x in qa])
+
+    def pack(parts, offs):
+        out = torch.zeros((MAX_DOF, int(offs[-1])), dtype=torch.float32, device=device)
+        for x, o in zip(parts, offs[:-1]):
+            out[:x.shape[0], int(o):int(o) + x.shape[1]] = x
+        return out
+    return dict(spaces=spaces, scenes=scs, q=pack(qv, offs_v), qs=pack(qa, offs_e), qe=pack(qb, offs_e),
+                offs_v=offs_v, offs_e=offs_e, n_free=n_free)

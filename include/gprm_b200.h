@@ -68,7 +68,15 @@ extern "C" {
 #define GPRM_MODE_FAST        2
 
 /* Edge evaluation (gprm_set_edge_policy). */
-/* Stop an edge at its first colliding step; res[e] is that step's code. */
+/* Stop an edge at its first colliding step; res[e] is that step's code
+ * (0: free).  "First" is the kernel's order, fixed for given inputs: the
+ * steps go in rounds of 32 (round r holds steps lane*R + r, R = rounds of
+ * the edge), each round pair by pair in the reference's pair order; the
+ * first round in which a step collides outside the FP64 band decides, at
+ * the lowest lane among the steps that collide at the earliest such pair,
+ * unless a lower lane of that round, or any step of an earlier round, was
+ * left in the band and collides in the FP64 check (then the lowest such
+ * round and lane).  The verdict (res != 0) is that of every other policy. */
 #define GPRM_EDGES_EARLY_EXIT 0
 /* Check every step; res[e] is the code of the last colliding step, exactly
  * what the reference CPU path writes (robotconfigspace.cpp:458,694-705). */
@@ -326,9 +334,19 @@ int  gprm_batch_replay(gprm_batch* b, int vertex_kernel, void* stream);
 /* Launch shape: threads per block (32..512); blocks fill every SM. */
 int  gprm_batch_set_launch(gprm_batch* b, int vertex_kernel, int threads);
 int  gprm_batch_get_launch(const gprm_batch* b, int vertex_kernel, int* threads, int* warps_per_sm);
-/* Times every launch shape (64, 128, 256, 512 threads) on this input,
- * `reps` runs each after one untimed run, and keeps the fastest.
- * Synchronous; the runs' counters are discarded. */
+/* Launch shape with a cap on the resident blocks per SM (0: as many as
+ * fit); a cap sets a shared-memory carveout just large enough for those
+ * blocks, so that the rest of the SM's storage serves as L1 for the
+ * scenes' tables.  gprm_batch_set_launch(b, k, t) = ..._shape(b, k, t, 0). */
+int  gprm_batch_set_launch_shape(gprm_batch* b, int vertex_kernel, int threads, int blocks_per_sm);
+int  gprm_batch_get_launch_shape(const gprm_batch* b, int vertex_kernel, int* threads, int* blocks_per_sm,
+                                 int* warps_per_sm);
+/* Times every launch shape on this input, `reps` runs each after one
+ * untimed run, and keeps the fastest: 64, 128, 256 and 512 threads per
+ * block, each with as many resident blocks per SM as fit and with 3/4 and
+ * 1/2 of them.  best_threads gets the winner's block size
+ * (gprm_batch_get_launch_shape gives the rest).  Synchronous; the runs'
+ * counters are discarded. */
 int  gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, const float* qb,
                          int* res, long long stride, int reps, int* best_threads, float* best_ms);
 int  gprm_batch_get_stats(const gprm_batch* b, gprm_stats* out);

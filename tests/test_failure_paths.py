@@ -3,8 +3,9 @@
 * FP64 queue overflow: a test hook caps the recheck queue far below the
   checks that need it; the overflow pass must complete the results on the
   stream, on the host-buffer, device-pointer and batched entry points alike
-  (all-steps codes and vertex codes identical, early-exit verdicts
-  identical), and count the recomputed items.
+  (vertex codes and the edge codes of both policies identical: the early
+  exit's code is that of the first colliding step in the check kernel's
+  order, overflowed or not), and count the recomputed items.
 * Device allocation failure: a test hook fails the n-th device allocation;
   the call returns GPRM_ERR_NOMEM and the handle works on the next call.
 * Tensor-core waits: a test hook shrinks the clock budget of the MLP
@@ -70,10 +71,7 @@ def test_queue_overflow_gives_complete_results(arith):
         for pol in (GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT):
             cs.set_edge_policy(pol)
             for got in (cs.check_edges(qs, qe), _device_edges(cs, qs, qe)):
-                if pol == GPRM_EDGES_ALL_STEPS:
-                    np.testing.assert_array_equal(got, want[pol])
-                else:
-                    np.testing.assert_array_equal(got != 0, want[pol] != 0)
+                np.testing.assert_array_equal(got, want[pol])
         np.testing.assert_array_equal(cs.check_configs(q), want_cfg)
         np.testing.assert_array_equal(_device_configs(cs, q), want_cfg)
     finally:
@@ -86,7 +84,8 @@ def test_queue_overflow_gives_complete_results(arith):
     assert cs.stats()["band_overflow_items"] == st1["band_overflow_items"]
 
 
-def test_batched_queue_overflow_gives_complete_results():
+@pytest.mark.parametrize("pol", [GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT])
+def test_batched_queue_overflow_gives_complete_results(pol):
     import torch
     from gpuprm_b200.batch import CONFIGS, EDGES, ProblemBatch, pack_items
     scs = [scenes.make_box4(41), scenes.make_hull6(42), scenes.make_box4(43)]
@@ -95,7 +94,7 @@ def test_batched_queue_overflow_gives_complete_results():
         cs = RobotConfigspace(sc, dq=0.02)
         cs.init()
         cs.set_mode(GPRM_MODE_FP64_BAND)
-        cs.set_edge_policy(GPRM_EDGES_ALL_STEPS)
+        cs.set_edge_policy(pol)
         spaces.append(cs)
     qv = [scenes.uniform_configs(sc, 700, 50 + i) for i, sc in enumerate(scs)]
     ed = [scenes.random_edges(sc, 150, 60 + i, 0.6) for i, sc in enumerate(scs)]
@@ -176,3 +175,39 @@ def test_mlp_wait_budget_expiry_is_reported_and_recovers():
     assert mlp.device_status() == 0
     np.testing.assert_array_equal(g1, g0)          # gradients reduce in a fixed order
     assert abs(l1 - l0) <= 1e-5 * abs(l0)           # the reported loss is summed atomically
+
+
+def test_queue_grows_to_the_demand_of_a_dense_band_scene():
+    """A cluttered scene where most edge steps end in the FP64 band (96% of
+    its configurations collide, most of them in shallow contact): the first
+    device-pointer call overflows the default queue and completes through
+    the overflow pass; the handle reads that demand back without a
+    synchronisation and sizes the next call's queue to it, so the same call
+    again overflows nothing and gives the same codes (both policies)."""
+    import torch
+    from gpuprm_b200.workloads import knn_pairs
+    sc = scenes.make_mixed(141)
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, 1 << 16, 7).T), device="cuda:0")
+    for pol in (GPRM_EDGES_EARLY_EXIT, GPRM_EDGES_ALL_STEPS):
+        cs = RobotConfigspace(sc, dq=0.01)
+        cs.init()
+        cs.set_mode(GPRM_MODE_FP64_BAND | GPRM_MODE_FAST)
+        cs.set_edge_policy(pol)
+        codes = torch.zeros(q.shape[1], dtype=torch.int32, device="cuda:0")
+        cs.check_configs_device(q, codes)
+        qf = q[:, codes == 0].T.contiguous()
+        i, j = knn_pairs(qf, 10)
+        qs, qe = qf[i].T.contiguous(), qf[j].T.contiguous()
+        n = qs.shape[1]
+        assert n > 10000
+        outs, ovf = [], []
+        for _ in range(3):
+            res = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+            before = cs.stats()["band_overflow_items"]
+            cs.check_edges_device(qs, qe, res)
+            torch.cuda.synchronize()
+            ovf.append(cs.stats()["band_overflow_items"] - before)
+            outs.append(res.cpu().numpy())
+        assert ovf[0] > 0 and ovf[1] == 0 and ovf[2] == 0
+        np.testing.assert_array_equal(outs[1], outs[0])
+        np.testing.assert_array_equal(outs[2], outs[0])
