@@ -762,27 +762,9 @@ def batch_leg(args, dev, policy):
     tune_v = T.autotune(CONFIGS, tq, None, torch.zeros(tq.shape[1], dtype=torch.int32, device=dev), reps=2)
     tune_e = T.autotune(EDGES, ta, tb, torch.zeros(ta.shape[1], dtype=torch.int32, device=dev), reps=2)
     t_tune = time.perf_counter() - t_tune
+    table = {"configs": T.tune_table(CONFIGS), "edges": T.tune_table(EDGES)}
     del T, tq, ta, tb
-    B.set_launch(CONFIGS, tune_v["threads"], tune_v["blocks_per_sm"])
-    B.set_launch(EDGES, tune_e["threads"], tune_e["blocks_per_sm"])
-    B.capture(CONFIGS, Q, None, rv)
-    B.capture(EDGES, A, Bq, re)
-    # per-problem views of the same inputs for the launch loop
-    ov, oe = ws["offs_v"], ws["offs_e"]
-    dofs = [sc.ndof for sc in ws["scenes"]]
-    pv = [Q[:d, ov[p]:ov[p + 1]] for p, d in enumerate(dofs)]
-    pa = [A[:d, oe[p]:oe[p + 1]] for p, d in enumerate(dofs)]
-    pb = [Bq[:d, oe[p]:oe[p + 1]] for p, d in enumerate(dofs)]
-    lv = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pv]
-    le = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pa]
     stream = torch.cuda.current_stream()
-
-    def loop(kind):
-        for p, cs in enumerate(spaces):
-            if kind == CONFIGS and lv[p].numel():
-                cs.check_configs_device(pv[p], lv[p])
-            elif kind == EDGES and le[p].numel():
-                cs.check_edges_device(pa[p], pb[p], le[p])
 
     def timed(fn, steps):
         fn()
@@ -794,6 +776,36 @@ def batch_leg(args, dev, policy):
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / steps
+
+    # the shape a new batch starts with, on the full set, before tuning
+    default = {"configs": B.get_launch(CONFIGS), "edges": B.get_launch(EDGES)}
+    t_dv = timed(lambda: B.check_configs_device(Q, rv), 1)
+    t_de = timed(lambda: B.check_edges_device(A, Bq, re), 1)
+    B.set_launch(CONFIGS, tune_v["threads"], tune_v["blocks_per_sm"])
+    B.set_launch(EDGES, tune_e["threads"], tune_e["blocks_per_sm"])
+    B.set_solo_threshold(CONFIGS, tune_v["solo"]["min_items"])
+    B.set_solo_threshold(EDGES, tune_e["solo"]["min_items"])
+    B.capture(CONFIGS, Q, None, rv)
+    B.capture(EDGES, A, Bq, re)
+    # rounds of 32 steps per edge (an edge split over warps pays only from
+    # a few rounds on)
+    tn = torch.floor(torch.linalg.vector_norm(Bq - A, dim=0) / workloads.MANY["dq"]) + 1
+    rounds = torch.ceil(tn / 32)
+    # per-problem views of the same inputs for the launch loop
+    ov, oe = ws["offs_v"], ws["offs_e"]
+    dofs = [sc.ndof for sc in ws["scenes"]]
+    pv = [Q[:d, ov[p]:ov[p + 1]] for p, d in enumerate(dofs)]
+    pa = [A[:d, oe[p]:oe[p + 1]] for p, d in enumerate(dofs)]
+    pb = [Bq[:d, oe[p]:oe[p + 1]] for p, d in enumerate(dofs)]
+    lv = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pv]
+    le = [torch.zeros(x.shape[1], dtype=torch.int32, device=dev) for x in pa]
+
+    def loop(kind):
+        for p, cs in enumerate(spaces):
+            if kind == CONFIGS and lv[p].numel():
+                cs.check_configs_device(pv[p], lv[p])
+            elif kind == EDGES and le[p].numel():
+                cs.check_edges_device(pa[p], pb[p], le[p])
 
     steps = 2
     s0 = B.stats()
@@ -817,8 +829,21 @@ def batch_leg(args, dev, policy):
         "batched": {"configs_per_s": nv / t_bv, "edge_steps_per_s": nominal / t_be,
                     "configs_ms": 1e3 * t_bv, "edges_ms": 1e3 * t_be, "graph_launches_per_step": 2,
                     "launch_shape": {"configs": B.get_launch(CONFIGS), "edges": B.get_launch(EDGES)},
+                    "solo": {"configs": B.get_solo_threshold(CONFIGS), "edges": B.get_solo_threshold(EDGES),
+                             "meaning": "problems with at least min_items items run in launches of their own "
+                                        "inside the captured graph; the rest share one persistent launch"},
                     "autotune": {"sub_batch": "every 8th problem (%d)" % len(sub), "seconds": t_tune,
-                                 "candidates": "threads 64/128/256/512 x resident blocks per SM all/3/4/half"},
+                                 "candidates": "threads 64/128/256/512 x resident blocks per SM all/3/4/half, "
+                                               "then solo threshold none/2^18/2^16/2^14/all items",
+                                 "sweep_ms_on_sub_batch": table,
+                                 "not_swept": "edge split over warps: the edges are %.2f rounds of 32 steps on "
+                                              "average (max %d), below the 2 rounds a segment needs; scene tables "
+                                              "in shared memory: the warps of a block check different problems, "
+                                              "so the tables go through L1, whose share the blocks-per-SM cap sets"
+                                              % (float(rounds.mean()), int(rounds.max()))},
+                    "default_shape": default,
+                    "default_configs_ms": 1e3 * t_dv, "default_edges_ms": 1e3 * t_de,
+                    "tuned_over_default_time": {"configs": t_bv / t_dv, "edges": t_be / t_de},
                     "timed_passes": steps},
         "per_problem_loop": {"configs_per_s": nv / t_lv, "edge_steps_per_s": nominal / t_le,
                              "configs_ms": 1e3 * t_lv, "edges_ms": 1e3 * t_le},

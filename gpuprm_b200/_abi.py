@@ -168,6 +168,10 @@ SIGNATURES = [
     ("gprm_batch_get_launch", C.c_int, [_P, C.c_int, _I, _I]),
     ("gprm_batch_set_launch_shape", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
     ("gprm_batch_get_launch_shape", C.c_int, [_P, C.c_int, _I, _I, _I]),
+    ("gprm_batch_get_tune_table", C.c_int, [_P, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            _I]),
+    ("gprm_batch_set_solo_threshold", C.c_int, [_P, C.c_int, C.c_longlong]),
+    ("gprm_batch_get_solo_threshold", C.c_int, [_P, C.c_int, C.POINTER(C.c_longlong), _I]),
     ("gprm_batch_autotune", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                                       _I, _F]),
     ("gprm_batch_get_stats", C.c_int, [_P, C.POINTER(Stats)]),

@@ -111,7 +111,31 @@ class ProblemBatch:
                                                  C.c_void_p(qb.data_ptr() if qb is not None else 0),
                                                  C.c_void_p(res.data_ptr()), int(qa.shape[1]), int(reps),
                                                  C.byref(t), C.byref(ms)))
-        return dict(self.get_launch(kind), ms=ms.value)
+        return dict(self.get_launch(kind), ms=ms.value, solo=self.get_solo_threshold(kind))
+
+    def tune_table(self, kind: int) -> list:
+        """The last autotune's candidates: [{threads, blocks_per_sm, ms}]."""
+        import numpy as np
+        cnt = C.c_int(0)
+        self._check(self.lib.gprm_batch_get_tune_table(self.h, int(kind), 0, None, None, None, None, C.byref(cnt)))
+        n = cnt.value
+        t, b, ms = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.float32)
+        so = np.zeros(n, np.int64)
+        if n:
+            self._check(self.lib.gprm_batch_get_tune_table(self.h, int(kind), n, t.ctypes.data, b.ctypes.data,
+                                                           so.ctypes.data, ms.ctypes.data, C.byref(cnt)))
+        return [{"threads": int(t[i]), "blocks_per_sm": int(b[i]), "solo_min_items": int(so[i]), "ms": float(ms[i])}
+                for i in range(n)]
+
+    def set_solo_threshold(self, kind: int, min_items: int) -> None:
+        """Problems with at least min_items items run in their own launches
+        (-1: none, 0: all); drops the kind's captured graph."""
+        self._check(self.lib.gprm_batch_set_solo_threshold(self.h, int(kind), int(min_items)))
+
+    def get_solo_threshold(self, kind: int) -> dict:
+        m, n = C.c_longlong(0), C.c_int(0)
+        self._check(self.lib.gprm_batch_get_solo_threshold(self.h, int(kind), C.byref(m), C.byref(n)))
+        return {"min_items": m.value, "solo_problems": n.value}
 
     def stats(self) -> dict:
         s = Stats()

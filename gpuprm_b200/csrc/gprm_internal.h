@@ -69,7 +69,14 @@ struct BatchView {
     const DevScene* scenes;   /* [S], device */
     const long long* offs;    /* [S+1], device */
     const int4* chunks;       /* vertex chunks, device */
-    long long nwork;          /* chunks (vertex) or edges (edge) */
+    long long nwork;          /* chunks (vertex) or edges (edge) of the shared launch */
+    /* edges of the shared launch: K ranges, range k = work items
+       woffs[k] .. woffs[k+1]-1 = edges wbase[k] .. of problem wprob[k]
+       (problems with their own launches are left out) */
+    const long long* woffs;   /* [K+1], device */
+    const long long* wbase;   /* [K], device */
+    const int* wprob;         /* [K], device */
+    int K;
     int S;
     int lane_floats;          /* per-lane shared floats: max over the problems */
     int fast;                 /* GPRM_MODE_FAST arithmetic (the problems share the mode) */

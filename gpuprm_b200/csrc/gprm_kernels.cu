@@ -1384,6 +1384,19 @@ __device__ __forceinline__ int problem_of(const BatchView& B, long long it)
     return lo;
 }
 
+/* Range of work item w of the shared edge launch: the k with
+ * woffs[k] <= w < woffs[k+1]. */
+__device__ __forceinline__ int range_of(const BatchView& B, long long w)
+{
+    int lo = 0, hi = B.K;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (B.woffs[mid] <= w) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 /* Makes problem p's descriptor the warp's current scene (warp-uniform p). */
 template <bool VERTEX>
 __device__ __forceinline__ void switch_scene(const BatchView& B, int p, DevScene* wsc, float* frames, SceneView& S)
@@ -1451,9 +1464,11 @@ __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __rest
         if (lane == 0) eu = atomicAdd(&ctl->next, 1ull);
         eu = __shfl_sync(FULL_MASK, eu, 0);
         if (eu >= (unsigned long long)B.nwork) break;
-        const int p = problem_of(B, (long long)eu);
+        const int k = range_of(B, (long long)eu);
+        const int p = B.wprob[k];
+        const long long e = B.wbase[k] + ((long long)eu - B.woffs[k]);
         if (p != cur) { switch_scene<false>(B, p, wsc, frames, S); cur = p; }
-        check_edge<POLICY, false, FAST>(*wsc, S, qs, qe, (long long)eu, offset, wsc->dq, key, band_on, band, bq, ctl,
+        check_edge<POLICY, false, FAST>(*wsc, S, qs, qe, e, offset, wsc->dq, key, band_on, band, bq, ctl,
                                         pc, exec, nominal);
     }
     flush_edge_counts(exec, nominal, pc, ctl);

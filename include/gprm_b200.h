@@ -341,14 +341,31 @@ int  gprm_batch_get_launch(const gprm_batch* b, int vertex_kernel, int* threads,
 int  gprm_batch_set_launch_shape(gprm_batch* b, int vertex_kernel, int threads, int blocks_per_sm);
 int  gprm_batch_get_launch_shape(const gprm_batch* b, int vertex_kernel, int* threads, int* blocks_per_sm,
                                  int* warps_per_sm);
-/* Times every launch shape on this input, `reps` runs each after one
- * untimed run, and keeps the fastest: 64, 128, 256 and 512 threads per
- * block, each with as many resident blocks per SM as fit and with 3/4 and
- * 1/2 of them.  best_threads gets the winner's block size
- * (gprm_batch_get_launch_shape gives the rest).  Synchronous; the runs'
- * counters are discarded. */
+/* Problems with at least min_items items (of the kind) are checked by the
+ * single-problem kernels in launches of their own, inside the same call
+ * (and captured graph): their scene sits in the kernel's constant bank and
+ * they keep their own launch shape, while the rest share one persistent
+ * launch that reads each warp's scene from shared memory.  -1 (the
+ * default): no problem runs alone; 0: every non-empty problem does.
+ * Changing it drops the kind's captured graph (capture again). */
+int  gprm_batch_set_solo_threshold(gprm_batch* b, int vertex_kernel, long long min_items);
+int  gprm_batch_get_solo_threshold(const gprm_batch* b, int vertex_kernel, long long* min_items,
+                                   int* solo_problems);
+/* Times the candidates on this input, `reps` runs each after one untimed
+ * run, and keeps the fastest: first the shared launch's shape (64, 128,
+ * 256 and 512 threads per block, each with as many resident blocks per SM
+ * as fit and with 3/4 and 1/2 of them), then with that shape the solo
+ * threshold (none, 2^18, 2^16, 2^14 items, every problem).  best_threads
+ * gets the winner's block size (gprm_batch_get_launch_shape and
+ * gprm_batch_get_solo_threshold give the rest).  Synchronous; drops the
+ * kind's captured graph; the runs' counters are discarded. */
 int  gprm_batch_autotune(gprm_batch* b, int vertex_kernel, const float* qa, const float* qb,
                          int* res, long long stride, int reps, int* best_threads, float* best_ms);
+/* The last autotune's candidates for a kind: up to cap rows of (threads per
+ * block, resident blocks per SM, solo threshold, ms per run); *count gets
+ * the number of candidates timed. */
+int  gprm_batch_get_tune_table(const gprm_batch* b, int vertex_kernel, int cap, int* threads,
+                               int* blocks_per_sm, long long* solo_min, float* ms, int* count);
 int  gprm_batch_get_stats(const gprm_batch* b, gprm_stats* out);
 
 /* ---- neighbour search on the device -------------------------------------

@@ -137,6 +137,27 @@ def test_graph_replay_and_autotune():
     assert tv["threads"] in (64, 128, 256, 512) and tv["ms"] > 0
     assert B.get_launch(EDGES)["threads"] == te["threads"]
     assert B.get_launch(EDGES)["blocks_per_sm"] == te["blocks_per_sm"] >= 1
+    table = B.tune_table(EDGES)
+    assert len(table) >= 4 and min(r["ms"] for r in table) == pytest.approx(te["ms"])
+    assert {r["threads"] for r in table} >= {64, 128, 256}
+    assert {r["solo_min_items"] for r in table} >= {-1, 0}
+    # problems in their own launches give the same results: all of them,
+    # the larger ones, none
+    for min_items in (0, 300, -1):
+        for kind in (CONFIGS, EDGES):
+            B.set_solo_threshold(kind, min_items)
+        st = B.get_solo_threshold(EDGES)
+        assert st["min_items"] == min_items
+        assert (st["solo_problems"] == 0) == (min_items < 0)
+        r4 = torch.full_like(r1, -9)
+        e4 = torch.full_like(e1, -9)
+        B.check_configs_device(Qd, r4)
+        B.check_edges_device(Ad, Bd, e4)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(r4.cpu().numpy(), r1.cpu().numpy())
+        np.testing.assert_array_equal(e4.cpu().numpy(), e1.cpu().numpy())
+    for kind in (CONFIGS, EDGES):
+        B.set_solo_threshold(kind, 300)
     # a capped shape (2 resident blocks per SM, the carveout as a launch
     # attribute) gives the same results, directly and in a captured graph
     for kind in (CONFIGS, EDGES):
@@ -163,7 +184,7 @@ def test_graph_replay_and_autotune():
     np.testing.assert_array_equal(e2.cpu().numpy(), e1.cpu().numpy())
     after = B.stats()
     assert after["vertex_checks"] == before["vertex_checks"] + 2 * Q.shape[1]
-    assert after["edge_steps_nominal"] == 2 * before["edge_steps_nominal"]
+    assert 5 * after["edge_steps_nominal"] == 7 * before["edge_steps_nominal"]   # 5 calls, then 2 replays
 
 
 @pytest.mark.gpu
