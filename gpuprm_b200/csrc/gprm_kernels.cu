@@ -903,16 +903,14 @@ __device__ __forceinline__ int check_config64(const DevScene& sc, const float* q
     return 0;
 }
 
-/* FP64 recheck of one queued item (vertex kind 0, edge step kind 1). */
-__device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2 it, const float* __restrict__ q,
-                                             const float* __restrict__ qs, const float* __restrict__ qe,
-                                             long long offset, float dq, int policy, int* __restrict__ res,
-                                             unsigned* __restrict__ key, unsigned long long& checks,
-                                             unsigned long long& flips)
+/* The item's configuration (vertex kind 0 or edge step kind 1); for an
+ * edge step also its step t and the edge's step count tn. */
+__device__ __forceinline__ void recheck_config(const DevScene& sc, int kind, uint2 it, const float* __restrict__ q,
+                                               const float* __restrict__ qs, const float* __restrict__ qe,
+                                               long long offset, float dq, float* qi, int& t, int& tn)
 {
-    const int code32 = (int)(it.y >> 27) - 1;
-    float qi[GPRM_MAX_FRAMES];
-    int t = 0, tn = 0;
+    t = 0;
+    tn = 0;
     if (kind == 0) {
         for (int j = 0; j < sc.ndof; ++j) qi[j] = q[(long long)it.x + offset * j];
     } else {
@@ -920,15 +918,19 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
         tn = edge_testnum(qs, qe, (long long)it.x, offset, sc.ndof, dq);
         edge_step_config(qs, qe, (long long)it.x, offset, sc.ndof, t, tn, qi);
     }
-    const int code = check_config64(sc, qi);
-    ++checks;
-    flips += ((code != 0) != (code32 != 0));
+}
+
+/* Writes an FP64 recheck's code: a configuration's result, or an edge
+ * step's key merge (the order of the check kernel for early exit). */
+__device__ __forceinline__ void recheck_store(int kind, uint2 it, int code, int t, int tn, int policy,
+                                              int* __restrict__ res, unsigned* __restrict__ key)
+{
     if (kind == 0) {
         res[it.x] = code;
     } else if (code != 0) {
         if (policy == EDGE_EARLY_EXIT) {
-            int R = (tn + 31) >> 5;
-            unsigned order = (unsigned)((t % R) * 32 + t / R);
+            const int R = (tn + 31) >> 5;
+            const unsigned order = (unsigned)((t % R) * 32 + t / R);
             atomicMin(&key[it.x], early_key(order, code));
         } else {
             atomicMax(&key[it.x], all_key(t, code));
@@ -1078,12 +1080,32 @@ __device__ __forceinline__ void overflow_item(const DevScene& sc, int kind, unsi
     key[x] = k;
 }
 
-__global__ void __launch_bounds__(128) k_recheck(DevScene sc, int kind, const float* __restrict__ q,
-                                                 const float* __restrict__ qs, const float* __restrict__ qe,
-                                                 long long offset, float dq, int policy,
-                                                 int* __restrict__ res, unsigned* __restrict__ key,
-                                                 const BandQueue bq,
-                                                 Control* ctl)
+/* The FP64 recheck of the queued items, one thread per item.  (A warp per
+ * item, the pairs spread over the lanes, ran 1.4x slower on the hull6
+ * edge workload: the items' own parallelism hides the FP64 latency better.) */
+constexpr int RECHECK_THREADS = 128;
+
+__device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2 it, const float* __restrict__ q,
+                                             const float* __restrict__ qs, const float* __restrict__ qe,
+                                             long long offset, float dq, int policy, int* __restrict__ res,
+                                             unsigned* __restrict__ key, unsigned long long& checks,
+                                             unsigned long long& flips)
+{
+    float qi[GPRM_MAX_FRAMES];
+    int t, tn;
+    recheck_config(sc, kind, it, q, qs, qe, offset, dq, qi, t, tn);
+    const int code = check_config64(sc, qi);
+    ++checks;
+    flips += ((code != 0) != ((int)(it.y >> 27) - 1 != 0));
+    recheck_store(kind, it, code, t, tn, policy, res, key);
+}
+
+__global__ void __launch_bounds__(RECHECK_THREADS) k_recheck(DevScene sc, int kind, const float* __restrict__ q,
+                                                             const float* __restrict__ qs,
+                                                             const float* __restrict__ qe, long long offset,
+                                                             float dq, int policy, int* __restrict__ res,
+                                                             unsigned* __restrict__ key, const BandQueue bq,
+                                                             Control* ctl)
 {
     unsigned cnt = ctl->qcount;
     if (cnt > bq.cap) cnt = bq.cap;
@@ -1339,7 +1361,7 @@ cudaError_t launch_recheck(const DevScene& sc, int blocks, int kind, const float
                            const float* qe, long long offset, float dq, int policy, int* res, unsigned* key,
                            BandQueue bq, Control* ctl, cudaStream_t st)
 {
-    k_recheck<<<blocks, 128, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, res, key, bq, ctl);
+    k_recheck<<<blocks, RECHECK_THREADS, 0, st>>>(sc, kind, q, qs, qe, offset, dq, policy, res, key, bq, ctl);
     return cudaGetLastError();
 }
 
@@ -1474,10 +1496,13 @@ __global__ void GPRM_BOUNDS k_check_edges_multi(BatchView B, const float* __rest
     flush_edge_counts(exec, nominal, pc, ctl);
 }
 
-__global__ void __launch_bounds__(128) k_recheck_multi(BatchView B, int kind, const float* __restrict__ q,
-                                                       const float* __restrict__ qs, const float* __restrict__ qe,
-                                                       long long offset, int policy, int* __restrict__ res,
-                                                       unsigned* __restrict__ key, BandQueue bq, Control* ctl)
+__global__ void __launch_bounds__(RECHECK_THREADS) k_recheck_multi(BatchView B, int kind,
+                                                                   const float* __restrict__ q,
+                                                                   const float* __restrict__ qs,
+                                                                   const float* __restrict__ qe, long long offset,
+                                                                   int policy, int* __restrict__ res,
+                                                                   unsigned* __restrict__ key, BandQueue bq,
+                                                                   Control* ctl)
 {
     unsigned cnt = ctl->qcount;
     if (cnt > bq.cap) cnt = bq.cap;
@@ -1623,7 +1648,7 @@ cudaError_t launch_recheck_multi(const BatchView& B, int blocks, int kind, const
                                  const float* qe, long long offset, int policy, int* res, unsigned* key,
                                  BandQueue bq, Control* ctl, cudaStream_t st)
 {
-    k_recheck_multi<<<blocks, 128, 0, st>>>(B, kind, q, qs, qe, offset, policy, res, key, bq, ctl);
+    k_recheck_multi<<<blocks, RECHECK_THREADS, 0, st>>>(B, kind, q, qs, qe, offset, policy, res, key, bq, ctl);
     return cudaGetLastError();
 }
 
