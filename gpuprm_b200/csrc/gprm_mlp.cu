@@ -1315,6 +1315,7 @@ __global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* 
     if (t < rows * kin) {
         const int o = t / kin, i = t % kin;
         float acc = 0.0f;
+#pragma unroll 8
         for (int s = 0; s < splits; ++s) acc += ws[(size_t)s * rows * ldw + (size_t)o * ldw + i];
         gw[t] = acc;
         return;
@@ -1323,6 +1324,7 @@ __global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* 
     if (cpart) {
         if (t < rows) {
             float acc = 0.0f;
+#pragma unroll 8
             for (int b = 0; b < cparts; ++b) acc += cpart[(size_t)b * rows + t];
             gb[t] = acc;
             return;
@@ -1336,20 +1338,28 @@ __global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* 
     }
 }
 
-/* dst[c][r] = src[r][c] for r < rows, c < cols (ld of dst = ldd); 32x32 tiles.
- * With colsum: colsum[blockIdx.y][c] = the sum of the tile's 32 rows of
- * column c (rows past the end count zero), for deterministic column sums. */
-__global__ void k_transpose_bf16(int rows, int cols, const __nv_bfloat16* __restrict__ src, int lds,
-                                 __nv_bfloat16* __restrict__ dst, int ldd, float* __restrict__ colsum = nullptr)
+/* Two transposes in one launch, 32x32 tiles: blocks x < xa write
+ * ta[c][r] = a[r][c] (cols_a columns) and colsum[blockIdx.y][c] = the sum
+ * of the tile's 32 rows of column c (rows past the end count zero: fixed
+ * order, deterministic column sums); the others tb[c][r] = b[r][c]
+ * (cols_b columns).  ldd: the leading dimension of ta and tb. */
+__global__ void k_transpose2_bf16(int rows, int xa, int cols_a, const __nv_bfloat16* __restrict__ a, int lda,
+                                  __nv_bfloat16* __restrict__ ta, float* __restrict__ colsum, int cols_b,
+                                  const __nv_bfloat16* __restrict__ b, int ldb, __nv_bfloat16* __restrict__ tb,
+                                  int ldd)
 {
     __shared__ __nv_bfloat16 t[32][33];
-    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const bool first = (int)blockIdx.x < xa;
+    const int cols = first ? cols_a : cols_b, lds = first ? lda : ldb;
+    const __nv_bfloat16* src = first ? a : b;
+    __nv_bfloat16* dst = first ? ta : tb;
+    const int r0 = blockIdx.y * 32, c0 = (first ? blockIdx.x : blockIdx.x - xa) * 32;
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int r = r0 + k, c = c0 + threadIdx.x;
         t[k][threadIdx.x] = (r < rows && c < cols) ? src[(size_t)r * lds + c] : __float2bfloat16(0.0f);
     }
     __syncthreads();
-    if (colsum && threadIdx.y == 0 && c0 + threadIdx.x < cols) {
+    if (first && colsum && threadIdx.y == 0 && c0 + threadIdx.x < cols) {
         float acc = 0.0f;
         for (int k = 0; k < 32; ++k) acc += __bfloat162float(t[k][threadIdx.x]);
         colsum[(size_t)blockIdx.y * cols + c0 + threadIdx.x] = acc;
@@ -1607,18 +1617,20 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
     int blocks = n < 1024 ? n : 1024;
     k_out_back<<<blocks, HID, 0, st>>>(n, h->H[NLAYER - 1], h->Z[NLAYER - 1], h->wbf + h->offWbf[NLAYER], h->dlogit,
                                        h->opart, h->dZ[NLAYER - 1]);
-    /* weight gradients: K = n split over CTAs, partials reduced in split order */
+    /* weight gradients: K = n split over CTAs, partials reduced in split
+       order (128 rows per split: 512-row splits made the step 1.4x slower,
+       the GEMM's longer K loop costing more than the partials it saves) */
     int splits = (n + 127) / 128;
     if (splits > TG_MAX_SPLITS) splits = TG_MAX_SPLITS;
     const int kps = ((n + splits - 1) / splits + 63) / 64 * 64;
     splits = (n + kps - 1) / kps;
-    const dim3 tgrid(HID / 32, (n + 31) / 32), tblock(32, 8);
+    const dim3 tblock(32, 8);
     for (int l = NLAYER - 1; l >= 0; --l) {
         const int kin = l == 0 ? IN_PAD : HID, kin_p = l == 0 ? 64 : HID;
         /* dW_l = dZ_l^T H_{l-1}: A = dZ_l^T [256 x n], B = H_{l-1}^T [kin_p x n] */
-        k_transpose_bf16<<<tgrid, tblock, 0, st>>>(n, HID, h->dZ[l], HID, h->Ta, h->ldT, h->cpart);
-        k_transpose_bf16<<<dim3(kin_p / 32, (n + 31) / 32), tblock, 0, st>>>(n, kin_p, l == 0 ? h->X64 : h->H[l - 1],
-                                                                             kin_p, h->Tb, h->ldT);
+        k_transpose2_bf16<<<dim3(HID / 32 + kin_p / 32, (n + 31) / 32), tblock, 0, st>>>(
+            n, HID / 32, HID, h->dZ[l], HID, h->Ta, h->cpart, kin_p, l == 0 ? h->X64 : h->H[l - 1], kin_p, h->Tb,
+            h->ldT);
         TgArgs a{};
         a.M = HID; a.N = kin_p; a.K = n; a.kps = kps; a.ws = h->ws; a.ldc = kin_p; a.err = h->dev_err; a.wait_cycles = wait_budget(h);
         if (l == 0)
