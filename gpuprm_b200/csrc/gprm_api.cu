@@ -843,15 +843,31 @@ int gprm_init(gprm_space* h, int rank, int size)
     CUDA_TRY(h, cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device));
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
 
-    /* d_scene: tab | pairs | pairs_b | far | scan_c | scan_b | ppoly | box | vtab | vinfo | cbin | cidx */
+    /* the candidate lists in fixed slots per (polytope, bin): cslots = the
+       longest list, shorter ones padded with their last entry */
+    h->cslots = 1;
+    for (unsigned hb : h->cbin) h->cslots = std::max(h->cslots, (int)(hb & 255u));
+    h->ccnt.assign(h->cbin.size(), 0);
+    h->ctab.assign(h->cbin.size() * (size_t)h->cslots, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (size_t kb = 0; kb < h->cbin.size(); ++kb) {
+        const int k = (int)(kb / GPRM_START_BINS), n = (int)(h->cbin[kb] & 255u);
+        const size_t off = h->cbin[kb] >> 8;
+        h->ccnt[kb] = (unsigned char)n;
+        for (int s = 0; s < h->cslots; ++s) {
+            const int idx = n > 0 ? h->cidx[off + (s < n ? s : n - 1)] : 0;
+            h->ctab[kb * h->cslots + s] = h->vtab[(size_t)h->vinfo[k].x + idx];
+        }
+    }
+
+    /* d_scene: tab | pairs | pairs_b | far | scan_c | scan_b | ppoly | box | vtab | vinfo | ctab | ccnt */
     size_t tb = h->tab.size() * sizeof(float4), pb = (size_t)h->npairs * sizeof(int4);
     size_t fsb = (size_t)h->npairs * sizeof(int2);
     size_t bxo = tb + 5 * pb + fsb, bxb = h->box.size() * sizeof(float4);
     bxo = (bxo + 15) & ~(size_t)15;
     const size_t vto = (bxo + bxb + 15) & ~(size_t)15, vtb = h->vtab.size() * sizeof(float4);
     const size_t vio = vto + vtb, vib = h->vinfo.size() * sizeof(int4);
-    const size_t cbo = (vio + vib + 15) & ~(size_t)15, cbb = h->cbin.size() * sizeof(unsigned);
-    const size_t cio = cbo + cbb, cib = h->cidx.size();
+    const size_t cbo = (vio + vib + 15) & ~(size_t)15, cbb = h->ctab.size() * sizeof(float4);
+    const size_t cio = cbo + cbb, cib = h->ccnt.size();
     CUDA_TRY(h, dev_malloc((void**)&h->d_scene, cio + cib + 64));
     char* base = (char*)h->d_scene;
     CUDA_TRY(h, cudaMemcpy(base, h->tab.data(), tb, cudaMemcpyHostToDevice));
@@ -864,8 +880,8 @@ int gprm_init(gprm_space* h, int rank, int size)
     if (bxb) CUDA_TRY(h, cudaMemcpy(base + bxo, h->box.data(), bxb, cudaMemcpyHostToDevice));
     if (vtb) CUDA_TRY(h, cudaMemcpy(base + vto, h->vtab.data(), vtb, cudaMemcpyHostToDevice));
     if (vib) CUDA_TRY(h, cudaMemcpy(base + vio, h->vinfo.data(), vib, cudaMemcpyHostToDevice));
-    if (cbb) CUDA_TRY(h, cudaMemcpy(base + cbo, h->cbin.data(), cbb, cudaMemcpyHostToDevice));
-    if (cib) CUDA_TRY(h, cudaMemcpy(base + cio, h->cidx.data(), cib, cudaMemcpyHostToDevice));
+    if (cbb) CUDA_TRY(h, cudaMemcpy(base + cbo, h->ctab.data(), cbb, cudaMemcpyHostToDevice));
+    if (cib) CUDA_TRY(h, cudaMemcpy(base + cio, h->ccnt.data(), cib, cudaMemcpyHostToDevice));
 
     DevScene& s = h->dsc;
     memset(&s, 0, sizeof(s));
@@ -892,8 +908,9 @@ int gprm_init(gprm_space* h, int rank, int size)
     s.box = bxb ? (const float4*)(base + bxo) : nullptr;
     s.vtab = (const float4*)(base + vto);
     s.vinfo = (const int4*)(base + vio);
-    s.cbin = cbb ? (const unsigned*)(base + cbo) : nullptr;
-    s.cidx = (const unsigned char*)(base + cio);
+    s.ctab = cbb ? (const float4*)(base + cbo) : nullptr;
+    s.ccnt = (const unsigned char*)(base + cio);
+    s.cslots = h->cslots;
     s.fast = (h->mode & GPRM_MODE_FAST) != 0;
     s.thr_dir = h->thr_dir;
     s.eps_dir = h->eps_dir;

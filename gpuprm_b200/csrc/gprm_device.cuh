@@ -86,10 +86,12 @@ struct DevScene {
        values (float bits), 0): the fast path's support search */
     const float4* vtab;
     const int4* vinfo;
-    /* per polytope and direction bin: (byte offset into cidx << 8 | count)
-       of the bin's support candidates, vertex indices in ascending order */
-    const unsigned* cbin;
-    const unsigned char* cidx;
+    /* per polytope and direction bin: its support candidates as vertex
+       entries (vtab's), ascending vertex index, in cslots slots (slots past
+       the count repeat the last candidate), and the count */
+    const float4* ctab;
+    const unsigned char* ccnt;
+    int cslots;
 };
 
 /* fields of a table entry's w word */
@@ -703,38 +705,37 @@ __device__ __forceinline__ bool fsupport_cand2(const DevScene& sc, int kP, int4 
                                                float pz, int kQ, int4 vQ, float4& cq, float qx, float qy, float qz)
 {
     const float tieP = __int_as_float(vP.z), tieQ = __int_as_float(vQ.z);
-    const unsigned hP = sc.cbin[kP * GPRM_START_BINS + dir_bin(px, py, pz)];
-    const unsigned hQ = sc.cbin[kQ * GPRM_START_BINS + dir_bin(qx, qy, qz)];
-    const unsigned char* LP = sc.cidx + (hP >> 8);
-    const unsigned char* LQ = sc.cidx + (hQ >> 8);
-    const int nP = (int)(hP & 255u), nQ = (int)(hQ & 255u);
-    const float4* VP = sc.vtab + vP.x;
-    const float4* VQ = sc.vtab + vQ.x;
-    int ip = LP[0], iq = LQ[0];
-    float4 u = VP[ip], v = VQ[iq];
+    /* the bin's slots and count are found from the bin alone: the count
+       and the first candidate load side by side */
+    const int bP = kP * GPRM_START_BINS + dir_bin(px, py, pz);
+    const int bQ = kQ * GPRM_START_BINS + dir_bin(qx, qy, qz);
+    const float4* CP = sc.ctab + (size_t)bP * sc.cslots;
+    const float4* CQ = sc.ctab + (size_t)bQ * sc.cslots;
+    const int nP = sc.ccnt[bP], nQ = sc.ccnt[bQ];
+    int ip = 0, iq = 0;
+    float4 u = CP[0], v = CQ[0];
     float bp = fdot3(u.x, u.y, u.z, px, py, pz), bq = fdot3(v.x, v.y, v.z, qx, qy, qz);
     const float ninf = __int_as_float(0xff800000);
     float sp = ninf, sq = ninf;   /* runners-up */
     const int n = nP > nQ ? nP : nQ;
-    /* branch-free top two; past its last candidate a list re-reads that
-       candidate and counts it as -infinity */
+    /* branch-free top two; past its count a list's slots repeat its last
+       candidate, counted as -infinity */
 #pragma unroll 1
     for (int c = 1; c < n; ++c) {
-        const int a = LP[c < nP ? c : nP - 1], b = LQ[c < nQ ? c : nQ - 1];
-        u = VP[a];
-        v = VQ[b];
+        u = CP[c];
+        v = CQ[c];
         float du = fdot3(u.x, u.y, u.z, px, py, pz), dv = fdot3(v.x, v.y, v.z, qx, qy, qz);
         du = c < nP ? du : ninf;
         dv = c < nQ ? dv : ninf;
-        ip = du > bp ? a : ip;
-        iq = dv > bq ? b : iq;
+        ip = du > bp ? c : ip;
+        iq = dv > bq ? c : iq;
         sp = fmaxf(sp, fminf(bp, du));
         sq = fmaxf(sq, fminf(bq, dv));
         bp = fmaxf(bp, du);
         bq = fmaxf(bq, dv);
     }
-    cp = VP[ip];
-    cq = VQ[iq];
+    cp = CP[ip];
+    cq = CQ[iq];
     return !(bp - sp > tieP) || !(bq - sq > tieQ);
 }
 

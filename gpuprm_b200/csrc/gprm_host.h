@@ -92,6 +92,11 @@ struct gprm_space {
     /* support candidates per polytope and direction bin (see fsupport_cand2) */
     std::vector<unsigned> cbin;
     std::vector<unsigned char> cidx;
+    /* the lists as the device reads them: per (polytope, bin) cslots
+       vertex entries (the list, then copies of its last entry) and the count */
+    std::vector<float4> ctab;
+    std::vector<unsigned char> ccnt;
+    int cslots = 1;
     double extent = 1.0;           /* length scale of the scene (m) */
     float thr_dir = 0, eps_dir = 0;
 
