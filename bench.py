@@ -27,7 +27,7 @@ Extra legs in the same line (not part of `value`):
              (2^20 samples, 1000 seeded queries; the predictor is trained on
              2^20 exact-checker labels by the library's BF16 kernels);
   prm_stress the same on the 7-DOF wall scene (512 obstacles, two walls with
-             a 0.12 m gap, dq 0.005, k 16, 2^17 samples);
+             a 0.12 m gap, dq 0.005, k 16, 2^20 samples);
   stress_edges  checker throughput on the 7-DOF wall scene at full size
              (2^22 samples, k=16, dq 0.005): vertex checks/s and edge-step
              checks/s on 2^21 of the roadmap's edges, with the reference CPU
@@ -92,7 +92,7 @@ def parse():
     ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
     ap.add_argument("--prm-samples", type=int, default=1 << 20)
     ap.add_argument("--no-stress", action="store_true", help="skip the 7-DOF wall planner comparison")
-    ap.add_argument("--stress-samples", type=int, default=1 << 17)
+    ap.add_argument("--stress-samples", type=int, default=1 << 20)
     ap.add_argument("--no-stress-edges", action="store_true", help="skip the 7-DOF wall checker throughput leg")
     ap.add_argument("--stress-edges", type=int, default=1 << 21, help="roadmap edges the stress leg checks")
     ap.add_argument("--no-batch", action="store_true", help="skip the many-problem batch leg")
