@@ -86,7 +86,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--policy", default="early", choices=["early", "all"])
+    ap.add_argument("--policy", default="all", choices=["early", "all"])
     ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
                     help="FP32 arithmetic of the checks: fast (GPRM_MODE_FAST) or the reference's exact operations")
     ap.add_argument("--no-prm", action="store_true", help="skip the PRM time-to-path comparison")
@@ -346,7 +346,8 @@ def run_ours(args, rank, world, local_rank):
         cpu, work, sample = cpu_reference_rate(ws["scene"], qs_r, qe_r, WORKLOAD["dq"], args.cpu_seconds,
                                                args.seed)
         parity = edge_parity(ws["scene"], qs_r, qe_r, WORKLOAD["dq"], WORKLOAD["band_m"], sample, res_np,
-                             "headline edges (FP64 band mode, early exit) vs the reference CPU checker")
+                             "headline edges (FP64 band mode, %s policy) vs the reference CPU checker"
+                             % ("early-exit" if args.policy == "early" else "last-colliding-step"))
     k_ms = prof["fp32_ms"] / max(1, prof["fp32_launches"])
     per = lambda key: (s1[key] - s0[key]) / max(1, args.steps)
     full_pl, cert_pl, exec_pl = per("pairs_tested"), per("pairs_certified"), executed / max(1, args.steps)

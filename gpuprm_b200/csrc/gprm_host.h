@@ -109,7 +109,7 @@ struct gprm_space {
     gprm::LaunchCfg cfg_v, cfg_e;
 
     int mode = GPRM_MODE_FP64_BAND;
-    int policy = GPRM_EDGES_EARLY_EXIT;
+    int policy = GPRM_EDGES_ALL_STEPS;
     int split_max = 16384;        /* edge batches up to this size split long edges */
     int split_rounds = 2;         /* rounds of 32 steps per segment */
     float band = 1e-5f;

@@ -42,7 +42,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import scenes
-from ._abi import GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT
+from ._abi import GPRM_EDGES_ALL_STEPS
 from .graph import RoadmapGraph
 from .neighbours import NeighbourIndex
 
@@ -117,7 +117,7 @@ class _Phases:
         self.last = now
 
 
-def _check_edges(cs, qa, qb, policy=GPRM_EDGES_EARLY_EXIT):
+def _check_edges(cs, qa, qb, policy=GPRM_EDGES_ALL_STEPS):
     """Exact verdicts (int32 codes) of edges qa[i] -> qb[i] ((n, ndof) CUDA tensors)."""
     import torch
     n = qa.shape[0]

@@ -78,8 +78,15 @@ extern "C" {
  * left in the band and collides in the FP64 check (then the lowest such
  * round and lane).  The verdict (res != 0) is that of every other policy. */
 #define GPRM_EDGES_EARLY_EXIT 0
-/* Check every step; res[e] is the code of the last colliding step, exactly
- * what the reference CPU path writes (robotconfigspace.cpp:458,694-705). */
+/* res[e] is the code of the last colliding step, exactly what the
+ * reference CPU path writes (robotconfigspace.cpp:458,694-705).  The steps
+ * go from the qs end in rounds of 32 consecutive steps; a round with a
+ * collision outside the FP64 band finishes its steps nearer qs and ends the
+ * edge, since the steps after it cannot hold the last colliding one.  The
+ * default: besides giving the reference's codes, its rounds of neighbouring
+ * steps let the warp-wide sweep certificates settle more pairs, and it ran
+ * faster than the early-exit order on every workload measured (headline
+ * edges 198 vs 218 ms, 7-DOF wall edges 1.64 vs 1.91 s). */
 #define GPRM_EDGES_ALL_STEPS  1
 
 /* ---- scene description --------------------------------------------- */
