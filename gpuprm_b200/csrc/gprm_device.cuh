@@ -589,8 +589,28 @@ __device__ __forceinline__ bool pair_certified(const DevScene& sc, const float4*
  * covers float rounding, which exceeds double rounding), and the first
  * direction is computed in double, so its error term only needs the
  * 1e-6 relative allowance. */
+/* box_support with the FP64 frames of check_config64 */
+__device__ __forceinline__ double box_support64(const float4* __restrict__ B, const Frame<double>* F, int f, double ux,
+                                                double uy, double uz)
+{
+    double lx = ux, ly = uy, lz = uz;
+    if (f) {
+        const Frame<double>& T = F[f];
+        lx = T.m[0] * ux + T.m[1] * uy + T.m[2] * uz;
+        ly = T.m[3] * ux + T.m[4] * uy + T.m[5] * uz;
+        lz = T.m[6] * ux + T.m[7] * uy + T.m[8] * uz;
+    }
+    double h = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float4 b = B[a];
+        h += (double)b.w * fabs((double)b.x * lx + (double)b.y * ly + (double)b.z * lz);
+    }
+    return h;
+}
+
 __device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float4* __restrict__ tab, int4 pr,
-                                                 float4 pb, const Frame<double>* F, const double* cen)
+                                                 float4 pb, const Frame<double>* F, const double* cen, int j)
 {
     /* ball centres: a moving polytope's from its slot (the FP64 transform of
        its ball centre, computed once per check), a static one's from the
@@ -617,7 +637,18 @@ __device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float
     const double inv = 1.0 / sqrt(n2);
     const double G = (sx * dx + sy * dy + sz * dz) * inv - (double)pb.x;
     const double err = (sqrt(d2) + (double)pb.x) * 1e-6;
-    return G - err > (double)sc.thr_dir;
+    if (G - err > (double)sc.thr_dir) return true;
+    /* the box test of pair_certified_dir: each polytope's support along the
+       first direction bounded by its box about the ball centre (the box
+       records are inflated for float rounding, which covers FP64 vertices
+       too); a moving polytope without a slot has no usable centre */
+    if (!sc.box || !((double)pb.x < 1e300)) return false;
+    const int2 pp = sc.ppoly[j];
+    const double ux = sx * inv, uy = sy * inv, uz = sz * inv;
+    const double hp = box_support64(sc.box + 3 * pp.x, F, pr.z, ux, uy, uz);
+    const double hq = box_support64(sc.box + 3 * pp.y, F, pr.w, ux, uy, uz);
+    const double Gb = (ux * dx + uy * dy + uz * dz) - (hp + hq) * (1.0 + 1e-5);
+    return Gb - err > (double)sc.thr_dir;
 }
 
 /* ---------------------------------------------------------------- */

@@ -895,7 +895,7 @@ __device__ __forceinline__ int check_config64(const DevScene& sc, const float* q
 #pragma unroll 1
     for (int j = 0; j < sc.npairs; ++j) {
         const int4 pr = sc.pairs[j];
-        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F, cen)) continue;
+        if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F, cen, j)) continue;
         double m;
         const int r = pair_test<PF64>(sc, sc.tab, pr, F[pr.z], F[pr.w], &m);
         if (r != 0) return r;
