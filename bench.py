@@ -64,9 +64,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes per edge of one k_check_edges launch on this workload at full
-# size (one launch captured by ncu with dram__bytes_read.sum and
-# dram__bytes_write.sum: 162.40 MB + 23.82 MB for 2,926,333 edges).
-DRAM_BYTES_PER_EDGE = 186.22e6 / 2926333
+# size (the default last-colliding-step policy, fast arithmetic; one launch
+# captured by ncu with dram__bytes_read.sum and dram__bytes_write.sum:
+# 159.34 MB + 29.60 MB for 2,926,333 edges).
+DRAM_BYTES_PER_EDGE = 188.94e6 / 2926333
 
 METRIC = "edge-step collision checks/s"
 UNIT = "edge-steps/s"
@@ -368,8 +369,8 @@ def run_ours(args, rank, world, local_rank):
         roof = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": DRAM_BYTES_PER_EDGE * E,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_check_edges launch "
-                                  "of this workload at full size (162.40 + 23.82 MB for 2,926,333 edges), per "
-                                  "edge x this run's edges",
+                                  "of this workload at full size (159.34 + 29.60 MB for 2,926,333 edges, default "
+                                  "policy), per edge x this run's edges",
                 "algorithmic_bytes": int(2 * qs.numel() * 4 + E * 4),
                 "peak_source": "measured FP32 FMA probe on this device (2 flops/FMA); "
                                "MEASURED_PEAKS.json has no FP32 entry",
