@@ -117,6 +117,7 @@ SIGNATURES = [
     ("gprm_indicator", C.c_int, [_P, _F, _I]),
     ("gprm_indicator_batch", C.c_int, [_P, _F, _I, C.c_int, C.c_int]),
     ("gprm_indicator2", C.c_int, [_P, _F, _F, _I, C.c_int, C.c_int]),
+    ("gprm_indicator2_compressed", C.c_int, [_P, _F, C.c_int, _F, _I, _I, _I, C.c_int]),
     ("gprm_indicator2_async", C.c_int, [_P, _F, _F, _I, C.c_int, C.c_int, _I]),
     ("gprm_indicator2_wait", C.c_int, [_P, C.c_int]),
     ("gprm_check_boundaries", C.c_int, [_P, _F, _I, C.c_int, C.c_int]),

@@ -176,6 +176,18 @@ class RobotConfigspace:
         return res
 
     # -- device buffers (torch tensors, SoA (ndof, n) float32 on the GPU) --------
+    def indicator2_compressed(self, qs, M: int, qe, res, posqe, numqe, offset: int) -> int:
+        """indicator2(qs, M, qe, res, posqe, numqe, offset): res[l] for the
+        edges qs[k] -> qe[l], l in posqe[k] .. posqe[k]+numqe[k]-1 (qs SoA
+        with row stride M, qe with row stride offset; host arrays)."""
+        a, b = _f32(qs), _f32(qe)
+        assert res.dtype == np.int32 and res.flags.c_contiguous
+        pos = np.ascontiguousarray(posqe, np.int32)
+        num = np.ascontiguousarray(numqe, np.int32)
+        _check(self.lib, self.h, self.lib.gprm_indicator2_compressed(self.h, fptr(a), int(M), fptr(b), iptr(res),
+                                                                    iptr(pos), iptr(num), int(offset)))
+        return 0
+
     def check_configs_device(self, q_soa, res, stream=None) -> None:
         """q_soa: (ndof, n) float32 CUDA tensor with unit column stride
         (a column slice of a wider SoA array works: its row stride is the

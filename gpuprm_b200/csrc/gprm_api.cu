@@ -15,6 +15,7 @@
  *   - every failure returns a status code and leaves a message instead of
  *     asserting (util.hpp:44-46).
  */
+#include <limits.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>
@@ -1073,6 +1074,41 @@ int gprm_indicator2(gprm_space* h, const float* qs, const float* qe, int* res, i
     int rc = gprm_indicator2_async(h, qs, qe, res, n, offset, &req);
     if (rc) return rc;
     return gprm_indicator2_wait(h, req);
+}
+
+int gprm_indicator2_compressed(gprm_space* h, const float* qs, int M, const float* qe, int* res, const int* posqe,
+                               const int* numqe, int offset)
+{
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (M < 0 || offset < 0 || (M > 0 && (!qs || !qe || !res || !posqe || !numqe)))
+        return fail(h, GPRM_ERR_ARG, "bad qs/qe/res/posqe/numqe/M/offset");
+    long long n = 0;
+    for (int k = 0; k < M; ++k) {
+        if (posqe[k] < 0 || numqe[k] < 0 || (long long)posqe[k] + numqe[k] > (long long)offset)
+            return fail(h, GPRM_ERR_ARG, "range %d: posqe %d, numqe %d outside the %d end configurations", k,
+                        posqe[k], numqe[k], offset);
+        n += numqe[k];
+    }
+    if (n == 0) return GPRM_OK;
+    if (n > (long long)INT_MAX) return fail(h, GPRM_ERR_ARG, "%lld edges exceed %d", n, INT_MAX);
+    /* the pairs as a plain edge batch (SoA, offset n), in (k, l) order */
+    const int nd = h->ndof;
+    std::vector<float> a((size_t)n * nd), b((size_t)n * nd);
+    std::vector<int> out((size_t)n), dst((size_t)n);
+    size_t e = 0;
+    for (int k = 0; k < M; ++k)
+        for (int l = posqe[k]; l < posqe[k] + numqe[k]; ++l, ++e) {
+            for (int j = 0; j < nd; ++j) {
+                a[e + (size_t)n * j] = qs[k + (size_t)M * j];
+                b[e + (size_t)n * j] = qe[l + (size_t)offset * j];
+            }
+            dst[e] = l;
+        }
+    rc = gprm_indicator2(h, a.data(), b.data(), out.data(), (int)n, (int)n);
+    if (rc) return rc;
+    for (size_t i = 0; i < (size_t)n; ++i) res[dst[i]] = out[i];   /* later ranges overwrite earlier ones */
+    return GPRM_OK;
 }
 
 int gprm_check_boundaries(gprm_space* h, const float* q, int* res, int n, int offset)

@@ -189,6 +189,20 @@ int gprm_indicator_batch(gprm_space* h, const float* q, int* res, int n, int off
  * step is free, else nonzero (see the edge policies above). */
 int gprm_indicator2(gprm_space* h, const float* qs, const float* qe, int* res, int n, int offset);
 
+/* The compressed edge check indicator2(qs, M, qe, res, posqe, numqe,
+ * offset) (configspace.hpp:29-32), which the reference's robot space
+ * declares and leaves unimplemented (robotconfigspace.cpp:764-772), with
+ * the meaning its 2-D array space gives it (arrayconfigspace.cpp:88-120):
+ * for k = 0..M-1 and l = posqe[k] .. posqe[k]+numqe[k]-1, res[l] = the
+ * code of the edge from qs[k + M*j] to qe[l + offset*j] (as
+ * gprm_indicator2, under the edge policy); a later k overwrites an earlier
+ * one's res[l]; entries of res that no range covers are left as they are.
+ * Star-shaped batches (one start, many ends) are what a planner's
+ * neighbour search produces.  Needs 0 <= posqe[k], numqe[k] >= 0 and
+ * posqe[k] + numqe[k] <= offset.  Host buffers; synchronous. */
+int gprm_indicator2_compressed(gprm_space* h, const float* qs, int M, const float* qe, int* res, const int* posqe,
+                               const int* numqe, int offset);
+
 /* indicator2_async / indicator2_async_wait (configspace.hpp:269-270,
  * robotconfigspace.cpp:617-742).  `qs`, `qe` are read before the call
  * returns; `res` must stay valid until gprm_indicator2_wait returns, which

@@ -67,7 +67,13 @@ public:
     int indicator2_async_wait(int request) { return throw_on_error(gprm_indicator2_wait(h_, request)); }
     /* the compressed form is declared but unimplemented in the reference
        too (robotconfigspace.cpp:765-772) */
-    int indicator2(const float*, const int, const float*, int*, const int*, const int*, const int) { return -1; }
+    /* the compressed edge check (unimplemented in the reference's robot
+       space; the meaning of its array space) */
+    int indicator2(const float* qs, const int M, const float* qe, int* res, const int* posqe, const int* numqe,
+                   const int offset)
+    {
+        return throw_on_error(gprm_indicator2_compressed(h_, qs, M, qe, res, posqe, numqe, offset));
+    }
     int check_boundaries(const float* q, int* res, const int N, const int offset)
     {
         return throw_on_error(gprm_check_boundaries(h_, q, res, N, offset));

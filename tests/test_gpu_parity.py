@@ -286,3 +286,37 @@ def test_handles_keep_their_launch_shapes():
     b = space(scenes.make_box4(3), 0.02, mode=GPRM_MODE_FP64_BAND)
     b.check_configs(scenes.uniform_configs(scenes.make_box4(3), 100, 1))
     np.testing.assert_array_equal(a.check_configs(z["q"]), want)
+
+
+@pytest.mark.gpu
+def test_compressed_edge_check_equals_the_expanded_pairs():
+    """indicator2(qs, M, qe, res, posqe, numqe, offset), the star-shaped
+    form the reference declares but leaves unimplemented in its robot space:
+    res[l] is the code of the edge qs[k] -> qe[l] for l in k's range (the
+    array space's meaning), later ranges overwrite earlier ones, uncovered
+    entries keep their value, and bad ranges are rejected."""
+    from gpuprm_b200.configspace import GprmError
+    sc, z = load_golden("hull6")
+    cs = RobotConfigspace(sc, dq=float(z["dq"]))
+    cs.init()
+    rng = np.random.default_rng(5)
+    M, L = 40, 300
+    qs = scenes.uniform_configs(sc, M, 11)
+    qe = scenes.uniform_configs(sc, L, 12)
+    qe = qe * 0.3 + np.repeat(qs, (L + M - 1) // M, axis=0)[:L] * 0.7     # ends near the starts
+    pos = rng.integers(0, L - 20, M).astype(np.int32)
+    num = rng.integers(0, 20, M).astype(np.int32)
+    num[3] = 0
+    res = np.full(L, -77, np.int32)
+    cs.indicator2_compressed(np.ascontiguousarray(qs.T), M, np.ascontiguousarray(qe.T), res, pos, num, L)
+    want = np.full(L, -77, np.int32)
+    for k in range(M):
+        ls = np.arange(pos[k], pos[k] + num[k])
+        if len(ls):
+            want[ls] = cs.check_edges(np.repeat(qs[k:k + 1], len(ls), axis=0), qe[ls])
+    np.testing.assert_array_equal(res, want)
+    assert (res != -77).sum() > 100 and (res == -77).any()
+    bad = num.copy()
+    bad[0] = L
+    with pytest.raises(GprmError):
+        cs.indicator2_compressed(np.ascontiguousarray(qs.T), M, np.ascontiguousarray(qe.T), res, pos, bad, L)
