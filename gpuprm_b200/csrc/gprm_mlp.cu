@@ -1446,18 +1446,26 @@ struct gprm_mlp {
     /* training on the tensor cores (k_tc_gemm) */
     int train_path = GPRM_MLP_TRAIN_TCGEN05;
     __nv_bfloat16* X64 = nullptr;       /* features padded to 64 columns [rows x 64] */
-    __nv_bfloat16 *Ta = nullptr, *Tb = nullptr;   /* transposes [256 x ldT] */
+    /* the weight-gradient chain of each layer (transposes, split-K GEMM,
+       ordered reduction) has its own buffers, so that the chains of
+       different layers can run side by side on st_w */
+    __nv_bfloat16 *Ta = nullptr, *Tb = nullptr;   /* transposes [NLAYER][256 x ldT] */
     int ldT = 0;
     __nv_bfloat16* w1p = nullptr;       /* W1 padded [256 x 64] */
     __nv_bfloat16* wt = nullptr;        /* W_l^T, layers 2..4 [3 x 256 x 256] */
-    float* ws = nullptr;                /* split-K partials [TG_MAX_SPLITS x 256 x 256] */
-    float* cpart = nullptr;             /* bias-gradient partials [max(1024, rows/32) x 256] */
+    float* ws = nullptr;                /* split-K partials [NLAYER][TG_MAX_SPLITS x 256 x 256] */
+    float* cpart = nullptr;             /* bias-gradient partials [NLAYER][cparts x 256] */
+    size_t cparts = 0;
+    cudaStream_t st_w = nullptr;        /* weight-gradient chains */
+    cudaEvent_t ev_dz[NLAYER] = {};     /* dZ_l written (on st) */
+    cudaEvent_t ev_w = nullptr;         /* every chain done (on st_w) */
     float* opart = nullptr;             /* output-layer gradient partials [1024 x 257] */
     int tc_n = -1;                      /* batch the tensor maps were made for */
     int tc_attr = 0;
     long long* d_ctl = nullptr;         /* training epoch: [row offset into perm, Adam step before it] */
     const long long* idx_off = nullptr; /* set while a training epoch is captured */
-    CUtensorMap m_x64, m_h[NLAYER - 1], m_dz[NLAYER], m_w1p, m_w[NLAYER - 1], m_wt[NLAYER - 1], m_ta, m_tb256, m_tb64;
+    CUtensorMap m_x64, m_h[NLAYER - 1], m_dz[NLAYER], m_w1p, m_w[NLAYER - 1], m_wt[NLAYER - 1], m_ta[NLAYER],
+        m_tb256[NLAYER], m_tb64;
     unsigned* dev_err = nullptr;
     long long wait_cycles = 0;          /* pipeline wait budget of the tensor-core kernels, 0 = default */
     int sms = 0;
@@ -1501,16 +1509,22 @@ int alloc_batch(gprm_mlp* h, int rows)
     cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb); cudaFree(h->cpart);
     h->cpart = nullptr;
     const size_t cparts = std::max<size_t>(1024, (R + 31) / 32);
-    MLP_TRY(h, cudaMalloc((void**)&h->cpart, cparts * HID * sizeof(float)));
+    h->cparts = cparts;
+    MLP_TRY(h, cudaMalloc((void**)&h->cpart, (size_t)NLAYER * cparts * HID * sizeof(float)));
     if (!h->opart) MLP_TRY(h, cudaMalloc((void**)&h->opart, (size_t)1024 * (HID + 1) * sizeof(float)));
     h->ldT = (rows + 63) / 64 * 64;
     MLP_TRY(h, cudaMalloc((void**)&h->X64, R * 64 * sizeof(__nv_bfloat16)));
-    MLP_TRY(h, cudaMalloc((void**)&h->Ta, (size_t)HID * h->ldT * sizeof(__nv_bfloat16)));
-    MLP_TRY(h, cudaMalloc((void**)&h->Tb, (size_t)HID * h->ldT * sizeof(__nv_bfloat16)));
+    MLP_TRY(h, cudaMalloc((void**)&h->Ta, (size_t)NLAYER * HID * h->ldT * sizeof(__nv_bfloat16)));
+    MLP_TRY(h, cudaMalloc((void**)&h->Tb, (size_t)NLAYER * HID * h->ldT * sizeof(__nv_bfloat16)));
     if (!h->w1p) {
         MLP_TRY(h, cudaMalloc((void**)&h->w1p, (size_t)HID * 64 * sizeof(__nv_bfloat16)));
         MLP_TRY(h, cudaMalloc((void**)&h->wt, (size_t)(NLAYER - 1) * HID * HID * sizeof(__nv_bfloat16)));
-        MLP_TRY(h, cudaMalloc((void**)&h->ws, (size_t)TG_MAX_SPLITS * HID * HID * sizeof(float)));
+        MLP_TRY(h, cudaMalloc((void**)&h->ws, (size_t)NLAYER * TG_MAX_SPLITS * HID * HID * sizeof(float)));
+    }
+    if (!h->st_w) {
+        MLP_TRY(h, cudaStreamCreateWithFlags(&h->st_w, cudaStreamNonBlocking));
+        for (int l = 0; l < NLAYER; ++l) MLP_TRY(h, cudaEventCreateWithFlags(&h->ev_dz[l], cudaEventDisableTiming));
+        MLP_TRY(h, cudaEventCreateWithFlags(&h->ev_w, cudaEventDisableTiming));
     }
     h->tc_n = -1;
     h->max_batch = rows;
@@ -1566,8 +1580,11 @@ int tc_maps(gprm_mlp* h, int n)
         if ((rc = tc_map(h, &h->m_wt[l - 1], h->wt + (size_t)(l - 1) * HID * HID, HID, HID, HID * 2, TG_BN_LAYER)))
             return rc;
     }
-    if ((rc = tc_map(h, &h->m_ta, h->Ta, N, HID, (uint64_t)h->ldT * 2, TC_ROWS))) return rc;
-    if ((rc = tc_map(h, &h->m_tb256, h->Tb, N, HID, (uint64_t)h->ldT * 2, HID))) return rc;
+    for (int l = 0; l < NLAYER; ++l) {
+        const size_t o = (size_t)l * HID * h->ldT;
+        if ((rc = tc_map(h, &h->m_ta[l], h->Ta + o, N, HID, (uint64_t)h->ldT * 2, TC_ROWS))) return rc;
+        if ((rc = tc_map(h, &h->m_tb256[l], h->Tb + o, N, HID, (uint64_t)h->ldT * 2, HID))) return rc;
+    }
     if ((rc = tc_map(h, &h->m_tb64, h->Tb, N, 64, (uint64_t)h->ldT * 2, 64))) return rc;
     if (!h->tc_attr) {
         MLP_TRY(h, cudaFuncSetAttribute(k_tc_gemm<TG_FWD, TG_BN_LAYER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1625,28 +1642,38 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
     const int kps = ((n + splits - 1) / splits + 63) / 64 * 64;
     splits = (n + kps - 1) / kps;
     const dim3 tblock(32, 8);
+    /* layer l's weight gradients (transposes, split-K GEMM, ordered
+       reduction) depend only on dZ_l and the forward activations: they run
+       on st_w, in their own buffers, while st carries the chain of backward
+       GEMMs dZ_l -> dZ_{l-1}; st waits for all of them at the end (a fork
+       and join that a captured graph keeps as dependencies) */
+    MLP_TRY(h, cudaEventRecord(h->ev_dz[NLAYER - 1], st));
     for (int l = NLAYER - 1; l >= 0; --l) {
         const int kin = l == 0 ? IN_PAD : HID, kin_p = l == 0 ? 64 : HID;
+        __nv_bfloat16* Ta = h->Ta + (size_t)l * HID * h->ldT;
+        __nv_bfloat16* Tb = h->Tb + (size_t)l * HID * h->ldT;
+        float* ws = h->ws + (size_t)l * TG_MAX_SPLITS * HID * HID;
+        float* cpart = h->cpart + (size_t)l * h->cparts * HID;
+        MLP_TRY(h, cudaStreamWaitEvent(h->st_w, h->ev_dz[l], 0));
         /* dW_l = dZ_l^T H_{l-1}: A = dZ_l^T [256 x n], B = H_{l-1}^T [kin_p x n] */
-        k_transpose2_bf16<<<dim3(HID / 32 + kin_p / 32, (n + 31) / 32), tblock, 0, st>>>(
-            n, HID / 32, HID, h->dZ[l], HID, h->Ta, h->cpart, kin_p, l == 0 ? h->X64 : h->H[l - 1], kin_p, h->Tb,
-            h->ldT);
+        k_transpose2_bf16<<<dim3(HID / 32 + kin_p / 32, (n + 31) / 32), tblock, 0, h->st_w>>>(
+            n, HID / 32, HID, h->dZ[l], HID, Ta, cpart, kin_p, l == 0 ? h->X64 : h->H[l - 1], kin_p, Tb, h->ldT);
         TgArgs a{};
-        a.M = HID; a.N = kin_p; a.K = n; a.kps = kps; a.ws = h->ws; a.ldc = kin_p; a.err = h->dev_err; a.wait_cycles = wait_budget(h);
+        a.M = HID; a.N = kin_p; a.K = n; a.kps = kps; a.ws = ws; a.ldc = kin_p; a.err = h->dev_err; a.wait_cycles = wait_budget(h);
         if (l == 0)
-            k_tc_gemm<TG_WPART, 64><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<64>::BYTES, st>>>(
-                h->m_ta, h->m_tb64, a);
+            k_tc_gemm<TG_WPART, 64><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<64>::BYTES, h->st_w>>>(
+                h->m_ta[0], h->m_tb64, a);
         else
-            k_tc_gemm<TG_WPART, HID><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<HID>::BYTES, st>>>(
-                h->m_ta, h->m_tb256, a);
+            k_tc_gemm<TG_WPART, HID><<<dim3(1, HID / TC_ROWS, splits), TG_THREADS, TgSmem<HID>::BYTES, h->st_w>>>(
+                h->m_ta[l], h->m_tb256[l], a);
         /* weights, this layer's biases (column sums of dZ_l from the transpose)
            and, with the last layer, the output layer's partials */
         const bool out_l = l == NLAYER - 1;
         const int red_threads = HID * kin + HID + (out_l ? HID + 1 : 0);
-        k_reduce_w<<<(red_threads + 255) / 256, 256, 0, st>>>(splits, HID, kin_p, kin, h->ws, h->g + h->offW[l],
-                                                              (n + 31) / 32, h->cpart, h->g + h->offB[l],
-                                                              out_l ? blocks : 0, out_l ? h->opart : nullptr,
-                                                              h->g + h->offW[NLAYER]);
+        k_reduce_w<<<(red_threads + 255) / 256, 256, 0, h->st_w>>>(splits, HID, kin_p, kin, ws, h->g + h->offW[l],
+                                                                   (n + 31) / 32, cpart, h->g + h->offB[l],
+                                                                   out_l ? blocks : 0, out_l ? h->opart : nullptr,
+                                                                   h->g + h->offW[NLAYER]);
         if (l > 0) {
             /* dZ_{l-1} = (dZ_l W_l) * gelu'(Z_{l-1}): A = dZ_l [n x 256], B = W_l^T [256 x 256] */
             TgArgs d{};
@@ -1656,8 +1683,11 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
             k_tc_gemm<TG_DH, TG_BN_LAYER><<<dim3(HID / TG_BN_LAYER, (n + TC_ROWS - 1) / TC_ROWS, 1), TG_THREADS,
                                             TgSmem<TG_BN_LAYER>::BYTES, st>>>(
                 h->m_dz[l], h->m_wt[l - 1], d);
+            MLP_TRY(h, cudaEventRecord(h->ev_dz[l - 1], st));
         }
     }
+    MLP_TRY(h, cudaEventRecord(h->ev_w, h->st_w));
+    MLP_TRY(h, cudaStreamWaitEvent(st, h->ev_w, 0));
     MLP_TRY(h, cudaGetLastError());
     return GPRM_OK;
 }
@@ -1915,6 +1945,13 @@ void gprm_mlp_destroy(gprm_mlp* h)
     cudaFree(h->X64); cudaFree(h->Ta); cudaFree(h->Tb); cudaFree(h->w1p); cudaFree(h->wt); cudaFree(h->ws);
     cudaFree(h->cpart); cudaFree(h->opart);
     cudaFree(h->d_ctl);
+    if (h->st_w) {
+        cudaStreamSynchronize(h->st_w);
+        cudaStreamDestroy(h->st_w);
+    }
+    for (int l = 0; l < NLAYER; ++l)
+        if (h->ev_dz[l]) cudaEventDestroy(h->ev_dz[l]);
+    if (h->ev_w) cudaEventDestroy(h->ev_w);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
