@@ -523,6 +523,24 @@ def predictor_errors(cs, scene, mlp, n=1 << 16, seed=0, prune=0.9):
             "accuracy": float(((p >= 0.5) == coll).float().mean().item())}
 
 
+def calibrate_prune(cs, scene, mlp, free_rate=0.005, n=1 << 16, seed=0, lo=0.9, hi=0.999):
+    """The prune threshold that removes at most `free_rate` of the free
+    configurations: the (1 - free_rate) quantile of the predictor's p over
+    exactly checked free held-out samples, kept within [lo, hi].  Pruning a
+    free sample costs connectivity (the planner then needs more samples to
+    reach the same success rate), so the threshold follows the predictor's
+    own confidence on free space instead of a fixed value."""
+    import torch
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(scene, n, seed + 777).T), device="cuda:0")
+    codes = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+    cs.check_configs_device(q, codes)
+    p = mlp.predict(q)[codes == 0]
+    if p.numel() == 0:
+        return hi
+    t = float(torch.quantile(p.float(), 1.0 - free_rate).item())
+    return min(max(t, lo), hi)
+
+
 def _summary(r):
     return {"success_rate": float(r.success.mean()), "time_to_path_ms": 1e3 * r.time_to_path,
             "batch_seconds": r.seconds, "edge_checks": r.edge_checks, "edge_steps": r.edge_steps,
@@ -537,7 +555,7 @@ def _median_run(fn, repeats):
 
 
 def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0, mlp=None, repeats=3,
-                     first=1, max_rounds=4):
+                     first=1, max_rounds=4, prune=None):
     """Plain (eager) PRM against the lazy PRM without guidance and the
     learned-guided lazy PRM, on the same seeded queries.  Each run is
     repeated (`repeats` timed runs after one untimed) and the median is
@@ -546,7 +564,8 @@ def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0,
     PRM prunes samples, which can change the roadmap: it runs on
     n_samples, then on 1.125x, 1.25x, ... samples until its success rate
     reaches the plain planner's, and the time of that run is the one
-    compared ("equal success rate")."""
+    compared ("equal success rate").  prune None: the threshold of
+    `calibrate_prune` (at most 0.5 % of the free configurations pruned)."""
     starts, goals = make_queries(cs, scene, n_queries, seed + 17)
     out = {}
     plain = _median_run(lambda: plain_prm(cs, scene, starts, goals, n_samples, k, seed), repeats)
@@ -555,11 +574,13 @@ def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0,
                                         max_rounds=max_rounds), repeats)
     out["lazy"] = _summary(lazy)
     if mlp is not None:
+        if prune is None:
+            prune = calibrate_prune(cs, scene, mlp, seed=seed)
         target = float(plain.success.mean())
         n, tries = n_samples, []
         for _ in range(8):
-            r = _median_run(lambda: lazy_prm(cs, scene, starts, goals, n, k, seed, mlp=mlp, first=first,
-                                             max_rounds=max_rounds), repeats)
+            r = _median_run(lambda: lazy_prm(cs, scene, starts, goals, n, k, seed, mlp=mlp, prune=prune,
+                                             first=first, max_rounds=max_rounds), repeats)
             tries.append({"samples": n, "success_rate": float(r.success.mean()), "time_to_path_ms": 1e3 * r.time_to_path})
             if r.success.mean() >= target:
                 break
@@ -568,7 +589,8 @@ def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0,
                               success_matched=bool(r.success.mean() >= target))
         out["learned_over_plain_time"] = out["learned"]["time_to_path_ms"] / out["plain"]["time_to_path_ms"]
         out["learned_over_lazy_time"] = out["learned"]["time_to_path_ms"] / out["lazy"]["time_to_path_ms"]
-        out["predictor_errors"] = predictor_errors(cs, scene, mlp, seed=seed)
+        out["predictor_errors"] = predictor_errors(cs, scene, mlp, seed=seed, prune=prune)
+        out["prune_threshold"] = prune
     out["lazy_over_plain_time"] = out["lazy"]["time_to_path_ms"] / out["plain"]["time_to_path_ms"]
     out["config"] = {"samples": n_samples, "queries": n_queries, "k": k, "seed": seed, "dq": float(cs.deltaq()),
                      "lazy_first": first, "lazy_rounds": max_rounds, "lazy_growth": 2, "lazy_attach": True}
