@@ -523,7 +523,7 @@ def predictor_errors(cs, scene, mlp, n=1 << 16, seed=0, prune=0.9):
             "accuracy": float(((p >= 0.5) == coll).float().mean().item())}
 
 
-def calibrate_prune(cs, scene, mlp, free_rate=0.005, n=1 << 16, seed=0, lo=0.9, hi=0.999):
+def calibrate_prune(cs, scene, mlp, free_rate=0.002, n=1 << 16, seed=0, lo=0.9, hi=0.999):
     """The prune threshold that removes at most `free_rate` of the free
     configurations: the (1 - free_rate) quantile of the predictor's p over
     exactly checked free held-out samples, kept within [lo, hi].  Pruning a
@@ -565,7 +565,7 @@ def compare_planners(cs, scene, n_samples=1 << 16, n_queries=1000, k=10, seed=0,
     n_samples, then on 1.125x, 1.25x, ... samples until its success rate
     reaches the plain planner's, and the time of that run is the one
     compared ("equal success rate").  prune None: the threshold of
-    `calibrate_prune` (at most 0.5 % of the free configurations pruned)."""
+    `calibrate_prune` (at most 0.2 % of the free configurations pruned)."""
     starts, goals = make_queries(cs, scene, n_queries, seed + 17)
     out = {}
     plain = _median_run(lambda: plain_prm(cs, scene, starts, goals, n_samples, k, seed), repeats)
