@@ -3,7 +3,7 @@
  *
  * No counterpart in GPUPRM.  A multilayer perceptron
  *     x (sin/cos of the joints, padded to 16) -> 256 -> 256 -> 256 -> 256 -> 1
- * with GELU (erf form, erfc by Abramowitz & Stegun 7.1.28) on the hidden
+ * with GELU (tanh form) on the hidden
  * layers and a sigmoid output, trained
  * with binary cross-entropy and Adam.  Weights are kept in FP32 (master)
  * and BF16 (the GEMM operands); activations are stored in BF16; every GEMM
@@ -58,52 +58,32 @@ struct EpiArgs {
     int ldc;
 };
 
-/* GELU(z) = z Phi(z), Phi the standard normal CDF, Phi(z) = (1 + erf(z/sqrt2))/2.
- * erfc by the approximation of Abramowitz & Stegun, Handbook of
- * Mathematical Functions, eq. 7.1.28: for x >= 0,
- *     erfc(x) = 1 - erf(x) = 1 / (1 + a1 x + a2 x^2 + ... + a6 x^6)^16,
- * |error| <= 3e-7, far below the BF16 rounding of the activations it
- * feeds.  The coefficients (with the 1) are scaled by 2^(1/16), so that the
- * reciprocal of the 16th power is h = erfc(x)/2 directly; with x = |z|/sqrt2,
- * Phi(z) = 1 - h for z >= 0 and h for z < 0, so
- *     GELU(z) = max(z, 0) - |z| h.
- * One approximate reciprocal is the only special-function instruction (the
- * multi-function unit's throughput and the issue rate bound the inference
- * epilogue).  For large x the 16th power overflows to infinity and h to 0,
- * its limit. */
-__device__ __forceinline__ float rcp_approx(float x)
+/* GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear
+ * Units", 2016, sec. 2):
+ *     GELU(z) = z/2 (1 + tanh(u)),   u = k (z + c z^3),  k = sqrt(2/pi), c = 0.044715,
+ * evaluated as u = z (k + kc z^2), GELU = hz + hz t with hz = z/2, t = tanh(u).
+ * The one special-function instruction is tanh.approx.f32 (relative error
+ * about 2^-11, below the BF16 rounding of the activations it feeds); the
+ * network is trained and evaluated with this same function, and the FP64
+ * oracle states it with an exact tanh.  Derivative:
+ *     GELU'(z) = (1 + t)/2 + hz (1 - t^2) k (1 + 3 c z^2). */
+constexpr float GELU_K = 0.7978845608028654f;              /* sqrt(2/pi) */
+constexpr float GELU_KC = 0.035677408136300125f;           /* sqrt(2/pi) * 0.044715 */
+constexpr float GELU_3KC = 0.10703222440890038f;           /* 3 sqrt(2/pi) * 0.044715 */
+
+__device__ __forceinline__ float tanh_approx(float x)
 {
     float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-__device__ __forceinline__ float gelu_h(float z)   /* erfc(|z|/sqrt2) / 2 = min(Phi(z), 1 - Phi(z)) */
-{
-    const float x = __fmul_rn(fabsf(z), 0.70710678118654752f);
-    float y = __fmaf_rn(4.497039844864048e-05f, x, 0.0002888118615373969f);
-    y = __fmaf_rn(y, x, 0.0001587445440236479f);
-    y = __fmaf_rn(y, x, 0.009680968709290028f);
-    y = __fmaf_rn(y, x, 0.04415399581193924f);
-    y = __fmaf_rn(y, x, 0.07364540547132492f);
-    y = __fmaf_rn(y, x, 1.0442737340927124f);
-    y = __fmul_rn(y, y);
-    y = __fmul_rn(y, y);
-    y = __fmul_rn(y, y);
-    y = __fmul_rn(y, y);                                   /* 2 P(x)^16 */
-    return rcp_approx(y);
-}
-
-__device__ __forceinline__ float ex2_approx(float x)
-{
-    float r;
-    asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
 
 __device__ __forceinline__ float gelu_f(float z)
 {
-    return __fmaf_rn(-fabsf(z), gelu_h(z), fmaxf(z, 0.0f));
+    const float u = __fmul_rn(z, __fmaf_rn(__fmul_rn(z, z), GELU_KC, GELU_K));
+    const float t = tanh_approx(u);
+    const float hz = __fmul_rn(z, 0.5f);
+    return __fmaf_rn(hz, t, hz);
 }
 
 /* Two lanes of FP32 in one 64-bit register for the packed FP32 x2
@@ -138,39 +118,26 @@ __device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsig
     return d;
 }
 
-/* gelu_f of (z0, z1) with packed x2 arithmetic: the same operations, half
- * the instructions for the polynomial and the squarings. */
+/* gelu_f of (z0, z1) with packed x2 arithmetic: the same operations in
+ * the same order, half the instructions. */
 __device__ __forceinline__ void gelu_f2(unsigned long long z, float& g0, float& g1)
 {
-    float z0, z1;
-    f2_unpack(z, z0, z1);
-    const unsigned long long az = f2_pack(fabsf(z0), fabsf(z1));
-    const unsigned long long x = f2_mul(az, f2_pack(0.70710678118654752f, 0.70710678118654752f));
-    unsigned long long y = f2_fma(f2_pack(4.497039844864048e-05f, 4.497039844864048e-05f), x,
-                                  f2_pack(0.0002888118615373969f, 0.0002888118615373969f));
-    y = f2_fma(y, x, f2_pack(0.0001587445440236479f, 0.0001587445440236479f));
-    y = f2_fma(y, x, f2_pack(0.009680968709290028f, 0.009680968709290028f));
-    y = f2_fma(y, x, f2_pack(0.04415399581193924f, 0.04415399581193924f));
-    y = f2_fma(y, x, f2_pack(0.07364540547132492f, 0.07364540547132492f));
-    y = f2_fma(y, x, f2_pack(1.0442737340927124f, 1.0442737340927124f));
-    y = f2_mul(y, y);
-    y = f2_mul(y, y);
-    y = f2_mul(y, y);
-    y = f2_mul(y, y);                                      /* 2 P(x)^16 */
-    float y0, y1;
-    f2_unpack(y, y0, y1);
-    const unsigned long long h = f2_pack(rcp_approx(y0), rcp_approx(y1));
-    const unsigned long long r = f2_fma(f2_pack(-fabsf(z0), -fabsf(z1)), h, f2_pack(fmaxf(z0, 0.0f), fmaxf(z1, 0.0f)));
-    f2_unpack(r, g0, g1);
+    const unsigned long long w = f2_fma(f2_mul(z, z), f2_pack(GELU_KC, GELU_KC), f2_pack(GELU_K, GELU_K));
+    float u0, u1;
+    f2_unpack(f2_mul(z, w), u0, u1);
+    const unsigned long long t = f2_pack(tanh_approx(u0), tanh_approx(u1));
+    const unsigned long long hz = f2_mul(z, f2_pack(0.5f, 0.5f));
+    f2_unpack(f2_fma(hz, t, hz), g0, g1);
 }
 
 __device__ __forceinline__ float gelu_grad(float z)
 {
-    /* Phi(z) + z pdf(z), pdf(z) = exp(-z^2/2) / sqrt(2 pi) = 2^(-z^2 log2(e) / 2) / sqrt(2 pi) */
-    const float h = gelu_h(z);
-    const float phi = z >= 0.0f ? 1.0f - h : h;
-    const float e = ex2_approx(__fmul_rn(__fmul_rn(z, z), -0.72134752044448170f));
-    return __fmaf_rn(z, 0.39894228040143268f * e, phi);
+    const float z2 = __fmul_rn(z, z);
+    const float t = tanh_approx(__fmul_rn(z, __fmaf_rn(z2, GELU_KC, GELU_K)));
+    const float du = __fmaf_rn(z2, GELU_3KC, GELU_K);                 /* k (1 + 3 c z^2) */
+    const float hz = __fmul_rn(z, 0.5f);
+    const float s = __fmaf_rn(-t, t, 1.0f);                           /* 1 - t^2 */
+    return __fmaf_rn(__fmul_rn(hz, s), du, __fmaf_rn(0.5f, t, 0.5f));
 }
 
 /* two floats -> a packed BF16 pair (a in the low half), round to nearest

@@ -1,7 +1,7 @@
 """The learned collision-probability predictor over the C ABI (gprm_mlp_*).
 
 Network: sin/cos of the joint angles (12 inputs for 6 joints, padded to 16)
--> 256 -> 256 -> 256 -> 256 -> 1, GELU hidden activations, sigmoid output,
+-> 256 -> 256 -> 256 -> 256 -> 1, GELU (tanh form) hidden activations, sigmoid output,
 binary cross-entropy, Adam.  Forward, backward and Adam run in the
 library's CUDA kernels (BF16 tensor-core GEMMs, FP32 accumulation).
 """

@@ -4,7 +4,7 @@ TEST INFRASTRUCTURE ONLY (tests import it as the checker of the CUDA MLP).
 
 The same network as gpuprm_b200/csrc/gprm_mlp.cu, in float64 numpy:
 features (sin q_j, cos q_j) padded to 16; Z_l = H_{l-1} W_l^T + b_l,
-H_l = gelu(Z_l) (erf form); logit = H_4 w5^T + b5; p = sigmoid(logit);
+H_l = gelu(Z_l) (tanh form, Hendrycks & Gimpel 2016); logit = H_4 w5^T + b5; p = sigmoid(logit);
 mean binary cross-entropy; Adam (beta 0.9/0.999, eps 1e-8).
 
 With emulate_bf16=True the values the kernels store in BF16 (inputs,
@@ -20,7 +20,8 @@ import math
 import numpy as np
 
 HID, IN_PAD, LAYERS = 256, 16, 4
-_erf = np.vectorize(math.erf, otypes=[np.float64])
+_K = math.sqrt(2.0 / math.pi)
+_C = 0.044715
 
 
 def bf16(x):
@@ -43,11 +44,13 @@ def features(q: np.ndarray) -> np.ndarray:
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """z/2 (1 + tanh(k (z + c z^3))), k = sqrt(2/pi), c = 0.044715."""
+    return 0.5 * z * (1.0 + np.tanh(_K * (z + _C * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    t = np.tanh(_K * (z + _C * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * _K * (1.0 + 3.0 * _C * z * z)
 
 
 def unpack(vec):
