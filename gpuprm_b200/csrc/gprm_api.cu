@@ -24,7 +24,6 @@
 
 #include <fstream>
 #include <map>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1319,25 +1318,16 @@ static_assert(sizeof(Control) <= NOALLOC_QUEUE_OFFSET, "control block outgrew it
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_QUEUE_OFFSET +
                                                                  (size_t)GPRM_NOALLOC_MAX_CONFIGS * sizeof(uint2)];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
-
-/* Device address of the scratch array on the current device (`dev`),
- * looked up once per device. */
-int noalloc_scratch(gprm_space* h, int dev, unsigned char** out)
+/* Device address of the scratch array in the current context, looked up
+ * on every call (a lookup, no allocation once the module is loaded), so that
+ * a context made again after a device reset gets the array's new address. */
+int noalloc_scratch(gprm_space* h, unsigned char** out)
 {
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-        return fail(h, GPRM_ERR_UNSUPPORTED, "device ordinal %d beyond %d", dev, NOALLOC_MAX_DEVICES);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(h, GPRM_ERR_CUDA, "cudaGetSymbolAddress(no-allocation scratch): %s", cudaGetErrorString(e));
-        g_noalloc_addr[dev] = p;
-    }
-    *out = (unsigned char*)g_noalloc_addr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(h, GPRM_ERR_CUDA, "cudaGetSymbolAddress(no-allocation scratch): %s", cudaGetErrorString(e));
+    *out = (unsigned char*)p;
     return GPRM_OK;
 }
 
@@ -1354,7 +1344,7 @@ extern "C" int gprm_indicator_batch_device_noalloc(gprm_space* h, const float* q
                     n, GPRM_NOALLOC_MAX_CONFIGS);
     if (n == 0) return GPRM_OK;
     unsigned char* base = nullptr;
-    rc = noalloc_scratch(h, h->device, &base);
+    rc = noalloc_scratch(h, &base);
     if (rc) return rc;
     Control* ctl = (Control*)base;
     /* one queue entry per configuration: the queue cannot overflow */

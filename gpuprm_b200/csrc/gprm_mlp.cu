@@ -118,16 +118,18 @@ __device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsig
     return d;
 }
 
-/* gelu_f of (z0, z1) with packed x2 arithmetic: the same operations in
- * the same order, half the instructions. */
-__device__ __forceinline__ void gelu_f2(unsigned long long z, float& g0, float& g1)
+/* gelu_f of (2 y0, 2 y1) from (y0, y1) = z/2, which k_mlp_fused's MMAs
+ * produce (weights and bias halved, exactly): u = y (2k + 8kc y^2) and
+ * GELU = y + y t.  Scaling by powers of two commutes with rounding, so each
+ * step equals gelu_f's on z = 2y bit for bit, with one multiply fewer. */
+__device__ __forceinline__ void gelu_half_f2(unsigned long long y, float& g0, float& g1)
 {
-    const unsigned long long w = f2_fma(f2_mul(z, z), f2_pack(GELU_KC, GELU_KC), f2_pack(GELU_K, GELU_K));
+    const unsigned long long w = f2_fma(f2_mul(y, y), f2_pack(8.0f * GELU_KC, 8.0f * GELU_KC),
+                                        f2_pack(2.0f * GELU_K, 2.0f * GELU_K));
     float u0, u1;
-    f2_unpack(f2_mul(z, w), u0, u1);
+    f2_unpack(f2_mul(y, w), u0, u1);
     const unsigned long long t = f2_pack(tanh_approx(u0), tanh_approx(u1));
-    const unsigned long long hz = f2_mul(z, f2_pack(0.5f, 0.5f));
-    f2_unpack(f2_fma(hz, t, hz), g0, g1);
+    f2_unpack(f2_fma(y, t, y), g0, g1);
 }
 
 __device__ __forceinline__ float gelu_grad(float z)
@@ -480,6 +482,23 @@ __device__ __forceinline__ void tc_ld16_wait(uint32_t* r)
                  :: "memory");
 }
 
+/* Stores 16 FP32 columns of this warp's 32 TMEM lanes, all lanes the same
+ * 16 values (a bias row), and waits for the stores. */
+__device__ __forceinline__ void tc_st16_bias(uint32_t taddr, const float* b)
+{
+    const float4 b0 = reinterpret_cast<const float4*>(b)[0], b1 = reinterpret_cast<const float4*>(b)[1];
+    const float4 b2 = reinterpret_cast<const float4*>(b)[2], b3 = reinterpret_cast<const float4*>(b)[3];
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+                 "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n"
+                 :: "r"(taddr), "f"(b0.x), "f"(b0.y), "f"(b0.z), "f"(b0.w), "f"(b1.x), "f"(b1.y), "f"(b1.z), "f"(b1.w),
+                    "f"(b2.x), "f"(b2.y), "f"(b2.z), "f"(b2.w), "f"(b3.x), "f"(b3.y), "f"(b3.z), "f"(b3.w)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_st_wait()
+{
+    asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+}
+
 /* shared memory of k_mlp_tc<K>: W | A | mbarrier | TMEM address | row partials */
 template <int K>
 struct TcSmem {
@@ -559,9 +578,17 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
                 *reinterpret_cast<uint4*>(As + (r / 8) * SBO + c * LBO + (r % 8) * 16) = v;
             }
         }
+        /* the accumulator starts at the bias: warp w writes its 32 lanes,
+           columns 128 (w / 4) .. +127 */
+#pragma unroll 1
+        for (int c = 0; c < 8; ++c)
+            tc_st16_bias(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * (warp >> 2) + 16 * c),
+                         bias + 128 * (warp >> 2) + 16 * c);
+        tc_st_wait();
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
         __syncthreads();
-        /* 2. the MMAs */
+        /* 2. the MMAs, accumulating onto the bias */
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const uint32_t a0 = smem_u32(As), b0 = smem_u32(Ws);
@@ -569,7 +596,7 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
             for (int s = 0; s < K / 16; ++s) {
                 const uint64_t ad = tc_sdesc(a0 + s * 2 * LBO, LBO, SBO);
                 const uint64_t bd = tc_sdesc(b0 + s * 2 * LBO, LBO, SBO);
-                const uint32_t acc = s > 0 ? 1u : 0u;
+                const uint32_t acc = 1u;
                 asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
                              :: "r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc),
@@ -578,7 +605,7 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                          :: "r"(mbar) : "memory");
         }
-        /* 3. accumulator -> bias, GELU -> out */
+        /* 3. accumulator (bias included) -> GELU -> out */
         const bool ok = tc_wait(mbar, phase);
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
@@ -603,7 +630,7 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
             uint32_t hp[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j)
-                hp[j] = pack_bf16(gelu_f(v[2 * j] + bias[col + 2 * j]), gelu_f(v[2 * j + 1] + bias[col + 2 * j + 1]));
+                hp[j] = pack_bf16(gelu_f(v[2 * j]), gelu_f(v[2 * j + 1]));
             if (LAST) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
@@ -646,7 +673,7 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
  * k_mlp_fused runs all layers of a 128-row tile on one SM; the hidden
  * activations never leave shared memory.  One persistent CTA per SM with
  * 22 warps in four roles:
- *   warps 0-15  epilogue: TMEM -> + bias, GELU -> BF16 activations (the
+ *   warps 0-15  epilogue: TMEM -> GELU -> BF16 activations (the
  *               next layer's A operand, written in place) or, after the
  *               last hidden layer, the output head.  Warp w reads TMEM
  *               lanes 32*(w%4).. (its rows) and, in round r = 0..3, the
@@ -666,7 +693,13 @@ k_mlp_tc(int n, const float* __restrict__ q, long long qoff, int ndof, const __n
  * columns 256*(l%2)..: MMA chunk c of layer l+1 (K columns 64c..64c+63)
  * is issued as soon as the epilogue's round c of layer l has written them, so the MMAs of a layer run under the
  * epilogue of the previous one, and the first layer of the next tile runs
- * under the last layer's epilogue.  The MMAs run in the same K order as
+ * under the last layer's epilogue.  Each accumulator starts at the bias of
+ * the layer that uses it (written by the epilogue warps with tcgen05.st
+ * when they have read the previous layer out), so the epilogue adds no
+ * bias.  Weights and biases are halved (exact in binary), so the
+ * accumulators hold z/2 and the GELU needs no multiply by 1/2; every step
+ * rounds like the per-layer kernels' GELU of z.  The MMAs start from the
+ * bias and run in the same K order as
  * k_mlp_tc and the output head uses the same split and order, so both
  * kernels give the same bits.  Every wait is bounded by a clock budget: an
  * expired wait sets *err and an abort flag that ends the other roles'
@@ -786,10 +819,25 @@ __device__ __forceinline__ void fu_commit(uint32_t bar)
                  : "memory");
 }
 
-/* Weights of hidden layers 2-4 in chunk order (layer, K chunk), each chunk
+/* Weights of hidden layers 2-4, halved (k_mlp_fused accumulates z/2), in chunk order (layer, K chunk), each chunk
  * [256 rows x 64 K] in the 128-byte-swizzled K-major layout (row n, k at
  * (n/8)*1024 + (n%8)*128 + ((k/8) ^ (n%8))*16 + (k%8)*2), then W1
  * [256 x 16] in the no-swizzle core-matrix order (SBO 256 B, LBO 128 B). */
+/* the 8 BF16 values of v times 1/2 (exact for normal values) */
+__device__ __forceinline__ uint4 half_bf16x8(uint4 v)
+{
+    const __nv_bfloat162 h = __float2bfloat162_rn(0.5f);
+    uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        __nv_bfloat162 x;
+        memcpy(&x, &w[i], 4);
+        x = __hmul2(x, h);
+        memcpy(&w[i], &x, 4);
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 __global__ void k_mlp_relayout(const __nv_bfloat16* __restrict__ wbf, long long o0, long long o1, long long o2,
                                long long o3, unsigned char* __restrict__ out)
 {
@@ -799,14 +847,14 @@ __global__ void k_mlp_relayout(const __nv_bfloat16* __restrict__ wbf, long long 
         const int l = t / per_layer, r = t % per_layer;
         const int nrow = r % HID, kg = r / HID;   /* kg: 8-element group of K, 0..31 */
         const long long off = l == 0 ? o1 : (l == 1 ? o2 : o3);
-        const uint4 v = *reinterpret_cast<const uint4*>(wbf + off + (long long)nrow * HID + kg * 8);
+        const uint4 v = half_bf16x8(*reinterpret_cast<const uint4*>(wbf + off + (long long)nrow * HID + kg * 8));
         unsigned char* dst = out + (size_t)(l * FU_CHUNKS + kg / 8) * FU_CHUNK_BYTES + (nrow / 8) * 1024 +
                              (nrow % 8) * 128 + (((kg % 8) ^ (nrow % 8)) * 16);
         *reinterpret_cast<uint4*>(dst) = v;
     } else if (t < (NLAYER - 1) * per_layer + HID * (IN_PAD / 8)) {
         const int r = t - (NLAYER - 1) * per_layer;
         const int nrow = r % HID, kg = r / HID;
-        const uint4 v = *reinterpret_cast<const uint4*>(wbf + o0 + (long long)nrow * IN_PAD + kg * 8);
+        const uint4 v = half_bf16x8(*reinterpret_cast<const uint4*>(wbf + o0 + (long long)nrow * IN_PAD + kg * 8));
         unsigned char* dst = out + (size_t)(NLAYER - 1) * FU_CHUNKS * FU_CHUNK_BYTES + (nrow / 8) * (IN_PAD * 16) +
                              kg * 128 + (nrow % 8) * 16;
         *reinterpret_cast<uint4*>(dst) = v;
@@ -839,7 +887,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
             reinterpret_cast<uint4*>(sm + L::W1)[i] = reinterpret_cast<const uint4*>(w1g)[i];
 #pragma unroll
         for (int l = 0; l < NLAYER; ++l)   /* constant indices keep P.bias out of local memory */
-            for (int i = tid; i < HID; i += FU_THREADS) bias_s[l * HID + i] = P.bias[l][i];
+            for (int i = tid; i < HID; i += FU_THREADS) bias_s[l * HID + i] = 0.5f * P.bias[l][i];
         for (int i = tid; i < HID; i += FU_THREADS) w5_s[i] = __bfloat162float(P.w5[i]);
         if (tid == 0) {
             *reinterpret_cast<float*>(sm + L::B5) = P.b5[0];
@@ -877,6 +925,21 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
         bool ok = true;
         /* this thread's row in the activation buffer: atom column kc at kc * 16 KB */
         unsigned char* hb_row = sm + L::BUF + (rl / 8) * 1024 + (rl % 8) * 128;
+        /* accumulator a starts at the bias of the layer that uses it next
+           (layers 0 and 1 first): this warp's lanes, columns 64r + 16q */
+        const uint32_t tlanes = tmem + ((uint32_t)(32 * g) << 16);
+#pragma unroll 1
+        for (int a = 0; a < 2; ++a)
+#pragma unroll 1
+            for (int r = 0; r < FU_CHUNKS; ++r)
+                tc_st16_bias(tlanes + (uint32_t)(a * TC_COLS + 64 * r + 16 * q), bias_s + a * HID + 64 * r + 16 * q);
+        tc_st_wait();
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+            fu_arrive(bar(FB_ACCEMPTY));
+            fu_arrive(bar(FB_ACCEMPTY + 1));
+        }
         for (int tile = blockIdx.x, it = 0; tile < ntiles && ok; tile += gridDim.x, ++it) {
             for (int l = 0; l < NLAYER; ++l) {
                 const int a = l & 1;
@@ -884,7 +947,6 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                 if (!ok) break;
                 af_ph ^= 1u << a;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                const float* bl = bias_s + l * HID;
                 float part = 0.0f;
                 /* round r: columns 64r + 16q .. +15, so that round r completes
                    K chunk r of the next layer's A operand; the TMEM load of
@@ -897,20 +959,11 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                 for (int r = 0; r < FU_CHUNKS; ++r) {
                     const int col = 64 * r + 16 * q;
                     if (r + 1 < FU_CHUNKS) tc_ld16_issue(tbase + (uint32_t)(64 * (r + 1)), acc[r + 1]);
-                    float v[16];
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(acc[r][j]);
-                    float bv[16];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float4 b4 = reinterpret_cast<const float4*>(bl + col)[j];
-                        bv[4 * j] = b4.x; bv[4 * j + 1] = b4.y; bv[4 * j + 2] = b4.z; bv[4 * j + 3] = b4.w;
-                    }
                     uint32_t hp[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
                         float g0, g1;
-                        gelu_f2(f2_add(f2_pack(v[2 * j], v[2 * j + 1]), f2_pack(bv[2 * j], bv[2 * j + 1])), g0, g1);
+                        gelu_half_f2(f2_pack(__uint_as_float(acc[r][2 * j]), __uint_as_float(acc[r][2 * j + 1])), g0, g1);
                         hp[j] = pack_bf16(g0, g1);
                     }
                     if (l < NLAYER - 1) {
@@ -932,6 +985,13 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                     }
                     if (r + 1 < FU_CHUNKS) tc_ld16_wait(acc[r + 1]);
                 }
+                /* the accumulator's next user is layer (l + 2) mod 4 (of the
+                   next tile for l >= 2): its bias goes in now */
+#pragma unroll 1
+                for (int r = 0; r < FU_CHUNKS; ++r)
+                    tc_st16_bias(tlanes + (uint32_t)(a * TC_COLS + 64 * r + 16 * q),
+                                 bias_s + ((l + 2) % NLAYER) * HID + 64 * r + 16 * q);
+                tc_st_wait();
                 asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
                 __syncwarp();
                 if (lane == 0) fu_arrive(bar(FB_ACCEMPTY + a));
@@ -984,25 +1044,23 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
     } else if (warp == FU_MMA_WARP) {
         /* ---------------- MMA issue ---------------- */
         if (lane == 0) {
-            uint32_t consumed = 0, fr_ph = 0u, ae_ph = 0u, hr_ph = 0u, used = 0u;   /* bit a: accumulator a */
+            uint32_t consumed = 0, fr_ph = 0u, ae_ph = 0u, hr_ph = 0u;   /* ae_ph bit a: accumulator a */
             bool ok = true;
             const uint64_t w1d = tc_sdesc(smem_u32(sm + L::W1), 128u, IN_PAD * 16u);
             const uint64_t fd = tc_sdesc(smem_u32(sm + L::FEAT), 128u, IN_PAD * 16u);
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 for (int l = 0; l < NLAYER && ok; ++l) {
                     const int a = l & 1;
-                    /* the accumulator's previous layer has been read out */
-                    if ((used >> a) & 1u) {
-                        if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), (ae_ph >> a) & 1u, abort_flag, P.err, P.wait_cycles))) break;
-                        ae_ph ^= 1u << a;
-                    }
-                    used |= 1u << a;
+                    /* the accumulator's previous layer has been read out and the
+                       bias of this layer written in (the first time: the bias only) */
+                    if (!(ok = fu_wait(bar(FB_ACCEMPTY + a), (ae_ph >> a) & 1u, abort_flag, P.err, P.wait_cycles))) break;
+                    ae_ph ^= 1u << a;
                     const uint32_t acc = tmem + (uint32_t)(a * TC_COLS);
                     if (l == 0) {
                         if (!(ok = fu_wait(bar(FB_FEATREADY), fr_ph, abort_flag, P.err, P.wait_cycles))) break;
                         fr_ph ^= 1u;
                         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                        fu_mma(acc, fd, w1d, 0u);
+                        fu_mma(acc, fd, w1d, 1u);
                         fu_commit(bar(FB_FEATEMPTY));
                     } else {
                         for (int c = 0; c < FU_CHUNKS; ++c, ++consumed) {
@@ -1017,7 +1075,7 @@ __global__ void __launch_bounds__(FU_THREADS, 1) k_mlp_fused(FuParams P)
                                 /* K step 4c + s2: 32 bytes into the swizzle atoms of column c */
                                 const uint64_t ad = tc_sdesc_sw128(buf0 + (uint32_t)c * (TC_ROWS * 128) + (uint32_t)s2 * 32u);
                                 const uint64_t bd = tc_sdesc_sw128(ring0 + st * FU_CHUNK_BYTES + (uint32_t)s2 * 32u);
-                                fu_mma(acc, ad, bd, (c | s2) != 0 ? 1u : 0u);
+                                fu_mma(acc, ad, bd, 1u);
                             }
                             fu_commit(bar(FB_WEMPTY + st));
                         }
@@ -1856,6 +1914,12 @@ int gprm_mlp_create(int ndof, unsigned long long seed, gprm_mlp** out)
         h->offB[l] = off; off += nout;
         h->offWbf[l] = offbf; offbf += (long long)nout * nin;
     }
+    /* the inference kernels read the hidden layers' biases as float4 */
+    for (int l = 0; l < NLAYER; ++l)
+        if (h->offB[l] % 4 != 0) {
+            delete h;
+            return GPRM_ERR_ARG;
+        }
     h->nparam = off;
     h->nbf = offbf;
     std::vector<float> w(off, 0.0f);
