@@ -505,6 +505,7 @@ void release_request(Request& r)
     cudaFree(r.d_key);
     cudaFree(r.d_seg);
     cudaFree(r.d_queue);
+    cudaFree(r.d_qpair);
     cudaFree(r.d_ovf);
     cudaFreeHost(r.ctl_host);
     cudaFreeHost(r.h_qwant);
@@ -554,8 +555,9 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
         size_t qcap = (need_q > r.cap_queue) ? need_q + need_q / 4 : r.cap_queue;
         if (qcap < cap * 4 + 65536) qcap = cap * 4 + 65536;
         cudaFree(r.d_a); cudaFree(r.d_b); cudaFree(r.d_res); cudaFree(r.d_key); cudaFree(r.d_queue);
-        cudaFree(r.d_ovf);
+        cudaFree(r.d_qpair); cudaFree(r.d_ovf);
         r.d_a = r.d_b = nullptr; r.d_res = nullptr; r.d_key = nullptr; r.d_queue = nullptr; r.d_ovf = nullptr;
+        r.d_qpair = nullptr;
         /* the capacities describe the buffers only once every one exists */
         r.cap_items = 0;
         r.cap_queue = 0;
@@ -563,6 +565,7 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
         CUDA_TRY(h, dev_malloc((void**)&r.d_res, cap * sizeof(int)));
         CUDA_TRY(h, dev_malloc((void**)&r.d_key, cap * sizeof(unsigned)));
         CUDA_TRY(h, dev_malloc((void**)&r.d_queue, qcap * sizeof(uint2)));
+        CUDA_TRY(h, dev_malloc((void**)&r.d_qpair, qcap * sizeof(unsigned)));
         CUDA_TRY(h, dev_malloc((void**)&r.d_ovf, (2 * cap + 2 * HOST_PARTS + 64) * sizeof(unsigned)));
         if (with_host) {
             CUDA_TRY(h, dev_malloc((void**)&r.d_a, cap * nd * sizeof(float)));
@@ -633,6 +636,9 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
     if (h->debug_qcap && h->debug_qcap < bq.cap) bq.cap = h->debug_qcap;
     bq.n = n;
     bq.ovf = nullptr;
+    /* pair indices fit 16 bits on every scene the library builds; a larger
+       pair list rechecks every pair */
+    bq.pair_range = h->dsc.npairs <= 65535 ? r.d_qpair : nullptr;
     if (band_on && r.d_ovf) {
         /* every part's keys start at its first item (key = d_key + c0) */
         bq.ovf = r.d_ovf + 2 * (size_t)(key - r.d_key);

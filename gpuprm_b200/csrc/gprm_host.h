@@ -38,6 +38,7 @@ struct Request {
     unsigned* d_key = nullptr;
     unsigned* d_seg = nullptr;    /* edge segment offsets (EDGE_SPLIT_MAX + 1) */
     uint2* d_queue = nullptr;
+    unsigned* d_qpair = nullptr;  /* pair range of each queue item's recheck (BandQueue) */
     unsigned* d_ovf = nullptr;    /* overflow record of the FP64 queue: 2 words per item (BandQueue) */
     float* h_a = nullptr;         /* pinned staging */
     float* h_b = nullptr;

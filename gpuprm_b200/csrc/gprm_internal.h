@@ -42,6 +42,14 @@ struct BandQueue {
     unsigned cap;
     unsigned* ovf;
     long long n;
+    /* per item (null: not recorded): the pairs the FP64 recheck has to
+       test, [lo, hi) packed as lo | hi << 16.  lo: the first pair that the
+       FP32 check decided within the band (every pair before it was decided
+       outside it); hi: one past the last such pair for a check the FP32
+       pass found free (every later pair was decided outside the band), the
+       pair count for one it found colliding (the pairs after the deciding
+       one were not tested) */
+    unsigned* pair_range = nullptr;
 };
 
 /* How a launch reads its scene. */

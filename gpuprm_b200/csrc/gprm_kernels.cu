@@ -438,6 +438,7 @@ struct LaneState {
     float mdec, mmin;
     bool active;
     int first_k;
+    int jrec, jlast;   /* first and last pair decided within the band (collision or margin < band) */
 };
 
 __device__ __forceinline__ void defer_push(unsigned* q, int& n, bool want, int k)
@@ -452,7 +453,7 @@ __device__ __forceinline__ void defer_push(unsigned* q, int& n, bool want, int k
  * owner apply its results; the remaining items move to the front. */
 template <bool FAST>
 __device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S, int j0, int& n, int cnt,
-                                          LaneState& st, PairCounts& pc)
+                                          LaneState& st, PairCounts& pc, float band)
 {
     const int lane = threadIdx.x & 31;
     unsigned* q = S.defer;
@@ -480,13 +481,19 @@ __device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S
         const unsigned it = q[t];
         if ((int)(it & 31u) == lane && st.first_k == DEFER_NONE) {
             const int ct = rcode[t];
+            const int jj = j0 + (int)(it >> 5);
             if (ct != 0) {
                 st.code = ct;
                 st.mdec = rm[t];
                 st.first_k = (int)(it >> 5);
                 st.active = false;
+                st.jrec = min(st.jrec, jj);
             } else {
                 st.mmin = min_nan(st.mmin, rm[t]);
+                if (!(rm[t] >= band)) {
+                    st.jrec = min(st.jrec, jj);
+                    st.jlast = max(st.jlast, jj);
+                }
             }
         }
     }
@@ -503,7 +510,7 @@ __device__ __forceinline__ void defer_run(const DevScene& sc, const SceneView& S
  * failed (need, from cert_scan) are queued in pair order. */
 template <bool FAST>
 __device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView& S, int j0, unsigned need,
-                                            unsigned todo, LaneState& st, PairCounts& pc)
+                                            unsigned todo, LaneState& st, PairCounts& pc, float band)
 {
     int n = 0;
     st.first_k = DEFER_NONE;
@@ -512,13 +519,21 @@ __device__ __forceinline__ void defer_chunk(const DevScene& sc, const SceneView&
         todo &= todo - 1u;
         const bool full = st.active && ((need >> k) & 1u);
         defer_push(S.defer, n, full, k);
-        if (n >= 32) defer_run<FAST>(sc, S, j0, n, 32, st, pc);
+        if (n >= 32) defer_run<FAST>(sc, S, j0, n, 32, st, pc, band);
     }
-    while (n > 0) defer_run<FAST>(sc, S, j0, n, n < 32 ? n : 32, st, pc);
+    while (n > 0) defer_run<FAST>(sc, S, j0, n, n < 32 ? n : 32, st, pc, band);
 }
 
-/* Appends the items of the lanes with `want` set, one atomic per warp. */
-__device__ __forceinline__ void warp_append(bool want, uint2 item, BandQueue bq,
+/* Appends the items of the lanes with `want` set, one atomic per warp;
+ * range: the pairs the item's FP64 recheck tests (BandQueue::pair_range). */
+__device__ __forceinline__ unsigned recheck_range(int code, int jfirst, int jlast, int npairs)
+{
+    if (jfirst >= npairs) return (unsigned)npairs << 16;          /* not recorded: every pair */
+    const int hi = code != 0 ? npairs : (jlast < npairs ? jlast + 1 : npairs);
+    return (unsigned)jfirst | ((unsigned)hi << 16);
+}
+
+__device__ __forceinline__ void warp_append(bool want, uint2 item, unsigned range, BandQueue bq,
                                             Control* ctl)
 {
     unsigned m = __ballot_sync(FULL_MASK, want);
@@ -531,6 +546,7 @@ __device__ __forceinline__ void warp_append(bool want, uint2 item, BandQueue bq,
         unsigned slot = base + __popc(m & ((1u << lane) - 1));
         if (slot < bq.cap) {
             bq.items[slot] = item;
+            if (bq.pair_range) bq.pair_range[slot] = range;
         } else {
             atomicOr(&ctl->flags, GPRM_DEVFLAG_QUEUE_FULL);
             const unsigned x = item.x;
@@ -573,7 +589,7 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
             if (qi[j] < sc.mins[j] || qi[j] > sc.maxs[j]) { code = 1; active = false; break; }
     }
     if (active) lane_fk<FAST>(sc, S, qi);
-    LaneState st{code, 0.0f, PF32::inf(), active, DEFER_NONE};
+    LaneState st{code, 0.0f, PF32::inf(), active, DEFER_NONE, 0x7fffffff, -1};
     /* pairs in chunks of 32: the order-free certificate scan, then the
        pairs left for the exact test in the reference's order, their exact
        tests deferred and run by the whole warp */
@@ -583,7 +599,7 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
         const int jn = min(32, sc.npairs - j0);
         const unsigned need = cert_scan<false>(sc, S, j0, jn, st.active, pc);
         const unsigned todo = __reduce_or_sync(FULL_MASK, need);
-        defer_chunk<FAST>(sc, S, j0, need, todo, st, pc);
+        defer_chunk<FAST>(sc, S, j0, need, todo, st, pc, band);
     }
     code = st.code;
     const float mmin = st.mmin, mdec = st.mdec;
@@ -592,7 +608,8 @@ __device__ __forceinline__ void check_config_chunk(const DevScene& sc, const Sce
         res[i] = code;
     }
     bool want = valid && band_on && code != 1 && in_band(code, code == 0 ? mmin : mdec, band);
-    warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27), bq, ctl);
+    warp_append(want, make_uint2((unsigned)i, (unsigned)(code + 1) << 27),
+                recheck_range(code, st.jrec, st.jlast, sc.npairs), bq, ctl);
 }
 
 template <bool SMEM, bool FAST>
@@ -708,6 +725,7 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
         float mmin = PF32::inf(), mdec = 0.0f;
         int cut = 32;   /* lanes above the highest-priority colliding lane no longer matter */
         int jend = 0;   /* pairs processed by the warp */
+        int jrec = 0x7fffffff, jlast = -1;   /* first and last pair decided within the band */
         bool stop = false;
         /* pairs in chunks of 32: the order-free certificate scan, then the
            pairs left for the exact test in the reference's order; a code can
@@ -724,8 +742,11 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
                 if (active && ((need >> k) & 1u)) {
                     float m;
                     const int rr = eval_pair<FAST>(sc, S, j0 + k, &m, pc);
-                    if (rr != 0) { code = rr; mdec = m; active = false; }
-                    else mmin = min_nan(mmin, m);
+                    if (rr != 0) { code = rr; mdec = m; active = false; jrec = min(jrec, j0 + k); }
+                    else {
+                        mmin = min_nan(mmin, m);
+                        if (!(m >= band)) { jrec = min(jrec, j0 + k); jlast = j0 + k; }
+                    }
                 }
                 jend = j0 + k + 1;
                 bool oobj = code != 0 && !(band_on && in_band(code, mdec, band));
@@ -749,7 +770,7 @@ __device__ __forceinline__ void check_edge(const DevScene& sc, const SceneView& 
            than the deciding step go to the FP64 queue */
         const bool want = inb && lane < L;
         warp_append(want, make_uint2((unsigned)e, (unsigned)t | ((unsigned)(code + 1) << 27)),
-                    bq, ctl);
+                    recheck_range(code, jrec, jlast, sc.npairs), bq, ctl);
         if (hits) {
             if (lane == L) {
                 const unsigned kv = (POLICY == EDGE_EARLY_EXIT) ? early_key(order, code) : all_key(t, code);
@@ -879,9 +900,13 @@ __global__ void __launch_bounds__(1024) k_edge_segments(const float* __restrict_
 /* ------------------------------------------------------------------ */
 
 /* The FP64 check of one configuration (in bounds): the reference's pair
- * loop in double with the FP64 certificates. */
-__device__ __forceinline__ int check_config64(const DevScene& sc, const float* qi)
+ * loop in double with the FP64 certificates, over pairs [j_start, j_end)
+ * (the pairs outside that range were decided separated outside the band by
+ * the FP32 check, so in FP64 they are separated too, and the first
+ * colliding pair, hence the code, is the same as over every pair). */
+__device__ __forceinline__ int check_config64(const DevScene& sc, const float* qi, int j_start = 0, int j_end = -1)
 {
+    if (j_end < 0 || j_end > sc.npairs) j_end = sc.npairs;
     Frame<double> F[GPRM_MAX_FRAMES];
     forward_kinematics<PF64>(sc, qi, F);
     /* slot ball centres in FP64, once per check (the same transform the
@@ -893,7 +918,7 @@ __device__ __forceinline__ int check_config64(const DevScene& sc, const float* q
         cen[3 * sl] = c.x; cen[3 * sl + 1] = c.y; cen[3 * sl + 2] = c.z;
     }
 #pragma unroll 1
-    for (int j = 0; j < sc.npairs; ++j) {
+    for (int j = j_start; j < j_end; ++j) {
         const int4 pr = sc.pairs[j];
         if (pair_certified64(sc, sc.tab, pr, sc.pairs_b[j], F, cen, j)) continue;
         double m;
@@ -1089,12 +1114,12 @@ __device__ __forceinline__ void recheck_item(const DevScene& sc, int kind, uint2
                                              const float* __restrict__ qs, const float* __restrict__ qe,
                                              long long offset, float dq, int policy, int* __restrict__ res,
                                              unsigned* __restrict__ key, unsigned long long& checks,
-                                             unsigned long long& flips)
+                                             unsigned long long& flips, unsigned range)
 {
     float qi[GPRM_MAX_FRAMES];
     int t, tn;
     recheck_config(sc, kind, it, q, qs, qe, offset, dq, qi, t, tn);
-    const int code = check_config64(sc, qi);
+    const int code = check_config64(sc, qi, (int)(range & 0xffffu), (int)(range >> 16));
     ++checks;
     flips += ((code != 0) != ((int)(it.y >> 27) - 1 != 0));
     recheck_store(kind, it, code, t, tn, policy, res, key);
@@ -1111,7 +1136,8 @@ __global__ void __launch_bounds__(RECHECK_THREADS) k_recheck(DevScene sc, int ki
     if (cnt > bq.cap) cnt = bq.cap;
     unsigned long long checks = 0, flips = 0;
     for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x)
-        recheck_item(sc, kind, bq.items[idx], q, qs, qe, offset, dq, policy, res, key, checks, flips);
+        recheck_item(sc, kind, bq.items[idx], q, qs, qe, offset, dq, policy, res, key, checks, flips,
+                     bq.pair_range ? bq.pair_range[idx] : 0xffff0000u);
     if (checks) atomicAdd(&ctl->band_checks, checks);
     if (flips) atomicAdd(&ctl->band_flips, flips);
 }
@@ -1510,7 +1536,8 @@ __global__ void __launch_bounds__(RECHECK_THREADS) k_recheck_multi(BatchView B, 
     for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
         const uint2 it = bq.items[idx];
         const DevScene& sc = B.scenes[problem_of(B, (long long)it.x)];
-        recheck_item(sc, kind, it, q, qs, qe, offset, sc.dq, policy, res, key, checks, flips);
+        recheck_item(sc, kind, it, q, qs, qe, offset, sc.dq, policy, res, key, checks, flips,
+                     bq.pair_range ? bq.pair_range[idx] : 0xffff0000u);
     }
     if (checks) atomicAdd(&ctl->band_checks, checks);
     if (flips) atomicAdd(&ctl->band_flips, flips);
