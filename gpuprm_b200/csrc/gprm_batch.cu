@@ -52,7 +52,9 @@ struct Layout {
     int graph_launches = 0;          /* kernels in the captured graph */
     unsigned* d_key = nullptr;       /* edges: per-edge decision key */
     uint2* d_queue = nullptr;
+    unsigned* d_qpair = nullptr;     /* pair range of each queue item's recheck (BandQueue) */
     size_t qcap = 0;
+    bool qpair_ok = false;           /* every problem's pair indices fit 16 bits */
     unsigned* d_ovf = nullptr;       /* overflow record of the queue (BandQueue), 2 words per item */
     cudaGraphExec_t graph = nullptr; /* captured call sequence */
 };
@@ -66,6 +68,7 @@ void free_layout(Layout& L)
     cudaFree(L.d_wprob);
     cudaFree(L.d_key);
     cudaFree(L.d_queue);
+    cudaFree(L.d_qpair);
     cudaFree(L.d_ovf);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     L = Layout();
@@ -163,6 +166,7 @@ int enqueue_batch(gprm_batch* b, int vertex_kernel, const float* qa, const float
         BandQueue bq;
         bq.items = L.d_queue;
         bq.cap = (unsigned)L.qcap;
+        bq.pair_range = L.qpair_ok ? L.d_qpair : nullptr;
         bq.ovf = band_on ? L.d_ovf + 2 * off : nullptr;
         bq.n = n;
         BATCH_TRY(b, cudaMemsetAsync(b->ctl, 0, sizeof(Control), st));
@@ -193,6 +197,7 @@ int enqueue_batch(gprm_batch* b, int vertex_kernel, const float* qa, const float
         BandQueue bq;
         bq.items = L.d_queue;
         bq.cap = (unsigned)L.qcap;
+        bq.pair_range = L.qpair_ok ? L.d_qpair : nullptr;
         bq.ovf = band_on ? L.d_ovf : nullptr;
         bq.n = L.total;
         BATCH_TRY(b, cudaMemsetAsync(b->ctl, 0, sizeof(Control), st));
@@ -410,6 +415,10 @@ int gprm_batch_set_layout(gprm_batch* b, int vertex_kernel, const long long* off
     BATCH_TRY(b, dev_malloc((void**)&L.d_offs, sizeof(long long) * (S + 1)));
     BATCH_TRY(b, cudaMemcpy(L.d_offs, offsets, sizeof(long long) * (S + 1), cudaMemcpyHostToDevice));
     BATCH_TRY(b, dev_malloc((void**)&L.d_queue, sizeof(uint2) * L.qcap));
+    BATCH_TRY(b, dev_malloc((void**)&L.d_qpair, sizeof(unsigned) * L.qcap));
+    L.qpair_ok = true;
+    for (int p = 0; p < S; ++p)
+        if (b->spaces[p]->dsc.npairs > 65535) L.qpair_ok = false;
     BATCH_TRY(b, dev_malloc((void**)&L.d_ovf, sizeof(unsigned) * (2 * (size_t)total + 64)));
     if (!vertex_kernel && total > 0) BATCH_TRY(b, dev_malloc((void**)&L.d_key, sizeof(unsigned) * total));
     const int rc = build_work(b, vertex_kernel, b->solo_min[vertex_kernel]);
