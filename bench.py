@@ -617,6 +617,31 @@ def stress_edges_leg(args, dev, policy):
                   "colliding_edges": int((res != 0).sum().item()),
                   "band_rechecks": int(s1["band_rechecks"] - s0["band_rechecks"])},
     }
+    # mid-size batches of these edges (a lazy planner's first round here is
+    # about 35k edges): one warp per edge against edges split into segments
+    # of 2 rounds over several warps
+    split = []
+    for mb in (35000, 140000):
+        if mb > m:
+            break
+        qs_b, qe_b = qs[:, :mb].contiguous(), qe[:, :mb].contiguous()
+        rb = {}
+        for name, smax in (("whole", 0), ("split", mb)):
+            cs.set_edge_split(smax, 2)
+            rr = torch.empty(mb, dtype=torch.int32, device=dev)
+            for _ in range(2):
+                cs.check_edges_device(qs_b, qe_b, rr)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            cs.check_edges_device(qs_b, qe_b, rr)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            rb[name] = (e0.elapsed_time(e1), rr.clone())
+        split.append({"edges": mb, "whole_ms": rb["whole"][0], "split_ms": rb["split"][0],
+                      "split_over_whole_time": rb["split"][0] / rb["whole"][0],
+                      "codes_identical": bool(torch.equal(rb["whole"][1], rb["split"][1]))})
+    cs.set_edge_split(16384, 2)
+    out["split_batches"] = split
     if not args.no_cpu_baseline:
         qs_r = np.ascontiguousarray(qs.T.cpu().numpy())
         qe_r = np.ascontiguousarray(qe.T.cpu().numpy())

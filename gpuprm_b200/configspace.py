@@ -86,7 +86,7 @@ class RobotConfigspace:
         _check(self.lib, self.h, self.lib.gprm_set_edge_policy(self.h, policy))
 
     def set_edge_split(self, max_edges: int, seg_rounds: int = 2) -> None:
-        """Edge batches of at most max_edges (<= 16384; 0 = never) split edges
+        """Edge batches of at most max_edges (<= 2^22; 0 = never) split edges
         longer than seg_rounds x 32 steps over several warps (same codes)."""
         _check(self.lib, self.h, self.lib.gprm_set_edge_split(self.h, max_edges, seg_rounds))
 

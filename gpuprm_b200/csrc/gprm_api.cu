@@ -15,6 +15,7 @@
  *   - every failure returns a status code and leaves a message instead of
  *     asserting (util.hpp:44-46).
  */
+#include <algorithm>
 #include <limits.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -533,8 +534,18 @@ int ensure_request(gprm_space* h, Request& r, int kind, size_t n, bool with_host
         CUDA_TRY(h, dev_malloc((void**)&r.ctl, HOST_PARTS * sizeof(Control)));
         CUDA_TRY(h, cudaHostAlloc((void**)&r.ctl_host, HOST_PARTS * sizeof(Control), cudaHostAllocDefault));
     }
-    if (kind == 1 && !r.d_seg)
-        CUDA_TRY(h, dev_malloc((void**)&r.d_seg, (size_t)(EDGE_SPLIT_MAX + 1) * sizeof(unsigned)));
+    /* segment offsets for the batches that split their edges */
+    if (kind == 1 && h->split_rounds > 0 && h->split_max > 0) {
+        const size_t want = (size_t)std::min<long long>((long long)n, (long long)h->split_max);
+        if (want > r.cap_seg || !r.d_seg) {
+            cudaFree(r.d_seg);
+            r.d_seg = nullptr;
+            r.cap_seg = 0;
+            const size_t cap = std::max<size_t>(want + want / 4, (size_t)EDGE_SPLIT_ONE_BLOCK);
+            CUDA_TRY(h, dev_malloc((void**)&r.d_seg, edge_seg_words((long long)cap) * sizeof(unsigned)));
+            r.cap_seg = cap;
+        }
+    }
     /* the demand of the last device-pointer edge call, once it has finished */
     if (r.q_pending) {
         const cudaError_t e = cudaEventQuery(r.ev_q);
@@ -658,10 +669,11 @@ int enqueue_part(gprm_space* h, Request& r, int kind, const float* a, const floa
         CUDA_TRY(h, launch_check_configs(h->dsc, h->cfg_v, a, n, offset, res, band_on, h->band, bq, ctl, st));
     else {
         /* small batches split their long edges over several warps */
-        const bool split = r.d_seg && h->split_rounds > 0 && n <= (long long)h->split_max;
+        const bool split = r.d_seg && h->split_rounds > 0 && n <= (long long)h->split_max &&
+                           (size_t)n <= r.cap_seg;
         CUDA_TRY(h, launch_check_edges(h->dsc, h->cfg_e, a, b, n, offset, h->dq, h->policy, key, band_on,
                                        h->band, bq, ctl, st, split ? r.d_seg : nullptr, split ? h->split_rounds : 0));
-        if (split) h->host_stats.launches += 1;
+        if (split) h->host_stats.launches += n <= EDGE_SPLIT_ONE_BLOCK ? 1 : 3;
     }
     if (e1) CUDA_TRY(h, cudaEventRecord(e1, st));
     if (band_on) {

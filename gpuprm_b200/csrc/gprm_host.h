@@ -36,7 +36,8 @@ struct Request {
     float* d_b = nullptr;         /* qe */
     int* d_res = nullptr;
     unsigned* d_key = nullptr;
-    unsigned* d_seg = nullptr;    /* edge segment offsets (EDGE_SPLIT_MAX + 1) */
+    unsigned* d_seg = nullptr;    /* edge segment offsets (edge_seg_words of cap_seg edges) */
+    size_t cap_seg = 0;           /* edges d_seg serves */
     uint2* d_queue = nullptr;
     unsigned* d_qpair = nullptr;  /* pair range of each queue item's recheck (BandQueue) */
     unsigned* d_ovf = nullptr;    /* overflow record of the FP64 queue: 2 words per item (BandQueue) */

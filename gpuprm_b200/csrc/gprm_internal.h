@@ -138,11 +138,17 @@ cudaError_t launch_check_configs(const DevScene& sc, const LaunchCfg& cfg, const
                                  BandQueue bq, Control* ctl, cudaStream_t st);
 
 /* Edge checks, FP32 pass: key[e] is set per the edge policy (see kernels).
- * seg_off (EDGE_SPLIT_MAX + 1 words of scratch) or null: with it, n <=
+ * seg_off (edge_seg_words(n) words of scratch) or null: with it, n <=
  * EDGE_SPLIT_MAX and every edge longer than seg_rounds rounds of 32 steps
- * is split into segments that different warps check (small batches of long
- * edges, where one warp per edge would leave the GPU idle). */
-constexpr long long EDGE_SPLIT_MAX = 16384;
+ * is split into segments that different warps check (batches of long
+ * edges, where one warp per edge would leave the GPU idle or wait on its
+ * longest edges).  Up to EDGE_SPLIT_ONE_BLOCK edges the segment offsets
+ * are scanned by one block; above, by a three-pass scan over
+ * EDGE_SEG_BLOCKS blocks whose sums follow the n + 1 offsets. */
+constexpr long long EDGE_SPLIT_MAX = 1ll << 22;
+constexpr long long EDGE_SPLIT_ONE_BLOCK = 16384;
+constexpr int EDGE_SEG_BLOCKS = 1024;
+inline size_t edge_seg_words(long long n) { return (size_t)n + 1 + EDGE_SEG_BLOCKS; }
 cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const float* qs,
                                const float* qe, long long n, long long offset, float dq, int policy,
                                unsigned* key, int band_on, float band, BandQueue bq,

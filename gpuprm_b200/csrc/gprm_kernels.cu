@@ -895,6 +895,89 @@ __global__ void __launch_bounds__(1024) k_edge_segments(const float* __restrict_
     if (tid == (int)blockDim.x - 1) seg_off[n] = base;
 }
 
+/* Segment count of edge e for the split kernels (a rejected edge counts
+ * one segment). */
+__device__ __forceinline__ unsigned edge_segs(const float* __restrict__ qs, const float* __restrict__ qe, long long e,
+                                              long long offset, int ndof, float dq, int seg_rounds)
+{
+    const int tn = edge_testnum(qs, qe, e, offset, ndof, dq);
+    return tn < 0 ? 1u : (unsigned)edge_seg_count((tn + 31) >> 5, seg_rounds);
+}
+
+/* Exclusive scan of x over the block (blockDim.x <= 1024, a multiple of
+ * 32); *total gets the block's sum.  wsum: 32 words of shared memory. */
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned x, unsigned* wsum, unsigned* total)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    unsigned v = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned y = __shfl_up_sync(FULL_MASK, v, d);
+        if (lane >= d) v += y;
+    }
+    if (lane == 31) wsum[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned w = lane < nw ? wsum[lane] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned y = __shfl_up_sync(FULL_MASK, w, d);
+            if (lane >= d) w += y;
+        }
+        if (lane < nw) wsum[lane] = w;                 /* inclusive warp totals */
+    }
+    __syncthreads();
+    const unsigned ex = v - x + (warp > 0 ? wsum[warp - 1] : 0u);
+    *total = wsum[nw - 1];
+    __syncthreads();
+    return ex;
+}
+
+/* Segment offsets of more than EDGE_SPLIT_ONE_BLOCK edges, in three
+ * passes: block b (of EDGE_SEG_BLOCKS) takes the edges [b c, (b+1) c),
+ * c = ceil(n / blocks), each thread a contiguous run of them.  Pass 0
+ * writes the block's segment count to bsum[b]; k_seg_scan_blocks turns
+ * bsum into exclusive offsets (and seg_off[n] into the total); pass 1
+ * writes seg_off[e] for the block's edges. */
+template <int PASS>
+__global__ void __launch_bounds__(256) k_seg_pass(const float* __restrict__ qs, const float* __restrict__ qe,
+                                                  long long n, long long offset, int ndof, float dq, int seg_rounds,
+                                                  unsigned* __restrict__ seg_off, unsigned* __restrict__ bsum)
+{
+    __shared__ unsigned wsum[32];
+    const long long chunk = (n + gridDim.x - 1) / gridDim.x;
+    const long long c0 = min(n, (long long)blockIdx.x * chunk), c1 = min(n, c0 + chunk);
+    const long long per = (c1 - c0 + blockDim.x - 1) / blockDim.x;
+    const long long b0 = min(c1, c0 + (long long)threadIdx.x * per), b1 = min(c1, b0 + per);
+    unsigned s = 0;
+    for (long long e = b0; e < b1; ++e) s += edge_segs(qs, qe, e, offset, ndof, dq, seg_rounds);
+    unsigned total = 0;
+    unsigned base = block_exclusive_scan(s, wsum, &total);
+    if (PASS == 0) {
+        if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+        return;
+    }
+    base += bsum[blockIdx.x];
+    for (long long e = b0; e < b1; ++e) {
+        seg_off[e] = base;
+        base += edge_segs(qs, qe, e, offset, ndof, dq, seg_rounds);
+    }
+}
+
+/* bsum[0..nb) -> exclusive offsets, *total_out = their sum (one block of
+ * 1024 threads, nb <= 1024). */
+__global__ void __launch_bounds__(1024) k_seg_scan_blocks(unsigned* __restrict__ bsum, int nb,
+                                                          unsigned* __restrict__ total_out)
+{
+    __shared__ unsigned wsum[32];
+    const int t = threadIdx.x;
+    const unsigned x = t < nb ? bsum[t] : 0u;
+    unsigned total = 0;
+    const unsigned ex = block_exclusive_scan(x, wsum, &total);
+    if (t < nb) bsum[t] = ex;
+    if (t == 0) *total_out = total;
+}
+
 /* ------------------------------------------------------------------ */
 /* FP64 recheck and finalisation                                        */
 /* ------------------------------------------------------------------ */
@@ -1354,7 +1437,15 @@ cudaError_t launch_check_edges(const DevScene& sc, const LaunchCfg& cfg, const f
     if (n <= 0) return cudaSuccess;
     if (seg_off && (seg_rounds < 1 || n > EDGE_SPLIT_MAX)) return cudaErrorInvalidValue;
     if (seg_off) {
-        k_edge_segments<<<1, 1024, 0, st>>>(qs, qe, n, offset, sc.ndof, dq, seg_rounds, seg_off);
+        if (n <= EDGE_SPLIT_ONE_BLOCK) {
+            k_edge_segments<<<1, 1024, 0, st>>>(qs, qe, n, offset, sc.ndof, dq, seg_rounds, seg_off);
+        } else {
+            static_assert(EDGE_SEG_BLOCKS <= 1024, "one block scans the block sums");
+            unsigned* bsum = seg_off + n + 1;   /* EDGE_SEG_BLOCKS words after the offsets */
+            k_seg_pass<0><<<EDGE_SEG_BLOCKS, 256, 0, st>>>(qs, qe, n, offset, sc.ndof, dq, seg_rounds, seg_off, bsum);
+            k_seg_scan_blocks<<<1, 1024, 0, st>>>(bsum, EDGE_SEG_BLOCKS, seg_off + n);
+            k_seg_pass<1><<<EDGE_SEG_BLOCKS, 256, 0, st>>>(qs, qe, n, offset, sc.ndof, dq, seg_rounds, seg_off, bsum);
+        }
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return err;
     }

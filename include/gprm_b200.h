@@ -159,10 +159,10 @@ const char* gprm_last_error(const gprm_space* h);
 
 int gprm_set_mode(gprm_space* h, int mode);
 int gprm_set_edge_policy(gprm_space* h, int policy);
-/* Edge batches of at most max_edges edges (0..16384, default 16384) check
- * each edge longer than seg_rounds x 32 steps (default 2) with several
- * warps, one per segment of about seg_rounds x 32 steps, so that a small
- * batch of long edges (lazy planning rounds, query attachment, path
+/* Edge batches of at most max_edges edges (0..4194304, default 16384)
+ * check each edge longer than seg_rounds x 32 steps (default 2) with
+ * several warps, one per segment of about seg_rounds x 32 steps, so that a
+ * small batch of long edges (lazy planning rounds, query attachment, path
  * verification) keeps the GPU busy; larger batches give each edge one
  * warp.  The codes do not depend on it.  No reference counterpart (the
  * reference runs one CUDA thread per edge step, robotconfigspace.cpp:362-595). */

@@ -143,10 +143,35 @@ def test_split_edges_match_whole_edges(policy, mode):
         np.testing.assert_array_equal(out[(16384, 1)][0][:48], want)
 
 
+@pytest.mark.parametrize("policy", [GPRM_EDGES_ALL_STEPS, GPRM_EDGES_EARLY_EXIT])
+def test_split_mid_size_batches_match_whole_edges(policy):
+    """Above 16384 edges the segment offsets come from the three-pass scan
+    (EDGE_SEG_BLOCKS blocks): 40000 edges of up to ~1000 steps, split into
+    segments of 1 or 2 rounds, give the codes and nominal step counts of
+    one warp per edge."""
+    sc = scenes.make_hull6(6)
+    dq = 0.005
+    qs, qe = scenes.random_edges(sc, 40000, 12, 5.0)
+    cs = space(sc, dq, mode=GPRM_MODE_FP64_BAND, policy=policy)
+    out = {}
+    for split in ((0, 2), (1 << 22, 2), (1 << 22, 1), (40000, 2)):
+        cs.set_edge_split(*split)
+        s0 = cs.stats()
+        out[split] = (cs.check_edges(qs, qe), cs.stats()["edge_steps_nominal"] - s0["edge_steps_nominal"],
+                      cs.stats()["launches"] - s0["launches"])
+    whole, steps, launches = out[(0, 2)]
+    assert (whole != 0).any() and (whole == 0).any()
+    for split, (codes, n, nl) in out.items():
+        np.testing.assert_array_equal(codes, whole, err_msg=str(split))
+        assert n == steps
+        if split[0] >= 40000:
+            assert nl == launches + 3          # the three scan passes
+
+
 def test_edge_split_arguments():
     sc = scenes.make_box4(1)
     cs = space(sc, 0.02)
-    for bad in ((-1, 4), (16385, 4), (100, 0)):
+    for bad in ((-1, 4), ((1 << 22) + 1, 4), (100, 0)):
         with pytest.raises(GprmError):
             cs.set_edge_split(*bad)
     cs.set_edge_split(0, 4)

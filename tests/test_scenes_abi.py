@@ -152,12 +152,13 @@ def test_queries_without_gpu_fail_cleanly():
 
 def test_edge_split_arguments_checked_on_host():
     cs = RobotConfigspace(scenes.make_box4(1), dq=0.02)
-    for bad in ((-1, 2), (16385, 2), (100, 0)):
+    for bad in ((-1, 2), ((1 << 22) + 1, 2), (100, 0)):
         with pytest.raises(GprmError) as e:
             cs.set_edge_split(*bad)
         assert e.value.status == -1
     cs.set_edge_split(0)
     cs.set_edge_split(16384, 4)
+    cs.set_edge_split(1 << 22, 2)
 
 
 REF_LIB_DIR = "/root/reference/prm/src/lib"
