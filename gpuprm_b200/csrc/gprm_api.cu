@@ -169,14 +169,19 @@ void compute_support_candidates(gprm_space* h, const gprm_scene_desc* d, const s
 {
     h->cbin.assign((size_t)GPRM_START_BINS * h->npoly, 0u);
     h->cidx.clear();
-    const double eps = 1e-2, lo[3] = {-1.0 - eps, -1.0 / 3.0 - eps, 1.0 / 3.0 - eps},
-                 hi[3] = {-1.0 / 3.0 + eps, 1.0 / 3.0 + eps, 1.0 + eps};
+    constexpr int C = GPRM_BIN_CELLS;
+    const double eps = 1e-2;
+    double lo[C], hi[C];
+    for (int i = 0; i < C; ++i) {
+        lo[i] = -1.0 + 2.0 * i / C - eps;
+        hi[i] = -1.0 + 2.0 * (i + 1) / C + eps;
+    }
     std::vector<double> poly;
     std::vector<unsigned char> list;
     for (int k = 0; k < h->npoly; ++k) {
         const int n = d->poly_n[k];
         for (int b = 0; b < GPRM_START_BINS; ++b) {
-            const int face = b / 9, iu = (b % 9) / 3, iv = b % 3;
+            const int face = b / (C * C), iu = (b % (C * C)) / C, iv = b % C;
             const double s = (face & 1) ? -1.0 : 1.0;
             const int ax = face / 2, bu = (ax + 1) % 3, bv = (ax + 2) % 3;   /* x:(y,z) y:(z,x) z:(x,y) */
             list.clear();

@@ -673,10 +673,14 @@ __device__ __forceinline__ bool pair_certified64(const DevScene& sc, const float
  * separation margin lies outside the FP64 band, which is what the band
  * exists for.  The exact policy (PF32) stays the drop-in default.
  */
-#define GPRM_START_BINS 54   /* direction bins: 6 cube faces x 3 x 3 cells */
+#ifndef GPRM_BIN_CELLS
+#define GPRM_BIN_CELLS 3     /* cells per axis of a cube face */
+#endif
+#define GPRM_START_BINS (6 * GPRM_BIN_CELLS * GPRM_BIN_CELLS)   /* direction bins: 6 faces x cells */
 
 /* Cube-map bin of a direction: the face of the largest |component| (with
- * its sign), then each of the other two components against a third of it.
+ * its sign), then each of the other two components against the cell
+ * borders m (-1 + 2k / GPRM_BIN_CELLS), m the largest |component|.
  * Any input, NaN included, gives a bin in [0, GPRM_START_BINS). */
 __host__ __device__ __forceinline__ int dir_bin(float x, float y, float z)
 {
@@ -686,9 +690,14 @@ __host__ __device__ __forceinline__ int dir_bin(float x, float y, float z)
     if (ax >= ay && ax >= az) { face = x < 0.0f ? 1 : 0; m = ax; u = y; v = z; }
     else if (ay >= az) { face = y < 0.0f ? 3 : 2; m = ay; u = z; v = x; }
     else { face = z < 0.0f ? 5 : 4; m = az; u = x; v = y; }
-    const float t = m * (1.0f / 3.0f);
-    const int iu = (u > t) - (u < -t) + 1, iv = (v > t) - (v < -t) + 1;
-    return face * 9 + iu * 3 + iv;
+    int iu = 0, iv = 0;
+#pragma unroll
+    for (int k = 1; k < GPRM_BIN_CELLS; ++k) {
+        const float t = m * (-1.0f + 2.0f * (float)k / (float)GPRM_BIN_CELLS);
+        iu += u > t;
+        iv += v > t;
+    }
+    return (face * GPRM_BIN_CELLS + iu) * GPRM_BIN_CELLS + iv;
 }
 
 __device__ __forceinline__ float fdot3(float ax, float ay, float az, float bx, float by, float bz)

@@ -2,7 +2,8 @@
 
 The fast exact test (GPRM_MODE_FAST) finds a polytope's support vertex
 along a direction as the maximum over the candidate list of the
-direction's bin (dir_bin: a cube face and a 3 x 3 cell of it).  The lists
+direction's bin (dir_bin: a cube face and a 3 x 3 cell of it, the cell
+borders at m (-1 + 2k/3), m the largest |component|).  The lists
 are built on the host from each vertex's normal cone; the property that
 makes the search exact is that, for every direction, the largest dot
 product over the list equals the largest over all the polytope's vertices
@@ -31,10 +32,13 @@ def dir_bin(d):
         face, m, u, v = (3 if y < 0 else 2), ay, z, x
     else:
         face, m, u, v = (5 if z < 0 else 4), az, x, y
-    t = np.float32(m * np.float32(1.0 / 3.0))
-    iu = int(u > t) - int(u < -t) + 1
-    iv = int(v > t) - int(v < -t) + 1
-    return face * 9 + iu * 3 + iv
+    iu = iv = 0
+    for k in range(1, 3):
+        c = np.float32(np.float32(-1.0) + np.float32(2.0) * np.float32(k) / np.float32(3.0))
+        t = np.float32(m * c)
+        iu += int(u > t)
+        iv += int(v > t)
+    return (face * 3 + iu) * 3 + iv
 
 
 def candidates(cs, k, b):
