@@ -429,6 +429,59 @@ static int check_config(const Scene& s, const float* q, float* check_margin)
     return 0;
 }
 
+/* The same pair loop over pairs [j0, j1) only (first nonzero result in
+ * pair order). */
+template <class P>
+static int check_config_range(const Scene& s, const float* q, int j0, int j1)
+{
+    typedef typename P::R R;
+    Frame<R> F[GPRM_MAX_DOF + 1];
+    forward_kinematics<P>(s, q, F);
+    for (int j = j0; j < j1 && j < s.M; ++j) {
+        int a = s.pfrom[j], b = s.pto[j];
+        PolyRef pa = {s.voff[a], s.n[a], s.moff[a]};
+        PolyRef pb = {s.voff[b], s.n[b], s.moff[b]};
+        R m = R(0.0f);
+        const int res = pair_test<P>(s, pa, pb, F[s.sys[a]], F[s.sys[b]], &m);
+        if (res != 0) return res;
+    }
+    return 0;
+}
+
+/* The pairs an FP64 recheck has to test, from the FP32 pair loop: lo = the
+ * first pair decided within the band (a collision, or a separation with
+ * margin below band); hi = one past the last such pair when the check is
+ * free, the pair count when it collides (the pairs after the deciding one
+ * are not tested in FP32).  Returns the FP32 code. */
+template <class P>
+static int band_pair_range(const Scene& s, const float* q, float band, int* lo, int* hi)
+{
+    typedef typename P::R R;
+    Frame<R> F[GPRM_MAX_DOF + 1];
+    forward_kinematics<P>(s, q, F);
+    *lo = s.M;
+    int last = -1;
+    for (int j = 0; j < s.M; ++j) {
+        int a = s.pfrom[j], b = s.pto[j];
+        PolyRef pa = {s.voff[a], s.n[a], s.moff[a]};
+        PolyRef pb = {s.voff[b], s.n[b], s.moff[b]};
+        R m = R(0.0f);
+        const int res = pair_test<P>(s, pa, pb, F[s.sys[a]], F[s.sys[b]], &m);
+        const float mf = P::to_f(m);
+        if (res != 0) {
+            if (j < *lo) *lo = j;
+            *hi = s.M;
+            return res;
+        }
+        if (!(mf >= band)) {
+            if (j < *lo) *lo = j;
+            last = j;
+        }
+    }
+    *hi = last + 1;
+    return 0;
+}
+
 /* check_boundaries(q) (robotconfigspace.cpp:795-802) */
 static int out_of_bounds(const Scene& s, const float* q)
 {
@@ -526,6 +579,35 @@ int orc_check_configs(void* h, const float* q, int n, int offset, int mode, floa
         }
         code[i] = c;
         if (margin) margin[i] = m;
+    }
+    return 0;
+}
+
+/* Pair ranges of an FP64 recheck (band_pair_range, FP32 with the
+ * kernels' trigonometry when mode & 4) and the FP64 check over a range:
+ * code[i] of configuration i over pairs [lo[i], hi[i]).  Configurations
+ * out of bounds get lo = hi = 0 and code 1. */
+int orc_band_pair_range(void* h, const float* q, int n, int offset, int mode, float band, int* lo, int* hi,
+                        int* code32)
+{
+    const Scene& s = *(const Scene*)h;
+    float qi[GPRM_MAX_DOF];
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < s.ndof; ++j) qi[j] = q[i + (size_t)offset * j];
+        if (out_of_bounds(s, qi)) { lo[i] = hi[i] = 0; code32[i] = 1; continue; }
+        code32[i] = (mode & 4) ? band_pair_range<F32D>(s, qi, band, &lo[i], &hi[i])
+                               : band_pair_range<F32>(s, qi, band, &lo[i], &hi[i]);
+    }
+    return 0;
+}
+
+int orc_check_configs64_range(void* h, const float* q, int n, int offset, const int* lo, const int* hi, int* code)
+{
+    const Scene& s = *(const Scene*)h;
+    float qi[GPRM_MAX_DOF];
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < s.ndof; ++j) qi[j] = q[i + (size_t)offset * j];
+        code[i] = out_of_bounds(s, qi) ? 1 : check_config_range<F64>(s, qi, lo[i], hi[i]);
     }
     return 0;
 }

@@ -59,6 +59,8 @@ def _load_oracle():
     lib.orc_edge_classify.argtypes = [C.c_void_p, _F, _F, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float,
                                       _U8, _I, _I]
     lib.orc_config_classify.argtypes = [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_float, _U8, _I]
+    lib.orc_band_pair_range.argtypes = [C.c_void_p, _F, C.c_int, C.c_int, C.c_int, C.c_float, _I, _I, _I]
+    lib.orc_check_configs64_range.argtypes = [C.c_void_p, _F, C.c_int, C.c_int, _I, _I, _I]
     return lib
 
 
@@ -95,6 +97,27 @@ class Oracle:
         self.lib.orc_check_configs(self.h, _f(buf), n, n, mode, band, _i(code), _f(margin),
                                    ib.ctypes.data_as(_U8))
         return code, margin, ib.astype(bool)
+
+    def band_pair_range(self, q: np.ndarray, mode: int = DEVICE_TRIG, band: float = 1e-5):
+        """The pairs [lo, hi) an FP64 recheck of each configuration has to
+        test, from its FP32 pair loop (first pair decided within the band;
+        one past the last such pair when free, the pair count when
+        colliding), and the FP32 codes."""
+        n = q.shape[0]
+        buf = soa(q)
+        lo, hi, code = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self.lib.orc_band_pair_range(self.h, _f(buf), n, n, mode, band, _i(lo), _i(hi), _i(code))
+        return lo, hi, code
+
+    def check_configs64_range(self, q: np.ndarray, lo: np.ndarray, hi: np.ndarray):
+        """FP64 codes of the configurations over their pairs [lo, hi)."""
+        n = q.shape[0]
+        buf = soa(q)
+        lo = np.ascontiguousarray(lo, np.int32)
+        hi = np.ascontiguousarray(hi, np.int32)
+        code = np.zeros(n, np.int32)
+        self.lib.orc_check_configs64_range(self.h, _f(buf), n, n, _i(lo), _i(hi), _i(code))
+        return code
 
     def check_edges(self, qs: np.ndarray, qe: np.ndarray, dq: float, mode: int = 0,
                     band: float = 1e-5):
