@@ -1329,11 +1329,11 @@ k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
 
 /* g_w[o][i] (i < kin) = sum over the splits of ws[s][o][i] (ld ldw), in split order. */
 /* Threads [0, rows*kin): gw = the split partials of ws added in split
- * order.  Then, with cpart, `rows` threads: gb[o] = sum over b < cparts of
- * cpart[b][o]; then, with opart, (HID + 1) x 32 threads: go[c] = sum over
- * b < oparts of opart[b][c] (the output layer's k_out_back partials), a
- * warp per column in a fixed order.  rows * kin and rows are multiples of
- * 32, so every warp lies in one segment. */
+ * order.  Then, with cpart, rows x 32 threads: gb[o] = sum over
+ * b < cparts of cpart[b][o]; then, with opart, (HID + 1) x 32 threads:
+ * go[c] = sum over b < oparts of opart[b][c] (the output layer's k_out_back
+ * partials); both a warp per column in a fixed order.  rows * kin is a
+ * multiple of 32, so every warp lies in one segment. */
 __global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* __restrict__ ws, float* __restrict__ gw,
                            int cparts, const float* __restrict__ cpart, float* __restrict__ gb,
                            int oparts, const float* __restrict__ opart, float* __restrict__ go)
@@ -1349,14 +1349,19 @@ __global__ void k_reduce_w(int splits, int rows, int ldw, int kin, const float* 
     }
     t -= rows * kin;
     if (cpart) {
-        if (t < rows) {
+        /* biases: one warp per column, lane l sums the partials l, l + 32,
+           ... in order, then a fixed shuffle tree adds the lanes */
+        if (t < rows * 32) {
+            const int c = t >> 5, lane = t & 31;
             float acc = 0.0f;
-#pragma unroll 8
-            for (int b = 0; b < cparts; ++b) acc += cpart[(size_t)b * rows + t];
-            gb[t] = acc;
+#pragma unroll 4
+            for (int b = lane; b < cparts; b += 32) acc += cpart[(size_t)b * rows + c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) gb[c] = acc;
             return;
         }
-        t -= rows;
+        t -= rows * 32;
     }
     /* output layer: one warp per column c (the segment starts at a multiple
        of 32 threads, so its warps are whole): lane l sums the partials
@@ -1703,7 +1708,7 @@ int backward_tc(gprm_mlp* h, int n, cudaStream_t st)
         /* weights, this layer's biases (column sums of dZ_l from the transpose)
            and, with the last layer, the output layer's partials */
         const bool out_l = l == NLAYER - 1;
-        const int red_threads = HID * kin + HID + (out_l ? (HID + 1) * 32 : 0);   /* segments of whole warps */
+        const int red_threads = HID * kin + HID * 32 + (out_l ? (HID + 1) * 32 : 0);   /* segments of whole warps */
         k_reduce_w<<<(red_threads + 255) / 256, 256, 0, h->st_w>>>(splits, HID, kin_p, kin, ws, h->g + h->offW[l],
                                                                    (n + 31) / 32, cpart, h->g + h->offB[l],
                                                                    out_l ? blocks : 0, out_l ? h->opart : nullptr,
