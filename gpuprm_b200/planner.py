@@ -523,7 +523,7 @@ def predictor_errors(cs, scene, mlp, n=1 << 16, seed=0, prune=0.9):
             "accuracy": float(((p >= 0.5) == coll).float().mean().item())}
 
 
-def calibrate_prune(cs, scene, mlp, free_rate=0.002, n=1 << 16, seed=0, lo=0.9, hi=0.999):
+def calibrate_prune(cs, scene, mlp, free_rate=0.002, n=1 << 16, seed=0, lo=0.9, hi=0.999, device="cuda:0"):
     """The prune threshold that removes at most `free_rate` of the free
     configurations: the (1 - free_rate) quantile of the predictor's p over
     exactly checked free held-out samples, kept within [lo, hi].  Pruning a
@@ -531,8 +531,8 @@ def calibrate_prune(cs, scene, mlp, free_rate=0.002, n=1 << 16, seed=0, lo=0.9, 
     reach the same success rate), so the threshold follows the predictor's
     own confidence on free space instead of a fixed value."""
     import torch
-    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(scene, n, seed + 777).T), device="cuda:0")
-    codes = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(scene, n, seed + 777).T), device=device)
+    codes = torch.zeros(n, dtype=torch.int32, device=device)
     cs.check_configs_device(q, codes)
     p = mlp.predict(q)[codes == 0]
     if p.numel() == 0:

@@ -150,3 +150,52 @@ def test_lazy_attachment_skips_missing_neighbours(monkeypatch):
     assert not bool(ok[:, -1].any())
     torch.testing.assert_close(_first_pairs(ok, label, nb.clamp_min(0), Q, kk),
                                _first_pairs(ok_all, label, nb.clamp_min(0), Q, kk))
+
+
+class _FakeSpace:
+    """Configurations with q[0] > 0 collide (code 4), the others are free."""
+
+    def check_configs_device(self, q, codes):
+        codes.copy_(torch.where(q[0] > 0, 4, 0).to(torch.int32))
+
+
+class _FakePredictor:
+    """p = a fixed function of the configuration, in [0, 1)."""
+
+    def __init__(self, scale=1.0):
+        self.scale = scale
+
+    def predict(self, q):
+        return self.scale * (0.5 + 0.5 * torch.sin(7.0 * q[1]) * torch.cos(3.0 * q[2])).clamp(0.0, 0.999)
+
+
+@pytest.mark.parametrize("free_rate", [0.002, 0.01, 0.05])
+def test_calibrated_prune_drops_at_most_the_free_rate(free_rate):
+    """The threshold is the (1 - free_rate) quantile of p over the free
+    held-out samples, clamped to [lo, hi]: at most free_rate of those
+    samples lie above it (when it is not clamped)."""
+    from gpuprm_b200 import scenes
+    sc = scenes.make_box4(1)
+    n = 1 << 14
+    t = planner.calibrate_prune(_FakeSpace(), sc, _FakePredictor(), free_rate=free_rate, n=n, seed=3,
+                                lo=0.0, hi=1.0, device="cpu")
+    q = torch.tensor(np.ascontiguousarray(scenes.uniform_configs(sc, n, 3 + 777).T))
+    p = _FakePredictor().predict(q)[q[0] <= 0]
+    assert 0.0 < t < 1.0
+    assert float((p > t).float().mean()) <= free_rate + 1e-3
+    assert float((p >= t).float().mean()) >= free_rate - 1e-3
+
+
+def test_calibrated_prune_is_clamped_and_handles_no_free_samples():
+    from gpuprm_b200 import scenes
+    sc = scenes.make_box4(1)
+    lo = planner.calibrate_prune(_FakeSpace(), sc, _FakePredictor(scale=0.1), n=4096, device="cpu")
+    assert lo == 0.9                                   # every p far below the floor
+    hi = planner.calibrate_prune(_FakeSpace(), sc, _FakePredictor(scale=1.0), free_rate=1e-6, n=4096,
+                                 hi=0.95, device="cpu")
+    assert hi == 0.95
+
+    class _AllColliding:
+        def check_configs_device(self, q, codes):
+            codes.fill_(4)
+    assert planner.calibrate_prune(_AllColliding(), sc, _FakePredictor(), n=1024, device="cpu") == 0.999
